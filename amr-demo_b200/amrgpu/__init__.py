@@ -1,0 +1,347 @@
+"""amrgpu -- Python host mirror of libamrgpu's C ABI.
+
+The reference (amr-demo) drives its physics through per-rank C entry points:
+``hpc_amr_initialize_solver``, ``hpc_amr_initialize_quadrant``,
+``hpc_amr_tag_feature``, ``hpc_amr_refine_operator_2d``,
+``hpc_amr_coarsen_operator_2d`` and ``hpc_amr_evolve_solver``
+(src/amr/src/amr_external.h:50-192). This package calls the same entry
+points of the B200 library with numpy arrays laid out exactly as
+``src/amr/src/amr_external.c`` lays them out, plus the library's extended
+API (device-resident sessions, the host forest, batched regrid kernels).
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (AmrGpuError, ConfigStruct, MeshStruct, ReportStruct, check, lib, LIB_PATH,
+                   PROTOTYPES)
+
+FORM_FP64_EXACT = 0
+FORM_FP32_FLUX = 1
+
+NFIELDS = 4
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def ip(a):
+    return _p(a, C.c_int)
+
+
+def dp(a):
+    return _p(a, C.c_double)
+
+
+def _iref(v):
+    return C.byref(C.c_int(int(v)))
+
+
+# --------------------------------------------------------------------- config
+class Config:
+    """The reference's physics configuration (physics_var_*.h) + extensions.
+
+    ``cfl`` is the *effective* CFL: reading an input.physics file applies
+    the reference's ``cfl = 0.25*cfl*time_scheme`` (physics_initialize.c:193);
+    :meth:`from_input` does the same for keyword arguments.
+    """
+
+    def __init__(self, **kw):
+        s = ConfigStruct()
+        lib().amrgpu_config_defaults(C.byref(s))
+        self._s = s
+        for k, v in kw.items():
+            self[k] = v
+
+    @classmethod
+    def from_input(cls, cfl=1.0, time_scheme=1, **kw):
+        """Build as physics_initialize.c does from input.physics values."""
+        c = cls(time_scheme=time_scheme, **kw)
+        c["cfl"] = 0.25 * cfl * time_scheme
+        return c
+
+    @classmethod
+    def read(cls, path):
+        c = cls()
+        check(lib().amrgpu_config_read(str(path).encode(), C.byref(c._s)), "config_read")
+        return c
+
+    @classmethod
+    def current(cls):
+        c = cls()
+        check(lib().amrgpu_config_get(C.byref(c._s)), "config_get")
+        return c
+
+    def apply(self):
+        """Make this the library's global configuration."""
+        check(lib().amrgpu_config_set(C.byref(self._s)), "config_set")
+        return self
+
+    def __setitem__(self, k, v):
+        if k in ("bc", "amr_tag_methods", "amr_tag_tolerances", "ic_params"):
+            arr = getattr(self._s, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(self._s, k, v)
+
+    def __getitem__(self, k):
+        v = getattr(self._s, k)
+        if k in ("bc", "amr_tag_methods", "amr_tag_tolerances", "ic_params"):
+            return list(v)
+        return v
+
+    def as_dict(self):
+        return {f: self[f] for f, _ in ConfigStruct._fields_}
+
+
+# --------------------------------------------------------------------- mesh
+class Mesh:
+    """Flat arrays of one mesh epoch, as src/amr/src/amr_external.c builds them."""
+
+    def __init__(self, n, cell_info, face_info, geom, nface, dof, nghost=0):
+        self.n = int(n)
+        self.cell_info = np.ascontiguousarray(cell_info, dtype=np.int32)
+        self.face_info = np.ascontiguousarray(face_info, dtype=np.int32)
+        self.geom = np.ascontiguousarray(geom, dtype=np.float64)
+        self.nface = int(nface)
+        self.dof = int(dof)
+        self.nghost = int(nghost)
+        self.ncell = len(self.cell_info) // 3 - self.nghost
+
+    @property
+    def ncells(self):
+        return self.ncell * self.n * self.n
+
+    def struct(self):
+        return MeshStruct(self.ncell, self.nghost, self.nface, self.dof, ip(self.cell_info),
+                          ip(self.face_info), dp(self.geom))
+
+    def levels(self):
+        return self.cell_info[1::3][: self.ncell].copy()
+
+
+class Forest:
+    """Host quadtree forest on a brick of trees (stands in for p4est)."""
+
+    def __init__(self, nx=1, ny=1, periodic=(0, 0), lo=(0.0, 0.0, 0.0), scale=1.0, level=0):
+        L = lib()
+        self._f = L.amrgpu_forest_new_brick(int(nx), int(ny), int(periodic[0]), int(periodic[1]),
+                                            float(lo[0]), float(lo[1]), float(lo[2]), float(scale),
+                                            int(level))
+        if not self._f:
+            raise AmrGpuError(L.amrgpu_last_error(), "forest_new_brick")
+        self.scale = float(scale)
+
+    def __del__(self):
+        f = getattr(self, "_f", None)
+        if f:
+            lib().amrgpu_forest_destroy(f)
+            self._f = None
+
+    @property
+    def num_quads(self):
+        return lib().amrgpu_forest_num_quads(self._f)
+
+    def quads(self):
+        n = self.num_quads
+        tree = np.zeros(n, np.int32)
+        level = np.zeros(n, np.int32)
+        x = np.zeros(n, np.int64)
+        y = np.zeros(n, np.int64)
+        check(lib().amrgpu_forest_quads(self._f, ip(tree), ip(level), _p(x, C.c_int64), _p(y, C.c_int64)))
+        return tree, level, x, y
+
+    def begin_regrid(self):
+        lib().amrgpu_forest_begin_regrid(self._f)
+
+    def refine(self, flags, max_level=30):
+        fl = np.ascontiguousarray(flags, dtype=np.int32)
+        assert len(fl) == self.num_quads
+        return lib().amrgpu_forest_refine(self._f, ip(fl), int(max_level))
+
+    def coarsen(self, flags, min_level=0):
+        fl = np.ascontiguousarray(flags, dtype=np.int32)
+        assert len(fl) == self.num_quads
+        return lib().amrgpu_forest_coarsen(self._f, ip(fl), int(min_level))
+
+    def balance(self):
+        r = lib().amrgpu_forest_balance(self._f)
+        if r < 0:
+            raise AmrGpuError(3, "forest_balance")
+        return r
+
+    def is_balanced(self):
+        return bool(lib().amrgpu_forest_is_balanced(self._f))
+
+    def set_tags(self, tags):
+        t = np.ascontiguousarray(tags, dtype=np.int32)
+        check(lib().amrgpu_forest_set_tags(self._f, ip(t)))
+
+    def get_tags(self):
+        t = np.zeros(self.num_quads, np.int32)
+        check(lib().amrgpu_forest_get_tags(self._f, ip(t)))
+        return t
+
+    def remap(self):
+        n = self.num_quads
+        kind = np.zeros(n, np.int32)
+        src = np.zeros(n, np.int32)
+        check(lib().amrgpu_forest_remap(self._f, ip(kind), ip(src)))
+        return kind, src
+
+    def mesh(self, n):
+        L = lib()
+        nq = self.num_quads
+        cell_info = np.zeros(3 * nq, np.int32)
+        face_info = np.full(11 * max(L.amrgpu_forest_max_faces(self._f), 1), -1, np.int32)
+        geom = np.zeros(12 * nq, np.float64)
+        nface = C.c_int(0)
+        dof = C.c_int(0)
+        check(L.amrgpu_forest_external(self._f, int(n), NFIELDS, ip(cell_info), ip(face_info), dp(geom),
+                                       C.byref(nface), C.byref(dof)), "forest_external")
+        return Mesh(n, cell_info, face_info[: 11 * nface.value].copy(), geom, nface.value, dof.value)
+
+    def initialize(self, n):
+        """Initial condition of every quad from the global configuration (AoS)."""
+        soln = np.zeros(NFIELDS * n * n * self.num_quads, np.float64)
+        check(lib().amrgpu_forest_initialize(self._f, int(n), dp(soln)), "forest_initialize")
+        return soln
+
+
+# --------------------------------------------------------------------- session
+class Session:
+    """Device-resident state of one mesh epoch (see amrgpu_session_* in amrgpu.h)."""
+
+    def __init__(self, mesh, config=None, form=None):
+        L = lib()
+        if config is not None:
+            if form is not None:
+                config["form"] = form
+            config.apply()
+        elif form is not None:
+            c = Config.current()
+            c["form"] = form
+            c.apply()
+        self.mesh = mesh
+        h = C.c_void_p()
+        ms = mesh.struct()
+        check(L.amrgpu_session_create(C.byref(h), C.byref(ms), None), "session_create")
+        self._s = h
+
+    def close(self):
+        if getattr(self, "_s", None):
+            lib().amrgpu_session_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        self.close()
+
+    def set_form(self, form):
+        check(lib().amrgpu_session_set_form(self._s, int(form)), "set_form")
+
+    def set_launch(self, qpb, threads):
+        check(lib().amrgpu_session_set_launch(self._s, int(qpb), int(threads)), "set_launch")
+
+    def upload(self, soln):
+        a = np.ascontiguousarray(soln, dtype=np.float64)
+        check(lib().amrgpu_session_upload(self._s, dp(a)), "upload")
+
+    def download(self):
+        out = np.empty(self.mesh.dof, np.float64)
+        check(lib().amrgpu_session_download(self._s, dp(out)), "download")
+        return out
+
+    def step(self, nsteps, graph_steps=0):
+        if graph_steps:
+            check(lib().amrgpu_session_step_graph(self._s, int(nsteps), int(graph_steps)), "step_graph")
+        else:
+            check(lib().amrgpu_session_step(self._s, int(nsteps)), "step")
+
+    def sync(self):
+        r = ReportStruct()
+        check(lib().amrgpu_session_sync(self._s, C.byref(r)), "sync")
+        return {"steps": r.steps_done, "time": r.time, "dt_last": r.dt_last,
+                "residual_norm": r.residual_norm, "error": r.error, "nan": r.nan_detected}
+
+    def rhs(self):
+        out = np.empty(self.mesh.dof, np.float64)
+        check(lib().amrgpu_session_rhs(self._s, dp(out)), "rhs")
+        return out
+
+    def cfl_dt(self):
+        v = C.c_double(0.0)
+        check(lib().amrgpu_session_cfl_dt(self._s, C.byref(v)), "cfl_dt")
+        return v.value
+
+    def totals(self):
+        t = np.zeros(4, np.float64)
+        check(lib().amrgpu_session_totals(self._s, dp(t)), "totals")
+        return t
+
+    def tag(self):
+        t = np.zeros(self.mesh.ncell, np.int32)
+        check(lib().amrgpu_session_tag(self._s, ip(t)), "tag")
+        return t
+
+    def remap_from(self, other, kind, src):
+        k = np.ascontiguousarray(kind, np.int32)
+        s = np.ascontiguousarray(src, np.int32)
+        check(lib().amrgpu_session_remap(self._s, other._s, ip(k), ip(s)), "remap")
+
+    def state_ptr(self, field):
+        return lib().amrgpu_session_state_device(self._s, int(field))
+
+    def stream(self):
+        return lib().amrgpu_session_stream(self._s)
+
+    def launch_count(self):
+        return lib().amrgpu_session_launch_count(self._s)
+
+
+# --------------------------------------------------------------------- reference ABI
+def initialize_solver(mesh_scale, nelem_subgrid, nlevels=0, rank=0):
+    """hpc_amr_initialize_solver: reads input.physics from the working directory."""
+    L = lib()
+    L.hpc_amr_initialize_solver(_iref(rank), _iref(2), C.byref(C.c_double(mesh_scale)), _iref(nlevels),
+                                _iref(NFIELDS), _iref(2), _iref(nelem_subgrid), _iref(3), _iref(11),
+                                _iref(0), _iref(0), _iref(2))
+    return L.amrgpu_last_error()
+
+
+def evolve_solver(mesh, soln, istep, entry="hpc_amr_evolve_solver"):
+    """One call of the reference's evolve entry point on host arrays.
+
+    ``soln`` (AoS, dof doubles) is updated in place. Returns a dict with
+    istep, the regrid/visualize/checkpoint/evolve_solution flags and the
+    three accumulated timers, as src/amr/src/amr_external.c:85-106 sees them.
+    """
+    L = lib()
+    fn = getattr(L, entry)
+    dim, uns, nf, n = C.c_int(2), C.c_int(0), C.c_int(NFIELDS), C.c_int(mesh.n)
+    ncell, nghost, nface, dof = C.c_int(mesh.ncell), C.c_int(0), C.c_int(mesh.nface), C.c_int(mesh.dof)
+    nsend, nrecv = C.c_int(0), C.c_int(0)
+    send = np.zeros(2, np.int32)
+    recv = np.zeros(2, np.int32)
+    sizes = np.full(max(mesh.ncell, 1), NFIELDS * mesh.n * mesh.n, np.int32)
+    ist = C.c_int(int(istep))
+    regrid, vis, chk, evo = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(1)
+    tt, ct, rt = C.c_double(0), C.c_double(0), C.c_double(0)
+    assert soln.dtype == np.float64 and soln.flags.c_contiguous
+    fn(C.byref(dim), C.byref(uns), C.byref(nf), C.byref(n), C.byref(ncell), C.byref(nghost), C.byref(nface),
+       C.byref(dof), ip(mesh.cell_info), ip(mesh.face_info), C.byref(nsend), C.byref(nrecv), ip(send), ip(recv),
+       ip(sizes), dp(mesh.geom), dp(soln), C.byref(ist), C.byref(regrid), C.byref(vis), C.byref(chk),
+       C.byref(evo), 0, C.byref(tt), C.byref(ct), C.byref(rt))
+    return {"istep": ist.value, "regrid": regrid.value, "visualize": vis.value, "checkpoint": chk.value,
+            "evolve_solution": evo.value, "total_time": tt.value, "compute_time": ct.value,
+            "residual_time": rt.value, "error": L.amrgpu_last_error()}
+
+
+def last_error():
+    L = lib()
+    return L.amrgpu_last_error(), L.amrgpu_last_error_message().decode(errors="replace")
+
+
+def clear_error():
+    lib().amrgpu_clear_error()

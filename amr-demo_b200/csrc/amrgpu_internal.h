@@ -1,0 +1,95 @@
+// amrgpu_internal.h -- declarations shared by the host C++ and CUDA sources
+// of libamrgpu. Nothing here is part of the public C ABI (include/amrgpu.h).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "amrgpu.h"
+
+namespace amrgpu {
+
+// ---------------------------------------------------------------- forest
+enum { kRemapCopy = 0, kRemapAverage = 1 };
+
+struct Leaf {
+    int tree;
+    int level;
+    int64_t x, y;   // lower corner in units of 2^-30 of the tree
+    int tag;        // refinement tag carried through a regrid
+    int type;       // cell type (cell_info[0])
+    int src;        // provenance within the current regrid (see forest_begin_regrid)
+    int src_kind;   // kRemapCopy: data of old leaf src; kRemapAverage: mean of old src..src+3
+};
+
+struct Forest;
+Forest *forest_new_brick(int nx, int ny, int px, int py, double xlo, double ylo, double zlo,
+                         double scale, int level);
+void forest_destroy(Forest *f);
+int forest_num_quads(const Forest *f);
+const std::vector<Leaf> &forest_leaves(const Forest *f);
+std::vector<Leaf> &forest_leaves_mut(Forest *f);
+void forest_begin_regrid(Forest *f);
+int forest_refine(Forest *f, const int *flags, int max_level);
+int forest_coarsen(Forest *f, const int *flags, int min_level);
+int forest_balance(Forest *f);
+bool forest_is_balanced(const Forest *f);
+void forest_quad_corners(const Forest *f, const Leaf &q, double xyz[12]);
+double forest_quad_h(const Forest *f, const Leaf &q);
+int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_info,
+                    int *face_info, double *geom, int *nface_out, int *dof_out);
+
+// ---------------------------------------------------------------- config
+// The reference's physics configuration (physics_var_physics.h,
+// physics_var_simulation.h, physics_var_interface.h), parsed with the same
+// keyword rules as physics_initialize.c:61-197.
+struct PhysicsConfig {
+    int dim = 2;
+    int nfields = 4;
+    int nfringe = 2;
+    int nelem_subgrid = 2;
+    int extern_cell_size = 3;
+    int extern_face_size = 11;
+    int extern_mpi_comm_size = 2;
+    int nlevels = 0;
+    double coarse_grid_h = 1.0;
+
+    int initial_condition = 1;
+    int bc[6] = {1, 1, 1, 1, 1, 1};
+    int amr_ntag_methods = 0;
+    std::vector<int> amr_tag_methods;
+    std::vector<double> amr_tag_tolerances;
+    double cfl = 1.0;  // already scaled by 0.25*time_scheme when read from a file
+    double mach = 0.1, alpha = 0.0, beta = 0.0, gamma = 1.4, density = 1.0, pressure = 1.0 / 1.4;
+
+    int checkpoint_interval = 2147483647;
+    int visualization_interval = 2147483647;
+    int regrid_interval = 2147483647;
+    int time_scheme = 1;
+    int time_steps = 1;
+    double dt = 0.001;
+
+    // extensions (no reference counterpart)
+    int form = AMRGPU_FORM_FP64_EXACT;
+    double final_time = 0.0;  // > 0: stop at this simulated time, last step clipped
+    int abort_on_nan = 0;
+    double ic_params[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t ic_seed = 0;
+    double noise_amplitude = 0.0;
+};
+
+PhysicsConfig &global_config();
+int parse_physics_file(const char *path, PhysicsConfig &cfg);
+
+// ---------------------------------------------------------------- errors
+void set_error(int code, const std::string &msg);
+int last_error();
+
+// ---------------------------------------------------------------- host ICs
+void initialize_quadrant_host(const PhysicsConfig &cfg, int nfields, int n, int *cell_type,
+                              double h, const double *geom, double *soln, int64_t first_cell_id);
+void shock_state(double gamma, double ms, double rho1, double p1, double out[4]);
+void tag_feature_host(const PhysicsConfig &cfg, int nfields, int n, const double *soln, int *tag);
+
+}  // namespace amrgpu

@@ -1,0 +1,56 @@
+// device_common.cuh -- device-side data layout shared by all kernels.
+//
+// State in HBM is structure-of-arrays: field f of cell c of quad q lives at
+// Q[f][q*n*n + j*n + i] (i fastest), so a quad's patch is four contiguous
+// n*n slabs of doubles. Per quad the kernels read a 128-byte QuadDesc with
+// its four sides' neighbour descriptions and its corner coordinates.
+#pragma once
+
+#include <cstdint>
+
+namespace amrgpu {
+
+enum SideKind : int {
+    kSideNone = 0,
+    kSideBoundary = 1,   // physical boundary: bc flux on this quad only
+    kSideFull = 2,       // conforming neighbour nbr0
+    kSideCoarseHang = 3, // this quad is coarse; fine neighbours nbr0, nbr1
+    kSideFineHang = 4    // this quad is one of two fine quads; coarse nbr0
+};
+
+struct SideDesc {
+    int kind;
+    int nbr0;
+    int nbr1;
+    int rank;   // position of the face in face_info: order of accumulation
+    int level;  // level whose cell_h sizes the face normal
+    int bc;     // boundary condition type for kSideBoundary
+};
+
+struct QuadDesc {
+    SideDesc side[4];   // 96 bytes
+    double corner[8];   // x,y of n1(-,-) n2(+,-) n3(-,+) n4(+,+): 64 bytes
+};
+static_assert(sizeof(QuadDesc) == 160, "QuadDesc layout");
+
+// Per-step scalars kept on the device, cycled over three slots so that a
+// step reads slot s%3, writes its successor's dt candidates into (s+1)%3 and
+// re-arms (s+2)%3 without racing concurrently running blocks.
+struct StepSlot {
+    unsigned long long dt_bits;  // min over cells of the CFL step, as uint64 image
+    double time;                 // simulated time at the start of the step
+};
+
+struct DeviceScalars {
+    StepSlot slot[3];
+    double norm_sq;           // sum of k^2 of the last stage of the last step
+    double dt_used;           // step size of the last step
+    unsigned int done_blocks; // last-block-done counter for the norm reduction
+    int flags;                // bit 0: non-finite residual, bit 1: rho<=0 or p<=0
+    int steps;                // steps taken with a positive step size
+    int pad;
+};
+
+enum { kFlagNonFinite = 1, kFlagNegative = 2 };
+
+}  // namespace amrgpu

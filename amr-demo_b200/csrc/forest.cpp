@@ -1,0 +1,493 @@
+// forest.cpp -- host quadtree forest on a brick of trees.
+//
+// Stands in for the p4est forest that the reference's AMR driver owns
+// (src/amr/src/amr_initialize.c:213-314, amr_regrid.c:101-125,
+// amr_external.c:211-508), which is not available here. It produces the
+// same flat arrays the reference hands to hpc_amr_evolve_solver:
+//   cell_info  3 ints per quad  {type, level, soln offset = 4 n^2 * id}
+//              (amr_external.c:358-360)
+//   face_info 11 ints per face  {ftype 1 boundary / 2 full / 3 hanging,
+//              side of the full (or only) quad, its id, 4 neighbour ids,
+//              4 neighbour sides}                (amr_external.c:389-507)
+//   geom      12 doubles per quad, corners n1(-,-) n2(+,-) n3(-,+) n4(+,+)
+//              (amr_p4est_utilities.c:15-81)
+//
+// Semantics kept from p4est: trees of a brick are numbered along the
+// Morton curve of their (tx,ty) position; leaves are ordered by tree, then
+// Morton index; refine replaces a leaf by its four z-ordered children;
+// coarsen replaces a complete family by its parent; balance enforces the
+// 2:1 condition across faces and corners (P4EST_CONNECT_FULL).
+//
+// Deliberate, documented choices where p4est's behaviour is not part of the
+// solver arithmetic: faces are listed in order of the first leaf (in Morton
+// order) that touches them, sides 0..3; for a full face side[0] follows
+// p4est's rule (lower quadrant inside a tree, lower tree / lower face
+// across trees); a refined child inherits its parent's tag.
+#include "amrgpu_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+namespace amrgpu {
+
+namespace {
+
+constexpr int kMaxLevel = 30;
+constexpr int64_t kRootLen = int64_t(1) << kMaxLevel;
+
+inline int64_t qlen(int level) { return int64_t(1) << (kMaxLevel - level); }
+
+inline uint64_t spread_bits(uint64_t v)
+{
+    v &= 0x3fffffffULL;
+    v = (v | (v << 16)) & 0x0000ffff0000ffffULL;
+    v = (v | (v << 8)) & 0x00ff00ff00ff00ffULL;
+    v = (v | (v << 4)) & 0x0f0f0f0f0f0f0f0fULL;
+    v = (v | (v << 2)) & 0x3333333333333333ULL;
+    v = (v | (v << 1)) & 0x5555555555555555ULL;
+    return v;
+}
+
+inline uint64_t morton(int64_t x, int64_t y) { return spread_bits(uint64_t(x)) | (spread_bits(uint64_t(y)) << 1); }
+
+struct Key {
+    int tree, level;
+    int64_t x, y;
+    bool operator==(const Key &o) const { return tree == o.tree && level == o.level && x == o.x && y == o.y; }
+};
+struct KeyHash {
+    size_t operator()(const Key &k) const
+    {
+        uint64_t h = morton(k.x >> 0, k.y >> 0) * 0x9E3779B97F4A7C15ULL;
+        h ^= uint64_t(k.tree) * 0xC2B2AE3D27D4EB4FULL + uint64_t(k.level);
+        return size_t(h ^ (h >> 29));
+    }
+};
+
+}  // namespace
+
+struct Forest {
+    int nx = 1, ny = 1;
+    int periodic[2] = {0, 0};
+    double xlo[3] = {0, 0, 0};
+    double scale = 1.0;
+    // tree id -> brick position and back
+    std::vector<int> tree_tx, tree_ty;
+    std::vector<int> tree_at;  // [ty*nx+tx] -> tree id
+    std::vector<Leaf> leaves;
+
+    int tree_of(int tx, int ty) const { return tree_at[size_t(ty) * nx + tx]; }
+
+    void sort_leaves()
+    {
+        std::sort(leaves.begin(), leaves.end(), [](const Leaf &a, const Leaf &b) {
+            if (a.tree != b.tree) return a.tree < b.tree;
+            return morton(a.x, a.y) < morton(b.x, b.y);
+        });
+    }
+
+    std::unordered_map<Key, int, KeyHash> index() const
+    {
+        std::unordered_map<Key, int, KeyHash> m;
+        m.reserve(leaves.size() * 2);
+        for (size_t i = 0; i < leaves.size(); ++i)
+            m.emplace(Key{leaves[i].tree, leaves[i].level, leaves[i].x, leaves[i].y}, int(i));
+        return m;
+    }
+
+    // Same-level neighbour region of (tree,level,x,y) across offset (dx,dy)
+    // in units of the quadrant length; false when it leaves the domain.
+    bool shifted(int tree, int level, int64_t x, int64_t y, int dx, int dy, Key &out) const
+    {
+        int64_t L = qlen(level);
+        int64_t nxq = x + dx * L, nyq = y + dy * L;
+        int tx = tree_tx[tree], ty = tree_ty[tree];
+        if (nxq < 0) { nxq += kRootLen; tx -= 1; }
+        if (nxq >= kRootLen) { nxq -= kRootLen; tx += 1; }
+        if (nyq < 0) { nyq += kRootLen; ty -= 1; }
+        if (nyq >= kRootLen) { nyq -= kRootLen; ty += 1; }
+        if (tx < 0 || tx >= nx) {
+            if (!periodic[0]) return false;
+            tx = (tx + nx) % nx;
+        }
+        if (ty < 0 || ty >= ny) {
+            if (!periodic[1]) return false;
+            ty = (ty + ny) % ny;
+        }
+        out = Key{tree_of(tx, ty), level, nxq, nyq};
+        return true;
+    }
+
+    // Leaf that equals or contains the region k; -1 when the region is
+    // subdivided further (or absent).
+    static int containing_leaf(const std::unordered_map<Key, int, KeyHash> &m, Key k)
+    {
+        for (int l = k.level; l >= 0; --l) {
+            int64_t L = qlen(l);
+            Key a{k.tree, l, (k.x / L) * L, (k.y / L) * L};
+            auto it = m.find(a);
+            if (it != m.end()) return it->second;
+        }
+        return -1;
+    }
+};
+
+namespace {
+
+void side_offset(int side, int &dx, int &dy)
+{
+    dx = 0; dy = 0;
+    switch (side) {
+    case 0: dx = -1; break;
+    case 1: dx = 1; break;
+    case 2: dy = -1; break;
+    case 3: dy = 1; break;
+    }
+}
+
+}  // namespace
+
+Forest *forest_new_brick(int nx, int ny, int px, int py, double xlo, double ylo, double zlo,
+                         double scale, int level)
+{
+    if (nx < 1 || ny < 1 || level < 0 || level > kMaxLevel) return nullptr;
+    Forest *f = new Forest;
+    f->nx = nx; f->ny = ny;
+    f->periodic[0] = px ? 1 : 0; f->periodic[1] = py ? 1 : 0;
+    f->xlo[0] = xlo; f->xlo[1] = ylo; f->xlo[2] = zlo;
+    f->scale = scale;
+    std::vector<std::pair<uint64_t, int>> order;
+    for (int ty = 0; ty < ny; ++ty)
+        for (int tx = 0; tx < nx; ++tx) order.push_back({morton(tx, ty), ty * nx + tx});
+    std::sort(order.begin(), order.end());
+    f->tree_tx.resize(order.size());
+    f->tree_ty.resize(order.size());
+    f->tree_at.resize(order.size());
+    for (size_t t = 0; t < order.size(); ++t) {
+        int lin = order[t].second;
+        f->tree_tx[t] = lin % nx;
+        f->tree_ty[t] = lin / nx;
+        f->tree_at[size_t(lin)] = int(t);
+    }
+    int64_t per = int64_t(1) << level;
+    int64_t L = qlen(level);
+    f->leaves.reserve(size_t(nx) * ny * per * per);
+    for (int t = 0; t < nx * ny; ++t)
+        for (int64_t j = 0; j < per; ++j)
+            for (int64_t i = 0; i < per; ++i) {
+                Leaf q;
+                q.tree = t; q.level = level; q.x = i * L; q.y = j * L;
+                q.tag = 0; q.type = 0;
+                f->leaves.push_back(q);
+            }
+    f->sort_leaves();
+    forest_begin_regrid(f);
+    return f;
+}
+
+void forest_destroy(Forest *f) { delete f; }
+
+int forest_num_quads(const Forest *f) { return int(f->leaves.size()); }
+
+const std::vector<Leaf> &forest_leaves(const Forest *f) { return f->leaves; }
+std::vector<Leaf> &forest_leaves_mut(Forest *f) { return f->leaves; }
+
+void forest_begin_regrid(Forest *f)
+{
+    for (size_t i = 0; i < f->leaves.size(); ++i) {
+        f->leaves[i].src = int(i);
+        f->leaves[i].src_kind = kRemapCopy;
+    }
+}
+
+int forest_refine(Forest *f, const int *flags, int max_level)
+{
+    std::vector<Leaf> out;
+    out.reserve(f->leaves.size() + 3 * f->leaves.size() / 4);
+    for (size_t i = 0; i < f->leaves.size(); ++i) {
+        const Leaf &p = f->leaves[i];
+        if (flags[i] && p.level < max_level && p.level < kMaxLevel) {
+            int64_t h = qlen(p.level + 1);
+            for (int c = 0; c < 4; ++c) {
+                Leaf ch = p;
+                ch.level = p.level + 1;
+                ch.x = p.x + (c & 1) * h;
+                ch.y = p.y + ((c >> 1) & 1) * h;
+                ch.tag = 1;  // children inherit the refine tag
+                out.push_back(ch);
+            }
+        } else {
+            out.push_back(p);
+        }
+    }
+    f->leaves.swap(out);
+    return int(f->leaves.size());
+}
+
+int forest_coarsen(Forest *f, const int *flags, int min_level)
+{
+    std::vector<Leaf> out;
+    out.reserve(f->leaves.size());
+    size_t i = 0, n = f->leaves.size();
+    while (i < n) {
+        const Leaf &a = f->leaves[i];
+        bool family = false;
+        if (a.level > 0 && a.level > min_level && i + 3 < n) {
+            int64_t L = qlen(a.level - 1);
+            int64_t px = (a.x / L) * L, py = (a.y / L) * L;
+            if (a.x == px && a.y == py) {
+                family = true;
+                for (int c = 0; c < 4 && family; ++c) {
+                    const Leaf &b = f->leaves[i + c];
+                    int64_t h = qlen(a.level);
+                    if (b.tree != a.tree || b.level != a.level || b.x != px + (c & 1) * h ||
+                        b.y != py + ((c >> 1) & 1) * h || !flags[i + c] ||
+                        b.src_kind != kRemapCopy || b.src != f->leaves[i].src + c)
+                        family = false;
+                }
+            }
+        }
+        if (family) {
+            Leaf p = a;
+            p.level = a.level - 1;
+            int64_t L = qlen(p.level);
+            p.x = (a.x / L) * L;
+            p.y = (a.y / L) * L;
+            p.type = f->leaves[i + 3].type;  // the reference keeps the last child's type
+            p.tag = 0;
+            p.src = a.src;
+            p.src_kind = kRemapAverage;
+            out.push_back(p);
+            i += 4;
+        } else {
+            out.push_back(a);
+            ++i;
+        }
+    }
+    f->leaves.swap(out);
+    return int(f->leaves.size());
+}
+
+int forest_balance(Forest *f)
+{
+    // Refine until every leaf's face and corner neighbours are at most one
+    // level coarser (2:1 across faces and corners).
+    for (int iter = 0; iter < 64; ++iter) {
+        auto m = f->index();
+        std::vector<int> flags(f->leaves.size(), 0);
+        bool any = false;
+        for (size_t i = 0; i < f->leaves.size(); ++i) {
+            const Leaf &q = f->leaves[i];
+            if (q.level < 2) continue;
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (!dx && !dy) continue;
+                    Key k;
+                    if (!f->shifted(q.tree, q.level, q.x, q.y, dx, dy, k)) continue;
+                    int c = Forest::containing_leaf(m, k);
+                    if (c >= 0 && f->leaves[size_t(c)].level < q.level - 1 && !flags[size_t(c)]) {
+                        flags[size_t(c)] = 1;
+                        any = true;
+                    }
+                }
+        }
+        if (!any) return int(f->leaves.size());
+        // balance refinement keeps the refined quad's own tag on its children
+        std::vector<Leaf> out;
+        out.reserve(f->leaves.size() * 2);
+        for (size_t i = 0; i < f->leaves.size(); ++i) {
+            const Leaf &p = f->leaves[i];
+            if (flags[i]) {
+                int64_t h = qlen(p.level + 1);
+                for (int c = 0; c < 4; ++c) {
+                    Leaf ch = p;
+                    ch.level = p.level + 1;
+                    ch.x = p.x + (c & 1) * h;
+                    ch.y = p.y + ((c >> 1) & 1) * h;
+                    out.push_back(ch);
+                }
+            } else {
+                out.push_back(p);
+            }
+        }
+        f->leaves.swap(out);
+    }
+    return -1;
+}
+
+bool forest_is_balanced(const Forest *f)
+{
+    auto m = f->index();
+    for (const Leaf &q : f->leaves) {
+        if (q.level < 2) continue;
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                if (!dx && !dy) continue;
+                Key k;
+                if (!f->shifted(q.tree, q.level, q.x, q.y, dx, dy, k)) continue;
+                int c = Forest::containing_leaf(m, k);
+                if (c >= 0 && f->leaves[size_t(c)].level < q.level - 1) return false;
+            }
+    }
+    return true;
+}
+
+// amr_p4est_utilities.c:15-81, 2D branch: corners of a quadrant through the
+// brick tree's vertices (vertex = integer brick position * scale + lo).
+void forest_quad_corners(const Forest *f, const Leaf &q, double xyz[12])
+{
+    const double intsize = 1.0 / double(kRootLen);
+    double h2 = 0.5 * intsize * double(qlen(q.level));
+    int tx = f->tree_tx[size_t(q.tree)], ty = f->tree_ty[size_t(q.tree)];
+    double v[4][3];
+    for (int k = 0; k < 4; ++k) {
+        int vx = tx + (k & 1), vy = ty + ((k >> 1) & 1);
+        v[k][0] = double(vx) * f->scale + f->xlo[0];
+        v[k][1] = double(vy) * f->scale + f->xlo[1];
+        v[k][2] = 0.0 * f->scale + f->xlo[2];
+    }
+    const double eta_z = 0.0;
+    int k = 0;
+    for (int yi = 0; yi < 2; ++yi) {
+        double eta_y = intsize * double(q.y) + h2 * (1.0 + (2 * yi - 1));
+        for (int xi = 0; xi < 2; ++xi) {
+            double eta_x = intsize * double(q.x) + h2 * (1.0 + (2 * xi - 1));
+            for (int j = 0; j < 3; ++j)
+                xyz[3 * k + j] = ((1. - eta_z) * ((1. - eta_y) * ((1. - eta_x) * v[0][j] + eta_x * v[1][j]) +
+                                                  eta_y * ((1. - eta_x) * v[2][j] + eta_x * v[3][j])));
+            ++k;
+        }
+    }
+}
+
+// amr_initialize.c:326 -- quadrant edge length used by the per-quad callbacks
+double forest_quad_h(const Forest *f, const Leaf &q)
+{
+    return f->scale * double(qlen(q.level)) / double(kRootLen);
+}
+
+int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_info,
+                    int *face_info, double *geom, int *nface_out, int *dof_out)
+{
+    const int nq = int(f->leaves.size());
+    const int nftm = nfields * nelem_subgrid * nelem_subgrid;
+    auto m = f->index();
+    for (int i = 0; i < nq; ++i) {
+        const Leaf &q = f->leaves[size_t(i)];
+        cell_info[3 * i + 0] = q.type;
+        cell_info[3 * i + 1] = q.level;
+        cell_info[3 * i + 2] = nftm * i;
+        forest_quad_corners(f, q, &geom[12 * i]);
+    }
+    // done[i*4+side]: this quad side already belongs to an emitted face
+    std::vector<unsigned char> done(size_t(nq) * 4, 0);
+    int nface = 0;
+    auto emit = [&](const int v[11]) {
+        for (int k = 0; k < 11; ++k) face_info[11 * nface + k] = v[k];
+        ++nface;
+    };
+    for (int i = 0; i < nq; ++i) {
+        const Leaf &q = f->leaves[size_t(i)];
+        for (int s = 0; s < 4; ++s) {
+            if (done[size_t(i) * 4 + s]) continue;
+            int dx, dy;
+            side_offset(s, dx, dy);
+            int opp = s ^ 1;
+            int v[11];
+            for (int k = 0; k < 11; ++k) v[k] = -1;
+            Key k;
+            if (!f->shifted(q.tree, q.level, q.x, q.y, dx, dy, k)) {
+                v[0] = 1; v[1] = s; v[2] = i;
+                done[size_t(i) * 4 + s] = 1;
+                emit(v);
+                continue;
+            }
+            auto it = m.find(k);
+            if (it != m.end()) {
+                int j = it->second;
+                // side[0]: lower quadrant inside a tree; across trees the
+                // lower tree id, then the lower face number.
+                bool this_first;
+                int tq = q.tree, tj = f->leaves[size_t(j)].tree;
+                if (tq == tj) {
+                    this_first = (s & 1) == 1;
+                } else {
+                    this_first = (tq < tj) || (tq == tj && s < opp);
+                }
+                if (i == j) this_first = (s & 1) == 0;
+                int a = this_first ? i : j, sa = this_first ? s : opp;
+                int b = this_first ? j : i, sb = this_first ? opp : s;
+                v[0] = 2; v[1] = sa; v[2] = a; v[3] = b; v[7] = sb;
+                done[size_t(i) * 4 + s] = 1;
+                done[size_t(j) * 4 + opp] = 1;
+                emit(v);
+                continue;
+            }
+            // coarser neighbour: this quad is one of two hanging quads
+            if (q.level > 0) {
+                int64_t Lp = qlen(q.level - 1);
+                Key kp{k.tree, q.level - 1, (k.x / Lp) * Lp, (k.y / Lp) * Lp};
+                auto ip = m.find(kp);
+                if (ip != m.end()) {
+                    int c = ip->second;
+                    // the two fine quads on this face, lower coordinate first
+                    int64_t L = qlen(q.level);
+                    int64_t base_x = (q.x / Lp) * Lp, base_y = (q.y / Lp) * Lp;
+                    int fine[2];
+                    for (int h = 0; h < 2; ++h) {
+                        Key kf{q.tree, q.level, base_x, base_y};
+                        if (s < 2) {
+                            kf.x = q.x;
+                            kf.y = base_y + h * L;
+                        } else {
+                            kf.x = base_x + h * L;
+                            kf.y = q.y;
+                        }
+                        auto ifn = m.find(kf);
+                        fine[h] = ifn == m.end() ? -1 : ifn->second;
+                    }
+                    if (fine[0] < 0 || fine[1] < 0) return -2;
+                    v[0] = 3; v[1] = opp; v[2] = c;
+                    v[3] = fine[0]; v[4] = fine[1]; v[7] = s; v[8] = s;
+                    done[size_t(c) * 4 + opp] = 1;
+                    done[size_t(fine[0]) * 4 + s] = 1;
+                    done[size_t(fine[1]) * 4 + s] = 1;
+                    emit(v);
+                    continue;
+                }
+            }
+            // finer neighbours: this quad is the full side of a hanging face
+            {
+                int64_t Lc = qlen(q.level + 1);
+                int fine[2];
+                for (int h = 0; h < 2; ++h) {
+                    Key kf{k.tree, q.level + 1, k.x, k.y};
+                    if (s < 2) {
+                        kf.x = (s == 0) ? k.x + Lc : k.x;
+                        kf.y = k.y + h * Lc;
+                    } else {
+                        kf.x = k.x + h * Lc;
+                        kf.y = (s == 2) ? k.y + Lc : k.y;
+                    }
+                    auto ifn = m.find(kf);
+                    fine[h] = ifn == m.end() ? -1 : ifn->second;
+                }
+                if (fine[0] < 0 || fine[1] < 0) return -3;  // not 2:1 balanced
+                v[0] = 3; v[1] = s; v[2] = i;
+                v[3] = fine[0]; v[4] = fine[1]; v[7] = opp; v[8] = opp;
+                done[size_t(i) * 4 + s] = 1;
+                done[size_t(fine[0]) * 4 + opp] = 1;
+                done[size_t(fine[1]) * 4 + opp] = 1;
+                emit(v);
+            }
+        }
+    }
+    *nface_out = nface;
+    *dof_out = nftm * nq;
+    return 0;
+}
+
+}  // namespace amrgpu

@@ -1,0 +1,744 @@
+// host_physics.cpp -- host side of the reference's physics layer that is
+// not on the GPU path: configuration (input.physics), error state, the
+// per-quadrant callbacks of the ABI (initial condition, tagging,
+// refine/coarsen operators, regrid points) and the host forest's C API.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "amrgpu_internal.h"
+
+namespace amrgpu {
+
+// ------------------------------------------------------------------ errors
+static thread_local int g_error = AMRGPU_OK;
+static thread_local std::string g_error_msg;
+
+void set_error(int code, const std::string &msg)
+{
+    g_error = code;
+    g_error_msg = msg;
+    if (code != AMRGPU_OK && std::getenv("AMRGPU_VERBOSE"))
+        std::fprintf(stderr, "[amrgpu] error %d: %s\n", code, msg.c_str());
+}
+
+int last_error() { return g_error; }
+
+// ------------------------------------------------------------------ config
+PhysicsConfig &global_config()
+{
+    static PhysicsConfig cfg;
+    return cfg;
+}
+
+// physics_utilities.c: a line containing the keyword is parsed from
+// offset strlen(keyword) of the line (not from the match position).
+static bool find_line(const char *path, const char *kw, std::string &rest)
+{
+    FILE *fp = std::fopen(path, "r");
+    if (!fp) return false;
+    char buff[1024];
+    size_t len = std::strlen(kw);
+    bool found = false;
+    while (std::fgets(buff, sizeof(buff), fp)) {
+        if (std::strstr(buff, kw)) {
+            size_t bl = std::strlen(buff);
+            rest = (len < bl) ? std::string(buff + len) : std::string();
+            found = true;
+            break;
+        }
+    }
+    std::fclose(fp);
+    return found;
+}
+
+static void kw_int(const char *path, const char *kw, int &v)
+{
+    std::string r;
+    if (find_line(path, kw, r)) v = std::atoi(r.c_str());
+}
+
+static void kw_double(const char *path, const char *kw, double &v)
+{
+    std::string r;
+    if (find_line(path, kw, r)) v = std::atof(r.c_str());
+}
+
+static int kw_ints(const char *path, const char *kw, int *v, int n)
+{
+    std::string r;
+    if (!find_line(path, kw, r)) return 1;
+    const char *p = r.c_str();
+    for (int i = 0; i < n; ++i) {
+        char *end;
+        long x = std::strtol(p, &end, 10);
+        if (end == p) break;
+        v[i] = int(x);
+        p = end;
+        while (*p == ',' || *p == ' ' || *p == '\t') ++p;
+    }
+    return 0;
+}
+
+static int kw_doubles(const char *path, const char *kw, double *v, int n)
+{
+    std::string r;
+    if (!find_line(path, kw, r)) return 1;
+    const char *p = r.c_str();
+    for (int i = 0; i < n; ++i) {
+        char *end;
+        double x = std::strtod(p, &end);
+        if (end == p) break;
+        v[i] = x;
+        p = end;
+        while (*p == ',' || *p == ' ' || *p == '\t') ++p;
+    }
+    return 0;
+}
+
+// physics_initialize.c:61-197 and :312-316
+int parse_physics_file(const char *path, PhysicsConfig &c)
+{
+    FILE *fp = std::fopen(path, "r");
+    if (!fp) return AMRGPU_ERR_CONFIG;
+    std::fclose(fp);
+    c.initial_condition = 1;
+    c.time_scheme = 1;
+    c.time_steps = 1;
+    c.dt = 0.001;
+    c.alpha = 0.0;
+    c.beta = 0.0;
+    for (int k = 0; k < 6; ++k) c.bc[k] = 1;
+    c.cfl = 1.0;
+    c.gamma = 1.4;
+    c.density = 1.0;
+    c.pressure = 1.0 / 1.4;
+    c.mach = 0.1;
+    c.amr_ntag_methods = 0;
+    c.amr_tag_methods.clear();
+    c.amr_tag_tolerances.clear();
+    int ci = 0, vi = 0, ri = 0;
+    kw_int(path, "checkpoint_interval:", ci);
+    kw_int(path, "visualization_interval:", vi);
+    kw_int(path, "regrid_interval:", ri);
+    int nt = 0;
+    std::string dummy;
+    if (find_line(path, "amr_ntag_methods:", dummy)) {
+        kw_int(path, "amr_ntag_methods:", nt);
+        if (nt == 0) {
+            c.amr_tag_methods = {0};
+            c.amr_tag_tolerances = {1.0};
+        } else if (nt >= 1 && nt <= 5) {
+            c.amr_tag_methods.assign(size_t(nt), 0);
+            c.amr_tag_tolerances.assign(size_t(nt), 0.0);
+            kw_ints(path, "amr_tag_methods:", c.amr_tag_methods.data(), nt);
+            kw_doubles(path, "amr_tag_tolerances:", c.amr_tag_tolerances.data(), nt);
+        }
+        c.amr_ntag_methods = nt;
+    }
+    kw_int(path, "initial_condition:", c.initial_condition);
+    kw_int(path, "time_scheme:", c.time_scheme);
+    kw_int(path, "time_steps:", c.time_steps);
+    kw_double(path, "dt:", c.dt);
+    kw_int(path, "bc_xlo:", c.bc[0]);
+    kw_int(path, "bc_xhi:", c.bc[1]);
+    kw_int(path, "bc_ylo:", c.bc[2]);
+    kw_int(path, "bc_yhi:", c.bc[3]);
+    kw_int(path, "bc_zlo:", c.bc[4]);
+    kw_int(path, "bc_zhi:", c.bc[5]);
+    kw_double(path, "alpha:", c.alpha);
+    kw_double(path, "beta:", c.beta);
+    kw_double(path, "cfl:", c.cfl);
+    kw_double(path, "gamma:", c.gamma);
+    kw_double(path, "density:", c.density);
+    kw_double(path, "pressure:", c.pressure);
+    kw_double(path, "mach:", c.mach);
+    c.cfl = 0.25 * c.cfl * c.time_scheme;
+    // extensions (keywords the reference does not read)
+    kw_int(path, "gpu_form:", c.form);
+    kw_double(path, "final_time:", c.final_time);
+    kw_doubles(path, "ic_params:", c.ic_params, 8);
+    {
+        std::string r;
+        if (find_line(path, "ic_seed:", r)) c.ic_seed = std::strtoull(r.c_str(), nullptr, 10);
+    }
+    kw_double(path, "noise_amplitude:", c.noise_amplitude);
+    const int MAX_INT = 2147483647;
+    c.checkpoint_interval = ci <= 0 ? MAX_INT : ci;
+    c.visualization_interval = vi <= 0 ? MAX_INT : vi;
+    c.regrid_interval = ri <= 0 ? MAX_INT : ri;
+    return AMRGPU_OK;
+}
+
+// ------------------------------------------------------------------ noise
+static inline uint64_t splitmix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ULL;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+    return x ^ (x >> 31);
+}
+
+// uniform in [-1, 1) from (seed, stream id)
+static inline double unit_noise(uint64_t seed, uint64_t id)
+{
+    uint64_t h = splitmix64(seed ^ splitmix64(id));
+    return double(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}
+
+static inline double uniform(uint64_t seed, uint64_t id, double lo, double hi)
+{
+    return lo + (hi - lo) * 0.5 * (unit_noise(seed, id) + 1.0);
+}
+
+// bilinear_node_2d_module.F90:14-36
+static void bilinear(const double *g, double xi, double eta, double out[2])
+{
+    double oneMxi = 0.5 * (1.0 - xi), onePxi = 0.5 * (1.0 + xi);
+    double oneMeta = 0.5 * (1.0 - eta), onePeta = 0.5 * (1.0 + eta);
+    for (int c = 0; c < 2; ++c)
+        out[c] = g[c] * oneMxi * oneMeta + g[c + 3] * onePxi * oneMeta + g[c + 6] * oneMxi * onePeta +
+                 g[c + 9] * onePxi * onePeta;
+}
+
+// Post-shock state of a planar shock of Mach ms running into gas at rest
+// (rho1, p1): Rankine-Hugoniot relations. Used by IC 5 and bc 3.
+void shock_state(double gamma, double ms, double rho1, double p1, double out[4])
+{
+    double c1 = std::sqrt(gamma * p1 / rho1);
+    double m2 = ms * ms;
+    double rho2 = rho1 * (gamma + 1.0) * m2 / ((gamma - 1.0) * m2 + 2.0);
+    double p2 = p1 * (1.0 + 2.0 * gamma / (gamma + 1.0) * (m2 - 1.0));
+    double u2 = ms * c1 * (1.0 - rho1 / rho2);
+    out[0] = rho2;
+    out[1] = rho2 * u2;
+    out[2] = 0.0;
+    out[3] = p2 / (gamma - 1.0) + 0.5 * rho2 * u2 * u2;
+}
+
+// initial_condition_2d_module.F90:12-131 for IC 0 and 1 (reference), and
+// the extension ICs 2-5 used by the benchmark workloads:
+//   2 planar Riemann: x < p0 (default 0.5) -> (1,0,0,1) else (0.125,0,0,0.1)
+//   3 four-quadrant Riemann split at (p0,p1) (default 0.5,0.5); per
+//     quadrant rho,p ~ U[0.1,1.5], u,v ~ U[-0.8,0.8] from ic_seed
+//   4 isentropic vortex of the reference's form centred at (p0,p1) with
+//     strength p2 (beta) and a = p3 (default 0.5), free stream from
+//     density/pressure/mach/alpha/beta
+//   5 shock-bubble: ambient (rho,p)=(1,1) at rest, Mach p0 (default 2)
+//     shock at x = p1 (default 0.1), bubble of density p2 (default 0.1375)
+//     radius p3 (default 0.2), centre drawn from ic_seed in
+//     [0.6,0.9]x[0.4,0.6]
+// plus uniform density noise of amplitude noise_amplitude keyed by
+// (ic_seed, global cell id).
+void initialize_quadrant_host(const PhysicsConfig &c, int nf, int n, int *cell_type, double h,
+                              const double *g, double *Q, int64_t first_cell_id)
+{
+    (void)h;
+    *cell_type = 0;
+    const double PI_DP = 3.141592653589793238462643383279502884197;
+    const double TWOPI_DP = 6.283185307179586476925286766559005768394;
+    double gamma = c.gamma;
+    double gm1 = gamma - 1.0;
+    double oneOgm1 = 1.0 / gm1;
+    double RT0 = c.pressure / c.density;
+    double C_0 = std::sqrt(gamma * RT0);
+    double V_0 = c.mach * C_0;
+    double u_in = V_0 * std::cos(c.alpha * PI_DP / 180.0) * std::cos(c.beta * PI_DP / 180.0);
+    double v_in = V_0 * std::sin(c.alpha * PI_DP / 180.0) * std::cos(c.beta * PI_DP / 180.0);
+    double rhou = c.density * u_in;
+    double rhov = c.density * v_in;
+    double rhoe = (c.pressure * oneOgm1) + 0.5 * c.density * (u_in * u_in + v_in * v_in);
+    double s = 2.0 / double(n);
+    auto at = [&](int f, int i, int j) -> double & { return Q[f + nf * ((i - 1) + n * (j - 1))]; };
+    auto centre = [&](int i, int j, double out[2]) {
+        double v1 = s * double(j - 1) - 1.0, v2 = s * double(j) - 1.0;
+        double w1 = s * double(i - 1) - 1.0, w2 = s * double(i) - 1.0;
+        bilinear(g, 0.5 * (w1 + w2), 0.5 * (v1 + v2), out);
+    };
+    auto set_prim = [&](int i, int j, double rho, double u, double v, double p) {
+        at(0, i, j) = rho;
+        at(1, i, j) = rho * u;
+        at(2, i, j) = rho * v;
+        at(3, i, j) = p * oneOgm1 + 0.5 * rho * (u * u + v * v);
+    };
+    const double *P = c.ic_params;
+    switch (c.initial_condition) {
+    case 0:
+        for (int j = 1; j <= n; ++j)
+            for (int i = 1; i <= n; ++i) {
+                at(0, i, j) = c.density;
+                at(1, i, j) = rhou;
+                at(2, i, j) = rhov;
+                at(3, i, j) = rhoe;
+            }
+        break;
+    case 1:
+    case 4: {
+        double xo = 0.0, yo = 0.0, a = 0.5, beta_L = 3.0;
+        if (c.initial_condition == 4) {
+            xo = P[0];
+            yo = P[1];
+            beta_L = P[2] != 0.0 ? P[2] : 5.0;
+            a = P[3] != 0.0 ? P[3] : 0.5;
+        }
+        double time = 0.0;
+        xo = xo + u_in * time;
+        yo = yo + v_in * time;
+        double two_a = 2.0 * a;
+        double dT1 = -(gm1 * beta_L * beta_L) / (16.0 * a * gamma * PI_DP * PI_DP);
+        double node[2];
+        for (int j = 1; j <= n; ++j)
+            for (int i = 1; i <= n; ++i) {
+                centre(i, j, node);
+                double u = u_in, v = v_in;
+                double radius2 = (node[0] - xo) * (node[0] - xo) + (node[1] - yo) * (node[1] - yo);
+                double dT = dT1 * std::exp(two_a * (1.0 - radius2));
+                double rho = std::pow(1.0 + dT, oneOgm1);
+                double ff = beta_L / TWOPI_DP * std::exp(a * (1.0 - radius2));
+                u = u - (node[1] - yo) * ff;
+                v = v + (node[0] - xo) * ff;
+                double p = c.pressure + std::pow(rho, gamma) - 1.0;
+                at(0, i, j) = rho;
+                at(1, i, j) = rho * u;
+                at(2, i, j) = rho * v;
+                at(3, i, j) = p * oneOgm1 + 0.5 * rho * (u * u + v * v);
+            }
+        break;
+    }
+    case 2: {
+        double x0 = P[0] != 0.0 ? P[0] : 0.5;
+        double node[2];
+        for (int j = 1; j <= n; ++j)
+            for (int i = 1; i <= n; ++i) {
+                centre(i, j, node);
+                if (node[0] < x0) set_prim(i, j, 1.0, 0.0, 0.0, 1.0);
+                else set_prim(i, j, 0.125, 0.0, 0.0, 0.1);
+            }
+        break;
+    }
+    case 3: {
+        double xs = P[0] != 0.0 ? P[0] : 0.5, ys = P[1] != 0.0 ? P[1] : 0.5;
+        double node[2];
+        for (int j = 1; j <= n; ++j)
+            for (int i = 1; i <= n; ++i) {
+                centre(i, j, node);
+                int k = (node[0] >= xs ? 1 : 0) + (node[1] >= ys ? 2 : 0);
+                double rho = uniform(c.ic_seed, 16 * k + 0, 0.1, 1.5);
+                double p = uniform(c.ic_seed, 16 * k + 1, 0.1, 1.5);
+                double u = uniform(c.ic_seed, 16 * k + 2, -0.8, 0.8);
+                double v = uniform(c.ic_seed, 16 * k + 3, -0.8, 0.8);
+                set_prim(i, j, rho, u, v, p);
+            }
+        break;
+    }
+    case 5: {
+        double ms = P[0] != 0.0 ? P[0] : 2.0;
+        double xsh = P[1] != 0.0 ? P[1] : 0.1;
+        double rb = P[2] != 0.0 ? P[2] : 0.1375;
+        double rad = P[3] != 0.0 ? P[3] : 0.2;
+        double cx = uniform(c.ic_seed, 101, 0.6, 0.9), cy = uniform(c.ic_seed, 102, 0.4, 0.6);
+        double post[4];
+        shock_state(gamma, ms, 1.0, 1.0, post);
+        double node[2];
+        for (int j = 1; j <= n; ++j)
+            for (int i = 1; i <= n; ++i) {
+                centre(i, j, node);
+                if (node[0] < xsh) {
+                    for (int f = 0; f < 4; ++f) at(f, i, j) = post[f];
+                } else {
+                    double dx = node[0] - cx, dy = node[1] - cy;
+                    double rho = (dx * dx + dy * dy < rad * rad) ? rb : 1.0;
+                    set_prim(i, j, rho, 0.0, 0.0, 1.0);
+                }
+            }
+        break;
+    }
+    default:
+        for (int k = 0; k < nf * n * n; ++k) Q[k] = 0.0;
+        break;
+    }
+    if (c.noise_amplitude != 0.0 && first_cell_id >= 0) {
+        for (int j = 1; j <= n; ++j)
+            for (int i = 1; i <= n; ++i) {
+                int64_t id = first_cell_id + (j - 1) * n + (i - 1);
+                at(0, i, j) += c.noise_amplitude * unit_noise(c.ic_seed + 0x5eedULL, uint64_t(id));
+            }
+    }
+}
+
+// solver_tag_feature.F90:9-52 + tagging_methods_module.F90:14-71
+void tag_feature_host(const PhysicsConfig &c, int nf, int n, const double *soln, int *tag)
+{
+    *tag = 0;
+    for (int m = 0; m < c.amr_ntag_methods; ++m) {
+        int meth = c.amr_tag_methods[size_t(m)];
+        double tol = c.amr_tag_tolerances[size_t(m)];
+        for (int k = 0; k < n * n; ++k) {
+            double r = soln[nf * k];
+            if ((meth == 1 && r <= tol) || (meth == 2 && r >= tol)) {
+                *tag = 1;
+                break;
+            }
+        }
+    }
+}
+
+}  // namespace amrgpu
+
+using namespace amrgpu;
+
+// ======================================================================
+// C ABI: errors and configuration
+// ======================================================================
+extern "C" {
+
+int amrgpu_last_error(void) { return amrgpu::last_error(); }
+
+const char *amrgpu_error_string(int code)
+{
+    switch (code) {
+    case AMRGPU_OK: return "ok";
+    case AMRGPU_ERR_ARG: return "invalid argument";
+    case AMRGPU_ERR_CUDA: return "CUDA runtime error";
+    case AMRGPU_ERR_MESH: return "inconsistent mesh arrays";
+    case AMRGPU_ERR_NONFINITE: return "non-finite residual";
+    case AMRGPU_ERR_UNSUPPORTED: return "unsupported input";
+    case AMRGPU_ERR_NO_DEVICE: return "no CUDA device";
+    case AMRGPU_ERR_CONFIG: return "configuration file missing or invalid";
+    case AMRGPU_ERR_TOO_LARGE: return "request above the stated maximum";
+    case AMRGPU_ERR_NEGATIVE: return "non-positive density or pressure";
+    default: return "unknown error";
+    }
+}
+
+const char *amrgpu_last_error_message(void) { return g_error_msg.c_str(); }
+
+void amrgpu_clear_error(void) { set_error(AMRGPU_OK, ""); }
+
+static void to_public(const PhysicsConfig &c, amrgpu_config_t *o)
+{
+    std::memset(o, 0, sizeof(*o));
+    o->dim = c.dim;
+    o->nfields = c.nfields;
+    o->nelem_subgrid = c.nelem_subgrid;
+    o->coarse_grid_h = c.coarse_grid_h;
+    o->initial_condition = c.initial_condition;
+    for (int k = 0; k < 6; ++k) o->bc[k] = c.bc[k];
+    o->time_scheme = c.time_scheme;
+    o->time_steps = c.time_steps;
+    o->dt = c.dt;
+    o->cfl = c.cfl;
+    o->mach = c.mach;
+    o->alpha = c.alpha;
+    o->beta = c.beta;
+    o->gamma = c.gamma;
+    o->density = c.density;
+    o->pressure = c.pressure;
+    o->checkpoint_interval = c.checkpoint_interval;
+    o->visualization_interval = c.visualization_interval;
+    o->regrid_interval = c.regrid_interval;
+    o->amr_ntag_methods = c.amr_ntag_methods;
+    for (int k = 0; k < c.amr_ntag_methods && k < 5; ++k) {
+        o->amr_tag_methods[k] = c.amr_tag_methods[size_t(k)];
+        o->amr_tag_tolerances[k] = c.amr_tag_tolerances[size_t(k)];
+    }
+    o->form = c.form;
+    o->final_time = c.final_time;
+    for (int k = 0; k < 8; ++k) o->ic_params[k] = c.ic_params[k];
+    o->ic_seed = c.ic_seed;
+    o->noise_amplitude = c.noise_amplitude;
+}
+
+static void from_public(const amrgpu_config_t *o, PhysicsConfig &c)
+{
+    c.dim = o->dim;
+    c.nfields = o->nfields;
+    c.nelem_subgrid = o->nelem_subgrid;
+    c.coarse_grid_h = o->coarse_grid_h;
+    c.initial_condition = o->initial_condition;
+    for (int k = 0; k < 6; ++k) c.bc[k] = o->bc[k];
+    c.time_scheme = o->time_scheme;
+    c.time_steps = o->time_steps;
+    c.dt = o->dt;
+    c.cfl = o->cfl;
+    c.mach = o->mach;
+    c.alpha = o->alpha;
+    c.beta = o->beta;
+    c.gamma = o->gamma;
+    c.density = o->density;
+    c.pressure = o->pressure;
+    c.checkpoint_interval = o->checkpoint_interval <= 0 ? 2147483647 : o->checkpoint_interval;
+    c.visualization_interval = o->visualization_interval <= 0 ? 2147483647 : o->visualization_interval;
+    c.regrid_interval = o->regrid_interval <= 0 ? 2147483647 : o->regrid_interval;
+    int nt = o->amr_ntag_methods < 0 ? 0 : (o->amr_ntag_methods > 5 ? 5 : o->amr_ntag_methods);
+    c.amr_ntag_methods = nt;
+    c.amr_tag_methods.assign(o->amr_tag_methods, o->amr_tag_methods + nt);
+    c.amr_tag_tolerances.assign(o->amr_tag_tolerances, o->amr_tag_tolerances + nt);
+    c.form = o->form;
+    c.final_time = o->final_time;
+    for (int k = 0; k < 8; ++k) c.ic_params[k] = o->ic_params[k];
+    c.ic_seed = o->ic_seed;
+    c.noise_amplitude = o->noise_amplitude;
+}
+
+void amrgpu_config_defaults(amrgpu_config_t *cfg)
+{
+    PhysicsConfig c;
+    to_public(c, cfg);
+}
+
+int amrgpu_config_read(const char *path, amrgpu_config_t *cfg)
+{
+    PhysicsConfig c = global_config();
+    int rc = parse_physics_file(path, c);
+    if (rc != AMRGPU_OK) {
+        set_error(rc, std::string("cannot read ") + path);
+        return rc;
+    }
+    to_public(c, cfg);
+    return AMRGPU_OK;
+}
+
+int amrgpu_config_get(amrgpu_config_t *cfg)
+{
+    if (!cfg) return AMRGPU_ERR_ARG;
+    to_public(global_config(), cfg);
+    return AMRGPU_OK;
+}
+
+int amrgpu_config_set(const amrgpu_config_t *cfg)
+{
+    if (!cfg) return AMRGPU_ERR_ARG;
+    from_public(cfg, global_config());
+    return AMRGPU_OK;
+}
+
+// ======================================================================
+// C ABI: the reference's per-quadrant callbacks
+// ======================================================================
+void hpc_amr_initialize_solver(int *rank, int *dim, double *mesh_scale, int *nlevels, int *nfields,
+                               int *nfringe, int *nsub_elem, int *extern_cell_size,
+                               int *extern_face_size, int *extern_edge_size,
+                               int *extern_node_size, int *extern_mpi_comm_size)
+{
+    (void)extern_edge_size;
+    (void)extern_node_size;
+    PhysicsConfig &c = global_config();
+    c.nlevels = *nlevels;
+    c.coarse_grid_h = *mesh_scale;
+    c.dim = *dim;
+    c.nfields = *nfields;
+    c.nfringe = *nfringe;
+    c.nelem_subgrid = *nsub_elem;
+    c.extern_cell_size = *extern_cell_size;
+    c.extern_face_size = *extern_face_size;
+    c.extern_mpi_comm_size = *extern_mpi_comm_size;
+    if (*rank == 0 && !std::getenv("AMRGPU_QUIET")) {
+        std::printf("\n+==========================================+\n");
+        std::printf("|        Physics Kernel (B200, sm_100a)    |\n");
+        std::printf("+==========================================+\n");
+        std::printf("[physics] Input file: input.physics\n");
+    }
+    int rc = parse_physics_file("input.physics", c);
+    if (rc != AMRGPU_OK) {
+        if (*rank == 0) std::printf("[physics] The physics input file does not exist!\n");
+        set_error(rc, "input.physics not found; defaults kept");
+    }
+}
+
+void hpc_amr_initialize_quadrant(int *dim, int *unstructured, int *nfields, int *nsub_elem,
+                                 int *cell_type, double *elem_h, double *elem_xyz, double *soln)
+{
+    if (*dim != 2 || *unstructured) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "initialize_quadrant: 2D structured only");
+        return;
+    }
+    initialize_quadrant_host(global_config(), *nfields, *nsub_elem, cell_type, *elem_h, elem_xyz,
+                             soln, -1);
+}
+
+void hpc_amr_regrid_points(int *construct_grid, int *nregrid_pts, double *regrid_width,
+                           double *regrid_xyzh)
+{
+    (void)regrid_xyzh;
+    *construct_grid = 0;
+    *nregrid_pts = 0;
+    *regrid_width = 0.0;
+}
+
+void hpc_amr_tag_feature(int *dim, int *unstructured, int *nfields, int *nsub_elem, int *cell_type,
+                         double *elem_h, double *elem_xyz, double *soln, int *tag)
+{
+    (void)cell_type;
+    (void)elem_h;
+    (void)elem_xyz;
+    (void)unstructured;
+    int n = *nsub_elem;
+    if (*dim != 2) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "tag_feature: 2D only");
+        *tag = 0;
+        return;
+    }
+    tag_feature_host(global_config(), *nfields, n, soln, tag);
+}
+
+void hpc_amr_coarsen_operator_2d(int *unstructured, int *nfields, int *nsub_elem, int *cell_type,
+                                 double *elem_h, double *elem_xyz, double *uc1, double *uc2,
+                                 double *uc3, double *uc4, double *soln)
+{
+    (void)unstructured; (void)cell_type; (void)elem_h; (void)elem_xyz;
+    int m = *nfields * *nsub_elem * *nsub_elem;
+    for (int k = 0; k < m; ++k) {
+        double s = uc1[k] + uc2[k] + uc3[k] + uc4[k];
+        soln[k] = 0.25 * s;
+    }
+}
+
+void hpc_amr_refine_operator_2d(int *unstructured, int *nfields, int *nsub_elem, int *cell_type,
+                                double *elem_h, double *elem_xyz, double *soln, double *uc1,
+                                double *uc2, double *uc3, double *uc4)
+{
+    (void)unstructured; (void)cell_type; (void)elem_h; (void)elem_xyz;
+    int m = *nfields * *nsub_elem * *nsub_elem;
+    for (int k = 0; k < m; ++k) {
+        uc1[k] = soln[k];
+        uc2[k] = soln[k];
+        uc3[k] = soln[k];
+        uc4[k] = soln[k];
+    }
+}
+
+// ======================================================================
+// C ABI: host forest
+// ======================================================================
+struct amrgpu_forest {
+    Forest *f;
+};
+
+amrgpu_forest_t *amrgpu_forest_new_brick(int nx, int ny, int periodic_x, int periodic_y, double xlo,
+                                         double ylo, double zlo, double scale, int level)
+{
+    Forest *f = forest_new_brick(nx, ny, periodic_x, periodic_y, xlo, ylo, zlo, scale, level);
+    if (!f) {
+        set_error(AMRGPU_ERR_ARG, "forest_new_brick: invalid arguments");
+        return nullptr;
+    }
+    return new amrgpu_forest{f};
+}
+
+void amrgpu_forest_destroy(amrgpu_forest_t *f)
+{
+    if (!f) return;
+    forest_destroy(f->f);
+    delete f;
+}
+
+int amrgpu_forest_num_quads(const amrgpu_forest_t *f) { return f ? forest_num_quads(f->f) : -1; }
+
+int amrgpu_forest_quads(const amrgpu_forest_t *f, int *tree, int *level, int64_t *x, int64_t *y)
+{
+    if (!f) return AMRGPU_ERR_ARG;
+    const auto &L = forest_leaves(f->f);
+    for (size_t i = 0; i < L.size(); ++i) {
+        if (tree) tree[i] = L[i].tree;
+        if (level) level[i] = L[i].level;
+        if (x) x[i] = L[i].x;
+        if (y) y[i] = L[i].y;
+    }
+    return AMRGPU_OK;
+}
+
+int amrgpu_forest_set_tags(amrgpu_forest_t *f, const int *tags)
+{
+    if (!f || !tags) return AMRGPU_ERR_ARG;
+    auto &L = forest_leaves_mut(f->f);
+    for (size_t i = 0; i < L.size(); ++i) L[i].tag = tags[i];
+    return AMRGPU_OK;
+}
+
+int amrgpu_forest_get_tags(const amrgpu_forest_t *f, int *tags)
+{
+    if (!f || !tags) return AMRGPU_ERR_ARG;
+    const auto &L = forest_leaves(f->f);
+    for (size_t i = 0; i < L.size(); ++i) tags[i] = L[i].tag;
+    return AMRGPU_OK;
+}
+
+void amrgpu_forest_begin_regrid(amrgpu_forest_t *f)
+{
+    if (f) forest_begin_regrid(f->f);
+}
+
+int amrgpu_forest_refine(amrgpu_forest_t *f, const int *flags, int max_level)
+{
+    if (!f || !flags) return -1;
+    return forest_refine(f->f, flags, max_level);
+}
+
+int amrgpu_forest_coarsen(amrgpu_forest_t *f, const int *flags, int min_level)
+{
+    if (!f || !flags) return -1;
+    return forest_coarsen(f->f, flags, min_level);
+}
+
+int amrgpu_forest_balance(amrgpu_forest_t *f)
+{
+    if (!f) return -1;
+    return forest_balance(f->f);
+}
+
+int amrgpu_forest_is_balanced(const amrgpu_forest_t *f) { return f && forest_is_balanced(f->f) ? 1 : 0; }
+
+int amrgpu_forest_remap(const amrgpu_forest_t *f, int *kind, int *src)
+{
+    if (!f) return AMRGPU_ERR_ARG;
+    const auto &L = forest_leaves(f->f);
+    for (size_t i = 0; i < L.size(); ++i) {
+        kind[i] = L[i].src_kind;
+        src[i] = L[i].src;
+    }
+    return AMRGPU_OK;
+}
+
+int amrgpu_forest_max_faces(const amrgpu_forest_t *f) { return f ? 4 * forest_num_quads(f->f) : 0; }
+
+int amrgpu_forest_external(const amrgpu_forest_t *f, int nelem_subgrid, int nfields, int *cell_info,
+                           int *face_info, double *geom, int *nface, int *dof)
+{
+    if (!f || nelem_subgrid < 1 || nfields < 1) return AMRGPU_ERR_ARG;
+    int rc = forest_external(f->f, nelem_subgrid, nfields, cell_info, face_info, geom, nface, dof);
+    if (rc != 0) {
+        set_error(AMRGPU_ERR_MESH, "forest is not 2:1 balanced");
+        return AMRGPU_ERR_MESH;
+    }
+    return AMRGPU_OK;
+}
+
+double amrgpu_forest_quad_h(const amrgpu_forest_t *f, int quad)
+{
+    if (!f) return 0.0;
+    return forest_quad_h(f->f, forest_leaves(f->f)[size_t(quad)]);
+}
+
+int amrgpu_forest_initialize(const amrgpu_forest_t *f, int nelem_subgrid, double *soln)
+{
+    if (!f || !soln) return AMRGPU_ERR_ARG;
+    const PhysicsConfig &c = global_config();
+    const auto &L = forest_leaves(f->f);
+    const int n = nelem_subgrid;
+    const int nftm = c.nfields * n * n;
+    for (size_t i = 0; i < L.size(); ++i) {
+        double xyz[12];
+        forest_quad_corners(f->f, L[i], xyz);
+        int type = 0;
+        initialize_quadrant_host(c, c.nfields, n, &type, forest_quad_h(f->f, L[i]), xyz,
+                                 soln + size_t(nftm) * i, int64_t(i) * n * n);
+        forest_leaves_mut(const_cast<amrgpu_forest_t *>(f)->f)[i].type = type;
+    }
+    return AMRGPU_OK;
+}
+
+}  // extern "C"

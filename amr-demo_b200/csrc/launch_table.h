@@ -1,0 +1,30 @@
+// launch_table.h -- the compiled stage-kernel variants. Each entry is one
+// (patch size n, quads per CTA, threads per CTA) instantiation of
+// stage_kernel; the host autotuner times the entries that match a mesh's n
+// and keeps the fastest.
+#pragma once
+
+#include <cstddef>
+
+namespace amrgpu {
+
+struct StageArgs;
+
+struct StageLaunch {
+    int n;
+    int qpb;
+    int threads;
+    int min_blocks;
+    size_t smem;
+    const void *kernel;  // __global__ void(StageArgs)
+};
+
+int stage_table_fp64(const StageLaunch **out);
+int stage_table_fp32(const StageLaunch **out);
+
+// CFL step of a state (prologue of a segment): min over cells of the
+// reference's candidate, folded into scal->slot[slot].dt_bits.
+struct CflArgs;
+const void *cfl_kernel_fp64(int n);
+
+}  // namespace amrgpu

@@ -1,0 +1,916 @@
+// session.cu -- host driver of the GPU time-step path.
+//
+// A session owns the device copy of one mesh epoch (quad descriptors built
+// from cell_info / face_info / geom), the SoA state buffers, the per-step
+// device scalars, the chosen stage-kernel variant and the CUDA graphs of
+// whole steps. hpc_amr_evolve_solver / physics_go_gpu keep one session
+// alive across calls and rebuild it when the mesh changes.
+//
+// The step loop replaces physics_runge_kutta_interface.c:23-357: the number
+// of steps of a segment is known on the host from istep and the interval
+// flags, dt never leaves the device (each step's last stage folds the next
+// step's CFL minimum), and the host synchronises once per segment to read
+// the residual norm and the error flags.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "amrgpu_internal.h"
+#include "device_common.cuh"
+#include "launch_table.h"
+#include "misc_kernels.h"
+#include "stage_kernel.cuh"
+
+using namespace amrgpu;
+
+namespace {
+
+enum { RX = 0, RY = 1, RZ = 2, RK = 3 };
+
+struct StagePlan {
+    int in, a0, a1, out0, out1;
+};
+
+// Buffer roles of each stage, per scheme (see DESIGN: state X, Y, Z and
+// one auxiliary K). A stage reads halos only from `in`; a0/a1 are read and
+// out0/out1 written for the thread's own cells only, so in-place roles are
+// race-free.
+const std::vector<StagePlan> &plan_of(int scheme, bool &swap_xy)
+{
+    static const std::vector<StagePlan> rk1 = {{RX, -1, -1, RY, -1}};
+    static const std::vector<StagePlan> rk2 = {{RX, -1, -1, RY, RK}, {RY, RK, -1, RX, -1}};
+    static const std::vector<StagePlan> rk3 = {{RX, -1, -1, RY, RK}, {RY, RX, RK, RX, RK}, {RX, RK, -1, RY, -1}};
+    static const std::vector<StagePlan> rk4 = {
+        {RX, -1, -1, RY, RK}, {RY, RX, RK, RZ, RK}, {RZ, RX, RK, RY, RK}, {RY, RX, RK, RX, -1}};
+    static const std::vector<StagePlan> ls = {
+        {RX, -1, -1, RY, RK}, {RY, RK, -1, RX, RK}, {RX, RK, -1, RY, RK}, {RY, RK, -1, RX, RK}, {RX, RK, -1, RY, RK}};
+    static const std::vector<StagePlan> so = {{RX, -1, -1, RY, -1}, {RY, RX, -1, RZ, -1}, {RZ, RX, -1, RX, -1}};
+    switch (scheme) {
+    case kSchemeRK1: swap_xy = true; return rk1;
+    case kSchemeRK2: swap_xy = false; return rk2;
+    case kSchemeRK3: swap_xy = true; return rk3;
+    case kSchemeRK4: swap_xy = false; return rk4;
+    case kSchemeLSERK45: swap_xy = true; return ls;
+    default: swap_xy = false; return so;
+    }
+}
+
+bool cuda_ok(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return true;
+    set_error(AMRGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+uint64_t fnv1a(const void *p, size_t bytes, uint64_t h = 1469598103934665603ULL)
+{
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < bytes; ++i) {
+        h ^= b[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+}  // namespace
+
+struct amrgpu_session {
+    PhysicsConfig cfg;
+    int n = 0, nquad = 0, nghost = 0, nface = 0, dof = 0;
+    long long ncells_total = 0, stride = 0;
+    std::vector<QuadDesc> h_quads;
+    QuadDesc *d_quads = nullptr;
+    double *buf[4] = {nullptr, nullptr, nullptr, nullptr};
+    int role[4] = {0, 1, 2, 3};
+    double *d_aos = nullptr;
+    DeviceScalars *d_scal = nullptr;
+    DeviceScalars h_scal{};
+    double *d_partials = nullptr;
+    int partial_cap = 0;
+    double *d_tot = nullptr;
+    cudaStream_t stream = nullptr;
+    int form = AMRGPU_FORM_FP64_EXACT;
+    const StageLaunch *launch = nullptr;
+    int grid = 0;
+    long long step_index = 0;
+    int64_t launches = 0;
+    std::map<int, cudaGraphExec_t> graphs;
+    bool primed = false;
+    double t0 = 0.0;
+    int sms = 148;
+};
+
+namespace {
+
+double *rolebuf(amrgpu_session *s, int r) { return r < 0 ? nullptr : s->buf[s->role[r]]; }
+
+int scheme_of(const amrgpu_session *s)
+{
+    int sc = s->cfg.time_scheme;
+    if (s->form == AMRGPU_FORM_FP32_FLUX && sc == 3) return kSchemeRK3ShuOsher;
+    return sc;
+}
+
+// face_info -> per-quad side descriptors, following the decode of
+// physics_rhs_structured.c:73-262 (side parity picks left/right, side_plus,
+// level_l / level_r for cell_h, ind < dof guards real quads).
+int decode_mesh(amrgpu_session *s, const amrgpu_mesh_t *m)
+{
+    const int nq = m->ncell, ntot = m->ncell + m->nghost;
+    const int n = s->n;
+    const int nftm = 4 * n * n;
+    s->h_quads.assign(size_t(nq), QuadDesc{});
+    for (int q = 0; q < ntot; ++q) {
+        int off = m->cell_info[3 * q + 2];
+        if (off != nftm * q) {
+            set_error(AMRGPU_ERR_MESH, "cell_info[2] is not 4*n*n*id (quads must be contiguous)");
+            return AMRGPU_ERR_MESH;
+        }
+    }
+    for (int q = 0; q < nq; ++q) {
+        for (int k = 0; k < 4; ++k) {
+            s->h_quads[size_t(q)].side[k].kind = kSideNone;
+            s->h_quads[size_t(q)].corner[2 * k] = m->geom[12 * q + 3 * k];
+            s->h_quads[size_t(q)].corner[2 * k + 1] = m->geom[12 * q + 3 * k + 1];
+        }
+    }
+    auto level = [&](int c) { return m->cell_info[3 * c + 1]; };
+    auto set_side = [&](int q, int side, int kind, int n0, int n1, int rank, int lvl, int bc) -> bool {
+        if (q < 0 || q >= ntot) return false;
+        if (q >= nq) return true;  // ghost: no residual
+        SideDesc &d = s->h_quads[size_t(q)].side[side];
+        if (d.kind != kSideNone) return false;
+        d.kind = kind;
+        d.nbr0 = n0;
+        d.nbr1 = n1;
+        d.rank = rank;
+        d.level = lvl;
+        d.bc = bc;
+        return true;
+    };
+    for (int f = 0; f < m->nface; ++f) {
+        const int *fi = m->face_info + 11 * f;
+        int ftype = fi[0], side = fi[1], cell = fi[2];
+        bool ok = side >= 0 && side < 4 && cell >= 0 && cell < ntot;
+        if (ok && ftype == 1) {
+            ok = set_side(cell, side, kSideBoundary, -1, -1, f, level(cell), s->cfg.bc[side]);
+        } else if (ok && ftype == 2) {
+            int left = (side % 2 == 0) ? fi[3] : cell;
+            int right = (side % 2 == 0) ? cell : fi[3];
+            int hs = (side % 2 == 0) ? side + 1 : side;
+            ok = left >= 0 && left < ntot && right >= 0 && right < ntot;
+            if (ok) {
+                int lvl = level(left);
+                ok = set_side(left, hs, kSideFull, right, -1, f, lvl, 0) &&
+                     set_side(right, hs - 1, kSideFull, left, -1, f, lvl, 0);
+            }
+        } else if (ok && ftype == 3) {
+            int f0 = fi[3], f1 = fi[4];
+            ok = f0 >= 0 && f0 < ntot && f1 >= 0 && f1 < ntot;
+            if (ok) {
+                int lvl = level(f0);
+                int fine_side = (side % 2 == 0) ? side + 1 : side - 1;
+                ok = set_side(cell, side, kSideCoarseHang, f0, f1, f, lvl, 0) &&
+                     set_side(f0, fine_side, kSideFineHang, cell, -1, f, lvl, 0) &&
+                     set_side(f1, fine_side, kSideFineHang, cell, -1, f, lvl, 0);
+            }
+        } else {
+            ok = false;
+        }
+        if (!ok) {
+            set_error(ftype == 5 ? AMRGPU_ERR_UNSUPPORTED : AMRGPU_ERR_MESH,
+                      "face " + std::to_string(f) + " cannot be decoded (type " + std::to_string(ftype) + ")");
+            return ftype == 5 ? AMRGPU_ERR_UNSUPPORTED : AMRGPU_ERR_MESH;
+        }
+    }
+    for (int q = 0; q < nq; ++q)
+        for (int k = 0; k < 4; ++k)
+            if (s->h_quads[size_t(q)].side[k].kind == kSideNone) {
+                set_error(AMRGPU_ERR_MESH, "quad " + std::to_string(q) + " side " + std::to_string(k) +
+                                               " belongs to no face");
+                return AMRGPU_ERR_MESH;
+            }
+    return AMRGPU_OK;
+}
+
+const StageLaunch *find_launch(int form, int n, int qpb, int threads)
+{
+    const StageLaunch *tab;
+    int cnt = (form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
+    for (int i = 0; i < cnt; ++i)
+        if (tab[i].n == n && (qpb <= 0 || tab[i].qpb == qpb) && (threads <= 0 || tab[i].threads == threads))
+            return &tab[i];
+    return nullptr;
+}
+
+int configure_launch(amrgpu_session *s, const StageLaunch *L)
+{
+    if (!L) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "no stage kernel for this patch size");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    if (!cuda_ok(cudaFuncSetAttribute(L->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L->smem)),
+                 "cudaFuncSetAttribute"))
+        return AMRGPU_ERR_CUDA;
+    int per_sm = 0;
+    if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->kernel, L->threads, L->smem),
+                 "occupancy"))
+        return AMRGPU_ERR_CUDA;
+    if (per_sm < 1) per_sm = 1;
+    int groups = (s->nquad + L->qpb - 1) / L->qpb;
+    int g = std::min(groups, per_sm * s->sms);
+    if (g < 1) g = 1;
+    if (g > s->partial_cap) {
+        cudaFree(s->d_partials);
+        s->d_partials = nullptr;
+        if (!cuda_ok(cudaMalloc(&s->d_partials, sizeof(double) * size_t(g)), "cudaMalloc partials"))
+            return AMRGPU_ERR_CUDA;
+        s->partial_cap = g;
+    }
+    s->launch = L;
+    s->grid = g;
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    return AMRGPU_OK;
+}
+
+int prime(amrgpu_session *s)
+{
+    // slots: s%3 holds the step about to run; the others are armed with the cap
+    int p = int(s->step_index % 3);
+    std::memset(&s->h_scal, 0, sizeof(s->h_scal));
+    double cap = s->cfg.dt;
+    for (int k = 0; k < 3; ++k) {
+        s->h_scal.slot[k].dt_bits = (unsigned long long)0;
+        std::memcpy(&s->h_scal.slot[k].dt_bits, &cap, sizeof(double));
+        s->h_scal.slot[k].time = s->t0;
+    }
+    (void)p;
+    if (!cuda_ok(cudaMemcpyAsync(s->d_scal, &s->h_scal, sizeof(DeviceScalars), cudaMemcpyHostToDevice, s->stream),
+                 "prime scalars"))
+        return AMRGPU_ERR_CUDA;
+    bool cfl_on = s->cfg.time_scheme != 2;
+    if (cfl_on && s->nquad > 0) {
+        CflArgs a;
+        a.quads = s->d_quads;
+        a.qin = rolebuf(s, RX);
+        a.scal = s->d_scal;
+        a.stride = s->stride;
+        a.nquad = s->nquad;
+        a.slot = p;
+        a.cfl = s->cfg.cfl;
+        const void *k = cfl_kernel_fp64(s->n);
+        long long cells = (long long)s->nquad * s->n * s->n;
+        int g = int(std::min<long long>((cells + 255) / 256, (long long)s->sms * 8));
+        void *args[] = {&a};
+        if (!cuda_ok(cudaLaunchKernel(k, dim3(g), dim3(256), args, 0, s->stream), "cfl kernel"))
+            return AMRGPU_ERR_CUDA;
+        s->launches++;
+    }
+    s->primed = true;
+    return AMRGPU_OK;
+}
+
+int enqueue_step(amrgpu_session *s)
+{
+    int scheme = scheme_of(s);
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme, swap_xy);
+    int p = int(s->step_index % 3);
+    StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.quads = s->d_quads;
+    a.partials = s->d_partials;
+    a.scal = s->d_scal;
+    a.stride = s->stride;
+    a.nquad = s->nquad;
+    a.scheme = scheme;
+    a.cfl_on = s->cfg.time_scheme != 2;
+    a.slot_read = p;
+    a.slot_write = (p + 1) % 3;
+    a.slot_reset = (p + 2) % 3;
+    a.h_base = s->cfg.coarse_grid_h;
+    a.cfl = s->cfg.cfl;
+    a.dt_cap = s->cfg.dt;
+    a.final_time = s->cfg.final_time;
+    for (int k = 0; k < 4; ++k) a.qinflow[k] = 0.0;
+    if (s->cfg.initial_condition == 5) {
+        double ms = s->cfg.ic_params[0] != 0.0 ? s->cfg.ic_params[0] : 2.0;
+        shock_state(s->cfg.gamma, ms, 1.0, 1.0, a.qinflow);
+    }
+    for (size_t st = 0; st < plan.size(); ++st) {
+        a.stage = int(st) + 1;
+        a.last_stage = (st + 1 == plan.size()) ? 1 : 0;
+        a.qin = rolebuf(s, plan[st].in);
+        a.a0 = rolebuf(s, plan[st].a0);
+        a.a1 = rolebuf(s, plan[st].a1);
+        a.out0 = rolebuf(s, plan[st].out0);
+        a.out1 = rolebuf(s, plan[st].out1);
+        void *args[] = {&a};
+        cudaError_t e = cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args,
+                                         s->launch->smem, s->stream);
+        if (!cuda_ok(e, "stage kernel")) return AMRGPU_ERR_CUDA;
+        s->launches++;
+    }
+    if (swap_xy) std::swap(s->role[RX], s->role[RY]);
+    s->step_index++;
+    return AMRGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const amrgpu_config_t *cfg)
+{
+    if (!out || !m || !m->cell_info || !m->geom || (m->nface > 0 && !m->face_info) || m->ncell < 0 ||
+        m->nghost < 0) {
+        set_error(AMRGPU_ERR_ARG, "session_create: null or negative arguments");
+        return AMRGPU_ERR_ARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error(AMRGPU_ERR_NO_DEVICE, "no CUDA device visible");
+        return AMRGPU_ERR_NO_DEVICE;
+    }
+    amrgpu_session *s = new amrgpu_session;
+    if (cfg) {
+        amrgpu_config_set(cfg);  // keeps global and session in step
+    }
+    s->cfg = global_config();
+    s->n = s->cfg.nelem_subgrid;
+    s->form = s->cfg.form;
+    if (s->cfg.dim != 2 || s->cfg.nfields != 4) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "only dim 2 with 4 fields");
+        delete s;
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    if (s->cfg.time_scheme < 1 || s->cfg.time_scheme > 5) {
+        set_error(AMRGPU_ERR_CONFIG, "time_scheme must be 1..5");
+        delete s;
+        return AMRGPU_ERR_CONFIG;
+    }
+    s->nquad = m->ncell;
+    s->nghost = m->nghost;
+    s->nface = m->nface;
+    s->dof = m->dof;
+    if (m->dof != 4 * s->n * s->n * m->ncell) {
+        set_error(AMRGPU_ERR_MESH, "dof != 4*n*n*ncell");
+        delete s;
+        return AMRGPU_ERR_MESH;
+    }
+    int rc = decode_mesh(s, m);
+    if (rc != AMRGPU_OK) {
+        delete s;
+        return rc;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, dev);
+    s->ncells_total = (long long)(m->ncell + m->nghost) * s->n * s->n;
+    s->stride = ((s->ncells_total + 31) / 32) * 32;
+    if (s->stride == 0) s->stride = 32;
+    bool ok = cuda_ok(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+    for (int k = 0; k < 4 && ok; ++k) {
+        ok = cuda_ok(cudaMalloc(&s->buf[k], sizeof(double) * 4 * size_t(s->stride)), "cudaMalloc state");
+        if (ok) ok = cuda_ok(cudaMemsetAsync(s->buf[k], 0, sizeof(double) * 4 * size_t(s->stride), s->stream), "memset");
+    }
+    if (ok) ok = cuda_ok(cudaMalloc(&s->d_aos, sizeof(double) * 4 * size_t(std::max<long long>(s->ncells_total, 1))), "cudaMalloc aos");
+    if (ok) ok = cuda_ok(cudaMalloc(&s->d_scal, sizeof(DeviceScalars)), "cudaMalloc scalars");
+    if (ok && s->nquad > 0) {
+        ok = cuda_ok(cudaMalloc(&s->d_quads, sizeof(QuadDesc) * size_t(s->nquad)), "cudaMalloc quads");
+        if (ok)
+            ok = cuda_ok(cudaMemcpy(s->d_quads, s->h_quads.data(), sizeof(QuadDesc) * size_t(s->nquad),
+                                    cudaMemcpyHostToDevice),
+                         "upload quads");
+    }
+    if (ok) ok = cuda_ok(cudaMalloc(&s->d_tot, sizeof(double) * 4 * size_t(totals_grid(std::max<long long>(s->ncells_total, 1)))), "cudaMalloc totals");
+    if (!ok) {
+        amrgpu_session_destroy(s);
+        return AMRGPU_ERR_CUDA;
+    }
+    const StageLaunch *L = find_launch(s->form, s->n, 0, 0);
+    const char *env_q = std::getenv("AMRGPU_QPB");
+    const char *env_t = std::getenv("AMRGPU_THREADS");
+    if (env_q || env_t) {
+        const StageLaunch *L2 = find_launch(s->form, s->n, env_q ? std::atoi(env_q) : 0, env_t ? std::atoi(env_t) : 0);
+        if (L2) L = L2;
+    }
+    rc = configure_launch(s, L);
+    if (rc != AMRGPU_OK) {
+        amrgpu_session_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return AMRGPU_OK;
+}
+
+void amrgpu_session_destroy(amrgpu_session_t *s)
+{
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    for (int k = 0; k < 4; ++k) cudaFree(s->buf[k]);
+    cudaFree(s->d_aos);
+    cudaFree(s->d_scal);
+    cudaFree(s->d_partials);
+    cudaFree(s->d_quads);
+    cudaFree(s->d_tot);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int amrgpu_session_set_form(amrgpu_session_t *s, int form)
+{
+    if (!s || (form != AMRGPU_FORM_FP64_EXACT && form != AMRGPU_FORM_FP32_FLUX)) return AMRGPU_ERR_ARG;
+    if (form == s->form) return AMRGPU_OK;
+    // keep the current state where the canonical X role points
+    s->form = form;
+    s->cfg.form = form;
+    return configure_launch(s, find_launch(form, s->n, 0, 0));
+}
+
+int amrgpu_session_set_launch(amrgpu_session_t *s, int qpb, int threads)
+{
+    if (!s) return AMRGPU_ERR_ARG;
+    const StageLaunch *L = find_launch(s->form, s->n, qpb, threads);
+    if (!L) {
+        set_error(AMRGPU_ERR_ARG, "no compiled variant with that shape");
+        return AMRGPU_ERR_ARG;
+    }
+    return configure_launch(s, L);
+}
+
+int amrgpu_session_upload(amrgpu_session_t *s, const double *soln)
+{
+    if (!s || !soln) return AMRGPU_ERR_ARG;
+    size_t bytes = sizeof(double) * 4 * size_t(s->ncells_total);
+    if (bytes) {
+        if (!cuda_ok(cudaMemcpyAsync(s->d_aos, soln, bytes, cudaMemcpyHostToDevice, s->stream), "H2D soln"))
+            return AMRGPU_ERR_CUDA;
+        if (!cuda_ok(launch_aos_to_soa(s->d_aos, rolebuf(s, RX), s->ncells_total, s->stride, s->stream), "aos_to_soa"))
+            return AMRGPU_ERR_CUDA;
+        s->launches++;
+    }
+    return prime(s);
+}
+
+int amrgpu_session_download(amrgpu_session_t *s, double *soln)
+{
+    if (!s || !soln) return AMRGPU_ERR_ARG;
+    long long cells = (long long)s->nquad * s->n * s->n;
+    if (cells) {
+        if (!cuda_ok(launch_soa_to_aos(rolebuf(s, RX), s->d_aos, cells, s->stride, s->stream), "soa_to_aos"))
+            return AMRGPU_ERR_CUDA;
+        s->launches++;
+        if (!cuda_ok(cudaMemcpyAsync(soln, s->d_aos, sizeof(double) * 4 * size_t(cells), cudaMemcpyDeviceToHost,
+                                     s->stream),
+                     "D2H soln"))
+            return AMRGPU_ERR_CUDA;
+    }
+    return cuda_ok(cudaStreamSynchronize(s->stream), "sync") ? AMRGPU_OK : AMRGPU_ERR_CUDA;
+}
+
+int amrgpu_session_step(amrgpu_session_t *s, int nsteps)
+{
+    if (!s || nsteps < 0) return AMRGPU_ERR_ARG;
+    if (!s->primed) {
+        int rc = prime(s);
+        if (rc) return rc;
+    }
+    if (s->nquad == 0) return AMRGPU_OK;
+    for (int k = 0; k < nsteps; ++k) {
+        int rc = enqueue_step(s);
+        if (rc) return rc;
+    }
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_step_graph(amrgpu_session_t *s, int nsteps, int graph_steps)
+{
+    if (!s || nsteps < 0) return AMRGPU_ERR_ARG;
+    if (graph_steps < 6) graph_steps = 6;
+    graph_steps -= graph_steps % 6;
+    if (!s->primed) {
+        int rc = prime(s);
+        if (rc) return rc;
+    }
+    if (s->nquad == 0) return AMRGPU_OK;
+    int done = 0;
+    // align to a 6-step boundary: slot phase (3) and buffer-role parity (2)
+    while (done < nsteps && (s->step_index % 6) != 0) {
+        int rc = enqueue_step(s);
+        if (rc) return rc;
+        ++done;
+    }
+    while (nsteps - done >= graph_steps) {
+        auto it = s->graphs.find(graph_steps);
+        if (it == s->graphs.end()) {
+            cudaGraph_t g;
+            long long si = s->step_index;
+            int roles[4];
+            std::memcpy(roles, s->role, sizeof(roles));
+            int64_t l0 = s->launches;
+            if (!cuda_ok(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture"))
+                return AMRGPU_ERR_CUDA;
+            for (int k = 0; k < graph_steps; ++k) enqueue_step(s);
+            if (!cuda_ok(cudaStreamEndCapture(s->stream, &g), "end capture")) return AMRGPU_ERR_CUDA;
+            cudaGraphExec_t ge;
+            if (!cuda_ok(cudaGraphInstantiate(&ge, g, 0), "graph instantiate")) return AMRGPU_ERR_CUDA;
+            cudaGraphDestroy(g);
+            s->graphs[graph_steps] = ge;
+            s->step_index = si;
+            std::memcpy(s->role, roles, sizeof(roles));
+            s->launches = l0;
+            it = s->graphs.find(graph_steps);
+        }
+        if (!cuda_ok(cudaGraphLaunch(it->second, s->stream), "graph launch")) return AMRGPU_ERR_CUDA;
+        // advance host-side bookkeeping exactly as the captured steps did
+        bool swap_xy = false;
+        const auto &plan = plan_of(scheme_of(s), swap_xy);
+        s->launches += (int64_t)graph_steps * (int64_t)plan.size();
+        if (swap_xy && (graph_steps % 2)) std::swap(s->role[RX], s->role[RY]);
+        s->step_index += graph_steps;
+        done += graph_steps;
+    }
+    while (done < nsteps) {
+        int rc = enqueue_step(s);
+        if (rc) return rc;
+        ++done;
+    }
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_sync(amrgpu_session_t *s, amrgpu_report_t *rep)
+{
+    if (!s) return AMRGPU_ERR_ARG;
+    if (!cuda_ok(cudaMemcpyAsync(&s->h_scal, s->d_scal, sizeof(DeviceScalars), cudaMemcpyDeviceToHost, s->stream),
+                 "D2H scalars"))
+        return AMRGPU_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return AMRGPU_ERR_CUDA;
+    int p = int(s->step_index % 3);
+    if (rep) {
+        rep->steps_done = s->h_scal.steps;
+        rep->time = s->h_scal.slot[p].time;
+        rep->dt_last = s->h_scal.dt_used;
+        rep->residual_norm = std::sqrt(s->h_scal.norm_sq);
+        rep->nan_detected = (s->h_scal.flags & kFlagNonFinite) ? 1 : 0;
+        rep->error = rep->nan_detected ? AMRGPU_ERR_NONFINITE
+                                       : ((s->h_scal.flags & kFlagNegative) ? AMRGPU_ERR_NEGATIVE : AMRGPU_OK);
+    }
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_rhs(amrgpu_session_t *s, double *rhs)
+{
+    if (!s || !rhs) return AMRGPU_ERR_ARG;
+    if (s->nquad == 0) return AMRGPU_OK;
+    StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.quads = s->d_quads;
+    a.qin = rolebuf(s, RX);
+    a.out0 = rolebuf(s, RZ);
+    a.partials = s->d_partials;
+    a.scal = s->d_scal;
+    a.stride = s->stride;
+    a.nquad = s->nquad;
+    a.scheme = kSchemeRhsOnly;
+    a.stage = 1;
+    a.last_stage = 0;
+    a.cfl_on = 0;
+    a.slot_read = int(s->step_index % 3);
+    a.slot_write = (a.slot_read + 1) % 3;
+    a.slot_reset = (a.slot_read + 2) % 3;
+    a.h_base = s->cfg.coarse_grid_h;
+    a.cfl = s->cfg.cfl;
+    a.dt_cap = s->cfg.dt;
+    if (s->cfg.initial_condition == 5) {
+        double ms = s->cfg.ic_params[0] != 0.0 ? s->cfg.ic_params[0] : 2.0;
+        amrgpu::shock_state(s->cfg.gamma, ms, 1.0, 1.0, a.qinflow);
+    }
+    void *args[] = {&a};
+    if (!cuda_ok(cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args, s->launch->smem,
+                                  s->stream),
+                 "rhs kernel"))
+        return AMRGPU_ERR_CUDA;
+    s->launches++;
+    long long cells = (long long)s->nquad * s->n * s->n;
+    if (!cuda_ok(launch_soa_to_aos(rolebuf(s, RZ), s->d_aos, cells, s->stride, s->stream), "soa_to_aos"))
+        return AMRGPU_ERR_CUDA;
+    s->launches++;
+    if (!cuda_ok(cudaMemcpyAsync(rhs, s->d_aos, sizeof(double) * 4 * size_t(cells), cudaMemcpyDeviceToHost, s->stream),
+                 "D2H rhs"))
+        return AMRGPU_ERR_CUDA;
+    return cuda_ok(cudaStreamSynchronize(s->stream), "sync") ? AMRGPU_OK : AMRGPU_ERR_CUDA;
+}
+
+int amrgpu_session_cfl_dt(amrgpu_session_t *s, double *dt)
+{
+    if (!s || !dt) return AMRGPU_ERR_ARG;
+    long long keep = s->step_index;
+    int rc = prime(s);
+    if (rc) return rc;
+    s->step_index = keep;
+    rc = amrgpu_session_sync(s, nullptr);
+    if (rc) return rc;
+    std::memcpy(dt, &s->h_scal.slot[s->step_index % 3].dt_bits, sizeof(double));
+    if (s->cfg.time_scheme == 2) *dt = s->cfg.dt;
+    return AMRGPU_OK;
+}
+
+const double *amrgpu_session_state_device(amrgpu_session_t *s, int field)
+{
+    if (!s || field < 0 || field > 3) return nullptr;
+    return rolebuf(s, RX) + size_t(field) * size_t(s->stride);
+}
+
+int amrgpu_session_cells(const amrgpu_session_t *s) { return s ? int((long long)s->nquad * s->n * s->n) : 0; }
+
+void *amrgpu_session_stream(amrgpu_session_t *s) { return s ? (void *)s->stream : nullptr; }
+
+int64_t amrgpu_session_launch_count(const amrgpu_session_t *s) { return s ? s->launches : 0; }
+
+int amrgpu_session_totals(amrgpu_session_t *s, double totals[4])
+{
+    if (!s || !totals) return AMRGPU_ERR_ARG;
+    long long cells = (long long)s->nquad * s->n * s->n;
+    int g = totals_grid(std::max<long long>(cells, 1));
+    if (!cuda_ok(launch_totals(s->n, s->d_quads, rolebuf(s, RX), s->stride, s->nquad, s->d_tot, g, s->stream),
+                 "totals"))
+        return AMRGPU_ERR_CUDA;
+    s->launches++;
+    std::vector<double> h(size_t(4 * g));
+    if (!cuda_ok(cudaMemcpyAsync(h.data(), s->d_tot, sizeof(double) * 4 * size_t(g), cudaMemcpyDeviceToHost, s->stream),
+                 "D2H totals"))
+        return AMRGPU_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return AMRGPU_ERR_CUDA;
+    for (int f = 0; f < 4; ++f) {
+        double t = 0.0;
+        for (int b = 0; b < g; ++b) t += h[size_t(4 * b + f)];
+        totals[f] = t;
+    }
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_tag(amrgpu_session_t *s, int *tags)
+{
+    if (!s || !tags) return AMRGPU_ERR_ARG;
+    if (s->nquad == 0) return AMRGPU_OK;
+    TagMethods m;
+    int nm = std::min(s->cfg.amr_ntag_methods, 5);
+    for (int k = 0; k < 5; ++k) {
+        m.method[k] = k < nm ? s->cfg.amr_tag_methods[size_t(k)] : 0;
+        m.tol[k] = k < nm ? s->cfg.amr_tag_tolerances[size_t(k)] : 0.0;
+    }
+    int *d_tags = nullptr;
+    if (!cuda_ok(cudaMallocAsync((void **)&d_tags, sizeof(int) * size_t(s->nquad), s->stream), "cudaMalloc tags"))
+        return AMRGPU_ERR_CUDA;
+    bool ok = cuda_ok(launch_tag(s->n, rolebuf(s, RX), s->nquad, nm, m, d_tags, s->stream), "tag kernel");
+    s->launches++;
+    if (ok)
+        ok = cuda_ok(cudaMemcpyAsync(tags, d_tags, sizeof(int) * size_t(s->nquad), cudaMemcpyDeviceToHost, s->stream),
+                     "D2H tags");
+    cudaFreeAsync(d_tags, s->stream);
+    if (ok) ok = cuda_ok(cudaStreamSynchronize(s->stream), "sync");
+    return ok ? AMRGPU_OK : AMRGPU_ERR_CUDA;
+}
+
+int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int *kind, const int *src_index)
+{
+    if (!dst || !src || !kind || !src_index || dst->n != src->n) return AMRGPU_ERR_ARG;
+    for (int q = 0; q < dst->nquad; ++q) {
+        int lim = kind[q] == 0 ? src->nquad - 1 : src->nquad - 4;
+        if (src_index[q] < 0 || src_index[q] > lim) {
+            set_error(AMRGPU_ERR_ARG, "remap source index out of range");
+            return AMRGPU_ERR_ARG;
+        }
+    }
+    cudaStreamSynchronize(src->stream);
+    int *d_kind = nullptr, *d_src = nullptr;
+    size_t nb = sizeof(int) * size_t(std::max(dst->nquad, 1));
+    bool ok = cuda_ok(cudaMallocAsync((void **)&d_kind, nb, dst->stream), "cudaMalloc remap") &&
+              cuda_ok(cudaMallocAsync((void **)&d_src, nb, dst->stream), "cudaMalloc remap");
+    if (ok)
+        ok = cuda_ok(cudaMemcpyAsync(d_kind, kind, sizeof(int) * size_t(dst->nquad), cudaMemcpyHostToDevice, dst->stream),
+                     "H2D remap") &&
+             cuda_ok(cudaMemcpyAsync(d_src, src_index, sizeof(int) * size_t(dst->nquad), cudaMemcpyHostToDevice,
+                                     dst->stream),
+                     "H2D remap");
+    if (ok && dst->nquad > 0) {
+        ok = cuda_ok(launch_remap(dst->n, rolebuf(src, RX), src->stride, rolebuf(dst, RX), dst->stride, d_kind, d_src,
+                                  dst->nquad, dst->stream),
+                     "remap kernel");
+        dst->launches++;
+    }
+    cudaFreeAsync(d_kind, dst->stream);
+    cudaFreeAsync(d_src, dst->stream);
+    if (!ok) return AMRGPU_ERR_CUDA;
+    dst->t0 = src->h_scal.slot[src->step_index % 3].time;
+    return prime(dst);
+}
+
+}  // extern "C"
+
+// ======================================================================
+// The reference's evolve entry points
+// ======================================================================
+namespace {
+
+struct EvolveCache {
+    amrgpu_session *s = nullptr;
+    uint64_t mesh_hash = 0;
+    uint64_t cfg_hash = 0;
+    double sim_time = 0.0;
+};
+
+EvolveCache &cache()
+{
+    static EvolveCache c;
+    return c;
+}
+
+uint64_t cfg_hash(const PhysicsConfig &c)
+{
+    uint64_t h = fnv1a(&c.time_scheme, sizeof(int));
+    h = fnv1a(&c.dt, sizeof(double), h);
+    h = fnv1a(&c.cfl, sizeof(double), h);
+    h = fnv1a(c.bc, sizeof(c.bc), h);
+    h = fnv1a(&c.form, sizeof(int), h);
+    h = fnv1a(&c.final_time, sizeof(double), h);
+    h = fnv1a(&c.coarse_grid_h, sizeof(double), h);
+    h = fnv1a(&c.nelem_subgrid, sizeof(int), h);
+    h = fnv1a(&c.initial_condition, sizeof(int), h);
+    h = fnv1a(c.ic_params, sizeof(c.ic_params), h);
+    return h;
+}
+
+void evolve(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *ncell, int *nghost, int *nface,
+            int *dof, int *cell_info, int *face_info, int *nsend, int *nrecv, int *sizes, double *geom, double *soln,
+            int *istep, int *regrid, int *visualize, int *checkpoint, int *evolve_solution, double *total_time,
+            double *compute_time, double *residual_time)
+{
+    (void)sizes;
+    PhysicsConfig &c = global_config();
+    // physics_go.c:66-69
+    if (*istep >= c.time_steps) {
+        *evolve_solution = 0;
+        return;
+    }
+    if (*dim != 2 || *unstructured != 0 || *nfields != 4) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "GPU path: 2D structured with 4 fields only");
+        *evolve_solution = 0;
+        return;
+    }
+    if (*nsend != 0 || *nrecv != 0 || *nghost != 0) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "GPU path: one rank, no ghost exchange");
+        *evolve_solution = 0;
+        return;
+    }
+    c.dim = *dim;
+    c.nfields = *nfields;
+    c.nelem_subgrid = *nelem_subgrid;
+    if (const char *f = std::getenv("AMRGPU_FORM")) c.form = std::atoi(f);
+
+    auto wall0 = std::chrono::steady_clock::now();
+    EvolveCache &ec = cache();
+    uint64_t mh = fnv1a(cell_info, sizeof(int) * 3 * size_t(*ncell + *nghost));
+    mh = fnv1a(face_info, sizeof(int) * 11 * size_t(*nface), mh);
+    mh = fnv1a(geom, sizeof(double) * 12 * size_t(*ncell + *nghost), mh);
+    mh = fnv1a(ncell, sizeof(int), mh);
+    uint64_t ch = cfg_hash(c);
+    if (!ec.s || ec.mesh_hash != mh || ec.cfg_hash != ch) {
+        if (ec.s) amrgpu_session_destroy(ec.s);
+        ec.s = nullptr;
+        amrgpu_mesh_t m{*ncell, *nghost, *nface, *dof, cell_info, face_info, geom};
+        amrgpu_session *s = nullptr;
+        if (amrgpu_session_create(&s, &m, nullptr) != AMRGPU_OK) {
+            *evolve_solution = 0;
+            return;
+        }
+        ec.s = s;
+        ec.mesh_hash = mh;
+        ec.cfg_hash = ch;
+    }
+    amrgpu_session *s = ec.s;
+    s->cfg = c;
+    s->t0 = ec.sim_time;
+    s->step_index = 0;
+    s->role[0] = 0; s->role[1] = 1; s->role[2] = 2; s->role[3] = 3;
+    if (amrgpu_session_upload(s, soln) != AMRGPU_OK) {
+        *evolve_solution = 0;
+        return;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s->stream);
+    // number of steps of this segment (physics_runge_kutta_interface.c:213-229)
+    int steps = 0;
+    int is = *istep;
+    for (;;) {
+        ++steps;
+        ++is;
+        if (is >= c.time_steps || is % c.regrid_interval == 0 || is % c.checkpoint_interval == 0 ||
+            is % c.visualization_interval == 0)
+            break;
+    }
+    amrgpu_report_t rep{};
+    int taken = 0;
+    if (c.final_time > 0.0) {
+        // the device clips dt at final_time; run in chunks and stop once reached
+        int left = steps;
+        while (left > 0) {
+            int chunk = std::min(left, 240);
+            if (amrgpu_session_step_graph(s, chunk, 60) != AMRGPU_OK) break;
+            left -= chunk;
+            amrgpu_session_sync(s, &rep);
+            taken = rep.steps_done;
+            if (rep.time >= c.final_time || rep.error) break;
+        }
+        if (rep.time >= c.final_time) *evolve_solution = 0;
+        steps = taken;
+    } else {
+        int rc = (steps >= 12) ? amrgpu_session_step_graph(s, steps, std::min(steps - steps % 6, 600))
+                               : amrgpu_session_step(s, steps);
+        if (rc == AMRGPU_OK) amrgpu_session_sync(s, &rep);
+    }
+    cudaEventRecord(e1, s->stream);
+    if (amrgpu_session_download(s, soln) != AMRGPU_OK) {
+        *evolve_solution = 0;
+        return;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ec.sim_time = rep.time;
+    *istep += steps;
+    if (*istep % c.regrid_interval == 0) *regrid = 1;
+    if (*istep % c.checkpoint_interval == 0) *checkpoint = 1;
+    if (*istep % c.visualization_interval == 0) *visualize = 1;
+    double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
+    *total_time += wall;
+    *compute_time += ms * 1e-3;
+    *residual_time += ms * 1e-3;
+    // physics_go.c:105-118 and physics_runtime_statistics.c:82-86
+    int cells = *dof / *nfields;
+    double resid = rep.residual_norm / std::pow(double(cells), 1.0 / double(*dim));
+    if (!std::getenv("AMRGPU_QUIET")) {
+        std::printf("[ amr ] istep: %d\n", *istep);
+        std::printf("[ amr ] processor dofs (min,max,avg,total): %d, %d, %d, %d \n", cells, cells, cells, cells);
+        std::printf("[physics] iterations: %d, gpu time: %e, residual: %1.15e\n", steps, ms * 1e-3, resid);
+        int nres = c.time_scheme;
+        if (steps > 0 && cells > 0)
+            std::printf("[physics] time/dof (gpu): %e\n", (ms * 1e-3) / double(cells) / double(steps) / double(nres));
+    }
+    if (rep.nan_detected || std::isnan(rep.residual_norm)) {
+        std::printf("[solve] nan detected in residual aborting\n");
+        set_error(AMRGPU_ERR_NONFINITE, "non-finite residual norm");
+        *evolve_solution = 0;
+        const char *ab = std::getenv("AMRGPU_ABORT_ON_NAN");
+        if (ab && std::atoi(ab) == 1) std::exit(3);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void hpc_amr_evolve_solver(int *dim, int *unstructured, int *nfields, int *nsub_elem, int *ncell, int *nghost,
+                           int *nface, int *dof, int *cell_info, int *face_info, int *nsend, int *nrecv, int *send,
+                           int *recv, int *sizes, double *geom, double *soln, int *istep, int *regrid,
+                           int *visualize, int *checkpoint, int *evolve_solution, amrgpu_comm_t mpicomm_ext,
+                           double *total_time, double *compute_time, double *residual_time)
+{
+    (void)send;
+    (void)recv;
+    (void)mpicomm_ext;
+    evolve(dim, unstructured, nfields, nsub_elem, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
+           sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, total_time, compute_time,
+           residual_time);
+}
+
+void physics_go_gpu(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *ncell, int *nghost,
+                    int *nface, int *dof, int *cell_info, int *face_info, int *nsend, int *nrecv, int *send,
+                    int *recv, int *sizes, double *geom, double *soln, int *istep, int *regrid, int *visualize,
+                    int *checkpoint, int *evolve_solution, amrgpu_comm_t mpicomm_ext, double *total_time,
+                    double *compute_time, double *residual_time)
+{
+    (void)send;
+    (void)recv;
+    (void)mpicomm_ext;
+    evolve(dim, unstructured, nfields, nelem_subgrid, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
+           sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, total_time, compute_time,
+           residual_time);
+}
+
+}  // extern "C"

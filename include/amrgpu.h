@@ -1,0 +1,260 @@
+/*
+ * amrgpu.h -- C ABI of libamrgpu, the B200 (sm_100a) implementation of the
+ * residual / Runge-Kutta / CFL time-step path of amr-demo.
+ *
+ * Part 1 is the reference's own solver-facing call surface (same names,
+ * same argument lists, same in/out meaning), so the reference's AMR driver
+ * links against libamrgpu.so in place of libhpc_phys.so + libhpc_solver.so.
+ * Part 2 is this library's extended API: device-resident sessions, forms,
+ * batched regrid kernels, the host forest and error reporting.
+ *
+ * All pointers are plain host pointers unless a name says "_device".
+ * Nothing here uses torch or C++ types.
+ */
+#ifndef AMRGPU_H
+#define AMRGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The communicator argument of the reference ABI. A caller built with MPI
+ * passes its MPI_Comm (see physics_go_gpu.h); this single-process library
+ * accepts it and does not use it. */
+#ifndef AMRGPU_COMM_T
+#define AMRGPU_COMM_T intptr_t
+#endif
+typedef AMRGPU_COMM_T amrgpu_comm_t;
+
+/* ======================================================================
+ * Part 1 -- the reference's ABI
+ * ====================================================================== */
+
+/* Replaces hpc_amr_initialize_solver (src/amr/src/amr_external.h:50,
+ * src/physics/src/hpc_amr_initialize_solver.c:16-28): stores the mesh
+ * constants and reads "input.physics" from the working directory with the
+ * reference's keyword rules (physics_initialize.c:61-197), including
+ * cfl <- 0.25*cfl*time_scheme and intervals <= 0 -> INT_MAX. Unlike the
+ * reference it does not exit() when the file is missing: it keeps the
+ * defaults and reports AMRGPU_ERR_CONFIG through amrgpu_last_error(). */
+void hpc_amr_initialize_solver(int *rank, int *dim, double *mesh_scale, int *nlevels,
+                               int *nfields, int *nfringe, int *nsub_elem,
+                               int *extern_cell_size, int *extern_face_size,
+                               int *extern_edge_size, int *extern_node_size,
+                               int *extern_mpi_comm_size);
+
+/* Replaces hpc_amr_initialize_quadrant (amr_external.h:67,
+ * hpc_amr_initialize_quadrant.c:15-21 -> initial_condition_2d_module.F90:12-131):
+ * fills one quadrant's AoS patch with the configured initial condition. */
+void hpc_amr_initialize_quadrant(int *dim, int *unstructured, int *nfields, int *nsub_elem,
+                                 int *cell_type, double *elem_h, double *elem_xyz,
+                                 double *soln);
+
+/* Replaces hpc_amr_regrid_points (amr_external.h:77,
+ * physics_regrid_points.c:28-36): no external points. */
+void hpc_amr_regrid_points(int *construct_grid, int *nregrid_pts, double *regrid_width,
+                           double *regrid_xyzh);
+
+/* Replaces hpc_amr_tag_feature (amr_external.h:92, hpc_amr_tag_feature.c:17-26
+ * -> solver_tag_feature.F90:9-52): density-threshold tagging of one quad. */
+void hpc_amr_tag_feature(int *dim, int *unstructured, int *nfields, int *nsub_elem,
+                         int *cell_type, double *elem_h, double *elem_xyz, double *soln,
+                         int *tag);
+
+/* Replaces hpc_amr_coarsen_operator_2d (amr_external.h:146,
+ * solver_coarsen_operator_2d.F90:29-53): same-index average of 4 children. */
+void hpc_amr_coarsen_operator_2d(int *unstructured, int *nfields, int *nsub_elem,
+                                 int *cell_type, double *elem_h, double *elem_xyz,
+                                 double *uc1, double *uc2, double *uc3, double *uc4,
+                                 double *soln);
+
+/* Replaces hpc_amr_refine_operator_2d (amr_external.h:189,
+ * solver_refine_operator_2d.F90:28-55): every child receives the parent patch. */
+void hpc_amr_refine_operator_2d(int *unstructured, int *nfields, int *nsub_elem,
+                                int *cell_type, double *elem_h, double *elem_xyz,
+                                double *soln, double *uc1, double *uc2, double *uc3,
+                                double *uc4);
+
+/* Replaces hpc_amr_evolve_solver (amr_external.h:124,
+ * hpc_amr_evolve_solver.c:16-49) and, behind it, physics_go
+ * (physics_go.c:16-132) with the whole time-step loop of
+ * physics_runge_kutta_interface.c:23-357 run on the GPU:
+ *   - returns with *evolve_solution = 0 when *istep >= time_steps;
+ *   - otherwise copies soln[0:dof) to the device, runs steps until
+ *     time_steps or a regrid / checkpoint / visualisation interval is hit,
+ *     sets those flags, advances *istep, copies soln back;
+ *   - accumulates *total_time, *compute_time, *residual_time (seconds).
+ * Device buffers persist across calls and are rebuilt when the mesh
+ * (cell_info / face_info / geom) changes. Errors are reported through
+ * amrgpu_last_error(); a non-finite residual sets AMRGPU_ERR_NONFINITE (and
+ * exits with code 3 when AMRGPU_ABORT_ON_NAN=1, as the reference's
+ * MPI_Abort(comm,3) does). Only 2D structured meshes on one rank
+ * (nsend == nrecv == 0) are accepted. */
+void hpc_amr_evolve_solver(int *dim, int *unstructured, int *nfields, int *nsub_elem,
+                           int *ncell, int *nghost, int *nface, int *dof, int *cell_info,
+                           int *face_info, int *nsend, int *nrecv, int *send, int *recv,
+                           int *sizes, double *geom, double *soln, int *istep, int *regrid,
+                           int *visualize, int *checkpoint, int *evolve_solution,
+                           amrgpu_comm_t mpicomm_ext, double *total_time,
+                           double *compute_time, double *residual_time);
+
+/* The reference's reserved GPU plug-point (physics_evolve_interface.c:42-46,
+ * declared by the missing physics_go_gpu.h, physics_evolve_interface.h:16-17);
+ * same signature as physics_go (physics_go.h:59). Same behaviour as
+ * hpc_amr_evolve_solver above. */
+void physics_go_gpu(int *dim, int *unstructured, int *nfields, int *nelem_subgrid,
+                    int *ncell, int *nghost, int *nface, int *dof, int *cell_info,
+                    int *face_info, int *nsend, int *nrecv, int *send, int *recv,
+                    int *sizes, double *geom, double *soln, int *istep, int *regrid,
+                    int *visualize, int *checkpoint, int *evolve_solution,
+                    amrgpu_comm_t mpicomm_ext, double *total_time, double *compute_time,
+                    double *residual_time);
+
+/* ======================================================================
+ * Part 2 -- extended API (no reference counterpart unless stated)
+ * ====================================================================== */
+
+enum {
+    AMRGPU_OK = 0,
+    AMRGPU_ERR_ARG = 1,          /* invalid argument */
+    AMRGPU_ERR_CUDA = 2,         /* CUDA runtime error */
+    AMRGPU_ERR_MESH = 3,         /* inconsistent cell_info / face_info */
+    AMRGPU_ERR_NONFINITE = 4,    /* NaN/Inf residual or state */
+    AMRGPU_ERR_UNSUPPORTED = 5,  /* 3D, unstructured, multi-rank, patch size */
+    AMRGPU_ERR_NO_DEVICE = 6,    /* no CUDA device */
+    AMRGPU_ERR_CONFIG = 7,       /* input.physics missing or invalid */
+    AMRGPU_ERR_TOO_LARGE = 8,    /* request above a stated maximum */
+    AMRGPU_ERR_NEGATIVE = 9      /* non-positive density or pressure */
+};
+
+enum {
+    AMRGPU_FORM_FP64_EXACT = 0, /* reference arithmetic in FP64, bit-exact order */
+    AMRGPU_FORM_FP32_FLUX = 1   /* FP32 flux, FP64 state / sums / RK (Shu-Osher RK3) */
+};
+
+int amrgpu_last_error(void);
+const char *amrgpu_error_string(int code);
+const char *amrgpu_last_error_message(void);
+void amrgpu_clear_error(void);
+
+/* Physics configuration, the fields of the reference's d_physics_fluid /
+ * d_physics_simulation / d_physics_interface globals plus extensions. */
+typedef struct {
+    int dim, nfields, nelem_subgrid;
+    double coarse_grid_h;        /* h of a level-0 quadrant (mesh_scale) */
+    int initial_condition;       /* 0 free stream, 1 Shu vortex; 2..5 extensions */
+    int bc[6];                   /* per side: 0 extrapolate, 1 slip, 2 no-slip, 3 inflow */
+    int time_scheme;             /* 1 RK1, 2 SSP-RK2, 3 SSP-RK3, 4 RK4, 5 LSERK45 */
+    int time_steps;
+    double dt;                   /* cap on the CFL step */
+    double cfl;                  /* effective (already scaled) CFL */
+    double mach, alpha, beta, gamma, density, pressure;
+    int checkpoint_interval, visualization_interval, regrid_interval;
+    int amr_ntag_methods;
+    int amr_tag_methods[5];
+    double amr_tag_tolerances[5];
+    int form;                    /* AMRGPU_FORM_* */
+    double final_time;           /* > 0: stop at this time, last step clipped */
+    double ic_params[8];         /* parameters of extension ICs */
+    uint64_t ic_seed;            /* seed of extension ICs and density noise */
+    double noise_amplitude;      /* uniform density noise amplitude */
+} amrgpu_config_t;
+
+void amrgpu_config_defaults(amrgpu_config_t *cfg);
+int amrgpu_config_read(const char *path, amrgpu_config_t *cfg);
+int amrgpu_config_get(amrgpu_config_t *cfg);
+int amrgpu_config_set(const amrgpu_config_t *cfg);
+
+/* ---------------- device-resident sessions ---------------- */
+typedef struct amrgpu_session amrgpu_session_t;
+
+typedef struct {
+    int ncell, nghost, nface, dof;
+    const int *cell_info;   /* 3*(ncell+nghost) */
+    const int *face_info;   /* 11*nface */
+    const double *geom;     /* 12*(ncell+nghost) */
+} amrgpu_mesh_t;
+
+typedef struct {
+    int steps_done;
+    double time;            /* simulated time advanced by this session */
+    double dt_last;         /* dt of the last step */
+    double residual_norm;   /* sqrt(sum k^2) of the last stage, as rk_*() reports */
+    int error;              /* AMRGPU_OK or an error code */
+    int nan_detected;
+} amrgpu_report_t;
+
+/* Builds device tables for a mesh and a configuration (config NULL: the
+ * global configuration). */
+int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *mesh,
+                          const amrgpu_config_t *cfg);
+void amrgpu_session_destroy(amrgpu_session_t *s);
+int amrgpu_session_set_form(amrgpu_session_t *s, int form);
+int amrgpu_session_set_launch(amrgpu_session_t *s, int quads_per_block, int threads);
+/* Host AoS soln (reference layout, dof + ghost tail) <-> device SoA state. */
+int amrgpu_session_upload(amrgpu_session_t *s, const double *soln_aos);
+int amrgpu_session_download(amrgpu_session_t *s, double *soln_aos);
+/* Advance nsteps on the device (async on the session stream). */
+int amrgpu_session_step(amrgpu_session_t *s, int nsteps);
+/* Same, recording the steps as a CUDA graph of graph_steps steps. */
+int amrgpu_session_step_graph(amrgpu_session_t *s, int nsteps, int graph_steps);
+int amrgpu_session_sync(amrgpu_session_t *s, amrgpu_report_t *rep);
+/* One residual evaluation rhs = -R(Q) of the current state (AoS, dof). */
+int amrgpu_session_rhs(amrgpu_session_t *s, double *rhs_aos);
+/* CFL time step of the current state, capped by the configured dt. */
+int amrgpu_session_cfl_dt(amrgpu_session_t *s, double *dt);
+/* Device pointer of field f of the SoA state; cells of quad q are
+ * [q*n*n, (q+1)*n*n), row-major (i fastest). */
+const double *amrgpu_session_state_device(amrgpu_session_t *s, int field);
+int amrgpu_session_cells(const amrgpu_session_t *s);
+void *amrgpu_session_stream(amrgpu_session_t *s);
+/* Kernel launches issued by this session so far. */
+int64_t amrgpu_session_launch_count(const amrgpu_session_t *s);
+/* Conservation totals sum(vol*Q_f) for the 4 fields, in FP64. */
+int amrgpu_session_totals(amrgpu_session_t *s, double totals[4]);
+
+/* ---------------- host forest (stands in for p4est) ---------------- */
+typedef struct amrgpu_forest amrgpu_forest_t;
+amrgpu_forest_t *amrgpu_forest_new_brick(int nx, int ny, int periodic_x, int periodic_y,
+                                         double xlo, double ylo, double zlo, double scale,
+                                         int level);
+void amrgpu_forest_destroy(amrgpu_forest_t *f);
+int amrgpu_forest_num_quads(const amrgpu_forest_t *f);
+/* Per quad: tree, level, x, y (units of 2^-30 of a tree), tag, type. */
+int amrgpu_forest_quads(const amrgpu_forest_t *f, int *tree, int *level, int64_t *x, int64_t *y);
+int amrgpu_forest_set_tags(amrgpu_forest_t *f, const int *tags);
+int amrgpu_forest_get_tags(const amrgpu_forest_t *f, int *tags);
+void amrgpu_forest_begin_regrid(amrgpu_forest_t *f);
+int amrgpu_forest_refine(amrgpu_forest_t *f, const int *flags, int max_level);
+int amrgpu_forest_coarsen(amrgpu_forest_t *f, const int *flags, int min_level);
+int amrgpu_forest_balance(amrgpu_forest_t *f);
+int amrgpu_forest_is_balanced(const amrgpu_forest_t *f);
+/* For every quad after the last begin_regrid: kind 0 = copy (injection)
+ * from old quad src, kind 1 = average of old quads src..src+3. */
+int amrgpu_forest_remap(const amrgpu_forest_t *f, int *kind, int *src);
+/* Upper bound of nface for amrgpu_forest_external (4 per quad). */
+int amrgpu_forest_max_faces(const amrgpu_forest_t *f);
+int amrgpu_forest_external(const amrgpu_forest_t *f, int nelem_subgrid, int nfields,
+                           int *cell_info, int *face_info, double *geom, int *nface,
+                           int *dof);
+double amrgpu_forest_quad_h(const amrgpu_forest_t *f, int quad);
+/* Initial condition of every quad through hpc_amr_initialize_quadrant
+ * semantics and the global configuration; soln is AoS (dof). */
+int amrgpu_forest_initialize(const amrgpu_forest_t *f, int nelem_subgrid, double *soln);
+
+/* ---------------- batched regrid kernels (GPU) ---------------- */
+/* Plain indicator of solver_tag_feature.F90:9-52 for every quad of the
+ * session's state, plus the density-jump extension (method 5). */
+int amrgpu_session_tag(amrgpu_session_t *s, int *tags);
+/* New SoA state for a remapped mesh: kind/src from amrgpu_forest_remap. */
+int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int *kind,
+                         const int *src_index);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMRGPU_H */
