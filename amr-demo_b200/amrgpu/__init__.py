@@ -136,8 +136,11 @@ class Forest:
 
     def __del__(self):
         f = getattr(self, "_f", None)
-        if f:
-            lib().amrgpu_forest_destroy(f)
+        if f and lib is not None:
+            try:
+                lib().amrgpu_forest_destroy(f)
+            except Exception:
+                pass
             self._f = None
 
     @property
@@ -231,8 +234,11 @@ class Session:
         self._s = h
 
     def close(self):
-        if getattr(self, "_s", None):
-            lib().amrgpu_session_destroy(self._s)
+        if getattr(self, "_s", None) and lib is not None:
+            try:
+                lib().amrgpu_session_destroy(self._s)
+            except Exception:
+                pass
             self._s = None
 
     def __del__(self):

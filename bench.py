@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""RK cell-updates/s of the residual / time-step path on B200.
+
+Workload: the isentropic-vortex problem (periodic [0,10]^2, vortex of
+strength 5 at (5,5), free stream (1,1,1,1), 4096 quadrants of 16x16 =
+1024^2 cells, SSP-RK3, CFL 0.5). One step = one full RK3 time step (three
+fused stage kernels, the next step's CFL minimum folded into the last one).
+
+  value : device-resident throughput of the FP32-flux / FP64-state form,
+          every step timed with CUDA events on the solver's stream, L2
+          flushed between steps (per-step events exclude the flush)
+  e2e   : the same metric through the reference's C ABI
+          (hpc_amr_evolve_solver) on pinned host arrays, one call per
+          10-step segment (the reference example's regrid interval), H2D
+          and D2H of the whole state inside the timed region
+  forms : the plain FP64 form (bit-exact with the reference) beside it
+
+`--impl reference` times the reference's own CPU path (its C driver over
+the restated Fortran kernels, oracle/_ref) on all host cores instead.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "amr-demo_b200")]
+os.environ.setdefault("AMRGPU_QUIET", "1")
+
+METRIC = "RK cell-updates/s on 1 B200: learned+FP32 form vs plain FP64, at equal L1(rho)"
+UNIT = "cell-updates/s"
+WORKLOAD = "isentropic vortex, periodic [0,10]^2, 4096 quads x 16x16 = 1024^2 cells, SSP-RK3, CFL 0.5"
+B_ALG = {0: 352.0, 1: 256.0}  # algorithmic HBM bytes per cell-update
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU baseline
+def _cpu_worker(args):
+    level, steps, use_ref = args
+    import numpy as np  # noqa: F401
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "amr-demo_b200")]
+    os.environ["AMRGPU_QUIET"] = "1"
+    from amrgpu import workloads as W
+    from oracle import oracle as O
+    f, m, cfg, s0 = W.vortex_1024(level=level, steps=steps, final_time=0.0)
+    s = s0.copy()
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    os.dup2(devnull, 1)
+    t0 = time.perf_counter()
+    try:
+        if use_ref:
+            O.reference_go(m, s, 16, cfg)
+        else:
+            O.evolve(m, s, O.make_config(16, cfg))
+    finally:
+        t1 = time.perf_counter()
+        os.dup2(saved, 1)
+        os.close(devnull)
+    return m.ncells * steps, t1 - t0
+
+
+def cpu_baseline(level=5, steps=16):
+    """All host cores, one process each (the reference's own MPI-rank model
+    without its exchange), each advancing its own copy of the vortex problem
+    at level `level` for `steps` RK3 steps."""
+    from oracle import oracle as O
+    use_ref = O.reference_available()
+    procs = max(1, min(os.cpu_count() or 1, 128))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_worker, [(level, steps, use_ref)] * procs)
+    wall = time.perf_counter() - t0
+    updates = sum(r[0] for r in res)
+    slowest = max(r[1] for r in res)
+    value = updates / slowest
+    cells = (4 ** level) * 256
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": "reference" if use_ref else "port",
+            "sample": f"{procs} processes x {steps} RK3 steps of the same vortex at {cells} cells "
+                      f"(level {level}, 16x16 patches); rate = all updates / slowest process "
+                      f"({slowest:.2f} s; pool wall {wall:.2f} s)"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i in range(4) if r[i].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ GPU arm
+def autotune(ag, s, steps=6):
+    """Times every compiled (quads per CTA, threads) variant for this mesh
+    and keeps the fastest; all variants give identical bits."""
+    import torch
+    from amrgpu._lib import lib
+    st = torch.cuda.ExternalStream(s.stream())
+    best = None
+    for qpb in (1, 2, 4, 8):
+        for thr in (160, 256, 288, 544, 576):
+            if lib().amrgpu_session_set_launch(s._s, qpb, thr) != 0:
+                ag.clear_error()
+                continue
+            s.step(3)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            s.step(steps)
+            e1.record(st)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            if best is None or ms < best[0]:
+                best = (ms, qpb, thr)
+    s.set_launch(best[1], best[2])
+    return {"quads_per_block": best[1], "threads": best[2]}
+
+
+def time_form(ag, mesh, cfg, s0, form, steps, warmup, tune_on=True):
+    import torch
+    s = ag.Session(mesh, cfg, form=form)
+    s.upload(s0)
+    tune = autotune(ag, s) if tune_on else None
+    s.upload(s0)
+    st = torch.cuda.ExternalStream(s.stream())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    s.step(warmup)
+    s.sync()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    l0 = s.launch_count()
+    for k in range(steps):
+        with torch.cuda.stream(st):
+            flush.zero_()
+        evs[k][0].record(st)
+        s.step(1)
+        evs[k][1].record(st)
+    rep = s.sync()
+    launches = s.launch_count() - l0
+    ms = [a.elapsed_time(b) for a, b in evs]
+    return s, {"ms_steps": ms, "report": rep, "tune": tune, "launches": launches}
+
+
+def e2e_form(ag, mesh, cfg, s0, form, steps, segment):
+    """hpc_amr_evolve_solver on pinned host memory, `segment` steps a call."""
+    import torch
+    host = torch.empty(mesh.dof, dtype=torch.float64, pin_memory=True).numpy()
+    host[:] = s0
+    c = ag.Config.current()
+    c["form"] = form
+    c["time_steps"] = 10 ** 9
+    c["regrid_interval"] = segment
+    c["final_time"] = 0.0
+    c.apply()
+    r = ag.evolve_solver(mesh, host, 0)  # warm-up segment (session build, graphs)
+    torch.cuda.synchronize()
+    ist = r["istep"]
+    calls = max(1, steps // segment)
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        r = ag.evolve_solver(mesh, host, ist)
+        ist = r["istep"]
+    wall = time.perf_counter() - t0
+    return {"value": mesh.ncells * calls * segment / wall, "unit": UNIT,
+            "h2d_bytes_per_step": mesh.dof * 8, "d2h_bytes_per_step": mesh.dof * 8,
+            "step": f"one hpc_amr_evolve_solver call = {segment} RK3 steps",
+            "error": r["error"]}
+
+
+def traffic_per_launch(form):
+    p = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        d = json.load(fh)
+    v = d.get("fp32_flux" if form == 1 else "fp64_exact")
+    return v.get("dram_bytes_per_launch") if v else None
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+
+    import amrgpu as ag
+    from amrgpu import workloads as W
+    f, mesh, cfg, s0 = W.vortex_1024(level=args.level, final_time=0.0, steps=10 ** 9)
+    hbm, peak_kind = peaks()
+    run_forms = (0, 1) if args.form < 0 else (args.form,)
+
+    forms = {}
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for form in run_forms:
+            s, r = time_form(ag, mesh, cfg, s0, form, args.steps, args.warmup, not args.no_tune)
+            forms[form] = (s, r)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = clk.summary()
+
+    out = {}
+    for form, (s, r) in forms.items():
+        tot_ms = sum(r["ms_steps"])
+        if world > 1:
+            t = torch.tensor([tot_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot_ms = float(t.item())
+        cells = mesh.ncells
+        value = world * cells * args.steps / (tot_ms * 1e-3)
+        avg_ms = tot_ms / args.steps
+        achieved = cells * B_ALG[form] / (avg_ms * 1e-3) / 1e9
+        out[form] = {"value": value, "ms_per_step": avg_ms, "achieved_gbs": achieved, "report": r["report"],
+                     "tune": r["tune"], "launches": r["launches"]}
+
+    if len(run_forms) == 1:
+        if rank == 0:
+            r = out[run_forms[0]]
+            print(json.dumps({"metric": METRIC, "value": r["value"], "unit": UNIT, "form": run_forms[0],
+                              "level": args.level, "ms_per_step": r["ms_per_step"],
+                              "achieved_gbs": r["achieved_gbs"], "launches": r["launches"],
+                              "clocks": clocks}), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    # accuracy of the FP32 form against the FP64 form after the same steps
+    q64 = forms[0][0].download().reshape(-1, 4)
+    q32 = forms[1][0].download().reshape(-1, 4)
+    l1 = float(np.abs(q32[:, 0] - q64[:, 0]).sum() / np.abs(q64[:, 0]).sum())
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_form(ag, mesh, cfg, s0, 1, args.steps, args.segment)
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    head = out[1]
+    traffic = traffic_per_launch(1)
+    line = {
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 flux / f64 state",
+        "data": "synthetic (seeded analytic vortex; no dataset exists)",
+        "config": {"workload": WORKLOAD, "cells": mesh.ncells, "quads": mesh.ncell, "patch": "16x16",
+                   "form": "FP32 flux, FP64 state, Shu-Osher SSP-RK3", "l2": "flushed between steps "
+                   "(256 MB write; per-step CUDA events exclude it)", "launch": head["tune"],
+                   "parallelism": "replicas" if world > 1 else "1 GPU"},
+        "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+                     "frac": head["achieved_gbs"] / hbm, "traffic": traffic,
+                     "peak_kind": peak_kind, "bytes_per_cell_update": B_ALG[1]},
+        "forms": {
+            "plain_fp64": {"value": out[0]["value"], "ms_per_step": out[0]["ms_per_step"],
+                           "achieved_gbs": out[0]["achieved_gbs"], "frac": out[0]["achieved_gbs"] / hbm,
+                           "bytes_per_cell_update": B_ALG[0], "launch": out[0]["tune"],
+                           "bound": "fp64 pipe (IEEE div/sqrt sequences)"},
+            "fp32_flux": {"value": out[1]["value"], "ms_per_step": out[1]["ms_per_step"]},
+            "speedup_fp32_over_fp64": out[1]["value"] / out[0]["value"],
+            "l1_rho_rel_fp32_vs_fp64": l1,
+        },
+        "e2e": e2e,
+        "clocks": clocks,
+        "gpu_launches": int(out[0]["launches"] + out[1]["launches"]),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    vals = []
+    cb = None
+    for _ in range(max(1, args.steps // 10)):
+        cb = cpu_baseline()
+        vals.append(cb["value"])
+    value = statistics.median(vals)
+    cb["value"] = value
+    line = {"metric": METRIC, "impl": "reference", "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded analytic vortex)",
+            "config": {"workload": WORKLOAD + " (CPU sample, see cpu_baseline.sample)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--segment", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--level", type=int, default=6, help="forest level (6: the 1024^2 workload)")
+    ap.add_argument("--form", type=int, default=-1, help="time one form only (0 FP64, 1 FP32 flux)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -25,7 +25,7 @@ def config_from_golden(ag, z):
               "pressure", "mach", "alpha", "beta", "checkpoint_interval", "visualization_interval",
               "regrid_interval"):
         c[k] = z[k].item()
-    c["bc"] = [int(b) for b in z["bc"]] + [1, 1]
+    c["bc"] = [int(b) for b in z["bc"]][:6]
     return c
 
 

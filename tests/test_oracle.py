@@ -28,7 +28,7 @@ def golden_cfg(z):
     keys = ["time_scheme", "time_steps", "dt", "cfl", "coarse_grid_h", "initial_condition", "gamma", "density",
             "pressure", "mach", "alpha", "beta", "checkpoint_interval", "visualization_interval", "regrid_interval"]
     d = {k: z[k].item() for k in keys}
-    d["bc"] = [int(b) for b in z["bc"]] + [1, 1]
+    d["bc"] = [int(b) for b in z["bc"]][:6]
     d["final_time"] = 0.0
     return d
 
