@@ -51,6 +51,6 @@ struct DeviceScalars {
     int pad;
 };
 
-enum { kFlagNonFinite = 1, kFlagNegative = 2 };
+enum { kFlagNonFinite = 1, kFlagNegative = 2, kFlagTimeout = 4 };
 
 }  // namespace amrgpu

@@ -78,6 +78,89 @@ __device__ __forceinline__ void roe_flux_fp32(const float ql[4], const float qr[
     flux[3] = ((b1 * fluxl - b2 * fluxr) * inv_db + disp) * mag;
 }
 
+// Per-cell FP32 record (8 floats, two float4 loads):
+// [0] rho [1] u [2] v [3] p [4] H [5] sqrt(rho) [6] rho*u [7] rho*v.
+// rho*E + p is recovered as rho*H.
+__device__ __forceinline__ void cell_prims_fp32(const double q[4], float P[8])
+{
+    float rho = (float)q[0];
+    float ru = (float)q[1], rv = (float)q[2], rE = (float)q[3];
+    float oneOrho = __frcp_rn(rho);
+    float u = ru * oneOrho, v = rv * oneOrho;
+    float p = 0.4f * (rE - 0.5f * rho * (u * u + v * v));
+    P[0] = rho;
+    P[1] = u;
+    P[2] = v;
+    P[3] = p;
+    P[4] = (rE + p) * oneOrho;
+    P[5] = sqrtf(rho);
+    P[6] = ru;
+    P[7] = rv;
+}
+
+// flux_roe_2d on FP32 records. Axis-aligned faces (every face of a brick
+// mesh) take the rotated form: with n = (h,0) the normal velocity is u and
+// the tangential-correction terms of rows 2/3 reduce to 0 and
+// rhobar*(v_R - v_L); Mcoeff = 1/(1+|un/a|) = a/(a+|un|). Five MUFU
+// operations per face. Other normals use roe_flux_fp32 on conserved states.
+__device__ __forceinline__ void roe_flux_prim_fp32(const float *L, const float *R, float n0, float n1,
+                                                   float flux[4])
+{
+    const bool xdir = (n1 == 0.0f);
+    const bool ydir = (n0 == 0.0f);
+    if (!(xdir || ydir)) {
+        float ql[4] = {L[0], L[6], L[7], L[0] * L[4] - L[3]};
+        float qr[4] = {R[0], R[6], R[7], R[0] * R[4] - R[3]};
+        roe_flux_fp32(ql, qr, n0, n1, flux);
+        return;
+    }
+    const float mag = xdir ? fabsf(n0) : fabsf(n1);
+    const float sgn = xdir ? (n0 > 0.0f ? 1.0f : -1.0f) : (n1 > 0.0f ? 1.0f : -1.0f);
+    const float rhol = L[0], ul = L[1], vl = L[2], pl = L[3], Hl = L[4], srl = L[5];
+    const float rhor = R[0], ur = R[1], vr = R[2], pr = R[3], Hr = R[4], srr = R[5];
+    // normal / tangential momentum components of each state
+    const float unl = sgn * (xdir ? ul : vl), unr = sgn * (xdir ? ur : vr);
+    const float inv = __frcp_rn(srl + srr);
+    const float rhobar = srl * srr;
+    const float ubar = (ul * srl + ur * srr) * inv;
+    const float vbar = (vl * srl + vr * srr) * inv;
+    const float Hbar = (Hl * srl + Hr * srr) * inv;
+    const float a2 = 0.4f * (Hbar - 0.5f * (ubar * ubar + vbar * vbar));
+    const float abar = sqrtf(a2);
+    const float unbar = sgn * (xdir ? ubar : vbar);
+    const float b1 = fmaxf(fmaxf(unbar + abar, unr + abar), 0.0f);
+    const float b2 = fminf(fminf(unbar - abar, unl - abar), 0.0f);
+    const float inv_db = __frcp_rn(b1 - b2);
+    const float bcoeff = b1 * b2 * inv_db;
+    const float delta1 = (rhor - rhol) - (pr - pl) * __frcp_rn(a2);
+    const float bM = bcoeff * abar * __frcp_rn(abar + fabsf(unbar));
+    // mass flux of each state through the face
+    const float ml = sgn * (xdir ? L[6] : L[7]);
+    const float mr = sgn * (xdir ? R[6] : R[7]);
+    const float rHl = rhol * Hl, rHr = rhor * Hr;
+    float fl, fr, d;
+    fl = ml;
+    fr = mr;
+    d = bcoeff * (rhor - rhol) - bM * delta1;
+    flux[0] = ((b1 * fl - b2 * fr) * inv_db + d) * mag;
+    fl = ml * ul + (xdir ? sgn * pl : 0.0f);
+    fr = mr * ur + (xdir ? sgn * pr : 0.0f);
+    d = bcoeff * (R[6] - L[6]) - bM * (delta1 * ubar + (xdir ? 0.0f : rhobar * (ur - ul)));
+    flux[1] = ((b1 * fl - b2 * fr) * inv_db + d) * mag;
+    fl = ml * vl + (xdir ? 0.0f : sgn * pl);
+    fr = mr * vr + (xdir ? 0.0f : sgn * pr);
+    d = bcoeff * (R[7] - L[7]) - bM * (delta1 * vbar + (xdir ? rhobar * (vr - vl) : 0.0f));
+    flux[2] = ((b1 * fl - b2 * fr) * inv_db + d) * mag;
+    fl = rHl * unl;
+    fr = rHr * unr;
+    d = bcoeff * (rHr - rHl) - bM * (delta1 * Hbar + rhobar * (Hr - Hl));
+    flux[3] = ((b1 * fl - b2 * fr) * inv_db + d) * mag;
+}
+
+// Boundary face on an FP32 record: conserved state rebuilt from the record.
+__device__ __forceinline__ void bc_flux_rec_fp32(int bc, const float *P, float n0, float n1,
+                                                 const float qin[4], float flux[4]);
+
 __device__ __forceinline__ void bc_flux_fp32(int bc, const float q[4], float n0, float n1,
                                              const float qin[4], float flux[4])
 {
@@ -110,6 +193,13 @@ __device__ __forceinline__ void bc_flux_fp32(int bc, const float q[4], float n0,
     flux[1] = (qb[1] * ub + p) * n0 + (qb[2] * ub) * n1;
     flux[2] = (qb[1] * vb) * n0 + (qb[2] * vb + p) * n1;
     flux[3] = (ub * n0 + vb * n1) * (qb[3] + p);
+}
+
+__device__ __forceinline__ void bc_flux_rec_fp32(int bc, const float *P, float n0, float n1,
+                                                 const float qin[4], float flux[4])
+{
+    float q[4] = {P[0], P[6], P[7], P[0] * P[4] - P[3]};
+    bc_flux_fp32(bc, q, n0, n1, qin, flux);
 }
 
 }  // namespace amrgpu

@@ -85,6 +85,100 @@ __device__ __forceinline__ void roe_flux_fp64(const double ql[4], const double q
     flux[3] = ((b1 * fluxl - b2 * fluxr) / db + disp) * mag;
 }
 
+// Per-cell primitive record shared by the four faces of a cell:
+// [0] rho [1] rho*u [2] rho*v [3] rho*E [4] u [5] v [6] p [7] H [8] sqrt(rho),
+// each computed by exactly the expression flux_roe_2d uses
+// (flux_2d_module.F90:93-99, 113-118), so reusing them is bit-exact.
+__device__ __forceinline__ void cell_prims_fp64(const double q[4], double P[9])
+{
+    const double gamma = 1.4;
+    const double half = 0.5;
+    double rho = q[0];
+    double oneOrho = 1.0 / rho;
+    double u = q[1] * oneOrho;
+    double v = q[2] * oneOrho;
+    double E = q[3] * oneOrho;
+    double p = (gamma - 1.0) * (q[3] - half * rho * (u * u + v * v));
+    P[0] = q[0];
+    P[1] = q[1];
+    P[2] = q[2];
+    P[3] = q[3];
+    P[4] = u;
+    P[5] = v;
+    P[6] = p;
+    P[7] = E + p * oneOrho;
+    P[8] = sqrt(rho);
+}
+
+// flux_roe_2d on primitive records. For an axis-aligned normal (one
+// component exactly zero) |n| = sqrt(n0*n0) is |n0| exactly in IEEE
+// round-to-nearest and n0/|n0| = +-1, n1/|n0| = n1 (a signed zero), so the
+// shortcut returns the same bits as the general path.
+__device__ __forceinline__ void roe_flux_prim_fp64(const double *L, const double *R, double n0, double n1,
+                                                   double flux[4])
+{
+    const double gm1 = 0.4;
+    const double half = 0.5;
+    double mag, nx, ny;
+    if (n1 == 0.0 && fabs(n0) > 1e-150) {
+        mag = fabs(n0);
+        nx = n0 > 0.0 ? 1.0 : -1.0;
+        ny = n1;
+    } else if (n0 == 0.0 && fabs(n1) > 1e-150) {
+        mag = fabs(n1);
+        nx = n0;
+        ny = n1 > 0.0 ? 1.0 : -1.0;
+    } else {
+        mag = sqrt(n0 * n0 + n1 * n1);
+        nx = n0 / mag;
+        ny = n1 / mag;
+    }
+    const double rhol = L[0], ul = L[4], vl = L[5], pl = L[6], Hl = L[7], srl = L[8];
+    const double rhor = R[0], ur = R[4], vr = R[5], pr = R[6], Hr = R[7], srr = R[8];
+    double unl = ul * nx + vl * ny;
+    double unr = ur * nx + vr * ny;
+    double oneOroe_fact = 1.0 / (srl + srr);
+    double rhobar = sqrt(rhol * rhor);
+    double ubar = (ul * srl + ur * srr) * oneOroe_fact;
+    double vbar = (vl * srl + vr * srr) * oneOroe_fact;
+    double Hbar = (Hl * srl + Hr * srr) * oneOroe_fact;
+    double abar = sqrt(gm1 * (Hbar - half * (ubar * ubar + vbar * vbar)));
+    double unbar = ubar * nx + vbar * ny;
+    double Mnbar = unbar / abar;
+    double eigp = unbar + abar;
+    double eigm = unbar - abar;
+    double eigp_max = unr + abar;
+    double eigm_min = unl - abar;
+    double b1 = (eigp > 0.0 || eigp_max > 0.0) ? ((eigp > eigp_max) ? eigp : eigp_max) : 0.0;
+    double b2 = (eigm < 0.0 || eigm_min < 0.0) ? ((eigm < eigm_min) ? eigm : eigm_min) : 0.0;
+    double bcoeff = b1 * b2 / (b1 - b2);
+    double delta1 = (rhor - rhol) - (pr - pl) / (abar * abar);
+    double Mcoeff = 1.0 / (1.0 + fabs(Mnbar));
+    double bM = bcoeff * Mcoeff;
+    double db = b1 - b2;
+    double fluxl, fluxr, disp;
+
+    fluxl = L[1] * nx + L[2] * ny;
+    fluxr = R[1] * nx + R[2] * ny;
+    disp = bcoeff * (rhor - rhol) - bM * delta1;
+    flux[0] = ((b1 * fluxl - b2 * fluxr) / db + disp) * mag;
+
+    fluxl = (L[1] * ul + pl) * nx + (L[2] * ul) * ny;
+    fluxr = (R[1] * ur + pr) * nx + (R[2] * ur) * ny;
+    disp = bcoeff * (R[1] - L[1]) - bM * (delta1 * ubar + rhobar * (ur - ul - nx * (unr - unl)));
+    flux[1] = ((b1 * fluxl - b2 * fluxr) / db + disp) * mag;
+
+    fluxl = (L[1] * vl) * nx + (L[2] * vl + pl) * ny;
+    fluxr = (R[1] * vr) * nx + (R[2] * vr + pr) * ny;
+    disp = bcoeff * (R[2] - L[2]) - bM * (delta1 * vbar + rhobar * (vr - vl - ny * (unr - unl)));
+    flux[2] = ((b1 * fluxl - b2 * fluxr) / db + disp) * mag;
+
+    fluxl = (L[3] + pl) * unl;
+    fluxr = (R[3] + pr) * unr;
+    disp = bcoeff * (rhor * Hr - rhol * Hl) - bM * (delta1 * Hbar + rhobar * (Hr - Hl));
+    flux[3] = ((b1 * fluxl - b2 * fluxr) / db + disp) * mag;
+}
+
 // Boundary face: ghost state of bc_2d, then the physical flux F.n of
 // flux_bc_2d. bc 3 (extension, no reference counterpart): prescribed state
 // qin, used for supersonic inflow.

@@ -201,6 +201,21 @@ int decode_mesh(amrgpu_session *s, const amrgpu_mesh_t *m)
     return AMRGPU_OK;
 }
 
+// The FP32-flux form takes face normals and volumes from each quad's
+// spacing, which needs axis-aligned rectangular quads (every brick mesh).
+bool quads_are_rectangles(const amrgpu_session *s)
+{
+    for (const QuadDesc &q : s->h_quads) {
+        const double *g = q.corner;
+        double sx = std::fabs(g[2] - g[0]) + std::fabs(g[5] - g[1]);
+        double tol = 1e-12 * sx;
+        if (std::fabs(g[0] - g[4]) > tol || std::fabs(g[2] - g[6]) > tol || std::fabs(g[1] - g[3]) > tol ||
+            std::fabs(g[5] - g[7]) > tol || !(g[2] > g[0]) || !(g[5] > g[1]))
+            return false;
+    }
+    return true;
+}
+
 const StageLaunch *find_launch(int form, int n, int qpb, int threads)
 {
     const StageLaunch *tab;
@@ -215,6 +230,10 @@ int configure_launch(amrgpu_session *s, const StageLaunch *L)
 {
     if (!L) {
         set_error(AMRGPU_ERR_UNSUPPORTED, "no stage kernel for this patch size");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    if (s->form == AMRGPU_FORM_FP32_FLUX && !quads_are_rectangles(s)) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "the FP32-flux form needs axis-aligned rectangular quads");
         return AMRGPU_ERR_UNSUPPORTED;
     }
     if (!cuda_ok(cudaFuncSetAttribute(L->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L->smem)),

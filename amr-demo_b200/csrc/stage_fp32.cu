@@ -12,15 +12,16 @@
 namespace amrgpu {
 
 struct FluxOpsFP32 {
+    __device__ static __forceinline__ void prims(const double *q, float *P) { cell_prims_fp32(q, P); }
     __device__ static __forceinline__ void roe(const float *l, const float *r, float n0, float n1,
                                                float *f)
     {
-        roe_flux_fp32(l, r, n0, n1, f);
+        roe_flux_prim_fp32(l, r, n0, n1, f);
     }
     __device__ static __forceinline__ void bc(int bc, const float *q, float n0, float n1,
                                               const float *qin, float *f)
     {
-        bc_flux_fp32(bc, q, n0, n1, qin, f);
+        bc_flux_rec_fp32(bc, q, n0, n1, qin, f);
     }
     __device__ static __forceinline__ double cfl(const double *q, double vol, double c)
     {
@@ -34,9 +35,10 @@ struct FluxOpsFP32 {
 
 static const StageLaunch kTable32[] = {
     AMRGPU_STAGE32(16, 1, 288, 3),
-    AMRGPU_STAGE32(16, 2, 544, 2),
-    AMRGPU_STAGE32(16, 1, 256, 3),
-    AMRGPU_STAGE32(16, 1, 160, 4),
+    AMRGPU_STAGE32(16, 1, 288, 2),
+    AMRGPU_STAGE32(16, 2, 544, 1),
+    AMRGPU_STAGE32(16, 2, 576, 1),
+    AMRGPU_STAGE32(16, 1, 544, 2),
     AMRGPU_STAGE32(8, 4, 288, 3),
     AMRGPU_STAGE32(8, 2, 160, 4),
     AMRGPU_STAGE32(8, 8, 576, 1),

@@ -12,10 +12,11 @@
 namespace amrgpu {
 
 struct FluxOpsFP64 {
+    __device__ static __forceinline__ void prims(const double *q, double *P) { cell_prims_fp64(q, P); }
     __device__ static __forceinline__ void roe(const double *l, const double *r, double n0, double n1,
                                                double *f)
     {
-        roe_flux_fp64(l, r, n0, n1, f);
+        roe_flux_prim_fp64(l, r, n0, n1, f);
     }
     __device__ static __forceinline__ void bc(int bc, const double *q, double n0, double n1,
                                               const double *qin, double *f)
@@ -85,13 +86,13 @@ const void *cfl_kernel_fp64(int n)
                 (const void *)stage_kernel<N, QPB, T, MINB, false, FluxOpsFP64>}
 
 static const StageLaunch kTable64[] = {
+    AMRGPU_STAGE64(16, 1, 288, 1),
     AMRGPU_STAGE64(16, 1, 288, 2),
+    AMRGPU_STAGE64(16, 2, 576, 1),
     AMRGPU_STAGE64(16, 1, 256, 2),
-    AMRGPU_STAGE64(16, 2, 544, 1),
-    AMRGPU_STAGE64(16, 1, 160, 3),
     AMRGPU_STAGE64(8, 4, 288, 2),
     AMRGPU_STAGE64(8, 2, 160, 3),
-    AMRGPU_STAGE64(8, 8, 576, 1),
+    AMRGPU_STAGE64(8, 4, 576, 1),
     AMRGPU_STAGE64(4, 8, 160, 3),
     AMRGPU_STAGE64(4, 16, 320, 2),
     AMRGPU_STAGE64(2, 16, 96, 4),

@@ -15,22 +15,29 @@
 //     physics_runge_kutta_interface.c:197-205) for the following step.
 //
 // Work decomposition: a persistent grid; each CTA owns QPB quadrants at a
-// time. Phase A stages the QPB patches (SoA, vectorised loads), the
-// neighbour edge strips and the (n+1)^2 bilinear nodes in shared memory.
-// Phase B evaluates every face flux of the patches once (interior faces
-// first, then the 4n edge faces; a coarse quad's hanging edge evaluates two
-// fluxes per edge cell). Phase C assembles each cell's residual in exactly
-// the reference's accumulation order -- edge-face contributions in
-// face_info order, then -F(x-1/2) +F(x+1/2) -F(y-1/2) +F(y+1/2) -- divides
-// by the volume, negates, and applies the stage update. Edge fluxes are
-// computed redundantly by both patches that share an edge, so there are no
-// atomics and both sides see bit-identical values (conservation holds
-// exactly as in the reference).
+// time and walks its groups in a software pipeline. While group k is being
+// computed, group k+1's four field slabs per quad (contiguous n*n doubles
+// each) arrive through 1D bulk copies (TMA engine) completed on an
+// mbarrier, its neighbour edge strips through cp.async, and group k+2's
+// descriptors through a bulk copy; the next stage's own-cell auxiliary
+// arrays are prefetched into L2.
+//   A  per-cell primitive records (rho, rho*u, rho*v, rho*E, u, v, p, H,
+//      sqrt(rho)) of the patches and strips, and the (n+1)^2 bilinear nodes
+//   B  every face flux once (interior faces first, then the 4n edge faces;
+//      a coarse quad's hanging edge evaluates two fluxes per edge cell)
+//   C  each cell's residual in exactly the reference's accumulation order
+//      -- edge-face contributions in face_info order, then -F(x-1/2)
+//      +F(x+1/2) -F(y-1/2) +F(y+1/2) -- divided by the volume, negated,
+//      and the stage update.
+// Edge fluxes are computed by both patches that share an edge, so there are
+// no atomics and both sides see bit-identical values; conservation holds
+// exactly as in the reference.
 #pragma once
 
 #include <cstdint>
 #include <type_traits>
 
+#include "async_copy.cuh"
 #include "device_common.cuh"
 
 namespace amrgpu {
@@ -111,7 +118,7 @@ __device__ __forceinline__ double cell_h_of(double h_base, int level, int n)
     return h_base * (1.0 / ldexp(1.0, level)) / (double)n;
 }
 
-// Volume of the sub-cell with nodes a=n1, b=n2, c=n3, d=n4:
+// Volume of the sub-cell with nodes n1..n4:
 // 0.5*sqrt(((n4-n1) x (n3-n2))**2), solver_residual_subgrid_2d_module.F90:152-160
 __device__ __forceinline__ double subcell_volume(double x1, double y1, double x2, double y2,
                                                  double x3, double y3, double x4, double y4)
@@ -139,49 +146,144 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-// Shared-memory footprint of one stage CTA.
+constexpr unsigned kWaitLimit = 1u << 22;  // bounded mbarrier polls
+
+// Per-cell records and per-face fluxes are stored array-of-structures in
+// shared memory so each is moved with 16-byte vector accesses:
+//   FP32 record: 8 floats (2 x float4), flux: float4
+//   FP64 record: 10 doubles (5 x double2, slot 9 unused), flux: 2 x double2
+template <bool F32>
+struct RecTraits;
+template <>
+struct RecTraits<true> {
+    using R = float;
+    using V = float4;
+    static constexpr int n = 8;
+    static constexpr int nv = 2;
+    static constexpr int fv = 1;  // vectors per flux
+};
+template <>
+struct RecTraits<false> {
+    using R = double;
+    using V = double2;
+    static constexpr int n = 10;
+    static constexpr int nv = 5;
+    static constexpr int fv = 2;
+};
+
+template <bool F32>
+__device__ __forceinline__ void load_rec(const typename RecTraits<F32>::R *base, int idx,
+                                         typename RecTraits<F32>::R *out)
+{
+    using T = RecTraits<F32>;
+    const typename T::V *src = reinterpret_cast<const typename T::V *>(base + (size_t)idx * T::n);
+    typename T::V *dst = reinterpret_cast<typename T::V *>(out);
+#pragma unroll
+    for (int k = 0; k < T::nv; ++k) dst[k] = src[k];
+}
+
+template <bool F32>
+__device__ __forceinline__ void store_flux(typename RecTraits<F32>::R *base, int idx,
+                                           const typename RecTraits<F32>::R *f)
+{
+    using T = RecTraits<F32>;
+    typename T::V *dst = reinterpret_cast<typename T::V *>(base + (size_t)idx * 4);
+    const typename T::V *src = reinterpret_cast<const typename T::V *>(f);
+#pragma unroll
+    for (int k = 0; k < T::fv; ++k) dst[k] = src[k];
+}
+
+template <bool F32>
+__device__ __forceinline__ void load_flux(const typename RecTraits<F32>::R *base, int idx, double out[4])
+{
+    using T = RecTraits<F32>;
+    alignas(16) typename T::R f[4];
+    const typename T::V *src = reinterpret_cast<const typename T::V *>(base + (size_t)idx * 4);
+    typename T::V *dst = reinterpret_cast<typename T::V *>(f);
+#pragma unroll
+    for (int k = 0; k < T::fv; ++k) dst[k] = src[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[k] = (double)f[k];
+}
+
+// Shared-memory carve-up of one stage CTA (all offsets 16-byte aligned).
 template <int N, int QPB, bool F32>
 struct StageSmem {
-    using R = typename std::conditional<F32, float, double>::type;
+    using R = typename RecTraits<F32>::R;
     static constexpr int NN = N * N;
     static constexpr int NP1 = N + 1;
-    static constexpr size_t desc = sizeof(QuadDesc) * QPB;
-    static constexpr size_t qs = sizeof(double) * QPB * 4 * NN;
-    static constexpr size_t qf = F32 ? sizeof(float) * QPB * 4 * NN : 0;
-    static constexpr size_t strip = sizeof(R) * QPB * 4 * 2 * 4 * N;
-    static constexpr size_t nodes = sizeof(double) * QPB * NP1 * NP1 * 2;
-    static constexpr size_t fx = sizeof(R) * QPB * 4 * N * NP1;
-    static constexpr size_t fy = sizeof(R) * QPB * 4 * NP1 * N;
-    static constexpr size_t fh = sizeof(R) * QPB * 4 * 4 * N;
+    static constexpr int NSTRIP = 4 * 2 * N;        // strip cells per quad: side x {nbr0,nbr1} x m
+    static constexpr int NPC = NN + NSTRIP;         // record cells per quad
+    static constexpr size_t al(size_t b) { return (b + 15) / 16 * 16; }
+    static constexpr size_t bar = 32;
+    static constexpr size_t desc = al(sizeof(QuadDesc) * QPB) * 3;
+    static constexpr size_t raw = al(sizeof(double) * QPB * 4 * NN) * 2;
+    static constexpr size_t rstrip = al(sizeof(double) * QPB * 4 * NSTRIP) * 2;
+    static constexpr size_t prim = al(sizeof(R) * QPB * RecTraits<F32>::n * NPC);
+    static constexpr size_t nodes = F32 ? 0 : al(sizeof(double) * QPB * NP1 * NP1 * 2);
+    static constexpr size_t geo = al(sizeof(double) * QPB * 4);
+    static constexpr size_t fx = al(sizeof(R) * QPB * 4 * N * NP1);
+    static constexpr size_t fy = al(sizeof(R) * QPB * 4 * NP1 * N);
+    static constexpr size_t fh = al(sizeof(R) * QPB * 4 * 4 * N);
     static constexpr size_t red = sizeof(double) * 64;
-    static constexpr size_t total = desc + qs + qf + strip + nodes + fx + fy + fh + red;
+    static constexpr size_t o_desc = bar;
+    static constexpr size_t o_raw = o_desc + desc;
+    static constexpr size_t o_rstrip = o_raw + raw;
+    static constexpr size_t o_prim = o_rstrip + rstrip;
+    static constexpr size_t o_nodes = o_prim + prim;
+    static constexpr size_t o_geo = o_nodes + nodes;
+    static constexpr size_t o_fx = o_geo + geo;
+    static constexpr size_t o_fy = o_fx + fx;
+    static constexpr size_t o_fh = o_fy + fy;
+    static constexpr size_t o_red = o_fh + fh;
+    static constexpr size_t total = o_red + red;
 };
+
+// The neighbour's cell facing side s at position m (its opposite edge).
+template <int N>
+__device__ __forceinline__ int facing_cell(int s, int m)
+{
+    if (s == 0) return m * N + (N - 1);
+    if (s == 1) return m * N;
+    if (s == 2) return (N - 1) * N + m;
+    return m;
+}
 
 template <int N, int QPB, int T, int MINB, bool F32, typename FluxOps>
 __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
 {
-    using R = typename std::conditional<F32, float, double>::type;
+    using Tr = RecTraits<F32>;
+    using R = typename Tr::R;
     using S = StageSmem<N, QPB, F32>;
+    constexpr int RS = Tr::n;
     constexpr int NN = N * N;
     constexpr int NP1 = N + 1;
-    constexpr int NINT = 2 * N * (N - 1);   // interior faces per quad
-    constexpr int NEDGE = 4 * N;            // edge faces per quad
-    constexpr int NWORK = NINT + NEDGE;
+    constexpr int NPC = S::NPC;
+    constexpr int NFACE = 2 * N * NP1;      // faces per quad (x and y, edges included)
+    constexpr int RB = (QPB * NFACE + T - 1) / T;   // face rounds per thread
+    static_assert(T % 32 == 0, "whole warps");
+    static_assert(N <= 32 && QPB <= 64, "face code packing");
 
-    extern __shared__ __align__(16) unsigned char smem[];
-    QuadDesc *sq = reinterpret_cast<QuadDesc *>(smem);
-    double *qs = reinterpret_cast<double *>(smem + S::desc);
-    R *qf = F32 ? reinterpret_cast<R *>(smem + S::desc + S::qs) : reinterpret_cast<R *>(qs);
-    R *strip = reinterpret_cast<R *>(smem + S::desc + S::qs + S::qf);
-    double *nodes = reinterpret_cast<double *>(smem + S::desc + S::qs + S::qf + S::strip);
-    R *fx = reinterpret_cast<R *>(smem + S::desc + S::qs + S::qf + S::strip + S::nodes);
-    R *fy = fx + QPB * 4 * N * NP1;
-    R *fh = fy + QPB * 4 * NP1 * N;
-    double *red = reinterpret_cast<double *>(smem + S::total - S::red);
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    QuadDesc *sdesc = reinterpret_cast<QuadDesc *>(smem + S::o_desc);
+    double *sraw = reinterpret_cast<double *>(smem + S::o_raw);
+    double *srstrip = reinterpret_cast<double *>(smem + S::o_rstrip);
+    R *prim = reinterpret_cast<R *>(smem + S::o_prim);
+    double *nodes = reinterpret_cast<double *>(smem + S::o_nodes);
+    double *geo = reinterpret_cast<double *>(smem + S::o_geo);
+    R *fx = reinterpret_cast<R *>(smem + S::o_fx);
+    R *fy = reinterpret_cast<R *>(smem + S::o_fy);
+    R *fh = reinterpret_cast<R *>(smem + S::o_fh);
+    double *red = reinterpret_cast<double *>(smem + S::o_red);
+    constexpr size_t desc_slot = S::desc / 3 / sizeof(QuadDesc);   // QuadDesc entries per slot
+    constexpr size_t raw_slot = S::raw / 2 / sizeof(double);
+    constexpr size_t rstrip_slot = S::rstrip / 2 / sizeof(double);
 
     const int tid = threadIdx.x;
     const long long stride = a.stride;
     const double scale_factor = 2.0 / (double)N;
+    const int ngroups = (a.nquad + QPB - 1) / QPB;
 
     // step scalars
     const StepSlot slot = a.scal->slot[a.slot_read];
@@ -197,164 +299,271 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
         a.scal->dt_used = dt;
         if (dt > 0.0) a.scal->steps += 1;
         a.scal->slot[a.slot_reset].dt_bits = (unsigned long long)__double_as_longlong(a.dt_cap);
-        if (!a.cfl_on) a.scal->slot[a.slot_write].dt_bits = (unsigned long long)__double_as_longlong(a.dt_cap);
+        if (!a.cfl_on)
+            a.scal->slot[a.slot_write].dt_bits = (unsigned long long)__double_as_longlong(a.dt_cap);
     }
 
     double my_dt_min = a.dt_cap;
     double my_norm = 0.0;
     int my_flags = 0;
 
-    for (int grp = blockIdx.x; grp * QPB < a.nquad; grp += gridDim.x) {
-        const int q0 = grp * QPB;
-        // ---------------- phase A: descriptors, patches, strips, nodes
-        {
-            const int *src = reinterpret_cast<const int *>(a.quads + q0);
-            int *dst = reinterpret_cast<int *>(sq);
-            constexpr int per = sizeof(QuadDesc) / 4;
-            const int lim = min(QPB, a.nquad - q0) * per;
-            for (int k = tid; k < lim; k += T) dst[k] = __ldg(src + k);
+    // Each thread's face work items are the same for every quad group:
+    // decode them once. code = ql | xd<<6 | fa<<7 | fb<<13 | valid<<19.
+    int fcode[RB];
+#pragma unroll
+    for (int rb = 0; rb < RB; ++rb) {
+        const int k = tid + rb * T;
+        if (k < QPB * NFACE) {
+            const int ql = k / NFACE;
+            const int r = k - ql * NFACE;
+            const int xd = r < N * NP1;
+            int fa, fb;
+            if (xd) { fb = r / NP1; fa = r - fb * NP1; }
+            else { const int r2 = r - N * NP1; fa = r2 / N; fb = r2 - fa * N; }
+            fcode[rb] = ql | (xd << 6) | (fa << 7) | (fb << 13) | (1 << 19);
+        } else {
+            fcode[rb] = 0;
         }
-        {
-            constexpr int H = NN / 2;  // double2 per field slab
-            for (int k = tid; k < QPB * 4 * H; k += T) {
-                int ql = k / (4 * H);
-                int rem = k - ql * 4 * H;
-                int f = rem / H;
-                int c2 = rem - f * H;
-                if (q0 + ql < a.nquad) {
-                    const double2 v = __ldg(reinterpret_cast<const double2 *>(
-                        a.qin + f * stride + (long long)(q0 + ql) * NN) + c2);
-                    double *d = qs + (ql * 4 + f) * NN + 2 * c2;
-                    d[0] = v.x;
-                    d[1] = v.y;
-                    if (F32) {
-                        qf[(ql * 4 + f) * NN + 2 * c2] = (R)v.x;
-                        qf[(ql * 4 + f) * NN + 2 * c2 + 1] = (R)v.y;
-                    }
+    }
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    // The CTA walks groups blockIdx.x, +G, +2G, ...; slot parities follow
+    // the iteration count. Descriptors of iteration 0, synchronously:
+    const int G = gridDim.x;
+    if ((int)blockIdx.x < ngroups) {
+        const int g0 = blockIdx.x;
+        const int *src = reinterpret_cast<const int *>(a.quads + (long long)g0 * QPB);
+        int *dst = reinterpret_cast<int *>(sdesc);
+        constexpr int per = sizeof(QuadDesc) / 4;
+        const int lim = min(QPB, a.nquad - g0 * QPB) * per;
+        for (int k = tid; k < lim; k += T) dst[k] = __ldg(src + k);
+    }
+    __syncthreads();
+    auto grp_of = [&](int it) { return (int)blockIdx.x + it * G; };
+    int niter = (ngroups - (int)blockIdx.x + G - 1) / G;
+    if (niter < 0) niter = 0;
+
+    // Issue iteration `it`: its slabs (bulk copies into raw slot it&1) and
+    // the next iteration's descriptors (desc slot (it+1)%3), completing on
+    // bars[it&1]; then its neighbour strips (cp.async, needs its own
+    // descriptors, already resident) and an L2 prefetch of its auxiliary
+    // own-cell inputs.
+    auto issue_iter = [&](int it) {
+        int gg = grp_of(it);
+        int gn = grp_of(it + 1);
+        if (tid == 0) {
+            uint64_t *bar = &bars[it & 1];
+            int nq = (it < niter) ? min(QPB, a.nquad - gg * QPB) : 0;
+            int nq1 = (it + 1 < niter) ? min(QPB, a.nquad - gn * QPB) : 0;
+            unsigned bytes = (unsigned)(nq * 4 * NN * sizeof(double) + nq1 * sizeof(QuadDesc));
+            mbar_arrive_expect_tx(bar, bytes);
+            double *dst = sraw + (size_t)(it & 1) * raw_slot;
+            for (int ql = 0; ql < nq; ++ql)
+                for (int f = 0; f < 4; ++f)
+                    bulk_g2s(dst + (ql * 4 + f) * NN, a.qin + f * stride + (long long)(gg * QPB + ql) * NN,
+                             (unsigned)(NN * sizeof(double)), bar);
+            if (nq1 > 0)
+                bulk_g2s(sdesc + (size_t)((it + 1) % 3) * desc_slot, a.quads + (long long)gn * QPB,
+                         (unsigned)(nq1 * sizeof(QuadDesc)), bar);
+        }
+        if (it < niter) {
+            const QuadDesc *dg = sdesc + (size_t)(it % 3) * desc_slot;
+            double *dst = srstrip + (size_t)(it & 1) * rstrip_slot;
+            for (int k = tid; k < QPB * 4 * S::NSTRIP; k += T) {
+                int m = k % N;
+                int kk = (k / N) % 2;
+                int s = (k / (2 * N)) % 4;
+                int f = (k / (8 * N)) % 4;
+                int ql = k / (32 * N);
+                if (gg * QPB + ql >= a.nquad) continue;
+                const SideDesc &d = dg[ql].side[s];
+                int nbr = -1;
+                if (d.kind == kSideFull || d.kind == kSideFineHang) nbr = (kk == 0) ? d.nbr0 : -1;
+                else if (d.kind == kSideCoarseHang) nbr = (kk == 0) ? d.nbr0 : d.nbr1;
+                if (nbr < 0) continue;
+                cp_async8(dst + k, a.qin + f * stride + (long long)nbr * NN + facing_cell<N>(s, m));
+            }
+            cp_async_commit();
+            if (a.a0 || a.a1) {
+                constexpr int LINES = NN * 8 / 128 > 0 ? NN * 8 / 128 : 1;
+                for (int k = tid; k < QPB * 4 * LINES * 2; k += T) {
+                    int which = k / (QPB * 4 * LINES);
+                    int r = k - which * QPB * 4 * LINES;
+                    int ql = r / (4 * LINES);
+                    int f = (r / LINES) % 4;
+                    int ln = r % LINES;
+                    const double *base = which ? a.a1 : a.a0;
+                    if (!base || gg * QPB + ql >= a.nquad) continue;
+                    prefetch_l2(base + f * stride + (long long)(gg * QPB + ql) * NN + ln * 16);
                 }
             }
         }
+    };
+
+    if (niter > 0) issue_iter(0);
+
+    for (int it = 0; it < niter; ++it) {
+        const int q0 = grp_of(it) * QPB;
+        // ---------------- wait for this group's data, then prefetch the next
+        if (!mbar_wait_bounded(&bars[it & 1], (unsigned)((it >> 1) & 1), kWaitLimit))
+            my_flags |= kFlagTimeout;
+        cp_async_wait_all();
         __syncthreads();
-        // neighbour edge strips: [ql][side][k][f][m]
-        for (int k = tid; k < QPB * 4 * 2 * 4 * N; k += T) {
-            int m = k % N;
-            int f = (k / N) % 4;
-            int kk = (k / (4 * N)) % 2;
-            int s = (k / (8 * N)) % 4;
-            int ql = k / (32 * N);
+        issue_iter(it + 1);
+
+        const QuadDesc *sq = sdesc + (size_t)(it % 3) * desc_slot;
+        const double *raw = sraw + (size_t)(it & 1) * raw_slot;
+        const double *rstrip = srstrip + (size_t)(it & 1) * rstrip_slot;
+
+        // ---------------- phase A: per-cell records, per-quad geometry
+        for (int k = tid; k < QPB * NPC; k += T) {
+            int ql = k / NPC;
+            int c = k - ql * NPC;
             if (q0 + ql >= a.nquad) continue;
-            const SideDesc &d = sq[ql].side[s];
-            int nbr = -1;
-            if (d.kind == kSideFull || d.kind == kSideFineHang) nbr = (kk == 0) ? d.nbr0 : -1;
-            else if (d.kind == kSideCoarseHang) nbr = (kk == 0) ? d.nbr0 : d.nbr1;
-            if (nbr < 0) continue;
-            // the neighbour's edge facing this side
-            int ci, cj;
-            if (s == 0) { ci = N - 1; cj = m; }
-            else if (s == 1) { ci = 0; cj = m; }
-            else if (s == 2) { ci = m; cj = N - 1; }
-            else { ci = m; cj = 0; }
-            strip[k] = (R)__ldg(a.qin + f * stride + (long long)nbr * NN + cj * N + ci);
+            double q[4];
+            if (c < NN) {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) q[f] = raw[(ql * 4 + f) * NN + c];
+            } else {
+                int e = c - NN;   // (s*2 + kk)*N + m
+                int s = e / (2 * N);
+                int kk = (e / N) % 2;
+                const SideDesc &d = sq[ql].side[s];
+                bool present = (d.kind == kSideFull || d.kind == kSideFineHang) ? (kk == 0)
+                               : (d.kind == kSideCoarseHang);
+                if (!present) continue;
+#pragma unroll
+                for (int f = 0; f < 4; ++f) q[f] = rstrip[ql * 4 * S::NSTRIP + f * S::NSTRIP + e];
+            }
+            alignas(16) R P[RS];
+            FluxOps::prims(q, P);
+            typename Tr::V *dst = reinterpret_cast<typename Tr::V *>(prim + (size_t)(ql * NPC + c) * RS);
+#pragma unroll
+            for (int v = 0; v < Tr::nv; ++v) dst[v] = reinterpret_cast<const typename Tr::V *>(P)[v];
         }
-        // bilinear nodes N(k,l) = map(s*k - 1, s*l - 1)
-        for (int k = tid; k < QPB * NP1 * NP1; k += T) {
-            int ql = k / (NP1 * NP1);
-            int r = k - ql * NP1 * NP1;
-            int l = r / NP1;
-            int kx = r - l * NP1;
-            if (q0 + ql >= a.nquad) continue;
-            double x, y;
-            bilinear_node(sq[ql].corner, scale_factor * (double)kx - 1.0,
-                          scale_factor * (double)l - 1.0, x, y);
-            nodes[2 * k] = x;
-            nodes[2 * k + 1] = y;
+        if (F32) {
+            // rectangle spacing: x-face normal (hy,0), y-face normal (0,hx), volume hx*hy
+            if (tid < QPB && q0 + tid < a.nquad) {
+                const double *g = sq[tid].corner;
+                double hx = (g[2] - g[0]) / (double)N, hy = (g[5] - g[1]) / (double)N;
+                geo[4 * tid + 0] = hx;
+                geo[4 * tid + 1] = hy;
+                geo[4 * tid + 2] = 1.0 / (hx * hy);
+                geo[4 * tid + 3] = hx * hy;
+            }
+        } else {
+            // The FP64 form takes normals and volumes from the (n+1)^2
+            // bilinear nodes, exactly as the reference.
+            for (int k = tid; k < QPB * NP1 * NP1; k += T) {
+                int ql = k / (NP1 * NP1);
+                int r = k - ql * NP1 * NP1;
+                int l = r / NP1;
+                int kx = r - l * NP1;
+                if (q0 + ql >= a.nquad) continue;
+                double x, y;
+                bilinear_node(sq[ql].corner, scale_factor * (double)kx - 1.0,
+                              scale_factor * (double)l - 1.0, x, y);
+                nodes[2 * k] = x;
+                nodes[2 * k + 1] = y;
+            }
         }
         __syncthreads();
 
         // ---------------- phase B: face fluxes
-        for (int k = tid; k < QPB * NWORK; k += T) {
-            int ql, r;
-            if (k < QPB * NINT) { ql = k / NINT; r = k - ql * NINT; }
-            else { int e = k - QPB * NINT; ql = e / NEDGE; r = NINT + (e - ql * NEDGE); }
+        // Faces of a quad: x-faces (row fb, position fa = 0..N) then y-faces
+        // (position fa = 0..N, column fb); fa = 0 / N are the edge faces.
+        // Edge and interior faces only differ in where the two states and
+        // the normal come from, so a warp mixing them runs one flux code
+        // path (only physical-boundary faces take the bc branch).
+#pragma unroll
+        for (int rb = 0; rb < RB; ++rb) {
+            const int code = fcode[rb];
+            if (!(code >> 19)) continue;
+            const int ql = code & 63;
             if (q0 + ql >= a.nquad) continue;
-            const R *qp = qf + ql * 4 * NN;
-            const double *nd = nodes + ql * NP1 * NP1 * 2;
-            R q_l[4], q_r[4], fl[4];
-            if (r < N * (N - 1)) {
-                // interior x-face between cells (ax-1, j) and (ax, j)
-                int j = r / (N - 1);
-                int ax = 1 + (r - j * (N - 1));
-                const double *p1 = nd + 2 * (j * NP1 + ax);
-                const double *p2 = nd + 2 * ((j + 1) * NP1 + ax);
-                R n0 = (R)(p2[1] - p1[1]);
-                R n1 = (R)(p1[0] - p2[0]);
-#pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    q_l[f] = qp[f * NN + j * N + ax - 1];
-                    q_r[f] = qp[f * NN + j * N + ax];
-                }
-                FluxOps::roe(q_l, q_r, n0, n1, fl);
-#pragma unroll
-                for (int f = 0; f < 4; ++f) fx[((ql * 4 + f) * N + j) * NP1 + ax] = fl[f];
-            } else if (r < NINT) {
-                // interior y-face between cells (i, ay-1) and (i, ay)
-                int r2 = r - N * (N - 1);
-                int ay = 1 + r2 / N;
-                int i = r2 - (ay - 1) * N;
-                const double *p1 = nd + 2 * (ay * NP1 + i + 1);
-                const double *p2 = nd + 2 * (ay * NP1 + i);
-                R n0 = (R)(p2[1] - p1[1]);
-                R n1 = (R)(p1[0] - p2[0]);
-#pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    q_l[f] = qp[f * NN + (ay - 1) * N + i];
-                    q_r[f] = qp[f * NN + ay * N + i];
-                }
-                FluxOps::roe(q_l, q_r, n0, n1, fl);
-#pragma unroll
-                for (int f = 0; f < 4; ++f) fy[((ql * 4 + f) * NP1 + ay) * N + i] = fl[f];
-            } else {
-                // edge face of side s at position m
-                int e = r - NINT;
-                int s = e / N;
-                int m = e - s * N;
+            const bool xd = (code >> 6) & 1;
+            const int fa = (code >> 7) & 63;
+            const int fb = (code >> 13) & 63;
+            const R *pq = prim + (size_t)ql * NPC * RS;
+            int li, ri, bcv = -1;
+            R n0, n1;
+            if (fa == 0 || fa == N) {
+                const int s = (xd ? 0 : 2) + (fa == N ? 1 : 0);
                 const SideDesc &d = sq[ql].side[s];
-                int ci = (s == 0) ? 0 : (s == 1) ? N - 1 : m;
-                int cj = (s == 2) ? 0 : (s == 3) ? N - 1 : m;
-                R own[4];
-#pragma unroll
-                for (int f = 0; f < 4; ++f) own[f] = qp[f * NN + cj * N + ci];
-                double ch = cell_h_of(a.h_base, d.level, N);
-                R h = (R)ch;
-                R n0 = (s < 2) ? h : (R)0;
-                R n1 = (s < 2) ? (R)0 : h;
+                const int own = xd ? (fb * N + (fa == 0 ? 0 : N - 1)) : ((fa == 0 ? 0 : N - 1) * N + fb);
+                const int nb = NN + (s * 2) * N + fb;
+                const R h = (R)cell_h_of(a.h_base, d.level, N);
                 if (d.kind == kSideBoundary) {
-                    if (s == 0) n0 = -h;
-                    if (s == 2) n1 = -h;
-                    R qin[4] = {(R)a.qinflow[0], (R)a.qinflow[1], (R)a.qinflow[2], (R)a.qinflow[3]};
-                    FluxOps::bc(d.bc, own, n0, n1, qin, fl);
+                    bcv = d.bc;
+                    li = own;
+                    ri = own;
+                    n0 = xd ? (fa == 0 ? -h : h) : (R)0;
+                    n1 = xd ? (R)0 : (fa == 0 ? -h : h);
                 } else {
-                    const R *sp = strip + ((ql * 4 + s) * 2) * 4 * N;
-                    R nb[4];
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) nb[f] = sp[f * N + m];
-                    if (s & 1) FluxOps::roe(own, nb, n0, n1, fl);
-                    else FluxOps::roe(nb, own, n0, n1, fl);
-                    if (d.kind == kSideCoarseHang) {
-                        R fl2[4];
-#pragma unroll
-                        for (int f = 0; f < 4; ++f) nb[f] = sp[4 * N + f * N + m];
-                        if (s & 1) FluxOps::roe(own, nb, n0, n1, fl2);
-                        else FluxOps::roe(nb, own, n0, n1, fl2);
-#pragma unroll
-                        for (int f = 0; f < 4; ++f) fh[((ql * 4 + s) * 4 + f) * N + m] = fl2[f];
-                    }
+                    li = (s & 1) ? own : nb;
+                    ri = (s & 1) ? nb : own;
+                    n0 = xd ? h : (R)0;
+                    n1 = xd ? (R)0 : h;
                 }
-#pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    if (s < 2) fx[((ql * 4 + f) * N + m) * NP1 + (s == 0 ? 0 : N)] = fl[f];
-                    else fy[((ql * 4 + f) * NP1 + (s == 2 ? 0 : N)) * N + m] = fl[f];
+            } else {
+                li = xd ? (fb * N + fa - 1) : ((fa - 1) * N + fb);
+                ri = xd ? (fb * N + fa) : (fa * N + fb);
+                if (F32) {
+                    n0 = xd ? (R)geo[4 * ql + 1] : (R)0;
+                    n1 = xd ? (R)0 : (R)geo[4 * ql + 0];
+                } else {
+                    const double *nd = nodes + ql * NP1 * NP1 * 2;
+                    const double *p1 = xd ? nd + 2 * (fb * NP1 + fa) : nd + 2 * (fa * NP1 + fb + 1);
+                    const double *p2 = xd ? nd + 2 * ((fb + 1) * NP1 + fa) : nd + 2 * (fa * NP1 + fb);
+                    n0 = (R)(p2[1] - p1[1]);
+                    n1 = (R)(p1[0] - p2[0]);
                 }
+            }
+            alignas(16) R Lp[RS];
+            alignas(16) R Rp[RS];
+            alignas(16) R fl[4];
+            load_rec<F32>(pq, li, Lp);
+            load_rec<F32>(pq, ri, Rp);
+            if (bcv < 0) {
+                FluxOps::roe(Lp, Rp, n0, n1, fl);
+            } else {
+                R qin[4] = {(R)a.qinflow[0], (R)a.qinflow[1], (R)a.qinflow[2], (R)a.qinflow[3]};
+                FluxOps::bc(bcv, Lp, n0, n1, qin, fl);
+            }
+            if (xd) store_flux<F32>(fx, (ql * N + fb) * NP1 + fa, fl);
+            else store_flux<F32>(fy, (ql * NP1 + fa) * N + fb, fl);
+        }
+        // second flux of each coarse hanging edge cell (only at level jumps)
+        bool any_hang = false;
+#pragma unroll
+        for (int ql = 0; ql < QPB; ++ql)
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                any_hang |= (q0 + ql < a.nquad) && sq[ql].side[s].kind == kSideCoarseHang;
+        if (any_hang) {
+            for (int k = tid; k < QPB * 4 * N; k += T) {
+                const int ql = k / (4 * N);
+                const int s = (k / N) % 4;
+                const int m = k % N;
+                if (q0 + ql >= a.nquad) continue;
+                const SideDesc &d = sq[ql].side[s];
+                if (d.kind != kSideCoarseHang) continue;
+                const R *pq = prim + (size_t)ql * NPC * RS;
+                const bool xd = s < 2;
+                const int own = xd ? (m * N + (s == 0 ? 0 : N - 1)) : ((s == 2 ? 0 : N - 1) * N + m);
+                const int nb = NN + (s * 2 + 1) * N + m;
+                const R h = (R)cell_h_of(a.h_base, d.level, N);
+                alignas(16) R Lp[RS];
+                alignas(16) R Rp[RS];
+                alignas(16) R fl[4];
+                load_rec<F32>(pq, (s & 1) ? own : nb, Lp);
+                load_rec<F32>(pq, (s & 1) ? nb : own, Rp);
+                FluxOps::roe(Lp, Rp, xd ? h : (R)0, xd ? (R)0 : h, fl);
+                store_flux<F32>(fh, (ql * 4 + s) * N + m, fl);
             }
         }
         __syncthreads();
@@ -367,6 +576,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             int i = c % N, j = c / N;
             const QuadDesc &qd = sq[ql];
             double r[4] = {0.0, 0.0, 0.0, 0.0};
+            double F[4];
             int sx = (i == 0) ? 0 : (i == N - 1) ? 1 : -1;
             int sy = (j == 0) ? 2 : (j == N - 1) ? 3 : -1;
             int first = sx, second = sy;
@@ -376,40 +586,57 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 int s = pass == 0 ? first : second;
                 if (s < 0) continue;
                 int kind = qd.side[s].kind;
+                int m = (s < 2) ? j : i;
+                if (s < 2) load_flux<F32>(fx, (ql * N + j) * NP1 + (s == 0 ? 0 : N), F);
+                else load_flux<F32>(fy, (ql * NP1 + (s == 2 ? 0 : N)) * N + i, F);
+                double F2[4] = {0.0, 0.0, 0.0, 0.0};
+                if (kind == kSideCoarseHang) load_flux<F32>(fh, (ql * 4 + s) * N + m, F2);
+                if (kind == kSideBoundary || (s & 1)) {
 #pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    double F = (s < 2) ? (double)fx[((ql * 4 + f) * N + j) * NP1 + (s == 0 ? 0 : N)]
-                                       : (double)fy[((ql * 4 + f) * NP1 + (s == 2 ? 0 : N)) * N + i];
-                    int m = (s < 2) ? j : i;
-                    if (kind == kSideBoundary || (s & 1)) {
-                        r[f] = r[f] + F;
-                        if (kind == kSideCoarseHang) r[f] = r[f] + (double)fh[((ql * 4 + s) * 4 + f) * N + m];
-                    } else {
-                        r[f] = r[f] - F;
-                        if (kind == kSideCoarseHang) r[f] = r[f] - (double)fh[((ql * 4 + s) * 4 + f) * N + m];
+                    for (int f = 0; f < 4; ++f) {
+                        r[f] = r[f] + F[f];
+                        if (kind == kSideCoarseHang) r[f] = r[f] + F2[f];
+                    }
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) {
+                        r[f] = r[f] - F[f];
+                        if (kind == kSideCoarseHang) r[f] = r[f] - F2[f];
                     }
                 }
             }
+            if (i > 0) {
+                load_flux<F32>(fx, (ql * N + j) * NP1 + i, F);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                if (i > 0) r[f] = r[f] - (double)fx[((ql * 4 + f) * N + j) * NP1 + i];
-                if (i < N - 1) r[f] = r[f] + (double)fx[((ql * 4 + f) * N + j) * NP1 + i + 1];
+                for (int f = 0; f < 4; ++f) r[f] = r[f] - F[f];
             }
+            if (i < N - 1) {
+                load_flux<F32>(fx, (ql * N + j) * NP1 + i + 1, F);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                if (j > 0) r[f] = r[f] - (double)fy[((ql * 4 + f) * NP1 + j) * N + i];
-                if (j < N - 1) r[f] = r[f] + (double)fy[((ql * 4 + f) * NP1 + j + 1) * N + i];
+                for (int f = 0; f < 4; ++f) r[f] = r[f] + F[f];
             }
-            const double *nd = nodes + ql * NP1 * NP1 * 2;
-            const double *n1p = nd + 2 * (j * NP1 + i);
-            const double *n3p = nd + 2 * ((j + 1) * NP1 + i);
-            double vol = subcell_volume(n1p[0], n1p[1], n1p[2], n1p[3], n3p[0], n3p[1], n3p[2], n3p[3]);
+            if (j > 0) {
+                load_flux<F32>(fy, (ql * NP1 + j) * N + i, F);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) r[f] = r[f] - F[f];
+            }
+            if (j < N - 1) {
+                load_flux<F32>(fy, (ql * NP1 + j + 1) * N + i, F);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) r[f] = r[f] + F[f];
+            }
+            double vol;
             double kv[4];
             if (F32) {
-                double inv = 1.0 / vol;
+                vol = geo[4 * ql + 3];
+                const double inv = geo[4 * ql + 2];
 #pragma unroll
                 for (int f = 0; f < 4; ++f) kv[f] = -(r[f] * inv);
             } else {
+                const double *nd = nodes + ql * NP1 * NP1 * 2;
+                const double *n1p = nd + 2 * (j * NP1 + i);
+                const double *n3p = nd + 2 * ((j + 1) * NP1 + i);
+                vol = subcell_volume(n1p[0], n1p[1], n1p[2], n1p[3], n3p[0], n3p[1], n3p[2], n3p[3]);
 #pragma unroll
                 for (int f = 0; f < 4; ++f) kv[f] = (r[f] / vol) * -1.0;
             }
@@ -417,7 +644,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             const long long gi = (long long)(q0 + ql) * NN + c;
             double q0v[4], qn[4];
 #pragma unroll
-            for (int f = 0; f < 4; ++f) q0v[f] = qs[(ql * 4 + f) * NN + c];
+            for (int f = 0; f < 4; ++f) q0v[f] = raw[(ql * 4 + f) * NN + c];
 
             switch (a.scheme) {
             case kSchemeRhsOnly:
@@ -548,24 +775,23 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                     if (cand < my_dt_min) my_dt_min = cand;
                 }
                 double rho = qn[0];
-                double pe = qn[3] - 0.5 * (qn[1] * qn[1] + qn[2] * qn[2]) / rho;
+                double pe = qn[3] * rho - 0.5 * (qn[1] * qn[1] + qn[2] * qn[2]);
                 if (!(rho > 0.0) || !(pe > 0.0)) my_flags |= kFlagNegative;
             }
         }
         __syncthreads();
     }
 
-    if (!a.last_stage) return;
-
-    // ---------------- block reductions: CFL min (one atomic per block) and
-    // the residual norm (per-block partials, summed in block order by the
-    // last block to finish, so the result does not depend on scheduling).
+    // ---------------- block reductions: CFL min (one atomic per block), the
+    // residual norm (per-block partials summed in block order by the last
+    // block to finish, so the result does not depend on scheduling), flags.
     const int lane = tid & 31, warp = tid >> 5;
+    int wflags = __reduce_or_sync(0xffffffffu, my_flags);
+    if (wflags && lane == 0) atomicOr(&a.scal->flags, wflags);
+    if (!a.last_stage) return;
     double wmin = warp_min(my_dt_min);
     double wsum = warp_sum(my_norm);
-    int wflags = __reduce_or_sync(0xffffffffu, my_flags);
     if (lane == 0) { red[warp] = wmin; red[32 + warp] = wsum; }
-    if (wflags && lane == 0) atomicOr(&a.scal->flags, wflags);
     __syncthreads();
     if (tid == 0) {
         double bmin = red[0], bsum = red[32];
