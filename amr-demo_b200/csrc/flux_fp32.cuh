@@ -103,6 +103,45 @@ __device__ __forceinline__ void cell_prims_fp32(const double q[4], float P[8])
 // the tangential-correction terms of rows 2/3 reduce to 0 and
 // rhobar*(v_R - v_L); Mcoeff = 1/(1+|un/a|) = a/(a+|un|). Five MUFU
 // operations per face. Other normals use roe_flux_fp32 on conserved states.
+// Axis-aligned face with a positive normal of length h, direction known at
+// compile time (DIR 0: n = (h,0), DIR 1: n = (0,h)): the same algebra as
+// roe_flux_prim_fp32 without any run-time selects.
+template <int DIR>
+__device__ __forceinline__ void roe_flux_axis_fp32(const float *L, const float *R, float h, float flux[4])
+{
+    const float rhol = L[0], ul = L[1], vl = L[2], pl = L[3], Hl = L[4], srl = L[5];
+    const float rhor = R[0], ur = R[1], vr = R[2], pr = R[3], Hr = R[4], srr = R[5];
+    const float unl = DIR == 0 ? ul : vl;
+    const float unr = DIR == 0 ? ur : vr;
+    const float inv = __frcp_rn(srl + srr);
+    const float rhobar = srl * srr;
+    const float ubar = (ul * srl + ur * srr) * inv;
+    const float vbar = (vl * srl + vr * srr) * inv;
+    const float Hbar = (Hl * srl + Hr * srr) * inv;
+    const float a2 = 0.4f * (Hbar - 0.5f * (ubar * ubar + vbar * vbar));
+    const float abar = sqrtf(a2);
+    const float unbar = DIR == 0 ? ubar : vbar;
+    const float b1 = fmaxf(fmaxf(unbar + abar, unr + abar), 0.0f);
+    const float b2 = fminf(fminf(unbar - abar, unl - abar), 0.0f);
+    const float inv_db = __frcp_rn(b1 - b2);
+    const float bcoeff = b1 * b2 * inv_db;
+    const float delta1 = (rhor - rhol) - (pr - pl) * __frcp_rn(a2);
+    const float bM = bcoeff * abar * __frcp_rn(abar + fabsf(unbar));
+    const float ml = DIR == 0 ? L[6] : L[7];
+    const float mr = DIR == 0 ? R[6] : R[7];
+    const float rHl = rhol * Hl, rHr = rhor * Hr;
+    const float hb1 = h * b1 * inv_db, hb2 = h * b2 * inv_db;
+    float d;
+    d = bcoeff * (rhor - rhol) - bM * delta1;
+    flux[0] = hb1 * ml - hb2 * mr + h * d;
+    d = bcoeff * (R[6] - L[6]) - bM * (delta1 * ubar + (DIR == 0 ? 0.0f : rhobar * (ur - ul)));
+    flux[1] = hb1 * (ml * ul + (DIR == 0 ? pl : 0.0f)) - hb2 * (mr * ur + (DIR == 0 ? pr : 0.0f)) + h * d;
+    d = bcoeff * (R[7] - L[7]) - bM * (delta1 * vbar + (DIR == 0 ? rhobar * (vr - vl) : 0.0f));
+    flux[2] = hb1 * (ml * vl + (DIR == 0 ? 0.0f : pl)) - hb2 * (mr * vr + (DIR == 0 ? 0.0f : pr)) + h * d;
+    d = bcoeff * (rHr - rHl) - bM * (delta1 * Hbar + rhobar * (Hr - Hl));
+    flux[3] = hb1 * (rHl * unl) - hb2 * (rHr * unr) + h * d;
+}
+
 __device__ __forceinline__ void roe_flux_prim_fp32(const float *L, const float *R, float n0, float n1,
                                                    float flux[4])
 {

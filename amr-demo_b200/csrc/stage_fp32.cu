@@ -18,6 +18,13 @@ struct FluxOpsFP32 {
     {
         roe_flux_prim_fp32(l, r, n0, n1, f);
     }
+    // axis-aligned face with positive normal: n0 = h (DIR 0) or n1 = h (DIR 1)
+    template <int DIR>
+    __device__ static __forceinline__ void roe_axis(const float *l, const float *r, float n0, float n1,
+                                                    float *f)
+    {
+        roe_flux_axis_fp32<DIR>(l, r, DIR == 0 ? n0 : n1, f);
+    }
     __device__ static __forceinline__ void bc(int bc, const float *q, float n0, float n1,
                                               const float *qin, float *f)
     {

@@ -18,6 +18,13 @@ struct FluxOpsFP64 {
     {
         roe_flux_prim_fp64(l, r, n0, n1, f);
     }
+    // the exact form evaluates every face through the general expression
+    template <int DIR>
+    __device__ static __forceinline__ void roe_axis(const double *l, const double *r, double n0, double n1,
+                                                    double *f)
+    {
+        roe_flux_prim_fp64(l, r, n0, n1, f);
+    }
     __device__ static __forceinline__ void bc(int bc, const double *q, double n0, double n1,
                                               const double *qin, double *f)
     {

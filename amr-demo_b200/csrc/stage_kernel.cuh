@@ -221,7 +221,8 @@ struct StageSmem {
     static constexpr size_t rstrip = al(sizeof(double) * QPB * 4 * NSTRIP) * 2;
     static constexpr size_t prim = al(sizeof(R) * QPB * RecTraits<F32>::n * NPC);
     static constexpr size_t nodes = F32 ? 0 : al(sizeof(double) * QPB * NP1 * NP1 * 2);
-    static constexpr size_t geo = al(sizeof(double) * QPB * 4);
+    // per quad: hx, hy, 1/vol, vol (FP32 form), cell_h of sides 0..3
+    static constexpr size_t geo = al(sizeof(double) * QPB * 8);
     static constexpr size_t fx = al(sizeof(R) * QPB * 4 * N * NP1);
     static constexpr size_t fy = al(sizeof(R) * QPB * 4 * NP1 * N);
     static constexpr size_t fh = al(sizeof(R) * QPB * 4 * 4 * N);
@@ -373,19 +374,35 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
         if (it < niter) {
             const QuadDesc *dg = sdesc + (size_t)(it % 3) * desc_slot;
             double *dst = srstrip + (size_t)(it & 1) * rstrip_slot;
-            for (int k = tid; k < QPB * 4 * S::NSTRIP; k += T) {
-                int m = k % N;
-                int kk = (k / N) % 2;
-                int s = (k / (2 * N)) % 4;
-                int f = (k / (8 * N)) % 4;
-                int ql = k / (32 * N);
+            // one strip row (quad, field, side, neighbour) per SCH threads;
+            // rows facing y-sides are contiguous in the neighbour's slab and
+            // move as 16-byte copies, x-side rows are columns (8-byte copies)
+            constexpr int SCH = (N >= 4) ? 4 : 1;     // threads per strip row
+            constexpr int SPT = N / SCH;              // elements per thread
+            for (int k = tid; k < QPB * 32 * SCH; k += T) {
+                const int row = k / SCH;              // ((ql*4 + f)*4 + s)*2 + kk
+                const int part = k - row * SCH;
+                const int kk = row & 1;
+                const int s = (row >> 1) & 3;
+                const int f = (row >> 3) & 3;
+                const int ql = row >> 5;
                 if (gg * QPB + ql >= a.nquad) continue;
                 const SideDesc &d = dg[ql].side[s];
                 int nbr = -1;
                 if (d.kind == kSideFull || d.kind == kSideFineHang) nbr = (kk == 0) ? d.nbr0 : -1;
                 else if (d.kind == kSideCoarseHang) nbr = (kk == 0) ? d.nbr0 : d.nbr1;
                 if (nbr < 0) continue;
-                cp_async8(dst + k, a.qin + f * stride + (long long)nbr * NN + facing_cell<N>(s, m));
+                const double *src = a.qin + f * stride + (long long)nbr * NN;
+                double *drow = dst + (size_t)row * N;
+                const int m0 = part * SPT;
+                if (s >= 2 && (SPT % 2) == 0) {
+                    const int base = (s == 2) ? (N - 1) * N : 0;
+#pragma unroll
+                    for (int m = m0; m < m0 + SPT; m += 2) cp_async16(drow + m, src + base + m);
+                } else {
+#pragma unroll
+                    for (int m = m0; m < m0 + SPT; ++m) cp_async8(drow + m, src + facing_cell<N>(s, m));
+                }
             }
             cp_async_commit();
             if (a.a0 || a.a1) {
@@ -445,17 +462,23 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
 #pragma unroll
             for (int v = 0; v < Tr::nv; ++v) dst[v] = reinterpret_cast<const typename Tr::V *>(P)[v];
         }
-        if (F32) {
-            // rectangle spacing: x-face normal (hy,0), y-face normal (0,hx), volume hx*hy
-            if (tid < QPB && q0 + tid < a.nquad) {
-                const double *g = sq[tid].corner;
-                double hx = (g[2] - g[0]) / (double)N, hy = (g[5] - g[1]) / (double)N;
-                geo[4 * tid + 0] = hx;
-                geo[4 * tid + 1] = hy;
-                geo[4 * tid + 2] = 1.0 / (hx * hy);
-                geo[4 * tid + 3] = hx * hy;
+        // per quad: rectangle spacing (FP32 form: x-face normal (hy,0),
+        // y-face normal (0,hx), volume hx*hy) and each side's cell_h
+        if (tid < 4 * QPB) {
+            const int ql = tid >> 2, s = tid & 3;
+            if (q0 + ql < a.nquad) {
+                geo[8 * ql + 4 + s] = cell_h_of(a.h_base, sq[ql].side[s].level, N);
+                if (F32 && s == 0) {
+                    const double *g = sq[ql].corner;
+                    double hx = (g[2] - g[0]) / (double)N, hy = (g[5] - g[1]) / (double)N;
+                    geo[8 * ql + 0] = hx;
+                    geo[8 * ql + 1] = hy;
+                    geo[8 * ql + 2] = 1.0 / (hx * hy);
+                    geo[8 * ql + 3] = hx * hy;
+                }
             }
-        } else {
+        }
+        if (!F32) {
             // The FP64 form takes normals and volumes from the (n+1)^2
             // bilinear nodes, exactly as the reference.
             for (int k = tid; k < QPB * NP1 * NP1; k += T) {
@@ -496,7 +519,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 const SideDesc &d = sq[ql].side[s];
                 const int own = xd ? (fb * N + (fa == 0 ? 0 : N - 1)) : ((fa == 0 ? 0 : N - 1) * N + fb);
                 const int nb = NN + (s * 2) * N + fb;
-                const R h = (R)cell_h_of(a.h_base, d.level, N);
+                const R h = (R)geo[8 * ql + 4 + s];
                 if (d.kind == kSideBoundary) {
                     bcv = d.bc;
                     li = own;
@@ -513,8 +536,8 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 li = xd ? (fb * N + fa - 1) : ((fa - 1) * N + fb);
                 ri = xd ? (fb * N + fa) : (fa * N + fb);
                 if (F32) {
-                    n0 = xd ? (R)geo[4 * ql + 1] : (R)0;
-                    n1 = xd ? (R)0 : (R)geo[4 * ql + 0];
+                    n0 = xd ? (R)geo[8 * ql + 1] : (R)0;
+                    n1 = xd ? (R)0 : (R)geo[8 * ql + 0];
                 } else {
                     const double *nd = nodes + ql * NP1 * NP1 * 2;
                     const double *p1 = xd ? nd + 2 * (fb * NP1 + fa) : nd + 2 * (fa * NP1 + fb + 1);
@@ -529,7 +552,8 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             load_rec<F32>(pq, li, Lp);
             load_rec<F32>(pq, ri, Rp);
             if (bcv < 0) {
-                FluxOps::roe(Lp, Rp, n0, n1, fl);
+                if (xd) FluxOps::template roe_axis<0>(Lp, Rp, n0, n1, fl);
+                else FluxOps::template roe_axis<1>(Lp, Rp, n0, n1, fl);
             } else {
                 R qin[4] = {(R)a.qinflow[0], (R)a.qinflow[1], (R)a.qinflow[2], (R)a.qinflow[3]};
                 FluxOps::bc(bcv, Lp, n0, n1, qin, fl);
@@ -556,13 +580,14 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 const bool xd = s < 2;
                 const int own = xd ? (m * N + (s == 0 ? 0 : N - 1)) : ((s == 2 ? 0 : N - 1) * N + m);
                 const int nb = NN + (s * 2 + 1) * N + m;
-                const R h = (R)cell_h_of(a.h_base, d.level, N);
+                const R h = (R)geo[8 * ql + 4 + s];
                 alignas(16) R Lp[RS];
                 alignas(16) R Rp[RS];
                 alignas(16) R fl[4];
                 load_rec<F32>(pq, (s & 1) ? own : nb, Lp);
                 load_rec<F32>(pq, (s & 1) ? nb : own, Rp);
-                FluxOps::roe(Lp, Rp, xd ? h : (R)0, xd ? (R)0 : h, fl);
+                if (xd) FluxOps::template roe_axis<0>(Lp, Rp, h, (R)0, fl);
+                else FluxOps::template roe_axis<1>(Lp, Rp, (R)0, h, fl);
                 store_flux<F32>(fh, (ql * 4 + s) * N + m, fl);
             }
         }
@@ -628,8 +653,8 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             double vol;
             double kv[4];
             if (F32) {
-                vol = geo[4 * ql + 3];
-                const double inv = geo[4 * ql + 2];
+                vol = geo[8 * ql + 3];
+                const double inv = geo[8 * ql + 2];
 #pragma unroll
                 for (int f = 0; f < 4; ++f) kv[f] = -(r[f] * inv);
             } else {

@@ -149,8 +149,8 @@ def autotune(ag, s, steps=6):
     from amrgpu._lib import lib
     st = torch.cuda.ExternalStream(s.stream())
     best = None
-    for qpb in (1, 2, 4, 8):
-        for thr in (160, 256, 288, 544, 576):
+    for qpb in (1, 2, 4, 8, 16):
+        for thr in (64, 128, 160, 192, 256, 288, 320, 384, 544, 576):
             if lib().amrgpu_session_set_launch(s._s, qpb, thr) != 0:
                 ag.clear_error()
                 continue
