@@ -112,6 +112,9 @@ PROTOTYPES = {
     "amrgpu_forest_external": (C.c_int, [C.c_void_p, C.c_int, C.c_int, i32p, i32p, f64p, i32p, i32p]),
     "amrgpu_forest_quad_h": (C.c_double, [C.c_void_p, C.c_int]),
     "amrgpu_forest_initialize": (C.c_int, [C.c_void_p, C.c_int, f64p]),
+    # allocation-free entry point
+    "amrgpu_totals_noalloc": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p, C.c_int, C.c_int, f64p,
+                                        C.c_void_p]),
 }
 
 

@@ -253,6 +253,32 @@ int amrgpu_session_tag(amrgpu_session_t *s, int *tags);
 int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int *kind,
                          const int *src_index);
 
+/* ---------------- allocation-free entry point ---------------- */
+/* No counterpart in the reference. Conservation totals sum(vol*Q_f), f =
+ * 0..3, of a device-resident SoA state, like amrgpu_session_totals, for
+ * callers that cannot let a library allocate: a driver that gives all
+ * device memory to its own pool at start-up, or one that checks
+ * conservation inside its time-step loop on a busy device, where the
+ * device-wide synchronisation of cudaMalloc/cudaFree would stall other
+ * streams. The function calls no cudaMalloc, cudaFree or other allocating
+ * routine: its scratch is a fixed array in the library's device image (one
+ * partial sum per quad, so at most AMRGPU_NOALLOC_MAX_QUADS quads; larger
+ * requests return AMRGPU_ERR_TOO_LARGE), held by every GPU that loads the
+ * library until the process exits.
+ *   q_device        field f of cell c at q_device[f*field_stride + c],
+ *                   cells of quad q at [q*n*n, (q+1)*n*n), row-major
+ *   corners_device  8 doubles per quad: x,y of n1(-,-) n2(+,-) n3(-,+) n4(+,+)
+ *   totals          host array of 4 doubles (written before return)
+ *   stream          cudaStream_t to run on (NULL: the legacy default stream)
+ * The first call on each device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) and must not be made during stream capture. All
+ * calls share the scratch array; calls that overlap on the GPU race. The
+ * call synchronises `stream` before returning. */
+#define AMRGPU_NOALLOC_MAX_QUADS 65536
+int amrgpu_totals_noalloc(const double *q_device, long long field_stride,
+                          const double *corners_device, int nquad, int n,
+                          double totals[4], void *stream);
+
 #ifdef __cplusplus
 }
 #endif
