@@ -1,0 +1,208 @@
+"""Host-side logic on CPU: the host forest (p4est stand-in), the reference
+ABI's configuration parsing and per-quad callbacks, and the library's
+exported symbols. No GPU needed."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import meshes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions(header):
+    txt = open(os.path.join(ROOT, "include", header)).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b([a-z_][a-z0-9_]*)\s*\(", txt)) - {"defined"})
+
+
+def test_library_exports_every_declared_symbol(ag):
+    L = ag.lib()
+    names = declared_functions("amrgpu.h")
+    assert "hpc_amr_evolve_solver" in names and "physics_go_gpu" in names
+    for name in names:
+        assert hasattr(L, name), name
+    for name in declared_functions("physics_go_gpu.h"):
+        assert hasattr(L, name), name
+    # the Python mirror binds every exported entry point with a prototype
+    assert set(names) <= set(ag.PROTOTYPES)
+
+
+def test_session_without_gpu_reports_no_device(ag):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    f = meshes.uniform(4, 1)
+    meshes.make_config(4).apply()
+    m = f.mesh(4)
+    with pytest.raises(ag.AmrGpuError) as e:
+        ag.Session(m)
+    assert e.value.code == 6
+
+
+def test_uniform_brick_counts():
+    import amrgpu as ag
+    for per in ((0, 0), (1, 0), (1, 1)):
+        f = ag.Forest(2, 1, periodic=per, lo=(0, 0, 0), scale=1.0, level=2)
+        assert f.num_quads == 2 * 16
+        m = f.mesh(4)
+        types = np.bincount(m.face_info[0::11], minlength=4)
+        nx, ny = 8, 4
+        full = (nx - (0 if per[0] else 1)) * ny + nx * (ny - (0 if per[1] else 1))
+        bnd = (0 if per[0] else 2 * ny) + (0 if per[1] else 2 * nx)
+        assert types[2] == full and types[1] == bnd and types[3] == 0
+
+
+def side_coverage(m):
+    cover = np.zeros((m.ncell, 4), int)
+    for row in m.face_info.reshape(-1, 11):
+        t, s, c = row[:3]
+        cover[c, s] += 1
+        if t == 2:
+            cover[row[3], row[7]] += 1
+        elif t == 3:
+            cover[row[3], row[7]] += 1
+            cover[row[4], row[8]] += 1
+    return cover
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_refinement_is_balanced_and_every_side_has_one_face(seed):
+    import amrgpu as ag
+    rng = np.random.default_rng(seed)
+    f = ag.Forest(int(rng.integers(1, 3)), int(rng.integers(1, 3)), periodic=(int(rng.integers(2)), int(rng.integers(2))),
+                  lo=(0, 0, 0), scale=1.0, level=2)
+    for _ in range(3):
+        fl = (rng.random(f.num_quads) < 0.2).astype(np.int32)
+        f.refine(fl, max_level=7)
+        f.balance()
+        assert f.is_balanced()
+    m = f.mesh(4)
+    assert np.all(side_coverage(m) == 1)
+    # cell_info offsets follow amr_external.c: 4 n^2 * local id
+    assert np.array_equal(m.cell_info[2::3], 64 * np.arange(m.ncell))
+
+
+def test_geometry_matches_quadrant_coordinates():
+    """geom corners (amr_p4est_utilities.c:15-81) against the quad's integer
+    position: x = lo + scale*(tree_x + qx/2^30)."""
+    import amrgpu as ag
+    f = ag.Forest(2, 2, periodic=(0, 0), lo=(-1.0, 2.0, 0.0), scale=0.5, level=3)
+    fl = np.zeros(f.num_quads, np.int32)
+    fl[::7] = 1
+    f.refine(fl)
+    f.balance()
+    m = f.mesh(2)
+    tree, lev, x, y = f.quads()
+    g = m.geom.reshape(-1, 4, 3)
+    L = 2.0 ** 30
+    # trees follow the Morton order of the 2x2 brick
+    tx = np.array([0, 1, 0, 1])[tree]
+    ty = np.array([0, 0, 1, 1])[tree]
+    x0 = -1.0 + 0.5 * (tx + x / L)
+    y0 = 2.0 + 0.5 * (ty + y / L)
+    h = 0.5 / 2.0 ** lev
+    assert np.allclose(g[:, 0, 0], x0) and np.allclose(g[:, 0, 1], y0)
+    assert np.allclose(g[:, 3, 0], x0 + h) and np.allclose(g[:, 3, 1], y0 + h)
+
+
+def test_hanging_faces_pair_the_coarse_quad_with_two_fine_quads():
+    f = meshes.hanging(4)
+    m = f.mesh(4)
+    lev = m.cell_info[1::3]
+    for row in m.face_info.reshape(-1, 11):
+        if row[0] != 3:
+            continue
+        coarse, f0, f1 = row[2], row[3], row[4]
+        assert lev[f0] == lev[f1] == lev[coarse] + 1
+        assert row[7] == row[8] == (row[1] ^ 1)
+
+
+def test_refine_then_coarsen_remap_and_operators(ag):
+    """Remap kinds from the forest and the reference's refine (injection)
+    and coarsen (same-index average) callbacks on host."""
+    f = ag.Forest(1, 1, periodic=(1, 1), lo=(0, 0, 0), scale=1.0, level=2)
+    f.begin_regrid()
+    fl = np.zeros(16, np.int32)
+    fl[5] = 1
+    f.refine(fl)
+    kind, src = f.remap()
+    assert f.num_quads == 19
+    assert list(src[5:9]) == [5] * 4 and np.all(kind == 0)
+    f.begin_regrid()
+    cf = np.zeros(f.num_quads, np.int32)
+    cf[5:9] = 1
+    f.coarsen(cf, min_level=0)
+    kind, src = f.remap()
+    assert f.num_quads == 16 and kind[5] == 1 and src[5] == 5
+    L = ag.lib()
+    n, nf = 2, 4
+    rng = np.random.default_rng(0)
+    parent = rng.random(nf * n * n)
+    kids = [np.zeros(nf * n * n) for _ in range(4)]
+    args = [C.byref(C.c_int(v)) for v in (0, nf, n, 0)] + [C.byref(C.c_double(0.1)), ag.dp(np.zeros(12))]
+    L.hpc_amr_refine_operator_2d(*args, ag.dp(parent), *[ag.dp(k) for k in kids])
+    assert all(np.array_equal(k, parent) for k in kids)
+    out = np.zeros(nf * n * n)
+    L.hpc_amr_coarsen_operator_2d(*args, *[ag.dp(k + i) for i, k in enumerate(kids)], ag.dp(out))
+    assert np.array_equal(out, 0.25 * (parent + (parent + 1) + (parent + 2) + (parent + 3)))
+
+
+def test_input_physics_keyword_rules(ag, tmp_path):
+    """physics_initialize.c:61-197: defaults, cfl <- 0.25*cfl*time_scheme,
+    intervals <= 0 become INT_MAX, extension keywords."""
+    p = tmp_path / "input.physics"
+    p.write_text("<SIMULATION PROPERTIES>\ncheckpoint_interval: 0\nvisualization_interval: 1000\n"
+                 "regrid_interval: 10\namr_ntag_methods: 2\namr_tag_methods: 1 2\n"
+                 "amr_tag_tolerances: 0.996, 1.5\ntime_scheme: 3\ntime_steps: 10000\ndt: 0.01000\n"
+                 "</SIMULATION PROPERTIES>\n<FLUID PROPERTIES>\ninitial_condition: 1\nbc_xlo: 2\ncfl: 0.5\n"
+                 "gamma: 1.4\npressure: 0.714286\nmach: 0.5\ngpu_form: 1\nfinal_time: 2.5\n</FLUID PROPERTIES>\n")
+    c = ag.Config.read(str(p))
+    assert c["time_scheme"] == 3 and c["time_steps"] == 10000 and c["dt"] == 0.01
+    assert c["cfl"] == 0.25 * 0.5 * 3
+    assert c["checkpoint_interval"] == 2147483647 and c["regrid_interval"] == 10
+    assert c["amr_ntag_methods"] == 2 and c["amr_tag_methods"][:2] == [1, 2]
+    assert c["amr_tag_tolerances"][:2] == [0.996, 1.5]
+    assert c["bc"][:4] == [2, 1, 1, 1] and c["mach"] == 0.5 and c["alpha"] == 0.0
+    assert c["form"] == 1 and c["final_time"] == 2.5
+
+
+def test_initialize_solver_reads_input_from_cwd(ag, tmp_path, monkeypatch):
+    (tmp_path / "input.physics").write_text("time_scheme: 2\ntime_steps: 7\ncfl: 1.0\n")
+    monkeypatch.chdir(tmp_path)
+    os.environ["AMRGPU_QUIET"] = "1"
+    ag.clear_error()
+    assert ag.initialize_solver(2.0, 8, nlevels=3) == 0
+    c = ag.Config.current()
+    assert c["time_scheme"] == 2 and c["time_steps"] == 7 and c["cfl"] == 0.5
+    assert c["coarse_grid_h"] == 2.0 and c["nelem_subgrid"] == 8
+    (tmp_path / "input.physics").unlink()
+    assert ag.initialize_solver(2.0, 8) == 7  # missing file: defaults kept, error reported
+    ag.clear_error()
+
+
+def test_host_tag_feature_matches_restated_fortran(ag, oracle):
+    L = ag.lib()
+    n, nf = 4, 4
+    rng = np.random.default_rng(3)
+    for meth, tol in ((1, 0.5), (2, 1.2)):
+        c = ag.Config.current()
+        c["amr_ntag_methods"] = 1
+        c["amr_tag_methods"] = [meth, 0, 0, 0, 0]
+        c["amr_tag_tolerances"] = [tol, 0, 0, 0, 0]
+        c.apply()
+        for _ in range(20):
+            soln = rng.uniform(0.4, 1.3, nf * n * n)
+            tag = C.c_int(-1)
+            L.hpc_amr_tag_feature(C.byref(C.c_int(2)), C.byref(C.c_int(0)), C.byref(C.c_int(nf)), C.byref(C.c_int(n)),
+                                  C.byref(C.c_int(0)), C.byref(C.c_double(0.1)), ag.dp(np.zeros(12)), ag.dp(soln),
+                                  C.byref(tag))
+            rho = soln[0::4]
+            expect = int((rho <= tol).any()) if meth == 1 else int((rho >= tol).any())
+            assert tag.value == expect
