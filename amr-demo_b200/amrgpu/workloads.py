@@ -40,6 +40,23 @@ def vortex_1024(level=6, n=16, time_scheme=3, final_time=10.0, form=0, steps=100
     return f, f.mesh(n), cfg, f.initialize(n)
 
 
+def four_quadrant(seed=0, min_level=4, max_level=9, n=16, form=1, jump_tol=0.05, time_scheme=3):
+    """Four-quadrant Riemann problem on the unit square split at (0.5,0.5),
+    each quadrant's (rho,p) ~ U[0.1,1.5] and (u,v) ~ U[-0.8,0.8] from the
+    seed; slip walls; CFL 0.5; density-jump tagging (method 5, relative jump
+    >= jump_tol) from min_level to max_level. Returns the forest after the
+    start-up refinement, its mesh, the configuration and the state."""
+    from .amr import host_tags, initial_forest
+    cfg = Config.from_input(cfl=0.5, time_scheme=time_scheme, nelem_subgrid=n, coarse_grid_h=1.0,
+                            initial_condition=3, time_steps=10 ** 9, dt=1.0, bc=[1] * 6, gamma=1.4,
+                            ic_seed=seed, form=form, amr_ntag_methods=1, amr_tag_methods=[5, 0, 0, 0, 0],
+                            amr_tag_tolerances=[jump_tol, 0, 0, 0, 0])
+    cfg.apply()
+    f = Forest(1, 1, periodic=(0, 0), lo=(0.0, 0.0, 0.0), scale=1.0, level=min_level)
+    soln = initial_forest(f, n, max_level, host_tags(n, jump_tol, 5), cfg)
+    return f, f.mesh(n), cfg, soln
+
+
 def vortex_exact(mesh, t, n=16, beta=5.0, a=0.5, center=(5.0, 5.0), L=10.0):
     """Exact translated vortex at time t (periodic images summed over the
     nearest copy), AoS like the solver state."""
