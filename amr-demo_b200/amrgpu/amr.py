@@ -26,7 +26,7 @@ def initial_forest(forest, n, max_level, tag_fn, config):
     config.apply()
     for _ in range(64):
         soln = forest.initialize(n)
-        tags = tag_fn(soln)
+        tags = tag_fn(soln, forest.mesh(n))
         _, lev, _, _ = forest.quads()
         flags = ((tags > 0) & (lev < max_level)).astype(np.int32)
         if not flags.any():
@@ -36,9 +36,50 @@ def initial_forest(forest, n, max_level, tag_fn, config):
     return forest.initialize(n)
 
 
+def side_table(mesh):
+    """Per-quad side neighbours decoded from face_info (the same decode as
+    the device quad descriptors): kind 0 none/boundary, 1 full or fine side
+    of a hanging face (one neighbour), 2 coarse side of a hanging face (two
+    fine neighbours)."""
+    nq = mesh.ncell
+    kind = np.zeros((nq, 4), np.int32)
+    nbr = np.zeros((nq, 4, 2), np.int64)
+    fi = mesh.face_info.reshape(-1, 11)[: mesh.nface]
+
+    def put(q, s, k, a, b):
+        if q < nq:
+            kind[q, s] = k
+            nbr[q, s] = (a, b)
+
+    for f in fi:
+        ftype, side, cell = int(f[0]), int(f[1]), int(f[2])
+        if ftype == 2:
+            left, right = (int(f[3]), cell) if side % 2 == 0 else (cell, int(f[3]))
+            hs = side + 1 if side % 2 == 0 else side
+            put(left, hs, 1, right, right)
+            put(right, hs - 1, 1, left, left)
+        elif ftype == 3:
+            fs = side + 1 if side % 2 == 0 else side - 1
+            put(cell, side, 2, int(f[3]), int(f[4]))
+            put(int(f[3]), fs, 1, cell, cell)
+            put(int(f[4]), fs, 1, cell, cell)
+    return kind, nbr
+
+
+def _edge(q, s, own):
+    """Edge cells of side s (own=True) or the opposite edge a neighbour
+    presents to side s (own=False); q is (nq, n_j, n_i)."""
+    if own:
+        return (q[:, :, 0], q[:, :, -1], q[:, 0, :], q[:, -1, :])[s]
+    return (q[:, :, -1], q[:, :, 0], q[:, -1, :], q[:, 0, :])[s]
+
+
 def host_tags(n, rho_tol, method=5):
-    """Host tagger on an AoS state, used only for the start-up build."""
-    def tag(soln):
+    """Host restatement of the library's plain indicator on an AoS state
+    (methods 1 and 2 of solver_tag_feature.F90:9-52; method 5 = relative
+    density jump inside the patch or across its faces, with the flux
+    kernels' cell pairing). Used for the start-up build and as a checker."""
+    def tag(soln, mesh=None):
         q = soln.reshape(-1, n, n, 4)[..., 0]
         if method == 1:
             return (q <= rho_tol).any(axis=(1, 2)).astype(np.int32)
@@ -46,7 +87,20 @@ def host_tags(n, rho_tol, method=5):
             return (q >= rho_tol).any(axis=(1, 2)).astype(np.int32)
         jx = np.abs(np.diff(q, axis=2)) / np.minimum(q[:, :, 1:], q[:, :, :-1])
         jy = np.abs(np.diff(q, axis=1)) / np.minimum(q[:, 1:, :], q[:, :-1, :])
-        return ((jx.max(axis=(1, 2)) >= rho_tol) | (jy.max(axis=(1, 2)) >= rho_tol)).astype(np.int32)
+        hit = (jx.max(axis=(1, 2)) >= rho_tol) | (jy.max(axis=(1, 2)) >= rho_tol)
+        if mesh is not None:
+            kind, nbr = side_table(mesh)
+            for s in range(4):
+                own = _edge(q, s, True)
+                for k in range(2):
+                    sel = kind[:, s] >= k + 1
+                    if not sel.any():
+                        continue
+                    other = _edge(q[nbr[sel, s, k]], s, False)
+                    mine = own[sel]
+                    jump = np.abs(mine - other) / np.minimum(mine, other)
+                    hit[np.nonzero(sel)[0]] |= (jump >= rho_tol).any(axis=1)
+        return hit.astype(np.int32)
     return tag
 
 

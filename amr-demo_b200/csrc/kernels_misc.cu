@@ -78,12 +78,17 @@ __global__ void __launch_bounds__(256) totals_kernel(const QuadDesc *quads, cons
     }
 }
 
+__device__ __forceinline__ double rel_jump(double a, double b) { return fabs(a - b) / fmin(a, b); }
+
 // Plain indicator of solver_tag_feature.F90:9-52 (methods 1: any rho <= tol,
 // 2: any rho >= tol; 3 and 4 are empty in the reference) plus method 5
-// (extension): largest relative density jump between adjacent cells of the
-// patch >= tol. One warp per quad.
+// (extension): largest relative density jump >= tol between adjacent cells
+// of the patch, or between an edge cell and the neighbour cell(s) it
+// exchanges a face flux with (the flux kernels' index pairing, hanging
+// faces included). One warp per quad.
 template <int N>
-__global__ void tag_kernel(const double *rho, int nquad, int nmeth, TagMethods m, int *tags)
+__global__ void tag_kernel(const double *rho, const QuadDesc *quads, int nquad, int nmeth, TagMethods m,
+                           int *tags)
 {
     constexpr int NN = N * N;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -101,9 +106,23 @@ __global__ void tag_kernel(const double *rho, int nquad, int nmeth, TagMethods m
             if (m.method[k] == 5) {
                 int i = c % N, j = c / N;
                 double jump = 0.0;
-                if (i + 1 < N) jump = fmax(jump, fabs(p[c + 1] - r) / fmin(p[c + 1], r));
-                if (j + 1 < N) jump = fmax(jump, fabs(p[c + N] - r) / fmin(p[c + N], r));
+                if (i + 1 < N) jump = fmax(jump, rel_jump(p[c + 1], r));
+                if (j + 1 < N) jump = fmax(jump, rel_jump(p[c + N], r));
                 if (jump >= tol) hit = 1;
+            }
+        }
+        if (m.method[k] == 5) {
+            for (int e = lane; e < 4 * N; e += 32) {
+                const int s = e / N, mm = e % N;
+                const SideDesc &d = quads[warp].side[s];
+                const int own = (s == 0) ? mm * N : (s == 1) ? mm * N + N - 1 : (s == 2) ? mm : (N - 1) * N + mm;
+                const int fc = facing_cell<N>(s, mm);
+                if (d.kind == kSideFull || d.kind == kSideFineHang || d.kind == kSideCoarseHang) {
+                    if (rel_jump(p[own], rho[(long long)d.nbr0 * NN + fc]) >= tol) hit = 1;
+                }
+                if (d.kind == kSideCoarseHang) {
+                    if (rel_jump(p[own], rho[(long long)d.nbr1 * NN + fc]) >= tol) hit = 1;
+                }
             }
         }
         if (__any_sync(0xffffffffu, hit)) tag = 1;
@@ -180,16 +199,16 @@ cudaError_t launch_totals(int n, const QuadDesc *quads, const double *q, long lo
     return cudaGetLastError();
 }
 
-cudaError_t launch_tag(int n, const double *rho, int nquad, int nmeth, const TagMethods &m, int *tags,
-                       cudaStream_t st)
+cudaError_t launch_tag(int n, const double *rho, const QuadDesc *quads, int nquad, int nmeth,
+                       const TagMethods &m, int *tags, cudaStream_t st)
 {
     int blocks = (nquad * 32 + 255) / 256;
     if (blocks < 1) blocks = 1;
     switch (n) {
-    case 2: tag_kernel<2><<<blocks, 256, 0, st>>>(rho, nquad, nmeth, m, tags); break;
-    case 4: tag_kernel<4><<<blocks, 256, 0, st>>>(rho, nquad, nmeth, m, tags); break;
-    case 8: tag_kernel<8><<<blocks, 256, 0, st>>>(rho, nquad, nmeth, m, tags); break;
-    case 16: tag_kernel<16><<<blocks, 256, 0, st>>>(rho, nquad, nmeth, m, tags); break;
+    case 2: tag_kernel<2><<<blocks, 256, 0, st>>>(rho, quads, nquad, nmeth, m, tags); break;
+    case 4: tag_kernel<4><<<blocks, 256, 0, st>>>(rho, quads, nquad, nmeth, m, tags); break;
+    case 8: tag_kernel<8><<<blocks, 256, 0, st>>>(rho, quads, nquad, nmeth, m, tags); break;
+    case 16: tag_kernel<16><<<blocks, 256, 0, st>>>(rho, quads, nquad, nmeth, m, tags); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -19,8 +19,8 @@ cudaError_t launch_soa_to_aos(const double *soa, double *aos, long long ncells, 
 int totals_grid(long long ncells);
 cudaError_t launch_totals(int n, const QuadDesc *quads, const double *q, long long stride, int nquad,
                           double *partials, int grid, cudaStream_t st);
-cudaError_t launch_tag(int n, const double *rho, int nquad, int nmeth, const TagMethods &m, int *tags,
-                       cudaStream_t st);
+cudaError_t launch_tag(int n, const double *rho, const QuadDesc *quads, int nquad, int nmeth,
+                       const TagMethods &m, int *tags, cudaStream_t st);
 cudaError_t launch_remap(int n, const double *qold, long long stride_old, double *qnew,
                          long long stride_new, const int *kind, const int *src, int nquad_new,
                          cudaStream_t st);

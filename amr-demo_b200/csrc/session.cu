@@ -39,8 +39,8 @@ struct StagePlan {
     int in, a0, a1, out0, out1;
 };
 
-// Buffer roles of each stage, per scheme (see DESIGN: state X, Y, Z and
-// one auxiliary K). A stage reads halos only from `in`; a0/a1 are read and
+// Buffer roles of each stage, per scheme, over three state buffers X, Y, Z
+// and one auxiliary K. A stage reads halos only from `in`; a0/a1 are read and
 // out0/out1 written for the thread's own cells only, so in-place roles are
 // race-free.
 const std::vector<StagePlan> &plan_of(int scheme, bool &swap_xy)
@@ -693,7 +693,7 @@ int amrgpu_session_tag(amrgpu_session_t *s, int *tags)
     int *d_tags = nullptr;
     if (!cuda_ok(cudaMallocAsync((void **)&d_tags, sizeof(int) * size_t(s->nquad), s->stream), "cudaMalloc tags"))
         return AMRGPU_ERR_CUDA;
-    bool ok = cuda_ok(launch_tag(s->n, rolebuf(s, RX), s->nquad, nm, m, d_tags, s->stream), "tag kernel");
+    bool ok = cuda_ok(launch_tag(s->n, rolebuf(s, RX), s->d_quads, s->nquad, nm, m, d_tags, s->stream), "tag kernel");
     s->launches++;
     if (ok)
         ok = cuda_ok(cudaMemcpyAsync(tags, d_tags, sizeof(int) * size_t(s->nquad), cudaMemcpyDeviceToHost, s->stream),

@@ -34,7 +34,11 @@ os.environ.setdefault("AMRGPU_QUIET", "1")
 METRIC = "RK cell-updates/s on 1 B200: learned+FP32 form vs plain FP64, at equal L1(rho)"
 UNIT = "cell-updates/s"
 WORKLOAD = "isentropic vortex, periodic [0,10]^2, 4096 quads x 16x16 = 1024^2 cells, SSP-RK3, CFL 0.5"
-B_ALG = {0: 352.0, 1: 256.0}  # algorithmic HBM bytes per cell-update
+# Algorithmic HBM bytes per cell-update (one RK step of one cell, summed over
+# its stages). FP64 exact SSP-RK3: stage 1 reads X, writes Y and K (96 B);
+# stage 2 reads Y, X, K, writes X, K (160 B); stage 3 reads X, K, writes Y
+# (96 B) = 352 B. FP32-flux Shu-Osher RK3 keeps no K: 64 + 96 + 96 = 256 B.
+B_ALG = {0: 352.0, 1: 256.0}
 
 
 def peaks():
