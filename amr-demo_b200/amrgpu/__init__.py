@@ -296,6 +296,14 @@ class Session:
         s = np.ascontiguousarray(src, np.int32)
         check(lib().amrgpu_session_remap(self._s, other._s, ip(k), ip(s)), "remap")
 
+    def regrid(self, mesh, kind, src):
+        """In place: take the new mesh and remap the state by kind/src."""
+        k = np.ascontiguousarray(kind, np.int32)
+        s = np.ascontiguousarray(src, np.int32)
+        ms = mesh.struct()
+        check(lib().amrgpu_session_regrid(self._s, C.byref(ms), ip(k), ip(s)), "regrid")
+        self.mesh = mesh
+
     def state_ptr(self, field):
         return lib().amrgpu_session_state_device(self._s, int(field))
 

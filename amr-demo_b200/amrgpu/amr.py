@@ -104,8 +104,9 @@ def host_tags(n, rho_tol, method=5):
     return tag
 
 
-def regrid(forest, session, n, min_level, max_level, config, form):
-    """One regrid; returns the new session with the remapped state."""
+def regrid(forest, session, n, min_level, max_level, config=None, form=None):
+    """One regrid of the session in place (its mesh and state follow the
+    forest); returns the session."""
     tags = session.tag()
     _, lev, _, _ = forest.quads()
     forest.begin_regrid()
@@ -116,10 +117,8 @@ def regrid(forest, session, n, min_level, max_level, config, form):
     forest.coarsen(((tags2 == 0) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
     forest.balance()
     kind, src = forest.remap()
-    mesh = forest.mesh(n)
-    new = Session(mesh, config, form=form)
-    new.remap_from(session, kind, src)
-    return new
+    session.regrid(forest.mesh(n), kind, src)
+    return session
 
 
 def run(forest, soln, n, config, form, final_time, regrid_interval, min_level, max_level, max_steps=10 ** 7):
@@ -150,9 +149,7 @@ def run(forest, soln, n, config, form, final_time, regrid_interval, min_level, m
             break
         if time_now >= final_time:
             break
-        s2 = regrid(forest, s, n, min_level, max_level, config, form)
-        s.close()
-        s = s2
+        regrid(forest, s, n, min_level, max_level)
         regrids += 1
         t_regrid += time.perf_counter() - t1
     return s, {"steps": steps, "time": time_now, "cell_updates": cell_updates, "solve_s": t_solve,

@@ -21,6 +21,7 @@ struct Leaf {
     int type;       // cell type (cell_info[0])
     int src;        // provenance within the current regrid (see forest_begin_regrid)
     int src_kind;   // kRemapCopy: data of old leaf src; kRemapAverage: mean of old src..src+3
+    int dirty = 0;  // created by refine / coarsen / balance since the last completed balance
 };
 
 struct Forest;

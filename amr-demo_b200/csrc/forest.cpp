@@ -28,7 +28,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <unordered_map>
 #include <vector>
 
 namespace amrgpu {
@@ -56,15 +55,6 @@ inline uint64_t morton(int64_t x, int64_t y) { return spread_bits(uint64_t(x)) |
 struct Key {
     int tree, level;
     int64_t x, y;
-    bool operator==(const Key &o) const { return tree == o.tree && level == o.level && x == o.x && y == o.y; }
-};
-struct KeyHash {
-    size_t operator()(const Key &k) const
-    {
-        uint64_t h = morton(k.x >> 0, k.y >> 0) * 0x9E3779B97F4A7C15ULL;
-        h ^= uint64_t(k.tree) * 0xC2B2AE3D27D4EB4FULL + uint64_t(k.level);
-        return size_t(h ^ (h >> 29));
-    }
 };
 
 }  // namespace
@@ -81,6 +71,12 @@ struct Forest {
 
     int tree_of(int tx, int ty) const { return tree_at[size_t(ty) * nx + tx]; }
 
+    // Morton index of each leaf's lower corner and the first leaf of each
+    // tree: leaves stay sorted by (tree, Morton) through refine, coarsen and
+    // balance, so point location is a binary search within the tree.
+    mutable std::vector<uint64_t> keys;
+    mutable std::vector<int> tree_begin;
+
     void sort_leaves()
     {
         std::sort(leaves.begin(), leaves.end(), [](const Leaf &a, const Leaf &b) {
@@ -89,17 +85,32 @@ struct Forest {
         });
     }
 
-    std::unordered_map<Key, int, KeyHash> index() const
+    void rebuild_keys() const
     {
-        std::unordered_map<Key, int, KeyHash> m;
-        m.reserve(leaves.size() * 2);
-        for (size_t i = 0; i < leaves.size(); ++i)
-            m.emplace(Key{leaves[i].tree, leaves[i].level, leaves[i].x, leaves[i].y}, int(i));
-        return m;
+        const size_t nl = leaves.size();
+        keys.resize(nl);
+        tree_begin.assign(size_t(nx) * ny + 1, int(nl));
+        for (size_t i = nl; i-- > 0;) {
+            keys[i] = morton(leaves[i].x, leaves[i].y);
+            tree_begin[size_t(leaves[i].tree)] = int(i);
+        }
+        for (size_t t = tree_begin.size() - 1; t-- > 0;)
+            tree_begin[t] = std::min(tree_begin[t], tree_begin[t + 1]);
+    }
+
+    // Leaf containing the point (x,y) of a tree: the last leaf of the tree
+    // whose corner precedes the point on the Morton curve.
+    int locate(int tree, int64_t x, int64_t y) const
+    {
+        const uint64_t m = morton(x, y);
+        const uint64_t *b = keys.data() + tree_begin[size_t(tree)];
+        const uint64_t *e = keys.data() + tree_begin[size_t(tree) + 1];
+        return int(std::upper_bound(b, e, m) - keys.data()) - 1;
     }
 
     // Same-level neighbour region of (tree,level,x,y) across offset (dx,dy)
     // in units of the quadrant length; false when it leaves the domain.
+    // At level kMaxLevel this moves a point by one finest unit.
     bool shifted(int tree, int level, int64_t x, int64_t y, int dx, int dy, Key &out) const
     {
         int64_t L = qlen(level);
@@ -121,17 +132,47 @@ struct Forest {
         return true;
     }
 
-    // Leaf that equals or contains the region k; -1 when the region is
-    // subdivided further (or absent).
-    static int containing_leaf(const std::unordered_map<Key, int, KeyHash> &m, Key k)
+    // Leaf two or more levels coarser than q holding q's neighbour region
+    // across (dx,dy) (q is the fine side of a 2:1 violation), else -1.
+    int too_coarse_neighbour(const Leaf &q, int dx, int dy) const
     {
-        for (int l = k.level; l >= 0; --l) {
-            int64_t L = qlen(l);
-            Key a{k.tree, l, (k.x / L) * L, (k.y / L) * L};
-            auto it = m.find(a);
-            if (it != m.end()) return it->second;
+        Key k;
+        if (!shifted(q.tree, q.level, q.x, q.y, dx, dy, k)) return -1;
+        int c = locate(k.tree, k.x, k.y);
+        return leaves[size_t(c)].level < q.level - 1 ? c : -1;
+    }
+
+    // True when a leaf touching q across a face or a corner is two or more
+    // levels finer (q is the coarse side of a 2:1 violation). Faces are
+    // walked leaf by leaf along the edge; corners take the diagonal point.
+    bool has_too_fine_neighbour(const Leaf &q) const
+    {
+        const int64_t L = qlen(q.level);
+        const int lim = q.level + 2;
+        for (int s = 0; s < 4; ++s) {
+            for (int64_t t = 0; t < L;) {
+                int64_t px = q.x, py = q.y;
+                int dx = 0, dy = 0;
+                if (s == 0) { py += t; dx = -1; }
+                if (s == 1) { px += L - 1; py += t; dx = 1; }
+                if (s == 2) { px += t; dy = -1; }
+                if (s == 3) { px += t; py += L - 1; dy = 1; }
+                Key k;
+                if (!shifted(q.tree, kMaxLevel, px, py, dx, dy, k)) break;
+                const Leaf &c = leaves[size_t(locate(k.tree, k.x, k.y))];
+                if (c.level >= lim) return true;
+                const int64_t len = qlen(c.level);
+                t += (s < 2) ? (c.y + len - k.y) : (c.x + len - k.x);
+            }
         }
-        return -1;
+        for (int dy = -1; dy <= 1; dy += 2)
+            for (int dx = -1; dx <= 1; dx += 2) {
+                Key k;
+                int64_t px = dx < 0 ? q.x : q.x + L - 1, py = dy < 0 ? q.y : q.y + L - 1;
+                if (!shifted(q.tree, kMaxLevel, px, py, dx, dy, k)) continue;
+                if (leaves[size_t(locate(k.tree, k.x, k.y))].level >= lim) return true;
+            }
+        return false;
     }
 };
 
@@ -217,6 +258,7 @@ int forest_refine(Forest *f, const int *flags, int max_level)
                 ch.x = p.x + (c & 1) * h;
                 ch.y = p.y + ((c >> 1) & 1) * h;
                 ch.tag = 1;  // children inherit the refine tag
+                ch.dirty = 1;
                 out.push_back(ch);
             }
         } else {
@@ -260,6 +302,7 @@ int forest_coarsen(Forest *f, const int *flags, int min_level)
             p.tag = 0;
             p.src = a.src;
             p.src_kind = kRemapAverage;
+            p.dirty = 1;
             out.push_back(p);
             i += 4;
         } else {
@@ -274,31 +317,44 @@ int forest_coarsen(Forest *f, const int *flags, int min_level)
 int forest_balance(Forest *f)
 {
     // Refine until every leaf's face and corner neighbours are at most one
-    // level coarser (2:1 across faces and corners).
+    // level coarser (2:1 across faces and corners). Leaves untouched since
+    // the last balance are pairwise balanced, so every violation has a
+    // dirty leaf on one side: each pass checks only dirty leaves, as the
+    // fine side (flag the too-coarse neighbour) and as the coarse side
+    // (flag itself); the children it creates are the next pass's dirty set.
+    // The result is the same minimal balanced refinement as checking every
+    // leaf on every pass.
     for (int iter = 0; iter < 64; ++iter) {
-        auto m = f->index();
-        std::vector<int> flags(f->leaves.size(), 0);
+        f->rebuild_keys();
+        const size_t nl = f->leaves.size();
+        std::vector<unsigned char> flags(nl, 0);
         bool any = false;
-        for (size_t i = 0; i < f->leaves.size(); ++i) {
+        for (size_t i = 0; i < nl; ++i) {
             const Leaf &q = f->leaves[i];
-            if (q.level < 2) continue;
-            for (int dy = -1; dy <= 1; ++dy)
-                for (int dx = -1; dx <= 1; ++dx) {
-                    if (!dx && !dy) continue;
-                    Key k;
-                    if (!f->shifted(q.tree, q.level, q.x, q.y, dx, dy, k)) continue;
-                    int c = Forest::containing_leaf(m, k);
-                    if (c >= 0 && f->leaves[size_t(c)].level < q.level - 1 && !flags[size_t(c)]) {
-                        flags[size_t(c)] = 1;
-                        any = true;
+            if (!q.dirty) continue;
+            if (q.level >= 2)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        if (!dx && !dy) continue;
+                        int c = f->too_coarse_neighbour(q, dx, dy);
+                        if (c >= 0 && !flags[size_t(c)]) {
+                            flags[size_t(c)] = 1;
+                            any = true;
+                        }
                     }
-                }
+            if (!flags[i] && q.level + 2 <= kMaxLevel && f->has_too_fine_neighbour(q)) {
+                flags[i] = 1;
+                any = true;
+            }
         }
-        if (!any) return int(f->leaves.size());
+        if (!any) {
+            for (Leaf &q : f->leaves) q.dirty = 0;
+            return int(f->leaves.size());
+        }
         // balance refinement keeps the refined quad's own tag on its children
         std::vector<Leaf> out;
-        out.reserve(f->leaves.size() * 2);
-        for (size_t i = 0; i < f->leaves.size(); ++i) {
+        out.reserve(nl + 3 * nl / 8);
+        for (size_t i = 0; i < nl; ++i) {
             const Leaf &p = f->leaves[i];
             if (flags[i]) {
                 int64_t h = qlen(p.level + 1);
@@ -307,10 +363,12 @@ int forest_balance(Forest *f)
                     ch.level = p.level + 1;
                     ch.x = p.x + (c & 1) * h;
                     ch.y = p.y + ((c >> 1) & 1) * h;
+                    ch.dirty = 1;
                     out.push_back(ch);
                 }
             } else {
                 out.push_back(p);
+                out.back().dirty = 0;
             }
         }
         f->leaves.swap(out);
@@ -320,17 +378,12 @@ int forest_balance(Forest *f)
 
 bool forest_is_balanced(const Forest *f)
 {
-    auto m = f->index();
+    f->rebuild_keys();
     for (const Leaf &q : f->leaves) {
         if (q.level < 2) continue;
         for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                if (!dx && !dy) continue;
-                Key k;
-                if (!f->shifted(q.tree, q.level, q.x, q.y, dx, dy, k)) continue;
-                int c = Forest::containing_leaf(m, k);
-                if (c >= 0 && f->leaves[size_t(c)].level < q.level - 1) return false;
-            }
+            for (int dx = -1; dx <= 1; ++dx)
+                if ((dx || dy) && f->too_coarse_neighbour(q, dx, dy) >= 0) return false;
     }
     return true;
 }
@@ -374,7 +427,13 @@ int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_i
 {
     const int nq = int(f->leaves.size());
     const int nftm = nfields * nelem_subgrid * nelem_subgrid;
-    auto m = f->index();
+    f->rebuild_keys();
+    // leaf exactly at (tree, level, x, y), else -1
+    auto find = [&](int tree, int level, int64_t x, int64_t y) {
+        int c = f->locate(tree, x, y);
+        const Leaf &l = f->leaves[size_t(c)];
+        return (l.level == level && l.x == x && l.y == y) ? c : -1;
+    };
     for (int i = 0; i < nq; ++i) {
         const Leaf &q = f->leaves[size_t(i)];
         cell_info[3 * i + 0] = q.type;
@@ -405,9 +464,10 @@ int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_i
                 emit(v);
                 continue;
             }
-            auto it = m.find(k);
-            if (it != m.end()) {
-                int j = it->second;
+            const int c0 = f->locate(k.tree, k.x, k.y);
+            const int lvl0 = f->leaves[size_t(c0)].level;
+            if (lvl0 == q.level) {
+                int j = c0;
                 // side[0]: lower quadrant inside a tree; across trees the
                 // lower tree id, then the lower face number.
                 bool this_first;
@@ -427,53 +487,37 @@ int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_i
                 continue;
             }
             // coarser neighbour: this quad is one of two hanging quads
-            if (q.level > 0) {
-                int64_t Lp = qlen(q.level - 1);
-                Key kp{k.tree, q.level - 1, (k.x / Lp) * Lp, (k.y / Lp) * Lp};
-                auto ip = m.find(kp);
-                if (ip != m.end()) {
-                    int c = ip->second;
-                    // the two fine quads on this face, lower coordinate first
-                    int64_t L = qlen(q.level);
-                    int64_t base_x = (q.x / Lp) * Lp, base_y = (q.y / Lp) * Lp;
-                    int fine[2];
-                    for (int h = 0; h < 2; ++h) {
-                        Key kf{q.tree, q.level, base_x, base_y};
-                        if (s < 2) {
-                            kf.x = q.x;
-                            kf.y = base_y + h * L;
-                        } else {
-                            kf.x = base_x + h * L;
-                            kf.y = q.y;
-                        }
-                        auto ifn = m.find(kf);
-                        fine[h] = ifn == m.end() ? -1 : ifn->second;
-                    }
-                    if (fine[0] < 0 || fine[1] < 0) return -2;
-                    v[0] = 3; v[1] = opp; v[2] = c;
-                    v[3] = fine[0]; v[4] = fine[1]; v[7] = s; v[8] = s;
-                    done[size_t(c) * 4 + opp] = 1;
-                    done[size_t(fine[0]) * 4 + s] = 1;
-                    done[size_t(fine[1]) * 4 + s] = 1;
-                    emit(v);
-                    continue;
+            if (lvl0 < q.level - 1) return -2;  // not 2:1 balanced
+            if (lvl0 == q.level - 1) {
+                const int c = c0;
+                // the two fine quads on this face, lower coordinate first
+                const int64_t Lp = qlen(q.level - 1), L = qlen(q.level);
+                const int64_t base_x = (q.x / Lp) * Lp, base_y = (q.y / Lp) * Lp;
+                int fine[2];
+                for (int h = 0; h < 2; ++h) {
+                    if (s < 2)
+                        fine[h] = find(q.tree, q.level, q.x, base_y + h * L);
+                    else
+                        fine[h] = find(q.tree, q.level, base_x + h * L, q.y);
                 }
+                if (fine[0] < 0 || fine[1] < 0) return -2;
+                v[0] = 3; v[1] = opp; v[2] = c;
+                v[3] = fine[0]; v[4] = fine[1]; v[7] = s; v[8] = s;
+                done[size_t(c) * 4 + opp] = 1;
+                done[size_t(fine[0]) * 4 + s] = 1;
+                done[size_t(fine[1]) * 4 + s] = 1;
+                emit(v);
+                continue;
             }
             // finer neighbours: this quad is the full side of a hanging face
             {
                 int64_t Lc = qlen(q.level + 1);
                 int fine[2];
                 for (int h = 0; h < 2; ++h) {
-                    Key kf{k.tree, q.level + 1, k.x, k.y};
-                    if (s < 2) {
-                        kf.x = (s == 0) ? k.x + Lc : k.x;
-                        kf.y = k.y + h * Lc;
-                    } else {
-                        kf.x = k.x + h * Lc;
-                        kf.y = (s == 2) ? k.y + Lc : k.y;
-                    }
-                    auto ifn = m.find(kf);
-                    fine[h] = ifn == m.end() ? -1 : ifn->second;
+                    if (s < 2)
+                        fine[h] = find(k.tree, q.level + 1, (s == 0) ? k.x + Lc : k.x, k.y + h * Lc);
+                    else
+                        fine[h] = find(k.tree, q.level + 1, k.x + h * Lc, (s == 2) ? k.y + Lc : k.y);
                 }
                 if (fine[0] < 0 || fine[1] < 0) return -3;  // not 2:1 balanced
                 v[0] = 3; v[1] = s; v[2] = i;

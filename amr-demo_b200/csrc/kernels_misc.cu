@@ -162,6 +162,27 @@ __global__ void remap_kernel(const double *__restrict__ qold, long long stride_o
     }
 }
 
+// Re-arms the step slots after an in-place mesh change without a host
+// round trip: the current step's start time is kept, every slot takes the
+// dt cap, and the per-segment counters restart (the device form of the
+// host-side priming that follows an upload).
+__global__ void rearm_kernel(DeviceScalars *s, int slot_now, double cap)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double t = s->slot[slot_now].time;
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(cap);
+    for (int k = 0; k < 3; ++k) {
+        s->slot[k].dt_bits = bits;
+        s->slot[k].time = t;
+    }
+    s->norm_sq = 0.0;
+    s->dt_used = 0.0;
+    s->done_blocks = 0u;
+    s->flags = 0;
+    s->steps = 0;
+    s->pad = 0;
+}
+
 static int grid_for(long long work, int block)
 {
     long long g = (work + block - 1) / block;
@@ -211,6 +232,12 @@ cudaError_t launch_tag(int n, const double *rho, const QuadDesc *quads, int nqua
     case 16: tag_kernel<16><<<blocks, 256, 0, st>>>(rho, quads, nquad, nmeth, m, tags); break;
     default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rearm(DeviceScalars *scal, int slot_now, double cap, cudaStream_t st)
+{
+    rearm_kernel<<<1, 32, 0, st>>>(scal, slot_now, cap);
     return cudaGetLastError();
 }
 

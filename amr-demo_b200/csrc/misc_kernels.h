@@ -6,6 +6,7 @@
 namespace amrgpu {
 
 struct QuadDesc;
+struct DeviceScalars;
 
 struct TagMethods {
     int method[5];
@@ -21,6 +22,7 @@ cudaError_t launch_totals(int n, const QuadDesc *quads, const double *q, long lo
                           double *partials, int grid, cudaStream_t st);
 cudaError_t launch_tag(int n, const double *rho, const QuadDesc *quads, int nquad, int nmeth,
                        const TagMethods &m, int *tags, cudaStream_t st);
+cudaError_t launch_rearm(DeviceScalars *scal, int slot_now, double cap, cudaStream_t st);
 cudaError_t launch_remap(int n, const double *qold, long long stride_old, double *qnew,
                          long long stride_new, const int *kind, const int *src, int nquad_new,
                          cudaStream_t st);

@@ -96,6 +96,13 @@ struct amrgpu_session {
     double *d_partials = nullptr;
     int partial_cap = 0;
     double *d_tot = nullptr;
+    long long cap_stride = 0;  // cells per field the state buffers hold
+    int cap_quads = 0;         // quads the descriptor, tag and remap arrays hold
+    int *d_tags = nullptr;
+    int *d_kind = nullptr;
+    int *d_src = nullptr;
+    const void *occ_kernel = nullptr;  // launch whose occupancy occ_per_sm is
+    int occ_per_sm = 0;
     cudaStream_t stream = nullptr;
     int form = AMRGPU_FORM_FP64_EXACT;
     const StageLaunch *launch = nullptr;
@@ -236,13 +243,18 @@ int configure_launch(amrgpu_session *s, const StageLaunch *L)
         set_error(AMRGPU_ERR_UNSUPPORTED, "the FP32-flux form needs axis-aligned rectangular quads");
         return AMRGPU_ERR_UNSUPPORTED;
     }
-    if (!cuda_ok(cudaFuncSetAttribute(L->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L->smem)),
-                 "cudaFuncSetAttribute"))
-        return AMRGPU_ERR_CUDA;
-    int per_sm = 0;
-    if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L->kernel, L->threads, L->smem),
-                 "occupancy"))
-        return AMRGPU_ERR_CUDA;
+    if (s->occ_kernel != L->kernel) {
+        if (!cuda_ok(cudaFuncSetAttribute(L->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L->smem)),
+                     "cudaFuncSetAttribute"))
+            return AMRGPU_ERR_CUDA;
+        int occ = 0;
+        if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->kernel, L->threads, L->smem),
+                     "occupancy"))
+            return AMRGPU_ERR_CUDA;
+        s->occ_kernel = L->kernel;
+        s->occ_per_sm = occ;
+    }
+    int per_sm = s->occ_per_sm;
     if (per_sm < 1) per_sm = 1;
     int groups = (s->nquad + L->qpb - 1) / L->qpb;
     int g = std::min(groups, per_sm * s->sms);
@@ -261,21 +273,28 @@ int configure_launch(amrgpu_session *s, const StageLaunch *L)
     return AMRGPU_OK;
 }
 
-int prime(amrgpu_session *s)
+// Arms the step slots (slot step_index % 3 holds the step about to run, the
+// others the dt cap) and folds the first step's CFL minimum. keep_time
+// re-arms on the device from the time already there (in-place regrid);
+// otherwise the slots start at t0 from the host.
+int prime(amrgpu_session *s, bool keep_time = false)
 {
-    // slots: s%3 holds the step about to run; the others are armed with the cap
     int p = int(s->step_index % 3);
-    std::memset(&s->h_scal, 0, sizeof(s->h_scal));
     double cap = s->cfg.dt;
-    for (int k = 0; k < 3; ++k) {
-        s->h_scal.slot[k].dt_bits = (unsigned long long)0;
-        std::memcpy(&s->h_scal.slot[k].dt_bits, &cap, sizeof(double));
-        s->h_scal.slot[k].time = s->t0;
+    if (keep_time) {
+        if (!cuda_ok(launch_rearm(s->d_scal, p, cap, s->stream), "rearm scalars")) return AMRGPU_ERR_CUDA;
+        s->launches++;
+    } else {
+        std::memset(&s->h_scal, 0, sizeof(s->h_scal));
+        for (int k = 0; k < 3; ++k) {
+            std::memcpy(&s->h_scal.slot[k].dt_bits, &cap, sizeof(double));
+            s->h_scal.slot[k].time = s->t0;
+        }
+        if (!cuda_ok(cudaMemcpyAsync(s->d_scal, &s->h_scal, sizeof(DeviceScalars), cudaMemcpyHostToDevice,
+                                     s->stream),
+                     "prime scalars"))
+            return AMRGPU_ERR_CUDA;
     }
-    (void)p;
-    if (!cuda_ok(cudaMemcpyAsync(s->d_scal, &s->h_scal, sizeof(DeviceScalars), cudaMemcpyHostToDevice, s->stream),
-                 "prime scalars"))
-        return AMRGPU_ERR_CUDA;
     bool cfl_on = s->cfg.time_scheme != 2;
     if (cfl_on && s->nquad > 0) {
         CflArgs a;
@@ -413,6 +432,10 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const 
                          "upload quads");
     }
     if (ok) ok = cuda_ok(cudaMalloc(&s->d_tot, sizeof(double) * 4 * size_t(totals_grid(std::max<long long>(s->ncells_total, 1)))), "cudaMalloc totals");
+    s->cap_stride = s->stride;
+    s->cap_quads = std::max(s->nquad, 1);
+    for (int **p : {&s->d_tags, &s->d_kind, &s->d_src})
+        if (ok) ok = cuda_ok(cudaMalloc(p, sizeof(int) * size_t(s->cap_quads)), "cudaMalloc quad arrays");
     if (!ok) {
         amrgpu_session_destroy(s);
         return AMRGPU_ERR_CUDA;
@@ -444,6 +467,9 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_partials);
     cudaFree(s->d_quads);
     cudaFree(s->d_tot);
+    cudaFree(s->d_tags);
+    cudaFree(s->d_kind);
+    cudaFree(s->d_src);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -690,15 +716,13 @@ int amrgpu_session_tag(amrgpu_session_t *s, int *tags)
         m.method[k] = k < nm ? s->cfg.amr_tag_methods[size_t(k)] : 0;
         m.tol[k] = k < nm ? s->cfg.amr_tag_tolerances[size_t(k)] : 0.0;
     }
-    int *d_tags = nullptr;
-    if (!cuda_ok(cudaMallocAsync((void **)&d_tags, sizeof(int) * size_t(s->nquad), s->stream), "cudaMalloc tags"))
-        return AMRGPU_ERR_CUDA;
-    bool ok = cuda_ok(launch_tag(s->n, rolebuf(s, RX), s->d_quads, s->nquad, nm, m, d_tags, s->stream), "tag kernel");
+    bool ok = cuda_ok(launch_tag(s->n, rolebuf(s, RX), s->d_quads, s->nquad, nm, m, s->d_tags, s->stream),
+                      "tag kernel");
     s->launches++;
     if (ok)
-        ok = cuda_ok(cudaMemcpyAsync(tags, d_tags, sizeof(int) * size_t(s->nquad), cudaMemcpyDeviceToHost, s->stream),
+        ok = cuda_ok(cudaMemcpyAsync(tags, s->d_tags, sizeof(int) * size_t(s->nquad), cudaMemcpyDeviceToHost,
+                                     s->stream),
                      "D2H tags");
-    cudaFreeAsync(d_tags, s->stream);
     if (ok) ok = cuda_ok(cudaStreamSynchronize(s->stream), "sync");
     return ok ? AMRGPU_OK : AMRGPU_ERR_CUDA;
 }
@@ -714,27 +738,149 @@ int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int
         }
     }
     cudaStreamSynchronize(src->stream);
-    int *d_kind = nullptr, *d_src = nullptr;
-    size_t nb = sizeof(int) * size_t(std::max(dst->nquad, 1));
-    bool ok = cuda_ok(cudaMallocAsync((void **)&d_kind, nb, dst->stream), "cudaMalloc remap") &&
-              cuda_ok(cudaMallocAsync((void **)&d_src, nb, dst->stream), "cudaMalloc remap");
-    if (ok)
-        ok = cuda_ok(cudaMemcpyAsync(d_kind, kind, sizeof(int) * size_t(dst->nquad), cudaMemcpyHostToDevice, dst->stream),
-                     "H2D remap") &&
-             cuda_ok(cudaMemcpyAsync(d_src, src_index, sizeof(int) * size_t(dst->nquad), cudaMemcpyHostToDevice,
-                                     dst->stream),
-                     "H2D remap");
+    bool ok = cuda_ok(cudaMemcpyAsync(dst->d_kind, kind, sizeof(int) * size_t(dst->nquad), cudaMemcpyHostToDevice,
+                                      dst->stream),
+                      "H2D remap") &&
+              cuda_ok(cudaMemcpyAsync(dst->d_src, src_index, sizeof(int) * size_t(dst->nquad),
+                                      cudaMemcpyHostToDevice, dst->stream),
+                      "H2D remap");
     if (ok && dst->nquad > 0) {
-        ok = cuda_ok(launch_remap(dst->n, rolebuf(src, RX), src->stride, rolebuf(dst, RX), dst->stride, d_kind, d_src,
-                                  dst->nquad, dst->stream),
+        ok = cuda_ok(launch_remap(dst->n, rolebuf(src, RX), src->stride, rolebuf(dst, RX), dst->stride, dst->d_kind,
+                                  dst->d_src, dst->nquad, dst->stream),
                      "remap kernel");
         dst->launches++;
     }
-    cudaFreeAsync(d_kind, dst->stream);
-    cudaFreeAsync(d_src, dst->stream);
     if (!ok) return AMRGPU_ERR_CUDA;
     dst->t0 = src->h_scal.slot[src->step_index % 3].time;
     return prime(dst);
+}
+
+int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int *kind, const int *src_index)
+{
+    if (!s || !m || !kind || !src_index || !m->cell_info || !m->geom || (m->nface > 0 && !m->face_info) ||
+        m->ncell < 0 || m->nghost < 0) {
+        set_error(AMRGPU_ERR_ARG, "session_regrid: null or negative arguments");
+        return AMRGPU_ERR_ARG;
+    }
+    if (m->nghost != 0) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "session_regrid: ghost quads need a ghost exchange after the remap");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    if (m->dof != 4 * s->n * s->n * m->ncell) {
+        set_error(AMRGPU_ERR_MESH, "dof != 4*n*n*ncell");
+        return AMRGPU_ERR_MESH;
+    }
+    for (int q = 0; q < m->ncell; ++q) {
+        int lim = kind[q] == 0 ? s->nquad - 1 : s->nquad - 4;
+        if ((kind[q] != 0 && kind[q] != 1) || src_index[q] < 0 || src_index[q] > lim) {
+            set_error(AMRGPU_ERR_ARG, "remap kind or source index out of range");
+            return AMRGPU_ERR_ARG;
+        }
+    }
+    std::vector<QuadDesc> old = std::move(s->h_quads);
+    int rc = decode_mesh(s, m);
+    if (rc == AMRGPU_OK && s->form == AMRGPU_FORM_FP32_FLUX && !quads_are_rectangles(s)) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "the FP32-flux form needs axis-aligned rectangular quads");
+        rc = AMRGPU_ERR_UNSUPPORTED;
+    }
+    if (rc != AMRGPU_OK) {
+        s->h_quads = std::move(old);
+        return rc;
+    }
+    const int nq = m->ncell;
+    const long long cells = (long long)nq * s->n * s->n;
+    const long long stride = std::max<long long>(((cells + 31) / 32) * 32, 32);
+    // per-quad arrays: grow by a quarter beyond the need so that a slowly
+    // growing mesh reallocates rarely (cudaFree synchronises the device)
+    if (nq > s->cap_quads) {
+        int cap = nq + nq / 4;
+        QuadDesc *dq = nullptr;
+        bool ok = cuda_ok(cudaMalloc(&dq, sizeof(QuadDesc) * size_t(cap)), "cudaMalloc quads");
+        int *arr[3] = {nullptr, nullptr, nullptr};
+        for (int k = 0; k < 3 && ok; ++k) ok = cuda_ok(cudaMalloc(&arr[k], sizeof(int) * size_t(cap)), "cudaMalloc quad arrays");
+        if (!ok) {
+            cudaFree(dq);
+            for (int *p : arr) cudaFree(p);
+            s->h_quads = std::move(old);
+            return AMRGPU_ERR_CUDA;
+        }
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->d_quads);
+        cudaFree(s->d_tags);
+        cudaFree(s->d_kind);
+        cudaFree(s->d_src);
+        s->d_quads = dq;
+        s->d_tags = arr[0];
+        s->d_kind = arr[1];
+        s->d_src = arr[2];
+        s->cap_quads = cap;
+    }
+    bool ok = cuda_ok(cudaMemcpyAsync(s->d_kind, kind, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, s->stream),
+                      "H2D remap") &&
+              cuda_ok(cudaMemcpyAsync(s->d_src, src_index, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice,
+                                      s->stream),
+                      "H2D remap");
+    // the new state goes to a buffer other than X: the spare Y of the same
+    // capacity, or a fresh set when the mesh outgrew the capacity
+    double *qold = rolebuf(s, RX);
+    const long long old_stride = s->stride;
+    double *fresh[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long cap = s->cap_stride;
+    if (ok && stride > s->cap_stride) {
+        cap = ((stride + stride / 4 + 31) / 32) * 32;
+        for (int k = 0; k < 4 && ok; ++k)
+            ok = cuda_ok(cudaMalloc(&fresh[k], sizeof(double) * 4 * size_t(cap)), "cudaMalloc state");
+        double *aos = nullptr;
+        double *tot = nullptr;
+        if (ok) ok = cuda_ok(cudaMalloc(&aos, sizeof(double) * 4 * size_t(cap)), "cudaMalloc aos");
+        if (ok) ok = cuda_ok(cudaMalloc(&tot, sizeof(double) * 4 * size_t(totals_grid(cap))), "cudaMalloc totals");
+        if (!ok) {
+            for (double *p : fresh) cudaFree(p);
+            cudaFree(aos);
+            cudaFree(tot);
+            s->h_quads = std::move(old);
+            return AMRGPU_ERR_CUDA;
+        }
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->d_aos);
+        cudaFree(s->d_tot);
+        s->d_aos = aos;
+        s->d_tot = tot;
+    }
+    double *qnew = fresh[0] ? fresh[0] : rolebuf(s, RY);
+    if (ok && nq > 0) {
+        ok = cuda_ok(launch_remap(s->n, qold, old_stride, qnew, stride, s->d_kind, s->d_src, nq, s->stream),
+                     "remap kernel");
+        s->launches++;
+    }
+    if (ok && nq > 0)
+        ok = cuda_ok(cudaMemcpyAsync(s->d_quads, s->h_quads.data(), sizeof(QuadDesc) * size_t(nq),
+                                     cudaMemcpyHostToDevice, s->stream),
+                     "upload quads");
+    if (!ok) {
+        for (double *p : fresh) cudaFree(p);
+        return AMRGPU_ERR_CUDA;
+    }
+    if (fresh[0]) {
+        cudaStreamSynchronize(s->stream);
+        for (int k = 0; k < 4; ++k) {
+            cudaFree(s->buf[k]);
+            s->buf[k] = fresh[k];
+            s->role[k] = k;
+        }
+        s->cap_stride = cap;
+    } else {
+        std::swap(s->role[RX], s->role[RY]);
+    }
+    s->nquad = nq;
+    s->nghost = 0;
+    s->nface = m->nface;
+    s->dof = m->dof;
+    s->ncells_total = cells;
+    s->stride = stride;
+    rc = configure_launch(s, s->launch);
+    if (rc != AMRGPU_OK) return rc;
+    return prime(s, s->primed);
 }
 
 }  // extern "C"

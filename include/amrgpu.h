@@ -252,6 +252,15 @@ int amrgpu_session_tag(amrgpu_session_t *s, int *tags);
 /* New SoA state for a remapped mesh: kind/src from amrgpu_forest_remap. */
 int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int *kind,
                          const int *src_index);
+/* In-place regrid: the session takes the new mesh m (no ghost quads) and
+ * its state is remapped by kind/src (amrgpu_forest_remap) into the spare
+ * state buffer; device arrays are reused while they are large enough and
+ * grow by a quarter beyond the need otherwise. Simulated time and the step
+ * counter carry over on the device; the first step's CFL minimum is folded
+ * for the new mesh. Replaces the per-regrid rebuild of the reference's
+ * amr_regrid.c:82-125 (new ghost layer, new face lists, new soln array). */
+int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int *kind,
+                          const int *src_index);
 
 /* ---------------- allocation-free entry point ---------------- */
 /* No counterpart in the reference. Conservation totals sum(vol*Q_f), f =

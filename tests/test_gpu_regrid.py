@@ -149,8 +149,67 @@ def test_amr_loop_fp64_bitwise_against_oracle(ag, oracle):
         fo.balance()
         kind, src = fo.remap()
         ref = numpy_remap(ref, kind, src, n)
-        s2 = regrid(fg, s, n, lo, hi, cfg, ag.FORM_FP64_EXACT)
-        s.close()
-        s = s2
+        regrid(fg, s, n, lo, hi)
         assert s.mesh.ncell == len(kind)
         assert np.array_equal(s.download(), ref)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_in_place_regrid_matches_new_session(ag, form):
+    """amrgpu_session_regrid (capacity reuse, spare-buffer remap, device-side
+    re-arm) against a fresh session filled by amrgpu_session_remap: same
+    state, same time, and bit-identical steps afterwards. The first regrid
+    grows past the capacity, the second shrinks into the spare buffer."""
+    n = 8
+    f = meshes.uniform(n, 2, periodic=(1, 1))
+    cfg = meshes.make_config(n)
+    cfg["time_steps"] = 10 ** 6
+    cfg.apply()
+    s0 = meshes.perturbed(f.initialize(n), 5, amp=5e-2)
+    a = ag.Session(f.mesh(n), cfg, form=form)
+    a.upload(s0)
+    a.step(2)
+    for flags_fn in (lambda lev: np.isin(np.arange(len(lev)), [0, 3, 5, 6, 9, 12]),
+                     lambda lev: lev > 2):
+        t_before = a.sync()["time"]
+        _, lev, _, _ = f.quads()
+        f.begin_regrid()
+        fl = flags_fn(lev).astype(np.int32)
+        if (lev > 2).any():
+            f.coarsen(fl, min_level=2)
+        else:
+            f.refine(fl, max_level=4)
+        f.balance()
+        kind, src = f.remap()
+        m1 = f.mesh(n)
+        b = ag.Session(m1, cfg, form=form)
+        b.remap_from(a, kind, src)
+        a.regrid(m1, kind, src)
+        assert np.array_equal(a.download(), b.download())
+        ra, rb = a.sync(), b.sync()
+        assert ra["time"] == rb["time"] == t_before
+        a.step(3)
+        b.step(3)
+        ra, rb = a.sync(), b.sync()
+        assert ra["steps"] == rb["steps"] == 3 and ra["time"] == rb["time"]
+        assert np.array_equal(a.download(), b.download())
+        b.close()
+    a.close()
+
+
+def test_in_place_regrid_rejects_bad_tables(ag):
+    n = 4
+    f = meshes.uniform(n, 1, periodic=(1, 1))
+    cfg = meshes.make_config(n)
+    cfg.apply()
+    a = ag.Session(f.mesh(n), cfg, form=0)
+    a.upload(f.initialize(n))
+    nq = f.num_quads
+    with pytest.raises(RuntimeError):
+        a.regrid(f.mesh(n), np.zeros(nq, np.int32), np.full(nq, nq, np.int32))
+    with pytest.raises(RuntimeError):
+        a.regrid(f.mesh(n), np.ones(nq, np.int32), np.full(nq, nq - 2, np.int32))
+    # the session is unchanged and still steps
+    a.step(1)
+    assert a.sync()["steps"] == 1
+    a.close()
