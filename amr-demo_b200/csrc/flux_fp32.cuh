@@ -8,18 +8,35 @@
 
 namespace amrgpu {
 
+// Reciprocal by the SFU's approximation (rcp.approx.ftz.f32, one MUFU
+// operation, within an ulp or so) instead of the correctly rounded sequence.
+__device__ __forceinline__ float frcp(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// 1/sqrt(x) by the SFU's approximation (rsqrt.approx.ftz.f32).
+__device__ __forceinline__ float frsqrt(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __device__ __forceinline__ void roe_flux_fp32(const float ql[4], const float qr[4], float n0,
                                               float n1, float flux[4])
 {
     const float gm1p = 0.4f;  // (gamma - 1) for the pressure
     const float gm1 = 0.4f;
     float mag = sqrtf(n0 * n0 + n1 * n1);
-    float inv_mag = __frcp_rn(mag);
+    float inv_mag = frcp(mag);
     float nx = n0 * inv_mag;
     float ny = n1 * inv_mag;
 
     float rhol = ql[0];
-    float oneOrhol = __frcp_rn(rhol);
+    float oneOrhol = frcp(rhol);
     float ul = ql[1] * oneOrhol;
     float vl = ql[2] * oneOrhol;
     float pl = gm1p * (ql[3] - 0.5f * rhol * (ul * ul + vl * vl));
@@ -27,7 +44,7 @@ __device__ __forceinline__ void roe_flux_fp32(const float ql[4], const float qr[
     float unl = ul * nx + vl * ny;
 
     float rhor = qr[0];
-    float oneOrhor = __frcp_rn(rhor);
+    float oneOrhor = frcp(rhor);
     float ur = qr[1] * oneOrhor;
     float vr = qr[2] * oneOrhor;
     float pr = gm1p * (qr[3] - 0.5f * rhor * (ur * ur + vr * vr));
@@ -36,7 +53,7 @@ __device__ __forceinline__ void roe_flux_fp32(const float ql[4], const float qr[
 
     float srl = sqrtf(rhol);
     float srr = sqrtf(rhor);
-    float oneOroe = __frcp_rn(srl + srr);
+    float oneOroe = frcp(srl + srr);
     float rhobar = srl * srr;
     float ubar = (ul * srl + ur * srr) * oneOroe;
     float vbar = (vl * srl + vr * srr) * oneOroe;
@@ -44,16 +61,16 @@ __device__ __forceinline__ void roe_flux_fp32(const float ql[4], const float qr[
     float a2 = gm1 * (Hbar - 0.5f * (ubar * ubar + vbar * vbar));
     float abar = sqrtf(a2);
     float unbar = ubar * nx + vbar * ny;
-    float Mnbar = unbar * __frcp_rn(abar);
+    float Mnbar = unbar * frcp(abar);
 
     float eigp = unbar + abar;
     float eigm = unbar - abar;
     float b1 = fmaxf(fmaxf(eigp, unr + abar), 0.0f);
     float b2 = fminf(fminf(eigm, unl - abar), 0.0f);
-    float inv_db = __frcp_rn(b1 - b2);
+    float inv_db = frcp(b1 - b2);
     float bcoeff = b1 * b2 * inv_db;
-    float delta1 = (rhor - rhol) - (pr - pl) * __frcp_rn(a2);
-    float bM = bcoeff * __frcp_rn(1.0f + fabsf(Mnbar));
+    float delta1 = (rhor - rhol) - (pr - pl) * frcp(a2);
+    float bM = bcoeff * frcp(1.0f + fabsf(Mnbar));
     float dun = unr - unl;
 
     float fluxl, fluxr, disp;
@@ -85,7 +102,7 @@ __device__ __forceinline__ void cell_prims_fp32(const double q[4], float P[8])
 {
     float rho = (float)q[0];
     float ru = (float)q[1], rv = (float)q[2], rE = (float)q[3];
-    float oneOrho = __frcp_rn(rho);
+    float oneOrho = frcp(rho);
     float u = ru * oneOrho, v = rv * oneOrho;
     float p = 0.4f * (rE - 0.5f * rho * (u * u + v * v));
     P[0] = rho;
@@ -101,8 +118,9 @@ __device__ __forceinline__ void cell_prims_fp32(const double q[4], float P[8])
 // flux_roe_2d on FP32 records. Axis-aligned faces (every face of a brick
 // mesh) take the rotated form: with n = (h,0) the normal velocity is u and
 // the tangential-correction terms of rows 2/3 reduce to 0 and
-// rhobar*(v_R - v_L); Mcoeff = 1/(1+|un/a|) = a/(a+|un|). Five MUFU
-// operations per face. Other normals use roe_flux_fp32 on conserved states.
+// rhobar*(v_R - v_L); Mcoeff = 1/(1+|un/a|) = a/(a+|un|). Four MUFU
+// operations per face (three approximate reciprocals, one reciprocal square
+// root). Other normals use roe_flux_fp32 on conserved states.
 // Axis-aligned face with a positive normal of length h, direction known at
 // compile time (DIR 0: n = (h,0), DIR 1: n = (0,h)): the same algebra as
 // roe_flux_prim_fp32 without any run-time selects.
@@ -113,20 +131,21 @@ __device__ __forceinline__ void roe_flux_axis_fp32(const float *L, const float *
     const float rhor = R[0], ur = R[1], vr = R[2], pr = R[3], Hr = R[4], srr = R[5];
     const float unl = DIR == 0 ? ul : vl;
     const float unr = DIR == 0 ? ur : vr;
-    const float inv = __frcp_rn(srl + srr);
+    const float inv = frcp(srl + srr);
     const float rhobar = srl * srr;
     const float ubar = (ul * srl + ur * srr) * inv;
     const float vbar = (vl * srl + vr * srr) * inv;
     const float Hbar = (Hl * srl + Hr * srr) * inv;
     const float a2 = 0.4f * (Hbar - 0.5f * (ubar * ubar + vbar * vbar));
-    const float abar = sqrtf(a2);
+    const float ra = frsqrt(a2);  // 1/abar: abar = a2/abar, 1/a2 = ra^2
+    const float abar = a2 * ra;
     const float unbar = DIR == 0 ? ubar : vbar;
     const float b1 = fmaxf(fmaxf(unbar + abar, unr + abar), 0.0f);
     const float b2 = fminf(fminf(unbar - abar, unl - abar), 0.0f);
-    const float inv_db = __frcp_rn(b1 - b2);
+    const float inv_db = frcp(b1 - b2);
     const float bcoeff = b1 * b2 * inv_db;
-    const float delta1 = (rhor - rhol) - (pr - pl) * __frcp_rn(a2);
-    const float bM = bcoeff * abar * __frcp_rn(abar + fabsf(unbar));
+    const float delta1 = (rhor - rhol) - (pr - pl) * (ra * ra);
+    const float bM = bcoeff * abar * frcp(abar + fabsf(unbar));
     const float ml = DIR == 0 ? L[6] : L[7];
     const float mr = DIR == 0 ? R[6] : R[7];
     const float rHl = rhol * Hl, rHr = rhor * Hr;
@@ -159,7 +178,7 @@ __device__ __forceinline__ void roe_flux_prim_fp32(const float *L, const float *
     const float rhor = R[0], ur = R[1], vr = R[2], pr = R[3], Hr = R[4], srr = R[5];
     // normal / tangential momentum components of each state
     const float unl = sgn * (xdir ? ul : vl), unr = sgn * (xdir ? ur : vr);
-    const float inv = __frcp_rn(srl + srr);
+    const float inv = frcp(srl + srr);
     const float rhobar = srl * srr;
     const float ubar = (ul * srl + ur * srr) * inv;
     const float vbar = (vl * srl + vr * srr) * inv;
@@ -169,10 +188,10 @@ __device__ __forceinline__ void roe_flux_prim_fp32(const float *L, const float *
     const float unbar = sgn * (xdir ? ubar : vbar);
     const float b1 = fmaxf(fmaxf(unbar + abar, unr + abar), 0.0f);
     const float b2 = fminf(fminf(unbar - abar, unl - abar), 0.0f);
-    const float inv_db = __frcp_rn(b1 - b2);
+    const float inv_db = frcp(b1 - b2);
     const float bcoeff = b1 * b2 * inv_db;
-    const float delta1 = (rhor - rhol) - (pr - pl) * __frcp_rn(a2);
-    const float bM = bcoeff * abar * __frcp_rn(abar + fabsf(unbar));
+    const float delta1 = (rhor - rhol) - (pr - pl) * frcp(a2);
+    const float bM = bcoeff * abar * frcp(abar + fabsf(unbar));
     // mass flux of each state through the face
     const float ml = sgn * (xdir ? L[6] : L[7]);
     const float mr = sgn * (xdir ? R[6] : R[7]);
@@ -204,7 +223,7 @@ __device__ __forceinline__ void bc_flux_fp32(int bc, const float q[4], float n0,
                                              const float qin[4], float flux[4])
 {
     float qb[4];
-    float oneOrho = __frcp_rn(q[0]);
+    float oneOrho = frcp(q[0]);
     float u = q[1] * oneOrho;
     float v = q[2] * oneOrho;
     if (bc == 1) {
@@ -225,7 +244,7 @@ __device__ __forceinline__ void bc_flux_fp32(int bc, const float q[4], float n0,
     } else {
         qb[0] = q[0]; qb[1] = q[1]; qb[2] = q[2]; qb[3] = q[3];
     }
-    float oor = __frcp_rn(qb[0]);
+    float oor = frcp(qb[0]);
     float ub = qb[1] * oor, vb = qb[2] * oor;
     float p = 0.4f * (qb[3] - 0.5f * qb[0] * (ub * ub + vb * vb));
     flux[0] = qb[1] * n0 + qb[2] * n1;
@@ -239,6 +258,21 @@ __device__ __forceinline__ void bc_flux_rec_fp32(int bc, const float *P, float n
 {
     float q[4] = {P[0], P[6], P[7], P[0] * P[4] - P[3]};
     bc_flux_fp32(bc, q, n0, n1, qin, flux);
+}
+
+// One cell's CFL step candidate cfl*sqrt(volume)/(|V| + c) of
+// solver_time_step_2d_module.F90:106-116, in FP32 with approximate square
+// roots and reciprocals (the FP32-flux form; the state stays FP64).
+__device__ __forceinline__ double cfl_candidate_fp32(const double q[4], double volume, double cfl)
+{
+    const float rho = (float)q[0];
+    const float oneOrho = frcp(rho);
+    const float u = (float)q[1] * oneOrho;
+    const float v = (float)q[2] * oneOrho;
+    const float V2 = u * u + v * v;
+    const float pOverRho = 0.4f * ((float)q[3] * oneOrho - 0.5f * V2);
+    const float eig = sqrtf(V2) + sqrtf(1.4f * pOverRho);
+    return (double)((float)cfl * sqrtf((float)volume) * frcp(eig));
 }
 
 }  // namespace amrgpu

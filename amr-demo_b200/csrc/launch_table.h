@@ -26,5 +26,6 @@ int stage_table_fp32(const StageLaunch **out);
 // reference's candidate, folded into scal->slot[slot].dt_bits.
 struct CflArgs;
 const void *cfl_kernel_fp64(int n);
+const void *cfl_kernel_fp32(int n);  // the FP32-flux form's candidate
 
 }  // namespace amrgpu

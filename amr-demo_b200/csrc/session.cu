@@ -305,7 +305,7 @@ int prime(amrgpu_session *s, bool keep_time = false)
         a.nquad = s->nquad;
         a.slot = p;
         a.cfl = s->cfg.cfl;
-        const void *k = cfl_kernel_fp64(s->n);
+        const void *k = s->form == AMRGPU_FORM_FP32_FLUX ? cfl_kernel_fp32(s->n) : cfl_kernel_fp64(s->n);
         long long cells = (long long)s->nquad * s->n * s->n;
         int g = int(std::min<long long>((cells + 255) / 256, (long long)s->sms * 8));
         void *args[] = {&a};

@@ -1,7 +1,7 @@
 // stage_fp32.cu -- FP32-flux instantiations of the stage kernel: face
-// fluxes, normals and boundary states in FP32; the conserved state, the
-// per-cell residual sums (hanging-face corrections included), the division
-// by the volume, the stage update and the CFL step stay in FP64.
+// fluxes, normals, boundary states and the CFL candidate in FP32; the
+// conserved state, the per-cell residual sums (hanging-face corrections
+// included), the division by the volume and the stage update stay in FP64.
 #include <cuda_runtime.h>
 
 #include "flux_fp32.cuh"
@@ -32,9 +32,50 @@ struct FluxOpsFP32 {
     }
     __device__ static __forceinline__ double cfl(const double *q, double vol, double c)
     {
-        return cfl_candidate_fp64(q, vol, c);
+        return cfl_candidate_fp32(q, vol, c);
     }
 };
+
+// CFL step of a state for the FP32-flux form (segment prologue): the same
+// candidate and rectangle volume as the stage kernel's last stage, so a step
+// takes the same dt whether or not it starts a segment.
+template <int N>
+__global__ void __launch_bounds__(256) cfl_kernel_f32(const CflArgs a)
+{
+    constexpr int NN = N * N;
+    __shared__ double red[8];
+    double best = __longlong_as_double((long long)a.scal->slot[a.slot].dt_bits);
+    const long long ncells = (long long)a.nquad * NN;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(c / NN);
+        const double *g = a.quads[q].corner;
+        const double hx = (g[2] - g[0]) / (double)N, hy = (g[5] - g[1]) / (double)N;
+        double q4[4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) q4[f] = a.qin[f * a.stride + c];
+        const double cand = cfl_candidate_fp32(q4, hx * hy, a.cfl);
+        if (cand < best) best = cand;
+    }
+    best = warp_min(best);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = (red[w] < best) ? red[w] : best;
+        atomicMin(&a.scal->slot[a.slot].dt_bits, (unsigned long long)__double_as_longlong(best));
+    }
+}
+
+const void *cfl_kernel_fp32(int n)
+{
+    switch (n) {
+    case 2: return (const void *)cfl_kernel_f32<2>;
+    case 4: return (const void *)cfl_kernel_f32<4>;
+    case 8: return (const void *)cfl_kernel_f32<8>;
+    case 16: return (const void *)cfl_kernel_f32<16>;
+    default: return nullptr;
+    }
+}
 
 #define AMRGPU_STAGE32(N, QPB, T, MINB)                                                        \
     StageLaunch{N, QPB, T, MINB, StageSmem<N, QPB, true>::total,                               \

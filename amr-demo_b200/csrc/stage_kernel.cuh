@@ -19,16 +19,18 @@
 // computed, group k+1's four field slabs per quad (contiguous n*n doubles
 // each) arrive through 1D bulk copies (TMA engine) completed on an
 // mbarrier, its neighbour edge strips through cp.async, and group k+2's
-// descriptors through a bulk copy; the next stage's own-cell auxiliary
-// arrays are prefetched into L2.
+// descriptors through a bulk copy; the FP32 form's first own-cell auxiliary
+// input comes with the slabs, the other auxiliary arrays are prefetched into
+// L2.
 //   A  per-cell primitive records (rho, rho*u, rho*v, rho*E, u, v, p, H,
 //      sqrt(rho)) of the patches and strips, and the (n+1)^2 bilinear nodes
 //   B  every face flux once (interior faces first, then the 4n edge faces;
 //      a coarse quad's hanging edge evaluates two fluxes per edge cell)
-//   C  each cell's residual in exactly the reference's accumulation order
-//      -- edge-face contributions in face_info order, then -F(x-1/2)
-//      +F(x+1/2) -F(y-1/2) +F(y+1/2) -- divided by the volume, negated,
-//      and the stage update.
+//   C  each cell's residual -- in the FP64 form in exactly the reference's
+//      accumulation order (edge-face contributions in face_info order, then
+//      -F(x-1/2) +F(x+1/2) -F(y-1/2) +F(y+1/2)); in the FP32 form the four
+//      faces alike, edges included, plus a coarse hanging edge's second flux
+//      -- divided by the volume, negated, and the stage update.
 // Edge fluxes are computed by both patches that share an edge, so there are
 // no atomics and both sides see bit-identical values; conservation holds
 // exactly as in the reference.
@@ -218,6 +220,9 @@ struct StageSmem {
     static constexpr size_t bar = 32;
     static constexpr size_t desc = al(sizeof(QuadDesc) * QPB) * 3;
     static constexpr size_t raw = al(sizeof(double) * QPB * 4 * NN) * 2;
+    // FP32 form: the stage's first own-cell auxiliary input (Q0 of the
+    // Shu-Osher stages) arrives with the slabs, double-buffered
+    static constexpr size_t aux = F32 ? al(sizeof(double) * QPB * 4 * NN) * 2 : 0;
     static constexpr size_t rstrip = al(sizeof(double) * QPB * 4 * NSTRIP) * 2;
     static constexpr size_t prim = al(sizeof(R) * QPB * RecTraits<F32>::n * NPC);
     static constexpr size_t nodes = F32 ? 0 : al(sizeof(double) * QPB * NP1 * NP1 * 2);
@@ -229,7 +234,8 @@ struct StageSmem {
     static constexpr size_t red = sizeof(double) * 64;
     static constexpr size_t o_desc = bar;
     static constexpr size_t o_raw = o_desc + desc;
-    static constexpr size_t o_rstrip = o_raw + raw;
+    static constexpr size_t o_aux = o_raw + raw;
+    static constexpr size_t o_rstrip = o_aux + aux;
     static constexpr size_t o_prim = o_rstrip + rstrip;
     static constexpr size_t o_nodes = o_prim + prim;
     static constexpr size_t o_geo = o_nodes + nodes;
@@ -269,6 +275,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     QuadDesc *sdesc = reinterpret_cast<QuadDesc *>(smem + S::o_desc);
     double *sraw = reinterpret_cast<double *>(smem + S::o_raw);
+    double *saux = reinterpret_cast<double *>(smem + S::o_aux);
     double *srstrip = reinterpret_cast<double *>(smem + S::o_rstrip);
     R *prim = reinterpret_cast<R *>(smem + S::o_prim);
     double *nodes = reinterpret_cast<double *>(smem + S::o_nodes);
@@ -279,6 +286,8 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
     double *red = reinterpret_cast<double *>(smem + S::o_red);
     constexpr size_t desc_slot = S::desc / 3 / sizeof(QuadDesc);   // QuadDesc entries per slot
     constexpr size_t raw_slot = S::raw / 2 / sizeof(double);
+    constexpr size_t aux_slot = S::aux / 2 / sizeof(double);
+    const bool stage_a0 = F32 && a.a0 != nullptr;
     constexpr size_t rstrip_slot = S::rstrip / 2 / sizeof(double);
 
     const int tid = threadIdx.x;
@@ -360,13 +369,21 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             uint64_t *bar = &bars[it & 1];
             int nq = (it < niter) ? min(QPB, a.nquad - gg * QPB) : 0;
             int nq1 = (it + 1 < niter) ? min(QPB, a.nquad - gn * QPB) : 0;
-            unsigned bytes = (unsigned)(nq * 4 * NN * sizeof(double) + nq1 * sizeof(QuadDesc));
+            unsigned bytes = (unsigned)(nq * 4 * NN * sizeof(double) * (stage_a0 ? 2 : 1) +
+                                        nq1 * sizeof(QuadDesc));
             mbar_arrive_expect_tx(bar, bytes);
             double *dst = sraw + (size_t)(it & 1) * raw_slot;
             for (int ql = 0; ql < nq; ++ql)
                 for (int f = 0; f < 4; ++f)
                     bulk_g2s(dst + (ql * 4 + f) * NN, a.qin + f * stride + (long long)(gg * QPB + ql) * NN,
                              (unsigned)(NN * sizeof(double)), bar);
+            if (stage_a0) {
+                double *dsta = saux + (size_t)(it & 1) * aux_slot;
+                for (int ql = 0; ql < nq; ++ql)
+                    for (int f = 0; f < 4; ++f)
+                        bulk_g2s(dsta + (ql * 4 + f) * NN, a.a0 + f * stride + (long long)(gg * QPB + ql) * NN,
+                                 (unsigned)(NN * sizeof(double)), bar);
+            }
             if (nq1 > 0)
                 bulk_g2s(sdesc + (size_t)((it + 1) % 3) * desc_slot, a.quads + (long long)gn * QPB,
                          (unsigned)(nq1 * sizeof(QuadDesc)), bar);
@@ -413,7 +430,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                     int ql = r / (4 * LINES);
                     int f = (r / LINES) % 4;
                     int ln = r % LINES;
-                    const double *base = which ? a.a1 : a.a0;
+                    const double *base = which ? a.a1 : (stage_a0 ? nullptr : a.a0);
                     if (!base || gg * QPB + ql >= a.nquad) continue;
                     prefetch_l2(base + f * stride + (long long)(gg * QPB + ql) * NN + ln * 16);
                 }
@@ -434,6 +451,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
 
         const QuadDesc *sq = sdesc + (size_t)(it % 3) * desc_slot;
         const double *raw = sraw + (size_t)(it & 1) * raw_slot;
+        const double *aux = saux + (size_t)(it & 1) * aux_slot;
         const double *rstrip = srstrip + (size_t)(it & 1) * rstrip_slot;
 
         // ---------------- phase A: per-cell records, per-quad geometry
@@ -557,6 +575,13 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             } else {
                 R qin[4] = {(R)a.qinflow[0], (R)a.qinflow[1], (R)a.qinflow[2], (R)a.qinflow[3]};
                 FluxOps::bc(bcv, Lp, n0, n1, qin, fl);
+                // FP32 form: a low-side boundary face is stored with the
+                // sign of the interior faces' convention (flux towards +x /
+                // +y), so that every cell sums its four faces alike
+                if (F32 && fa == 0) {
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) fl[f] = -fl[f];
+                }
             }
             if (xd) store_flux<F32>(fx, (ql * N + fb) * NP1 + fa, fl);
             else store_flux<F32>(fy, (ql * NP1 + fa) * N + fb, fl);
@@ -602,53 +627,79 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             const QuadDesc &qd = sq[ql];
             double r[4] = {0.0, 0.0, 0.0, 0.0};
             double F[4];
-            int sx = (i == 0) ? 0 : (i == N - 1) ? 1 : -1;
-            int sy = (j == 0) ? 2 : (j == N - 1) ? 3 : -1;
-            int first = sx, second = sy;
-            if (sx >= 0 && sy >= 0 && qd.side[sy].rank < qd.side[sx].rank) { first = sy; second = sx; }
+            if constexpr (F32) {
+                // FP32-flux form: -F(x-1/2) +F(x+1/2) -F(y-1/2) +F(y+1/2),
+                // edge faces included (low-side boundary faces were stored
+                // negated), summed in FP64; a coarse hanging edge adds its
+                // second flux with the edge's sign.
+                double G[4];
+                load_flux<F32>(fx, (ql * N + j) * NP1 + i, F);
+                load_flux<F32>(fx, (ql * N + j) * NP1 + i + 1, G);
 #pragma unroll
-            for (int pass = 0; pass < 2; ++pass) {
-                int s = pass == 0 ? first : second;
-                if (s < 0) continue;
-                int kind = qd.side[s].kind;
-                int m = (s < 2) ? j : i;
-                if (s < 2) load_flux<F32>(fx, (ql * N + j) * NP1 + (s == 0 ? 0 : N), F);
-                else load_flux<F32>(fy, (ql * NP1 + (s == 2 ? 0 : N)) * N + i, F);
-                double F2[4] = {0.0, 0.0, 0.0, 0.0};
-                if (kind == kSideCoarseHang) load_flux<F32>(fh, (ql * 4 + s) * N + m, F2);
-                if (kind == kSideBoundary || (s & 1)) {
+                for (int f = 0; f < 4; ++f) r[f] = G[f] - F[f];
+                load_flux<F32>(fy, (ql * NP1 + j) * N + i, F);
+                load_flux<F32>(fy, (ql * NP1 + j + 1) * N + i, G);
 #pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        r[f] = r[f] + F[f];
-                        if (kind == kSideCoarseHang) r[f] = r[f] + F2[f];
-                    }
-                } else {
+                for (int f = 0; f < 4; ++f) r[f] = (r[f] - F[f]) + G[f];
+                if (any_hang) {
 #pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        r[f] = r[f] - F[f];
-                        if (kind == kSideCoarseHang) r[f] = r[f] - F2[f];
+                    for (int s = 0; s < 4; ++s) {
+                        const bool on = (s == 0) ? i == 0 : (s == 1) ? i == N - 1 : (s == 2) ? j == 0 : j == N - 1;
+                        if (!on || qd.side[s].kind != kSideCoarseHang) continue;
+                        load_flux<F32>(fh, (ql * 4 + s) * N + ((s < 2) ? j : i), F);
+#pragma unroll
+                        for (int f = 0; f < 4; ++f) r[f] = (s & 1) ? r[f] + F[f] : r[f] - F[f];
                     }
                 }
-            }
-            if (i > 0) {
-                load_flux<F32>(fx, (ql * N + j) * NP1 + i, F);
+            } else {
+                int sx = (i == 0) ? 0 : (i == N - 1) ? 1 : -1;
+                int sy = (j == 0) ? 2 : (j == N - 1) ? 3 : -1;
+                int first = sx, second = sy;
+                if (sx >= 0 && sy >= 0 && qd.side[sy].rank < qd.side[sx].rank) { first = sy; second = sx; }
 #pragma unroll
-                for (int f = 0; f < 4; ++f) r[f] = r[f] - F[f];
-            }
-            if (i < N - 1) {
-                load_flux<F32>(fx, (ql * N + j) * NP1 + i + 1, F);
+                for (int pass = 0; pass < 2; ++pass) {
+                    int s = pass == 0 ? first : second;
+                    if (s < 0) continue;
+                    int kind = qd.side[s].kind;
+                    int m = (s < 2) ? j : i;
+                    if (s < 2) load_flux<F32>(fx, (ql * N + j) * NP1 + (s == 0 ? 0 : N), F);
+                    else load_flux<F32>(fy, (ql * NP1 + (s == 2 ? 0 : N)) * N + i, F);
+                    double F2[4] = {0.0, 0.0, 0.0, 0.0};
+                    if (kind == kSideCoarseHang) load_flux<F32>(fh, (ql * 4 + s) * N + m, F2);
+                    if (kind == kSideBoundary || (s & 1)) {
 #pragma unroll
-                for (int f = 0; f < 4; ++f) r[f] = r[f] + F[f];
-            }
-            if (j > 0) {
-                load_flux<F32>(fy, (ql * NP1 + j) * N + i, F);
+                        for (int f = 0; f < 4; ++f) {
+                            r[f] = r[f] + F[f];
+                            if (kind == kSideCoarseHang) r[f] = r[f] + F2[f];
+                        }
+                    } else {
 #pragma unroll
-                for (int f = 0; f < 4; ++f) r[f] = r[f] - F[f];
-            }
-            if (j < N - 1) {
-                load_flux<F32>(fy, (ql * NP1 + j + 1) * N + i, F);
+                        for (int f = 0; f < 4; ++f) {
+                            r[f] = r[f] - F[f];
+                            if (kind == kSideCoarseHang) r[f] = r[f] - F2[f];
+                        }
+                    }
+                }
+                if (i > 0) {
+                    load_flux<F32>(fx, (ql * N + j) * NP1 + i, F);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) r[f] = r[f] + F[f];
+                    for (int f = 0; f < 4; ++f) r[f] = r[f] - F[f];
+                }
+                if (i < N - 1) {
+                    load_flux<F32>(fx, (ql * N + j) * NP1 + i + 1, F);
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) r[f] = r[f] + F[f];
+                }
+                if (j > 0) {
+                    load_flux<F32>(fy, (ql * NP1 + j) * N + i, F);
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) r[f] = r[f] - F[f];
+                }
+                if (j < N - 1) {
+                    load_flux<F32>(fy, (ql * NP1 + j + 1) * N + i, F);
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) r[f] = r[f] + F[f];
+                }
             }
             double vol;
             double kv[4];
@@ -667,6 +718,12 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             }
 
             const long long gi = (long long)(q0 + ql) * NN + c;
+            // the first auxiliary input: staged in shared memory (FP32 form)
+            // or read from HBM
+            auto A0 = [&](int f) -> double {
+                if constexpr (F32) return aux[(ql * 4 + f) * NN + c];
+                else return a.a0[f * stride + gi];
+            };
             double q0v[4], qn[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) q0v[f] = raw[(ql * 4 + f) * NN + c];
@@ -694,7 +751,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 } else {
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
-                        qn[f] = a.a0[f * stride + gi] + beta2 * kv[f];
+                        qn[f] = A0(f) + beta2 * kv[f];
                         a.out0[f * stride + gi] = qn[f];
                     }
                 }
@@ -713,7 +770,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 } else if (a.stage == 2) {
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
-                        double Q0 = a.a0[f * stride + gi];
+                        double Q0 = A0(f);
                         double k1 = a.a1[f * stride + gi];
                         qn[f] = Q0 + alpha21 * k1 + alpha22 * kv[f];
                         double C = Q0 + beta1 * k1 + beta2 * kv[f];
@@ -723,7 +780,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 } else {
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
-                        qn[f] = a.a0[f * stride + gi] + beta3 * kv[f];
+                        qn[f] = A0(f) + beta3 * kv[f];
                         a.out0[f * stride + gi] = qn[f];
                     }
                 }
@@ -742,7 +799,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                     double al = (a.stage == 2) ? alpha2 : alpha3;
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
-                        double Q0 = a.a0[f * stride + gi];
+                        double Q0 = A0(f);
                         double K = a.a1[f * stride + gi];
                         qn[f] = Q0 + al * kv[f];
                         a.out0[f * stride + gi] = qn[f];
@@ -751,7 +808,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 } else {
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
-                        double Q0 = a.a0[f * stride + gi];
+                        double Q0 = A0(f);
                         double K = a.a1[f * stride + gi];
                         qn[f] = Q0 + beta1 * (K + kv[f]);
                         a.out0[f * stride + gi] = qn[f];
@@ -764,7 +821,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 lserk_coeff(a.stage, ra, rb);
 #pragma unroll
                 for (int f = 0; f < 4; ++f) {
-                    double qsv = (a.stage == 1) ? dt * kv[f] : a.a0[f * stride + gi] * ra + dt * kv[f];
+                    double qsv = (a.stage == 1) ? dt * kv[f] : A0(f) * ra + dt * kv[f];
                     qn[f] = q0v[f] + rb * qsv;
                     a.out1[f * stride + gi] = qsv;
                     a.out0[f * stride + gi] = qn[f];
@@ -778,13 +835,13 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
                 } else if (a.stage == 2) {
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
-                        qn[f] = 0.75 * a.a0[f * stride + gi] + 0.25 * (q0v[f] + dt * kv[f]);
+                        qn[f] = 0.75 * A0(f) + 0.25 * (q0v[f] + dt * kv[f]);
                         a.out0[f * stride + gi] = qn[f];
                     }
                 } else {
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
-                        qn[f] = (1.0 / 3.0) * a.a0[f * stride + gi] + (2.0 / 3.0) * (q0v[f] + dt * kv[f]);
+                        qn[f] = (1.0 / 3.0) * A0(f) + (2.0 / 3.0) * (q0v[f] + dt * kv[f]);
                         a.out0[f * stride + gi] = qn[f];
                     }
                 }
@@ -808,8 +865,10 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
     }
 
     // ---------------- block reductions: CFL min (one atomic per block), the
-    // residual norm (per-block partials summed in block order by the last
-    // block to finish, so the result does not depend on scheduling), flags.
+    // residual norm (per-block partials, summed by the last block to finish
+    // in a fixed order -- strided per thread, then warp and block trees -- so
+    // the result does not depend on scheduling), flags.
+    __shared__ int s_last;
     const int lane = tid & 31, warp = tid >> 5;
     int wflags = __reduce_or_sync(0xffffffffu, my_flags);
     if (wflags && lane == 0) atomicOr(&a.scal->flags, wflags);
@@ -828,15 +887,23 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
             atomicMin(&a.scal->slot[a.slot_write].dt_bits, (unsigned long long)__double_as_longlong(bmin));
         a.partials[blockIdx.x] = bsum;
         __threadfence();
-        unsigned ticket = atomicAdd(&a.scal->done_blocks, 1u);
-        if (ticket == gridDim.x - 1) {
-            __threadfence();
-            double tot = 0.0;
-            for (int b = 0; b < (int)gridDim.x; ++b) tot += ((volatile double *)a.partials)[b];
-            a.scal->norm_sq = tot;
-            if (!isfinite(tot)) atomicOr(&a.scal->flags, kFlagNonFinite);
-            a.scal->done_blocks = 0u;
-        }
+        const unsigned ticket = atomicAdd(&a.scal->done_blocks, 1u);
+        s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double part = 0.0;
+    for (int b = tid; b < (int)gridDim.x; b += T) part += __ldcg(a.partials + b);
+    part = warp_sum(part);
+    if (lane == 0) red[warp] = part;
+    __syncthreads();
+    if (tid == 0) {
+        double tot = red[0];
+        for (int w = 1; w < T / 32; ++w) tot += red[w];
+        a.scal->norm_sq = tot;
+        if (!isfinite(tot)) atomicOr(&a.scal->flags, kFlagNonFinite);
+        a.scal->done_blocks = 0u;
     }
 }
 
