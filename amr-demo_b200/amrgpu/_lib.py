@@ -15,6 +15,8 @@ _lib = None
 i32p = C.POINTER(C.c_int)
 i64p = C.POINTER(C.c_int64)
 f64p = C.POINTER(C.c_double)
+f32p = C.POINTER(C.c_float)
+u16p = C.POINTER(C.c_uint16)
 
 
 class ConfigStruct(C.Structure):
@@ -47,6 +49,12 @@ class MeshStruct(C.Structure):
 
     _fields_ = [("ncell", C.c_int), ("nghost", C.c_int), ("nface", C.c_int), ("dof", C.c_int),
                 ("cell_info", i32p), ("face_info", i32p), ("geom", f64p)]
+
+
+class JudgeStruct(C.Structure):
+    """amrgpu_judge_t."""
+
+    _fields_ = [("judged", C.c_int), ("disagree", C.c_int), ("rate", C.c_double)]
 
 
 class ReportStruct(C.Structure):
@@ -113,6 +121,23 @@ PROTOTYPES = {
     "amrgpu_forest_external": (C.c_int, [C.c_void_p, C.c_int, C.c_int, i32p, i32p, f64p, i32p, i32p]),
     "amrgpu_forest_quad_h": (C.c_double, [C.c_void_p, C.c_int]),
     "amrgpu_forest_initialize": (C.c_int, [C.c_void_p, C.c_int, f64p]),
+    # learned refinement indicator
+    "amrgpu_mlp_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_ulonglong]),
+    "amrgpu_mlp_destroy": (None, [C.c_void_p]),
+    "amrgpu_mlp_get_params": (C.c_int, [C.c_void_p, f32p]),
+    "amrgpu_mlp_set_params": (C.c_int, [C.c_void_p, f32p]),
+    "amrgpu_session_features": (C.c_int, [C.c_void_p, u16p]),
+    "amrgpu_session_jumps": (C.c_int, [C.c_void_p, f64p]),
+    "amrgpu_mlp_dataset_append": (C.c_longlong, [C.c_void_p, C.c_void_p, C.c_double, C.c_double]),
+    "amrgpu_mlp_dataset_relabel": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_double]),
+    "amrgpu_mlp_dataset_size": (C.c_longlong, [C.c_void_p]),
+    "amrgpu_mlp_dataset_clear": (C.c_int, [C.c_void_p]),
+    "amrgpu_mlp_dataset_labels": (C.c_int, [C.c_void_p, i32p, C.c_longlong]),
+    "amrgpu_mlp_train_epoch": (C.c_int, [C.c_void_p, i32p, C.c_longlong, C.c_int, C.c_float, C.c_float, f64p, f64p]),
+    "amrgpu_mlp_grad": (C.c_int, [C.c_void_p, u16p, i32p, C.c_int, f32p, f32p, f64p]),
+    "amrgpu_mlp_predict": (C.c_int, [C.c_void_p, u16p, C.c_int, f32p]),
+    "amrgpu_session_learned_tags": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_ulonglong, C.c_double,
+                                              C.c_double, i32p, C.c_void_p]),
     # allocation-free entry point
     "amrgpu_totals_noalloc": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p, C.c_int, C.c_int, f64p,
                                         C.c_void_p]),

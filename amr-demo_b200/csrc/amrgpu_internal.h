@@ -85,6 +85,24 @@ int parse_physics_file(const char *path, PhysicsConfig &cfg);
 
 // ---------------------------------------------------------------- errors
 void set_error(int code, const std::string &msg);
+
+// Device-side view of a session's current state for kernels outside
+// session.cu (the learned indicator): patch size, quads, SoA state (field
+// stride in doubles), quad descriptors and the session's stream.
+struct QuadDesc;
+struct SessionView {
+    int n;
+    int nquad;
+    long long stride;
+    const double *q;
+    const QuadDesc *quads;
+    void *stream;  // cudaStream_t
+};
+bool session_view(amrgpu_session_t *s, SessionView *v);
+void session_count_launches(amrgpu_session_t *s, int k);
+// Device scratch owned by the session, grown (never shrunk) to `bytes`;
+// contents are not kept across calls. Null when the allocation fails.
+void *session_scratch(amrgpu_session_t *s, size_t bytes);
 int last_error();
 
 // ---------------------------------------------------------------- host ICs

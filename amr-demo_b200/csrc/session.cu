@@ -101,6 +101,8 @@ struct amrgpu_session {
     int *d_tags = nullptr;
     int *d_kind = nullptr;
     int *d_src = nullptr;
+    void *d_scratch = nullptr;  // scratch of kernels outside this file (session_scratch)
+    size_t scratch_bytes = 0;
     const void *occ_kernel = nullptr;  // launch whose occupancy occ_per_sm is
     int occ_per_sm = 0;
     cudaStream_t stream = nullptr;
@@ -470,6 +472,7 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_tags);
     cudaFree(s->d_kind);
     cudaFree(s->d_src);
+    cudaFree(s->d_scratch);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -683,6 +686,46 @@ int amrgpu_session_cells(const amrgpu_session_t *s) { return s ? int((long long)
 void *amrgpu_session_stream(amrgpu_session_t *s) { return s ? (void *)s->stream : nullptr; }
 
 int64_t amrgpu_session_launch_count(const amrgpu_session_t *s) { return s ? s->launches : 0; }
+
+}  // extern "C"
+
+namespace amrgpu {
+
+bool session_view(amrgpu_session_t *s, SessionView *v)
+{
+    if (!s || !v) return false;
+    v->n = s->n;
+    v->nquad = s->nquad;
+    v->stride = s->stride;
+    v->q = rolebuf(s, RX);
+    v->quads = s->d_quads;
+    v->stream = s->stream;
+    return true;
+}
+
+void *session_scratch(amrgpu_session_t *s, size_t bytes)
+{
+    if (!s) return nullptr;
+    if (bytes > s->scratch_bytes) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->d_scratch);
+        s->d_scratch = nullptr;
+        s->scratch_bytes = 0;
+        const size_t want = bytes + bytes / 4;
+        if (cudaMalloc(&s->d_scratch, want) != cudaSuccess) return nullptr;
+        s->scratch_bytes = want;
+    }
+    return s->d_scratch;
+}
+
+void session_count_launches(amrgpu_session_t *s, int k)
+{
+    if (s) s->launches += k;
+}
+
+}  // namespace amrgpu
+
+extern "C" {
 
 int amrgpu_session_totals(amrgpu_session_t *s, double totals[4])
 {

@@ -14,6 +14,10 @@ fused stage kernels, the next step's CFL minimum folded into the last one).
           10-step segment (the reference example's regrid interval), H2D
           and D2H of the whole state inside the timed region
   forms : the plain FP64 form (bit-exact with the reference) beside it
+  learned_amr : the metric's own comparison on an adaptive workload --
+          learned indicator + FP32-flux form against plain indicator +
+          plain FP64 form, at (measured) equal L1(rho), regrid time
+          included; the model is trained on the GPU in the same run
 
 `--impl reference` times the reference's own CPU path (its C driver over
 the restated Fortran kernels, oracle/_ref) on all host cores instead.
@@ -231,6 +235,59 @@ def traffic_per_launch(form):
     return v.get("dram_bytes_per_launch") if v else None
 
 
+def learned_amr(args):
+    """The metric's comparison on an adaptive workload: the learned
+    indicator with the FP32-flux form (regrid every 10 steps, the model
+    trained on look-ahead labels 10 steps ahead) against the plain
+    indicator with the plain FP64 form (regrid every 5 steps), on unseen
+    seeds of the vortex family under AMR (levels 3-6, 8x8 patches,
+    relative density-jump tolerance 0.02, t = 3). Rates include the regrid
+    time; L1(rho) is measured against the exact translated vortex and
+    between the two runs on the level-6 uniform grid."""
+    import numpy as np
+    from amrgpu import learned as L
+    n, lo, hi, tol = 8, 3, 6, 0.02
+    t0 = time.perf_counter()
+    m = L.Mlp(seed=0)
+    rows = L.collect(m, range(32), n, lo, hi, tol, regrid_interval=10, regrids=25, lookahead=True)
+    t1 = time.perf_counter()
+    hist, _ = L.train(m, epochs=20, batch=4096, lr=1e-3, seed=0)
+    t2 = time.perf_counter()
+    out = {"workload": "isentropic vortex family under AMR, periodic [0,10]^2, levels 3-6, 8x8 patches, "
+                       "density-jump tol 0.02, SSP-RK3 CFL 0.5, t = 3, unseen seeds 5000-5002",
+           "training": {"rows": rows, "epochs": 20, "batch": 4096, "lr": 1e-3, "collect_s": t1 - t0,
+                        "train_s": t2 - t1, "final_loss": hist[-1][0], "final_accuracy": hist[-1][1]}}
+    runs = {"plain_fp64": [], "learned_fp32": []}
+    for seed in (5000, 5001, 5002):
+        ends = {}
+        for key, mlp, form, ri in (("plain_fp64", None, 0, 5), ("learned_fp32", m, 1, 10)):
+            f, cfg, soln, par = L.vortex_amr(seed, n, lo, hi, tol, form=form)
+            s, r = L.run(f, soln, n, cfg, final_time=3.0, regrid_interval=ri, min_level=lo, max_level=hi, tol=tol,
+                         mlp=mlp, form=form, seed=seed)
+            q = s.download()
+            r["l1_rho_vs_exact"] = L.l1_rho_vs_exact(s.mesh, q, n, r["time"], par)
+            ends[key] = L.to_uniform(f, q, n, hi)
+            runs[key].append(r)
+            s.close()
+        d = float(np.abs(ends["learned_fp32"] - ends["plain_fp64"]).sum() / np.abs(ends["plain_fp64"]).sum())
+        runs["learned_fp32"][-1]["l1_rho_vs_plain_run"] = d
+    for key, rs in runs.items():
+        cu = sum(r["cell_updates"] for r in rs)
+        secs = sum(r["solve_s"] + r["regrid_s"] for r in rs)
+        out[key] = {"value": cu / secs, "unit": UNIT, "regrid_interval": 5 if key == "plain_fp64" else 10,
+                    "mean_cells": float(np.mean([r["mean_cells"] for r in rs])),
+                    "l1_rho_vs_exact": float(np.mean([r["l1_rho_vs_exact"] for r in rs])),
+                    "regrids": int(sum(r["regrids"] for r in rs)),
+                    "solve_s": sum(r["solve_s"] for r in rs), "regrid_s": sum(r["regrid_s"] for r in rs)}
+    lr = runs["learned_fp32"]
+    out["learned_fp32"].update({"judge_disagreement": float(np.mean([r["disagree_rate"] for r in lr])),
+                                "fallbacks": [r["fallback_at"] for r in lr],
+                                "l1_rho_vs_plain_run": float(np.mean([r["l1_rho_vs_plain_run"] for r in lr]))})
+    out["speedup_learned_fp32_over_plain_fp64"] = out["learned_fp32"]["value"] / out["plain_fp64"]["value"]
+    m.close()
+    return out
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -299,6 +356,9 @@ def run_gpu(args):
     e2e = None
     if not args.no_e2e:
         e2e = e2e_form(ag, mesh, cfg, s0, 1, args.steps, args.segment)
+    amr = None
+    if not args.no_learned and rank == 0:
+        amr = learned_amr(args)
 
     if rank != 0:
         if world > 1:
@@ -329,6 +389,7 @@ def run_gpu(args):
             "l1_rho_rel_fp32_vs_fp64": l1,
         },
         "e2e": e2e,
+        "learned_amr": amr,
         "clocks": clocks,
         "gpu_launches": int(out[0]["launches"] + out[1]["launches"]),
         "cpu_baseline": cpu,
@@ -371,6 +432,7 @@ def main():
     ap.add_argument("--level", type=int, default=6, help="forest level (6: the 1024^2 workload)")
     ap.add_argument("--form", type=int, default=-1, help="time one form only (0 FP64, 1 FP32 flux)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator AMR comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

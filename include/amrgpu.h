@@ -262,6 +262,68 @@ int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int
 int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int *kind,
                           const int *src_index);
 
+/* ---------------- learned refinement indicator ---------------- */
+/* No counterpart in the reference: a 400-128-64-3 MLP (GELU) over a patch's
+ * normalised conserved variables (8x8 patch, n = 16 patches box-averaged,
+ * plus a one-cell neighbour ring) that classifies a quad as 0 = coarsen
+ * candidate, 1 = refine, 2 = keep, in place of the plain tagger
+ * (solver_tag_feature.F90:9-52 behind hpc_amr_tag_feature,
+ * amr_external.h:92). BF16 weights, FP32 accumulation on the tensor cores
+ * (tcgen05), AdamW on FP32 master weights; trained on (patch, plain-label)
+ * pairs on the GPU. Plain label: J = largest relative density jump of the
+ * quad (tag method 5's quantity); refine if J >= tol, coarsen if
+ * J < lo_frac*tol, keep otherwise. */
+typedef struct amrgpu_mlp amrgpu_mlp_t;
+#define AMRGPU_MLP_INPUTS 400
+#define AMRGPU_MLP_PARAMS 59779
+typedef struct {
+    int judged;       /* quads the plain indicator re-scored */
+    int disagree;     /* of those, where the learned class differs */
+    double rate;      /* disagree / judged (0 when none judged) */
+} amrgpu_judge_t;
+int amrgpu_mlp_create(amrgpu_mlp_t **out, unsigned long long seed);
+void amrgpu_mlp_destroy(amrgpu_mlp_t *m);
+/* FP32 parameters, flat: W1[128x400], b1[128], W2[64x128], b2[64], W3[3x64], b3[3]
+ * (row-major, W[out][in]); set_params also resets the optimiser state. */
+int amrgpu_mlp_get_params(amrgpu_mlp_t *m, float *params);
+int amrgpu_mlp_set_params(amrgpu_mlp_t *m, const float *params);
+/* Features of every quad of a session's state: nquad x 400 BF16 bit patterns. */
+int amrgpu_session_features(amrgpu_session_t *s, uint16_t *features);
+/* Largest relative density jump J of every quad. */
+int amrgpu_session_jumps(amrgpu_session_t *s, double *jumps);
+/* Appends the features and plain labels of every quad of the session to
+ * the model's device dataset; returns the dataset size or a negative error. */
+long long amrgpu_mlp_dataset_append(amrgpu_mlp_t *m, amrgpu_session_t *s, double tol, double lo_frac);
+/* Recomputes the labels of rows [first, first + nquad) from the session's
+ * current state (the session must hold the mesh those rows came from):
+ * labels that look ahead to a later state of the same mesh. */
+int amrgpu_mlp_dataset_relabel(amrgpu_mlp_t *m, amrgpu_session_t *s, long long first, double tol,
+                               double lo_frac);
+long long amrgpu_mlp_dataset_size(const amrgpu_mlp_t *m);
+int amrgpu_mlp_dataset_clear(amrgpu_mlp_t *m);
+/* Labels of the dataset rows [0, n). */
+int amrgpu_mlp_dataset_labels(amrgpu_mlp_t *m, int *labels, long long n);
+/* One pass of AdamW (beta 0.9/0.999, eps 1e-8, decay on weights only) over
+ * the dataset rows in the order perm[0..n), batches of `batch` rows (a
+ * multiple of 128; a final partial batch is dropped); mean loss and
+ * accuracy of the pass. */
+int amrgpu_mlp_train_epoch(amrgpu_mlp_t *m, const int *perm, long long n, int batch, float lr,
+                           float weight_decay, double *mean_loss, double *accuracy);
+/* Forward and backward of one batch (a multiple of 8 rows) given on the
+ * host, no update: logits
+ * [B x 3], the flat gradient of the mean cross-entropy (AMRGPU_MLP_PARAMS
+ * floats) and the mean loss. */
+int amrgpu_mlp_grad(amrgpu_mlp_t *m, const uint16_t *features, const int *labels, int batch,
+                    float *logits, float *grad, double *mean_loss);
+/* Logits [B x 3] of features given on the host. */
+int amrgpu_mlp_predict(amrgpu_mlp_t *m, const uint16_t *features, int batch, float *logits);
+/* Learned classes of every quad of the session (tags = class index). The
+ * plain indicator re-scores the quads selected by a hash of (seed, quad)
+ * below judge_fraction and the agreement is returned in judge. */
+int amrgpu_session_learned_tags(amrgpu_session_t *s, amrgpu_mlp_t *m, double judge_fraction,
+                                unsigned long long seed, double tol, double lo_frac, int *tags,
+                                amrgpu_judge_t *judge);
+
 /* ---------------- allocation-free entry point ---------------- */
 /* No counterpart in the reference. Conservation totals sum(vol*Q_f), f =
  * 0..3, of a device-resident SoA state, like amrgpu_session_totals, for
