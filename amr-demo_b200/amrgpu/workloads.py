@@ -57,6 +57,27 @@ def four_quadrant(seed=0, min_level=4, max_level=9, n=16, form=1, jump_tol=0.05,
     return f, f.mesh(n), cfg, soln
 
 
+def shock_bubble(seed=0, min_level=5, max_level=11, n=16, form=1, jump_tol=0.1, time_scheme=3):
+    """Shock-bubble interaction on [0,2]x[0,1] (a brick of 2x1 trees):
+    ambient (rho,p) = (1,1) at rest, a Mach-2 planar shock at x = 0.1
+    entering from the left (post-shock state from the Rankine-Hugoniot
+    relations, also the inflow state of the left boundary, bc 3), a bubble
+    of density 0.1375 and radius 0.2 in pressure equilibrium, centre
+    ~ U([0.6,0.9]x[0.4,0.6]) from the seed; outflow (bc 0) on the right,
+    slip walls top and bottom; density-jump tagging (method 5) from
+    min_level to max_level; SSP-RK3, CFL 0.5. Returns the forest after the
+    start-up refinement, its mesh, the configuration and the state."""
+    from .amr import host_tags, initial_forest
+    cfg = Config.from_input(cfl=0.5, time_scheme=time_scheme, nelem_subgrid=n, coarse_grid_h=1.0,
+                            initial_condition=5, time_steps=10 ** 9, dt=1.0, bc=[3, 0, 1, 1, 1, 1], gamma=1.4,
+                            ic_seed=seed, ic_params=[2.0, 0.1, 0.1375, 0.2], form=form, amr_ntag_methods=1,
+                            amr_tag_methods=[5, 0, 0, 0, 0], amr_tag_tolerances=[jump_tol, 0, 0, 0, 0])
+    cfg.apply()
+    f = Forest(2, 1, periodic=(0, 0), lo=(0.0, 0.0, 0.0), scale=1.0, level=min_level)
+    soln = initial_forest(f, n, max_level, host_tags(n, jump_tol, 5), cfg)
+    return f, f.mesh(n), cfg, soln
+
+
 def vortex_exact(mesh, t, n=16, beta=5.0, a=0.5, center=(5.0, 5.0), L=10.0):
     """Exact translated vortex at time t (periodic images summed over the
     nearest copy), AoS like the solver state."""

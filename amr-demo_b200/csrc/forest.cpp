@@ -27,12 +27,47 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace amrgpu {
 
 namespace {
+
+// Host threads for the forest's per-leaf loops: AMRGPU_HOST_THREADS, else
+// the hardware's count, at most 16.
+int host_threads()
+{
+    static const int n = [] {
+        if (const char *e = std::getenv("AMRGPU_HOST_THREADS")) {
+            const int v = std::atoi(e);
+            if (v >= 1) return std::min(v, 64);
+        }
+        const unsigned hw = std::thread::hardware_concurrency();
+        return int(std::max(1u, std::min(hw, 16u)));
+    }();
+    return n;
+}
+
+// fn(begin, end, chunk) over [0, n) in contiguous chunks, one thread each;
+// one chunk (no thread) below `grain` items per thread.
+template <typename Fn>
+int parallel_chunks(size_t n, size_t grain, Fn fn)
+{
+    int nt = int(std::min<size_t>(size_t(host_threads()), std::max<size_t>(1, n / std::max<size_t>(grain, 1))));
+    if (nt <= 1) {
+        fn(size_t(0), n, 0);
+        return 1;
+    }
+    std::vector<std::thread> th;
+    th.reserve(size_t(nt));
+    for (int c = 0; c < nt; ++c)
+        th.emplace_back(fn, n * size_t(c) / size_t(nt), n * size_t(c + 1) / size_t(nt), c);
+    for (auto &t : th) t.join();
+    return nt;
+}
 
 constexpr int kMaxLevel = 30;
 constexpr int64_t kRootLen = int64_t(1) << kMaxLevel;
@@ -324,29 +359,37 @@ int forest_balance(Forest *f)
     // (flag itself); the children it creates are the next pass's dirty set.
     // The result is the same minimal balanced refinement as checking every
     // leaf on every pass.
+    // The checks of one pass only read the forest: they run on host threads
+    // over the dirty leaves, each thread listing the leaves it flags.
     for (int iter = 0; iter < 64; ++iter) {
         f->rebuild_keys();
         const size_t nl = f->leaves.size();
+        std::vector<int> dirty;
+        for (size_t i = 0; i < nl; ++i)
+            if (f->leaves[i].dirty) dirty.push_back(int(i));
+        std::vector<std::vector<int>> hits((size_t)host_threads());
+        parallel_chunks(dirty.size(), 512, [&](size_t b, size_t e, int t) {
+            std::vector<int> &h = hits[size_t(t)];
+            for (size_t k = b; k < e; ++k) {
+                const int i = dirty[k];
+                const Leaf &q = f->leaves[size_t(i)];
+                if (q.level >= 2)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            if (!dx && !dy) continue;
+                            const int c = f->too_coarse_neighbour(q, dx, dy);
+                            if (c >= 0) h.push_back(c);
+                        }
+                if (q.level + 2 <= kMaxLevel && f->has_too_fine_neighbour(q)) h.push_back(i);
+            }
+        });
         std::vector<unsigned char> flags(nl, 0);
         bool any = false;
-        for (size_t i = 0; i < nl; ++i) {
-            const Leaf &q = f->leaves[i];
-            if (!q.dirty) continue;
-            if (q.level >= 2)
-                for (int dy = -1; dy <= 1; ++dy)
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        if (!dx && !dy) continue;
-                        int c = f->too_coarse_neighbour(q, dx, dy);
-                        if (c >= 0 && !flags[size_t(c)]) {
-                            flags[size_t(c)] = 1;
-                            any = true;
-                        }
-                    }
-            if (!flags[i] && q.level + 2 <= kMaxLevel && f->has_too_fine_neighbour(q)) {
-                flags[i] = 1;
+        for (const auto &h : hits)
+            for (int c : h) {
+                flags[size_t(c)] = 1;
                 any = true;
             }
-        }
         if (!any) {
             for (Leaf &q : f->leaves) q.dirty = 0;
             return int(f->leaves.size());
@@ -441,93 +484,97 @@ int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_i
         cell_info[3 * i + 2] = nftm * i;
         forest_quad_corners(f, q, &geom[12 * i]);
     }
-    // done[i*4+side]: this quad side already belongs to an emitted face
-    std::vector<unsigned char> done(size_t(nq) * 4, 0);
-    int nface = 0;
-    auto emit = [&](const int v[11]) {
-        for (int k = 0; k < 11; ++k) face_info[11 * nface + k] = v[k];
-        ++nface;
+    // Faces are listed in order of the first leaf (by index) that takes part
+    // in them, sides 0..3 at that leaf: leaf i emits the face on its side s
+    // when no participant of that face has a smaller index (a leaf that is
+    // its own periodic neighbour emits from its even side). Every (leaf,
+    // side) is decided independently, so leaves are split among host
+    // threads and the per-chunk face lists are concatenated in leaf order.
+    struct Part {
+        std::vector<int> rec;
+        int err = 0;
     };
-    for (int i = 0; i < nq; ++i) {
-        const Leaf &q = f->leaves[size_t(i)];
-        for (int s = 0; s < 4; ++s) {
-            if (done[size_t(i) * 4 + s]) continue;
-            int dx, dy;
-            side_offset(s, dx, dy);
-            int opp = s ^ 1;
-            int v[11];
-            for (int k = 0; k < 11; ++k) v[k] = -1;
-            Key k;
-            if (!f->shifted(q.tree, q.level, q.x, q.y, dx, dy, k)) {
-                v[0] = 1; v[1] = s; v[2] = i;
-                done[size_t(i) * 4 + s] = 1;
-                emit(v);
-                continue;
-            }
-            const int c0 = f->locate(k.tree, k.x, k.y);
-            const int lvl0 = f->leaves[size_t(c0)].level;
-            if (lvl0 == q.level) {
-                int j = c0;
-                // side[0]: lower quadrant inside a tree; across trees the
-                // lower tree id, then the lower face number.
-                bool this_first;
-                int tq = q.tree, tj = f->leaves[size_t(j)].tree;
-                if (tq == tj) {
-                    this_first = (s & 1) == 1;
+    std::vector<Part> parts((size_t)host_threads());
+    parallel_chunks(size_t(nq), 2048, [&](size_t b, size_t e, int t) {
+        Part &P = parts[size_t(t)];
+        P.rec.reserve((e - b) * 2 * 11);
+        for (size_t ii = b; ii < e && !P.err; ++ii) {
+            const int i = int(ii);
+            const Leaf &q = f->leaves[ii];
+            for (int s = 0; s < 4; ++s) {
+                int dx, dy;
+                side_offset(s, dx, dy);
+                const int opp = s ^ 1;
+                int v[11];
+                for (int k = 0; k < 11; ++k) v[k] = -1;
+                bool emit = true;
+                Key k;
+                if (!f->shifted(q.tree, q.level, q.x, q.y, dx, dy, k)) {
+                    v[0] = 1; v[1] = s; v[2] = i;
                 } else {
-                    this_first = (tq < tj) || (tq == tj && s < opp);
+                    const int c0 = f->locate(k.tree, k.x, k.y);
+                    const int lvl0 = f->leaves[size_t(c0)].level;
+                    if (lvl0 == q.level) {
+                        const int j = c0;
+                        // side[0]: lower quadrant inside a tree; across trees
+                        // the lower tree id, then the lower face number.
+                        bool this_first;
+                        const int tq = q.tree, tj = f->leaves[size_t(j)].tree;
+                        if (tq == tj) this_first = (s & 1) == 1;
+                        else this_first = (tq < tj) || (tq == tj && s < opp);
+                        if (i == j) this_first = (s & 1) == 0;
+                        const int a = this_first ? i : j, sa = this_first ? s : opp;
+                        const int bq = this_first ? j : i, sb = this_first ? opp : s;
+                        v[0] = 2; v[1] = sa; v[2] = a; v[3] = bq; v[7] = sb;
+                        emit = (i < j) || (i == j && (s & 1) == 0);
+                    } else if (lvl0 < q.level - 1) {
+                        P.err = -2;  // not 2:1 balanced
+                        break;
+                    } else if (lvl0 == q.level - 1) {
+                        // coarser neighbour: this quad is one of two hanging quads
+                        const int c = c0;
+                        const int64_t Lp = qlen(q.level - 1), L = qlen(q.level);
+                        const int64_t base_x = (q.x / Lp) * Lp, base_y = (q.y / Lp) * Lp;
+                        int fine[2];
+                        for (int h = 0; h < 2; ++h) {
+                            if (s < 2) fine[h] = find(q.tree, q.level, q.x, base_y + h * L);
+                            else fine[h] = find(q.tree, q.level, base_x + h * L, q.y);
+                        }
+                        if (fine[0] < 0 || fine[1] < 0) {
+                            P.err = -2;
+                            break;
+                        }
+                        v[0] = 3; v[1] = opp; v[2] = c;
+                        v[3] = fine[0]; v[4] = fine[1]; v[7] = s; v[8] = s;
+                        emit = i == std::min(c, std::min(fine[0], fine[1]));
+                    } else {
+                        // finer neighbours: this quad is the full side of a hanging face
+                        const int64_t Lc = qlen(q.level + 1);
+                        int fine[2];
+                        for (int h = 0; h < 2; ++h) {
+                            if (s < 2)
+                                fine[h] = find(k.tree, q.level + 1, (s == 0) ? k.x + Lc : k.x, k.y + h * Lc);
+                            else
+                                fine[h] = find(k.tree, q.level + 1, k.x + h * Lc, (s == 2) ? k.y + Lc : k.y);
+                        }
+                        if (fine[0] < 0 || fine[1] < 0) {
+                            P.err = -3;  // not 2:1 balanced
+                            break;
+                        }
+                        v[0] = 3; v[1] = s; v[2] = i;
+                        v[3] = fine[0]; v[4] = fine[1]; v[7] = opp; v[8] = opp;
+                        emit = i < std::min(fine[0], fine[1]);
+                    }
                 }
-                if (i == j) this_first = (s & 1) == 0;
-                int a = this_first ? i : j, sa = this_first ? s : opp;
-                int b = this_first ? j : i, sb = this_first ? opp : s;
-                v[0] = 2; v[1] = sa; v[2] = a; v[3] = b; v[7] = sb;
-                done[size_t(i) * 4 + s] = 1;
-                done[size_t(j) * 4 + opp] = 1;
-                emit(v);
-                continue;
-            }
-            // coarser neighbour: this quad is one of two hanging quads
-            if (lvl0 < q.level - 1) return -2;  // not 2:1 balanced
-            if (lvl0 == q.level - 1) {
-                const int c = c0;
-                // the two fine quads on this face, lower coordinate first
-                const int64_t Lp = qlen(q.level - 1), L = qlen(q.level);
-                const int64_t base_x = (q.x / Lp) * Lp, base_y = (q.y / Lp) * Lp;
-                int fine[2];
-                for (int h = 0; h < 2; ++h) {
-                    if (s < 2)
-                        fine[h] = find(q.tree, q.level, q.x, base_y + h * L);
-                    else
-                        fine[h] = find(q.tree, q.level, base_x + h * L, q.y);
-                }
-                if (fine[0] < 0 || fine[1] < 0) return -2;
-                v[0] = 3; v[1] = opp; v[2] = c;
-                v[3] = fine[0]; v[4] = fine[1]; v[7] = s; v[8] = s;
-                done[size_t(c) * 4 + opp] = 1;
-                done[size_t(fine[0]) * 4 + s] = 1;
-                done[size_t(fine[1]) * 4 + s] = 1;
-                emit(v);
-                continue;
-            }
-            // finer neighbours: this quad is the full side of a hanging face
-            {
-                int64_t Lc = qlen(q.level + 1);
-                int fine[2];
-                for (int h = 0; h < 2; ++h) {
-                    if (s < 2)
-                        fine[h] = find(k.tree, q.level + 1, (s == 0) ? k.x + Lc : k.x, k.y + h * Lc);
-                    else
-                        fine[h] = find(k.tree, q.level + 1, k.x + h * Lc, (s == 2) ? k.y + Lc : k.y);
-                }
-                if (fine[0] < 0 || fine[1] < 0) return -3;  // not 2:1 balanced
-                v[0] = 3; v[1] = s; v[2] = i;
-                v[3] = fine[0]; v[4] = fine[1]; v[7] = opp; v[8] = opp;
-                done[size_t(i) * 4 + s] = 1;
-                done[size_t(fine[0]) * 4 + opp] = 1;
-                done[size_t(fine[1]) * 4 + opp] = 1;
-                emit(v);
+                if (emit) P.rec.insert(P.rec.end(), v, v + 11);
             }
         }
+    });
+    int nface = 0;
+    for (const Part &P : parts) {
+        if (P.err) return P.err;
+        std::memcpy(face_info + 11 * size_t(nface), P.rec.data(), sizeof(int) * P.rec.size());
+        nface += int(P.rec.size() / 11);
     }
     *nface_out = nface;
     *dof_out = nftm * nq;

@@ -249,7 +249,7 @@ def learned_amr(args):
     n, lo, hi, tol = 8, 3, 6, 0.02
     t0 = time.perf_counter()
     m = L.Mlp(seed=0)
-    rows = L.collect(m, range(32), n, lo, hi, tol, regrid_interval=10, regrids=25, lookahead=True)
+    rows = L.collect(m, range(args.learned_seeds), n, lo, hi, tol, regrid_interval=10, regrids=25, lookahead=True)
     t1 = time.perf_counter()
     hist, _ = L.train(m, epochs=20, batch=4096, lr=1e-3, seed=0)
     t2 = time.perf_counter()
@@ -286,6 +286,57 @@ def learned_amr(args):
     out["speedup_learned_fp32_over_plain_fp64"] = out["learned_fp32"]["value"] / out["plain_fp64"]["value"]
     m.close()
     return out
+
+
+def amr_workload(args):
+    """One adaptive workload through the library's AMR loop (regrid every 5
+    steps: GPU tagging by the density jump, host forest refine / coarsen /
+    2:1 balance, in-place GPU remap). --warmup steps untimed, then --steps
+    steps timed: cell-updates/s with the regrid time included (the
+    metric's definition for adaptive runs) and of the solve alone."""
+    import amrgpu as ag
+    from amrgpu import amr, workloads as W
+    t0 = time.perf_counter()
+    if args.workload == "four_quadrant":
+        f, mesh, cfg, soln = W.four_quadrant(seed=0, min_level=4, max_level=9, n=16, form=args.amr_form)
+        desc = ("four-quadrant Riemann problem, unit square, levels 4-9, 16x16 patches, density-jump tol 0.05, "
+                "SSP-RK3 CFL 0.5, regrid every 5 steps")
+        lo, hi = 4, 9
+    else:
+        f, mesh, cfg, soln = W.shock_bubble(seed=0, min_level=5, max_level=args.max_level, n=16, form=args.amr_form)
+        desc = (f"Mach-2 shock-bubble interaction, [0,2]x[0,1] (2x1 trees), levels 5-{args.max_level}, 16x16 "
+                "patches, density-jump tol 0.1, SSP-RK3 CFL 0.5, regrid every 5 steps")
+        lo, hi = 5, args.max_level
+    t_setup = time.perf_counter() - t0
+    cells0 = mesh.ncells
+    cfg["final_time"] = 0.0
+    s = ag.Session(mesh, cfg, form=args.amr_form)
+    s.upload(soln)
+    for _ in range(max(1, args.warmup // 5)):
+        s.step(5)
+        s.sync()
+        amr.regrid(f, s, 16, lo, hi)
+    solve = reg = 0.0
+    cu = steps = 0
+    cells = []
+    for _ in range(max(1, args.steps // 5)):
+        a = time.perf_counter()
+        s.step(5)
+        rep = s.sync()
+        b = time.perf_counter()
+        cu += rep["steps"] * s.mesh.ncells
+        steps += rep["steps"]
+        cells.append(s.mesh.ncells)
+        amr.regrid(f, s, 16, lo, hi)
+        solve += b - a
+        reg += time.perf_counter() - b
+    err = rep["error"]
+    s.close()
+    return {"metric": METRIC, "workload": args.workload, "config": {"workload": desc},
+            "form": "FP32 flux, FP64 state" if args.amr_form == 1 else "plain FP64 (bit-exact)",
+            "value": cu / (solve + reg), "unit": UNIT, "solve_only": cu / solve, "steps": steps,
+            "regrids": steps // 5, "cells_start": cells0, "cells_min": min(cells), "cells_max": max(cells),
+            "solve_s": solve, "regrid_s": reg, "setup_s": t_setup, "error": err}
 
 
 def run_gpu(args):
@@ -433,11 +484,23 @@ def main():
     ap.add_argument("--form", type=int, default=-1, help="time one form only (0 FP64, 1 FP32 flux)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator AMR comparison")
+    ap.add_argument("--learned-only", action="store_true", help="run only the learned-indicator AMR comparison")
+    ap.add_argument("--learned-seeds", type=int, default=32, help="seeded runs that make the training set")
+    ap.add_argument("--workload", choices=["vortex", "four_quadrant", "shock_bubble"], default="vortex",
+                    help="vortex: the headline line; the others time one adaptive workload")
+    ap.add_argument("--amr-form", type=int, default=1, help="form of the adaptive workloads (0 FP64, 1 FP32 flux)")
+    ap.add_argument("--max-level", type=int, default=11, help="finest level of the shock-bubble workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "vortex":
+        sys.path[:0] = [ROOT, os.path.join(ROOT, "amr-demo_b200")]
+        print(json.dumps(amr_workload(args)), flush=True)
+    elif args.learned_only:
+        sys.path[:0] = [ROOT, os.path.join(ROOT, "amr-demo_b200")]
+        print(json.dumps({"metric": METRIC, "learned_amr": learned_amr(args)}), flush=True)
     else:
         run_gpu(args)
 
