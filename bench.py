@@ -316,10 +316,14 @@ def amr_workload(args):
         s.step(5)
         s.sync()
         amr.regrid(f, s, 16, lo, hi)
+    import numpy as np
     solve = reg = 0.0
     cu = steps = 0
     cells = []
-    for _ in range(max(1, args.steps // 5)):
+    parts = dict(tag=0.0, forest=0.0, balance=0.0, mesh=0.0, session_regrid=0.0)
+    cycles = max(1, args.steps // 5)
+    for _ in range(cycles):
+        # the regrid of amr.regrid, timed part by part
         a = time.perf_counter()
         s.step(5)
         rep = s.sync()
@@ -327,16 +331,36 @@ def amr_workload(args):
         cu += rep["steps"] * s.mesh.ncells
         steps += rep["steps"]
         cells.append(s.mesh.ncells)
-        amr.regrid(f, s, 16, lo, hi)
+        tags = s.tag()
+        c = time.perf_counter()
+        _, lev, _, _ = f.quads()
+        f.begin_regrid()
+        f.set_tags(tags)
+        f.refine(((tags > 0) & (lev < hi)).astype(np.int32), max_level=hi)
+        t2 = f.get_tags()
+        _, lev2, _, _ = f.quads()
+        f.coarsen(((t2 == 0) & (lev2 > lo)).astype(np.int32), min_level=lo)
+        d = time.perf_counter()
+        f.balance()
+        e = time.perf_counter()
+        kind, src = f.remap()
+        m2 = f.mesh(16)
+        g = time.perf_counter()
+        s.regrid(m2, kind, src)
+        h = time.perf_counter()
+        for k, v in zip(parts, (c - b, d - c, e - d, g - e, h - g)):
+            parts[k] += v
         solve += b - a
-        reg += time.perf_counter() - b
+        reg += h - b
     err = rep["error"]
     s.close()
     return {"metric": METRIC, "workload": args.workload, "config": {"workload": desc},
             "form": "FP32 flux, FP64 state" if args.amr_form == 1 else "plain FP64 (bit-exact)",
             "value": cu / (solve + reg), "unit": UNIT, "solve_only": cu / solve, "steps": steps,
             "regrids": steps // 5, "cells_start": cells0, "cells_min": min(cells), "cells_max": max(cells),
-            "solve_s": solve, "regrid_s": reg, "setup_s": t_setup, "error": err}
+            "solve_s": solve, "regrid_s": reg, "setup_s": t_setup, "error": err,
+            "regrid_ms": {k: 1e3 * v / cycles for k, v in parts.items()},
+            "solve_ms_per_5_steps": 1e3 * solve / cycles}
 
 
 def run_gpu(args):
