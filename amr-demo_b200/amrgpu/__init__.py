@@ -147,6 +147,31 @@ class Forest:
     def num_quads(self):
         return lib().amrgpu_forest_num_quads(self._f)
 
+    def write_vtk(self, path, n, soln, subgrid=False):
+        """Unstructured VTK (.vtu) of the forest and an AoS state (amrgpu_write_vtk)."""
+        a = np.ascontiguousarray(soln, np.float64)
+        check(lib().amrgpu_write_vtk(str(path).encode(), self._f, int(n), dp(a), int(bool(subgrid))), "write_vtk")
+
+    def save_checkpoint(self, path, n, soln, istep=0, time=0.0):
+        a = np.ascontiguousarray(soln, np.float64)
+        check(lib().amrgpu_checkpoint_write(str(path).encode(), self._f, int(n), dp(a), int(istep), float(time)),
+              "checkpoint_write")
+
+    @classmethod
+    def load_checkpoint(cls, path):
+        """(forest, n, soln, istep, time) from amrgpu_checkpoint_write's file."""
+        nq, n, ist = C.c_int(0), C.c_int(0), C.c_int(0)
+        t = C.c_double(0.0)
+        check(lib().amrgpu_checkpoint_read_header(str(path).encode(), C.byref(nq), C.byref(n), C.byref(ist),
+                                                  C.byref(t)), "checkpoint_read_header")
+        soln = np.zeros(4 * n.value * n.value * nq.value, np.float64)
+        h = C.c_void_p()
+        check(lib().amrgpu_checkpoint_read(str(path).encode(), C.byref(h), dp(soln), soln.size), "checkpoint_read")
+        f = cls.__new__(cls)
+        f._f = h.value
+        f.scale = None
+        return f, n.value, soln, ist.value, t.value
+
     def quads(self):
         n = self.num_quads
         tree = np.zeros(n, np.int32)

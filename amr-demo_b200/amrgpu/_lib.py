@@ -121,6 +121,11 @@ PROTOTYPES = {
     "amrgpu_forest_external": (C.c_int, [C.c_void_p, C.c_int, C.c_int, i32p, i32p, f64p, i32p, i32p]),
     "amrgpu_forest_quad_h": (C.c_double, [C.c_void_p, C.c_int]),
     "amrgpu_forest_initialize": (C.c_int, [C.c_void_p, C.c_int, f64p]),
+    # output
+    "amrgpu_write_vtk": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, f64p, C.c_int]),
+    "amrgpu_checkpoint_write": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, f64p, C.c_int, C.c_double]),
+    "amrgpu_checkpoint_read_header": (C.c_int, [C.c_char_p, i32p, i32p, i32p, f64p]),
+    "amrgpu_checkpoint_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p), f64p, C.c_longlong]),
     # learned refinement indicator
     "amrgpu_mlp_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_ulonglong]),
     "amrgpu_mlp_destroy": (None, [C.c_void_p]),

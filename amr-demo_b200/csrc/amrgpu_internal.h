@@ -37,6 +37,11 @@ int forest_coarsen(Forest *f, const int *flags, int min_level);
 int forest_balance(Forest *f);
 bool forest_is_balanced(const Forest *f);
 void forest_quad_corners(const Forest *f, const Leaf &q, double xyz[12]);
+// Checkpoint image of a forest: brick, periodicity, origin, scale and the
+// leaves (tree, level, x, y, tag, type); forest_load returns null on a
+// malformed image.
+std::vector<unsigned char> forest_save(const Forest *f);
+Forest *forest_load(const unsigned char *data, size_t size);
 double forest_quad_h(const Forest *f, const Leaf &q);
 int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_info,
                     int *face_info, double *geom, int *nface_out, int *dof_out);
@@ -112,3 +117,8 @@ void shock_state(double gamma, double ms, double rho1, double p1, double out[4])
 void tag_feature_host(const PhysicsConfig &cfg, int nfields, int n, const double *soln, int *tag);
 
 }  // namespace amrgpu
+
+// The C ABI's forest handle (amrgpu_forest_t of include/amrgpu.h).
+struct amrgpu_forest {
+    amrgpu::Forest *f;
+};

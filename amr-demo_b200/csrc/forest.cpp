@@ -465,6 +465,112 @@ double forest_quad_h(const Forest *f, const Leaf &q)
     return f->scale * double(qlen(q.level)) / double(kRootLen);
 }
 
+namespace {
+
+constexpr uint64_t kForestMagic = 0x31464741524d4147ULL;  // "GAMRAGF1"
+
+template <typename T>
+void put(std::vector<unsigned char> &o, const T &v)
+{
+    const unsigned char *p = reinterpret_cast<const unsigned char *>(&v);
+    o.insert(o.end(), p, p + sizeof(T));
+}
+
+template <typename T>
+bool get(const unsigned char *&p, const unsigned char *end, T &v)
+{
+    if (size_t(end - p) < sizeof(T)) return false;
+    std::memcpy(&v, p, sizeof(T));
+    p += sizeof(T);
+    return true;
+}
+
+}  // namespace
+
+std::vector<unsigned char> forest_save(const Forest *f)
+{
+    std::vector<unsigned char> o;
+    put(o, kForestMagic);
+    put(o, int32_t(f->nx));
+    put(o, int32_t(f->ny));
+    put(o, int32_t(f->periodic[0]));
+    put(o, int32_t(f->periodic[1]));
+    for (double v : f->xlo) put(o, v);
+    put(o, f->scale);
+    put(o, int64_t(f->leaves.size()));
+    for (const Leaf &q : f->leaves) {
+        put(o, int32_t(q.tree));
+        put(o, int32_t(q.level));
+        put(o, int64_t(q.x));
+        put(o, int64_t(q.y));
+        put(o, int32_t(q.tag));
+        put(o, int32_t(q.type));
+    }
+    return o;
+}
+
+Forest *forest_load(const unsigned char *data, size_t size)
+{
+    const unsigned char *p = data, *end = data + size;
+    uint64_t magic = 0;
+    int32_t nx, ny, px, py;
+    double xlo[3], scale;
+    int64_t nl;
+    if (!get(p, end, magic) || magic != kForestMagic || !get(p, end, nx) || !get(p, end, ny) || !get(p, end, px) ||
+        !get(p, end, py) || !get(p, end, xlo[0]) || !get(p, end, xlo[1]) || !get(p, end, xlo[2]) ||
+        !get(p, end, scale) || !get(p, end, nl))
+        return nullptr;
+    if (nx < 1 || ny < 1 || nl < 1 || int64_t(size_t(end - p)) < nl * 32) return nullptr;
+    Forest *f = forest_new_brick(nx, ny, px, py, xlo[0], xlo[1], xlo[2], scale, 0);
+    if (!f) return nullptr;
+    f->leaves.clear();
+    f->leaves.reserve(size_t(nl));
+    for (int64_t k = 0; k < nl; ++k) {
+        int32_t tree, level, tag, type;
+        int64_t x, y;
+        get(p, end, tree);
+        get(p, end, level);
+        get(p, end, x);
+        get(p, end, y);
+        get(p, end, tag);
+        get(p, end, type);
+        const bool ok = tree >= 0 && tree < nx * ny && level >= 0 && level <= kMaxLevel && x >= 0 && y >= 0 &&
+                        x < kRootLen && y < kRootLen && x % qlen(level) == 0 && y % qlen(level) == 0;
+        if (!ok) {
+            delete f;
+            return nullptr;
+        }
+        Leaf q;
+        q.tree = tree;
+        q.level = level;
+        q.x = x;
+        q.y = y;
+        q.tag = tag;
+        q.type = type;
+        q.src = int(k);
+        q.src_kind = kRemapCopy;
+        f->leaves.push_back(q);
+    }
+    // the leaves must tile every tree in (tree, Morton) order
+    unsigned __int128 covered = 0;  // in units of a level-30 quadrant
+    for (size_t k = 0; k < f->leaves.size(); ++k) {
+        const Leaf &q = f->leaves[k];
+        if (k > 0) {
+            const Leaf &a = f->leaves[k - 1];
+            if (a.tree > q.tree || (a.tree == q.tree && morton(a.x, a.y) >= morton(q.x, q.y))) {
+                delete f;
+                return nullptr;
+            }
+        }
+        covered += (unsigned __int128)1 << (2 * (kMaxLevel - q.level));
+    }
+    if (covered != (unsigned __int128)(nx * ny) << (2 * kMaxLevel)) {
+        delete f;
+        return nullptr;
+    }
+    return f;
+}
+
 int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_info,
                     int *face_info, double *geom, int *nface_out, int *dof_out)
 {

@@ -410,6 +410,7 @@ const char *amrgpu_error_string(int code)
     case AMRGPU_ERR_CONFIG: return "configuration file missing or invalid";
     case AMRGPU_ERR_TOO_LARGE: return "request above the stated maximum";
     case AMRGPU_ERR_NEGATIVE: return "non-positive density or pressure";
+    case AMRGPU_ERR_IO: return "file input/output error";
     default: return "unknown error";
     }
 }
@@ -614,10 +615,6 @@ void hpc_amr_refine_operator_2d(int *unstructured, int *nfields, int *nsub_elem,
 // ======================================================================
 // C ABI: host forest
 // ======================================================================
-struct amrgpu_forest {
-    Forest *f;
-};
-
 amrgpu_forest_t *amrgpu_forest_new_brick(int nx, int ny, int periodic_x, int periodic_y, double xlo,
                                          double ylo, double zlo, double scale, int level)
 {

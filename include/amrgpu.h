@@ -127,7 +127,8 @@ enum {
     AMRGPU_ERR_NO_DEVICE = 6,    /* no CUDA device */
     AMRGPU_ERR_CONFIG = 7,       /* input.physics missing or invalid */
     AMRGPU_ERR_TOO_LARGE = 8,    /* request above a stated maximum */
-    AMRGPU_ERR_NEGATIVE = 9      /* non-positive density or pressure */
+    AMRGPU_ERR_NEGATIVE = 9,     /* non-positive density or pressure */
+    AMRGPU_ERR_IO = 10           /* file cannot be written / read, or is malformed */
 };
 
 enum {
@@ -261,6 +262,27 @@ int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int
  * amr_regrid.c:82-125 (new ghost layer, new face lists, new soln array). */
 int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int *kind,
                           const int *src_index);
+
+/* ---------------- output: visualisation and checkpoint ---------------- */
+/* Unstructured VTK (.vtu, ASCII) of a forest and its AoS state (soln[f +
+ * 4*(c + n*n*q)]): as the reference's vtk_write_solution
+ * (src/amr/src/amr_vtk.c:23-106) one quad per quadrant, corners shrunk by
+ * 0.99999, cell data treeid / level / mpirank and point data rho, rhou,
+ * rhov, rhoe = the patch average at every corner (interpolate_solution,
+ * amr_vtk.c:109-217); subgrid != 0 writes every subgrid cell as a quad
+ * with its own values as cell data instead. */
+int amrgpu_write_vtk(const char *path, const amrgpu_forest_t *forest, int n, const double *soln,
+                     int subgrid);
+/* Checkpoint of the forest, the AoS state, the step and the time (the
+ * reference saves the forest and quadrant data with p4est_save,
+ * amr_evolve.c:61-64, and has no reader). read_header gives the sizes;
+ * read restores a new forest (destroy it with amrgpu_forest_destroy) and
+ * fills soln (capacity in doubles, at least 4*n*n*nquad). */
+int amrgpu_checkpoint_write(const char *path, const amrgpu_forest_t *forest, int n,
+                            const double *soln, int istep, double time);
+int amrgpu_checkpoint_read_header(const char *path, int *nquad, int *n, int *istep, double *time);
+int amrgpu_checkpoint_read(const char *path, amrgpu_forest_t **forest, double *soln,
+                           long long soln_capacity);
 
 /* ---------------- learned refinement indicator ---------------- */
 /* No counterpart in the reference: a 400-128-64-3 MLP (GELU) over a patch's
