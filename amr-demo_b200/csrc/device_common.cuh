@@ -45,10 +45,10 @@ struct DeviceScalars {
     StepSlot slot[3];
     double norm_sq;           // sum of k^2 of the last stage of the last step
     double dt_used;           // step size of the last step
-    unsigned int done_blocks; // last-block-done counter for the norm reduction
+    unsigned int done_blocks; // last-block-done counter (norm reduction, work counter reset)
     int flags;                // bit 0: non-finite residual, bit 1: rho<=0 or p<=0
     int steps;                // steps taken with a positive step size
-    int pad;
+    unsigned int work_next;   // dynamic quad counter of the row-sweep kernel (reset by its last block)
 };
 
 enum { kFlagNonFinite = 1, kFlagNegative = 2, kFlagTimeout = 4 };

@@ -95,22 +95,37 @@ __device__ __forceinline__ void roe_flux_fp32(const float ql[4], const float qr[
     flux[3] = ((b1 * fluxl - b2 * fluxr) * inv_db + disp) * mag;
 }
 
+// Every operation of the per-cell record and of the axis-aligned flux below
+// is written with an explicitly rounded intrinsic (__fmul_rn, __fadd_rn,
+// __fsub_rn, __fmaf_rn) or an SFU instruction in inline PTX, so that the
+// compiler cannot contract or reorder them differently at different
+// inlined call sites: a face that two quads evaluate from their own sides
+// (or one kernel in two places) gets bit-identical values, which exact
+// conservation needs.
+__device__ __forceinline__ float fsqrt_approx(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Per-cell FP32 record (8 floats, two float4 loads):
 // [0] rho [1] u [2] v [3] p [4] H [5] sqrt(rho) [6] rho*u [7] rho*v.
 // rho*E + p is recovered as rho*H.
 __device__ __forceinline__ void cell_prims_fp32(const double q[4], float P[8])
 {
-    float rho = (float)q[0];
-    float ru = (float)q[1], rv = (float)q[2], rE = (float)q[3];
-    float oneOrho = frcp(rho);
-    float u = ru * oneOrho, v = rv * oneOrho;
-    float p = 0.4f * (rE - 0.5f * rho * (u * u + v * v));
+    const float rho = __double2float_rn(q[0]);
+    const float ru = __double2float_rn(q[1]), rv = __double2float_rn(q[2]), rE = __double2float_rn(q[3]);
+    const float oneOrho = frcp(rho);
+    const float u = __fmul_rn(ru, oneOrho), v = __fmul_rn(rv, oneOrho);
+    const float ke = __fmul_rn(__fmul_rn(0.5f, rho), __fmaf_rn(u, u, __fmul_rn(v, v)));
+    const float p = __fmul_rn(0.4f, __fsub_rn(rE, ke));
     P[0] = rho;
     P[1] = u;
     P[2] = v;
     P[3] = p;
-    P[4] = (rE + p) * oneOrho;
-    P[5] = sqrtf(rho);
+    P[4] = __fmul_rn(__fadd_rn(rE, p), oneOrho);
+    P[5] = fsqrt_approx(rho);
     P[6] = ru;
     P[7] = rv;
 }
@@ -131,34 +146,42 @@ __device__ __forceinline__ void roe_flux_axis_fp32(const float *L, const float *
     const float rhor = R[0], ur = R[1], vr = R[2], pr = R[3], Hr = R[4], srr = R[5];
     const float unl = DIR == 0 ? ul : vl;
     const float unr = DIR == 0 ? ur : vr;
-    const float inv = frcp(srl + srr);
-    const float rhobar = srl * srr;
-    const float ubar = (ul * srl + ur * srr) * inv;
-    const float vbar = (vl * srl + vr * srr) * inv;
-    const float Hbar = (Hl * srl + Hr * srr) * inv;
-    const float a2 = 0.4f * (Hbar - 0.5f * (ubar * ubar + vbar * vbar));
+    const float inv = frcp(__fadd_rn(srl, srr));
+    const float rhobar = __fmul_rn(srl, srr);
+    const float ubar = __fmul_rn(__fmaf_rn(ul, srl, __fmul_rn(ur, srr)), inv);
+    const float vbar = __fmul_rn(__fmaf_rn(vl, srl, __fmul_rn(vr, srr)), inv);
+    const float Hbar = __fmul_rn(__fmaf_rn(Hl, srl, __fmul_rn(Hr, srr)), inv);
+    const float a2 =
+        __fmul_rn(0.4f, __fsub_rn(Hbar, __fmul_rn(0.5f, __fmaf_rn(ubar, ubar, __fmul_rn(vbar, vbar)))));
     const float ra = frsqrt(a2);  // 1/abar: abar = a2/abar, 1/a2 = ra^2
-    const float abar = a2 * ra;
+    const float abar = __fmul_rn(a2, ra);
     const float unbar = DIR == 0 ? ubar : vbar;
-    const float b1 = fmaxf(fmaxf(unbar + abar, unr + abar), 0.0f);
-    const float b2 = fminf(fminf(unbar - abar, unl - abar), 0.0f);
-    const float inv_db = frcp(b1 - b2);
-    const float bcoeff = b1 * b2 * inv_db;
-    const float delta1 = (rhor - rhol) - (pr - pl) * (ra * ra);
-    const float bM = bcoeff * abar * frcp(abar + fabsf(unbar));
+    const float b1 = fmaxf(fmaxf(__fadd_rn(unbar, abar), __fadd_rn(unr, abar)), 0.0f);
+    const float b2 = fminf(fminf(__fsub_rn(unbar, abar), __fsub_rn(unl, abar)), 0.0f);
+    const float inv_db = frcp(__fsub_rn(b1, b2));
+    const float bcoeff = __fmul_rn(__fmul_rn(b1, b2), inv_db);
+    const float drho = __fsub_rn(rhor, rhol);
+    const float delta1 = __fsub_rn(drho, __fmul_rn(__fsub_rn(pr, pl), __fmul_rn(ra, ra)));
+    const float bM = __fmul_rn(__fmul_rn(bcoeff, abar), frcp(__fadd_rn(abar, fabsf(unbar))));
     const float ml = DIR == 0 ? L[6] : L[7];
     const float mr = DIR == 0 ? R[6] : R[7];
-    const float rHl = rhol * Hl, rHr = rhor * Hr;
-    const float hb1 = h * b1 * inv_db, hb2 = h * b2 * inv_db;
-    float d;
-    d = bcoeff * (rhor - rhol) - bM * delta1;
-    flux[0] = hb1 * ml - hb2 * mr + h * d;
-    d = bcoeff * (R[6] - L[6]) - bM * (delta1 * ubar + (DIR == 0 ? 0.0f : rhobar * (ur - ul)));
-    flux[1] = hb1 * (ml * ul + (DIR == 0 ? pl : 0.0f)) - hb2 * (mr * ur + (DIR == 0 ? pr : 0.0f)) + h * d;
-    d = bcoeff * (R[7] - L[7]) - bM * (delta1 * vbar + (DIR == 0 ? rhobar * (vr - vl) : 0.0f));
-    flux[2] = hb1 * (ml * vl + (DIR == 0 ? 0.0f : pl)) - hb2 * (mr * vr + (DIR == 0 ? 0.0f : pr)) + h * d;
-    d = bcoeff * (rHr - rHl) - bM * (delta1 * Hbar + rhobar * (Hr - Hl));
-    flux[3] = hb1 * (rHl * unl) - hb2 * (rHr * unr) + h * d;
+    const float rHl = __fmul_rn(rhol, Hl), rHr = __fmul_rn(rhor, Hr);
+    const float hb1 = __fmul_rn(__fmul_rn(h, b1), inv_db), hb2 = __fmul_rn(__fmul_rn(h, b2), inv_db);
+    // flux = hb1 * fl - hb2 * fr + h * d with d = bcoeff * jump - bM * corr
+    auto row = [&](float fl, float fr, float jump, float corr) {
+        const float d = __fsub_rn(__fmul_rn(bcoeff, jump), __fmul_rn(bM, corr));
+        return __fmaf_rn(h, d, __fsub_rn(__fmul_rn(hb1, fl), __fmul_rn(hb2, fr)));
+    };
+    const float tang = DIR == 0 ? __fmul_rn(rhobar, __fsub_rn(vr, vl)) : __fmul_rn(rhobar, __fsub_rn(ur, ul));
+    flux[0] = row(ml, mr, drho, delta1);
+    flux[1] = row(DIR == 0 ? __fmaf_rn(ml, ul, pl) : __fmul_rn(ml, ul),
+                  DIR == 0 ? __fmaf_rn(mr, ur, pr) : __fmul_rn(mr, ur), __fsub_rn(R[6], L[6]),
+                  DIR == 0 ? __fmul_rn(delta1, ubar) : __fmaf_rn(delta1, ubar, tang));
+    flux[2] = row(DIR == 0 ? __fmul_rn(ml, vl) : __fmaf_rn(ml, vl, pl),
+                  DIR == 0 ? __fmul_rn(mr, vr) : __fmaf_rn(mr, vr, pr), __fsub_rn(R[7], L[7]),
+                  DIR == 0 ? __fmaf_rn(delta1, vbar, tang) : __fmul_rn(delta1, vbar));
+    flux[3] = row(__fmul_rn(rHl, unl), __fmul_rn(rHr, unr), __fsub_rn(rHr, rHl),
+                  __fmaf_rn(delta1, Hbar, __fmul_rn(rhobar, __fsub_rn(Hr, Hl))));
 }
 
 __device__ __forceinline__ void roe_flux_prim_fp32(const float *L, const float *R, float n0, float n1,

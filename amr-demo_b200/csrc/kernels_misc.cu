@@ -180,7 +180,7 @@ __global__ void rearm_kernel(DeviceScalars *s, int slot_now, double cap)
     s->done_blocks = 0u;
     s->flags = 0;
     s->steps = 0;
-    s->pad = 0;
+    s->work_next = 0u;
 }
 
 static int grid_for(long long work, int block)

@@ -256,6 +256,137 @@ __device__ __forceinline__ int facing_cell(int s, int m)
     return m;
 }
 
+// The stage update of one cell for every scheme, with the reference's
+// coefficients and summation order (rk_time_integrators.c:22-540; the
+// Shu-Osher RK3 of the FP32-flux form is the extension). kv is the cell's
+// residual, q0v its input state, A0(f) the first auxiliary input; writes
+// the outputs at gi and returns the new state in qn.
+template <typename A0F>
+__device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long long stride, long long gi,
+                                          const double q0v[4], const double kv[4], A0F A0, double qn[4])
+{
+    switch (a.scheme) {
+    case kSchemeRhsOnly:
+#pragma unroll
+        for (int f = 0; f < 4; ++f) { a.out0[f * stride + gi] = kv[f]; qn[f] = q0v[f]; }
+        break;
+    case kSchemeRK1: {
+        double beta1 = 1.0 * dt;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) { qn[f] = q0v[f] + beta1 * kv[f]; a.out0[f * stride + gi] = qn[f]; }
+        break;
+    }
+    case kSchemeRK2: {
+        double alpha1 = 1.0 * dt, beta1 = 0.5 * dt, beta2 = 0.5 * dt;
+        if (a.stage == 1) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                qn[f] = q0v[f] + alpha1 * kv[f];
+                a.out0[f * stride + gi] = qn[f];
+                a.out1[f * stride + gi] = q0v[f] + beta1 * kv[f];
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                qn[f] = A0(f) + beta2 * kv[f];
+                a.out0[f * stride + gi] = qn[f];
+            }
+        }
+        break;
+    }
+    case kSchemeRK3: {
+        double alpha1 = 1.00 * dt, alpha21 = 0.25 * dt, alpha22 = 0.25 * dt;
+        double beta1 = 1.0 / 6.0 * dt, beta2 = 1.0 / 6.0 * dt, beta3 = 2.0 / 3.0 * dt;
+        if (a.stage == 1) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                qn[f] = q0v[f] + alpha1 * kv[f];
+                a.out0[f * stride + gi] = qn[f];
+                a.out1[f * stride + gi] = kv[f];
+            }
+        } else if (a.stage == 2) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                double Q0 = A0(f);
+                double k1 = a.a1[f * stride + gi];
+                qn[f] = Q0 + alpha21 * k1 + alpha22 * kv[f];
+                double C = Q0 + beta1 * k1 + beta2 * kv[f];
+                a.out0[f * stride + gi] = qn[f];
+                a.out1[f * stride + gi] = C;
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                qn[f] = A0(f) + beta3 * kv[f];
+                a.out0[f * stride + gi] = qn[f];
+            }
+        }
+        break;
+    }
+    case kSchemeRK4: {
+        double alpha1 = 0.5 * dt, alpha2 = 0.5 * dt, alpha3 = 1.0 * dt, beta1 = 1.0 / 6.0 * dt;
+        if (a.stage == 1) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                qn[f] = q0v[f] + alpha1 * kv[f];
+                a.out0[f * stride + gi] = qn[f];
+                a.out1[f * stride + gi] = kv[f];
+            }
+        } else if (a.stage < 4) {
+            double al = (a.stage == 2) ? alpha2 : alpha3;
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                double Q0 = A0(f);
+                double K = a.a1[f * stride + gi];
+                qn[f] = Q0 + al * kv[f];
+                a.out0[f * stride + gi] = qn[f];
+                a.out1[f * stride + gi] = K + 2.0 * kv[f];
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                double Q0 = A0(f);
+                double K = a.a1[f * stride + gi];
+                qn[f] = Q0 + beta1 * (K + kv[f]);
+                a.out0[f * stride + gi] = qn[f];
+            }
+        }
+        break;
+    }
+    case kSchemeLSERK45: {
+        double ra, rb;
+        lserk_coeff(a.stage, ra, rb);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            double qsv = (a.stage == 1) ? dt * kv[f] : A0(f) * ra + dt * kv[f];
+            qn[f] = q0v[f] + rb * qsv;
+            a.out1[f * stride + gi] = qsv;
+            a.out0[f * stride + gi] = qn[f];
+        }
+        break;
+    }
+    default: {  // kSchemeRK3ShuOsher
+        if (a.stage == 1) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) { qn[f] = q0v[f] + dt * kv[f]; a.out0[f * stride + gi] = qn[f]; }
+        } else if (a.stage == 2) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                qn[f] = 0.75 * A0(f) + 0.25 * (q0v[f] + dt * kv[f]);
+                a.out0[f * stride + gi] = qn[f];
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                qn[f] = (1.0 / 3.0) * A0(f) + (2.0 / 3.0) * (q0v[f] + dt * kv[f]);
+                a.out0[f * stride + gi] = qn[f];
+            }
+        }
+        break;
+    }
+    }
+}
+
 template <int N, int QPB, int T, int MINB, bool F32, typename FluxOps>
 __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
 {
@@ -728,126 +859,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
 #pragma unroll
             for (int f = 0; f < 4; ++f) q0v[f] = raw[(ql * 4 + f) * NN + c];
 
-            switch (a.scheme) {
-            case kSchemeRhsOnly:
-#pragma unroll
-                for (int f = 0; f < 4; ++f) { a.out0[f * stride + gi] = kv[f]; qn[f] = q0v[f]; }
-                break;
-            case kSchemeRK1: {
-                double beta1 = 1.0 * dt;
-#pragma unroll
-                for (int f = 0; f < 4; ++f) { qn[f] = q0v[f] + beta1 * kv[f]; a.out0[f * stride + gi] = qn[f]; }
-                break;
-            }
-            case kSchemeRK2: {
-                double alpha1 = 1.0 * dt, beta1 = 0.5 * dt, beta2 = 0.5 * dt;
-                if (a.stage == 1) {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        qn[f] = q0v[f] + alpha1 * kv[f];
-                        a.out0[f * stride + gi] = qn[f];
-                        a.out1[f * stride + gi] = q0v[f] + beta1 * kv[f];
-                    }
-                } else {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        qn[f] = A0(f) + beta2 * kv[f];
-                        a.out0[f * stride + gi] = qn[f];
-                    }
-                }
-                break;
-            }
-            case kSchemeRK3: {
-                double alpha1 = 1.00 * dt, alpha21 = 0.25 * dt, alpha22 = 0.25 * dt;
-                double beta1 = 1.0 / 6.0 * dt, beta2 = 1.0 / 6.0 * dt, beta3 = 2.0 / 3.0 * dt;
-                if (a.stage == 1) {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        qn[f] = q0v[f] + alpha1 * kv[f];
-                        a.out0[f * stride + gi] = qn[f];
-                        a.out1[f * stride + gi] = kv[f];
-                    }
-                } else if (a.stage == 2) {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        double Q0 = A0(f);
-                        double k1 = a.a1[f * stride + gi];
-                        qn[f] = Q0 + alpha21 * k1 + alpha22 * kv[f];
-                        double C = Q0 + beta1 * k1 + beta2 * kv[f];
-                        a.out0[f * stride + gi] = qn[f];
-                        a.out1[f * stride + gi] = C;
-                    }
-                } else {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        qn[f] = A0(f) + beta3 * kv[f];
-                        a.out0[f * stride + gi] = qn[f];
-                    }
-                }
-                break;
-            }
-            case kSchemeRK4: {
-                double alpha1 = 0.5 * dt, alpha2 = 0.5 * dt, alpha3 = 1.0 * dt, beta1 = 1.0 / 6.0 * dt;
-                if (a.stage == 1) {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        qn[f] = q0v[f] + alpha1 * kv[f];
-                        a.out0[f * stride + gi] = qn[f];
-                        a.out1[f * stride + gi] = kv[f];
-                    }
-                } else if (a.stage < 4) {
-                    double al = (a.stage == 2) ? alpha2 : alpha3;
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        double Q0 = A0(f);
-                        double K = a.a1[f * stride + gi];
-                        qn[f] = Q0 + al * kv[f];
-                        a.out0[f * stride + gi] = qn[f];
-                        a.out1[f * stride + gi] = K + 2.0 * kv[f];
-                    }
-                } else {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        double Q0 = A0(f);
-                        double K = a.a1[f * stride + gi];
-                        qn[f] = Q0 + beta1 * (K + kv[f]);
-                        a.out0[f * stride + gi] = qn[f];
-                    }
-                }
-                break;
-            }
-            case kSchemeLSERK45: {
-                double ra, rb;
-                lserk_coeff(a.stage, ra, rb);
-#pragma unroll
-                for (int f = 0; f < 4; ++f) {
-                    double qsv = (a.stage == 1) ? dt * kv[f] : A0(f) * ra + dt * kv[f];
-                    qn[f] = q0v[f] + rb * qsv;
-                    a.out1[f * stride + gi] = qsv;
-                    a.out0[f * stride + gi] = qn[f];
-                }
-                break;
-            }
-            default: {  // kSchemeRK3ShuOsher
-                if (a.stage == 1) {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) { qn[f] = q0v[f] + dt * kv[f]; a.out0[f * stride + gi] = qn[f]; }
-                } else if (a.stage == 2) {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        qn[f] = 0.75 * A0(f) + 0.25 * (q0v[f] + dt * kv[f]);
-                        a.out0[f * stride + gi] = qn[f];
-                    }
-                } else {
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        qn[f] = (1.0 / 3.0) * A0(f) + (2.0 / 3.0) * (q0v[f] + dt * kv[f]);
-                        a.out0[f * stride + gi] = qn[f];
-                    }
-                }
-                break;
-            }
-            }
+            rk_update(a, dt, stride, gi, q0v, kv, A0, qn);
 
             if (a.last_stage) {
 #pragma unroll

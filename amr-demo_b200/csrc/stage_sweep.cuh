@@ -1,0 +1,298 @@
+// stage_sweep.cuh -- the FP32-flux form's RK stage for 16x16 patches as a
+// row sweep: one warp per quadrant, no shared-memory records and no
+// block-wide barriers between phases.
+//
+// Same arithmetic as stage_kernel<16, ..., FP32> (the reference's
+// flux_roe_2d, flux_2d_module.F90:63-182, and boundary flux, bc_2d_module.F90,
+// in FP32 on per-cell records; FP64 residual sums, stage update, norm and
+// conservation; FP32 CFL candidate), reorganised for the register file:
+//
+//   lane = (i, h): column i = lane & 15 of the patch, rows 8h .. 8h+7.
+//   edges   per quad, the 4 x 16 edge faces (each lane one per round: the
+//           own edge cell's record, the neighbour cell(s) the reference
+//           pairs it with, the Roe or boundary flux, a coarse hanging edge's
+//           two fluxes summed in FP64) and the 16 faces between rows 7 and 8
+//           go to a small per-warp table, in the interior sign convention
+//           (a cell adds -F at its low face and +F at its high face);
+//   sweep   8 steps; at step t lane (i, h) loads cell (i, 8h+t) straight
+//           from HBM (16 lanes read 128 contiguous bytes per field), builds
+//           its record in registers, computes the x-face flux at i-1/2 with
+//           the left neighbour's record taken by a warp shuffle, hands that
+//           flux to lane i-1 (which needs it as its i+1/2 face) by a second
+//           shuffle, and the y-face flux at j-1/2 from the record it kept of
+//           the row below. Row j-1 is then complete: -F(x-1/2) +F(x+1/2)
+//           -F(y-1/2) +F(y+1/2), summed in FP64, divided by the volume,
+//           negated, and the stage update is written.
+//
+// Per cell-stage this is about 2.1 flux evaluations, one record, 12
+// shuffles and the update: no per-face index decoding, no record stores and
+// reloads, no barrier between the record, face and cell phases.
+#pragma once
+
+#include "flux_fp32.cuh"
+#include "stage_kernel.cuh"
+
+namespace amrgpu {
+
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageArgs a)
+{
+    constexpr int N = 16, NN = N * N;
+    constexpr unsigned FULL = 0xffffffffu;
+    // edge fluxes per warp: [side 0..3, 4 = faces between rows 7 and 8][position][field]
+    __shared__ double sedge[WARPS][5][N][4];
+    __shared__ double red[64];
+    __shared__ int s_last;
+
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int i = lane & 15, h = lane >> 4;
+    const long long stride = a.stride;
+
+    // step scalars (as stage_kernel)
+    const StepSlot slot = a.scal->slot[a.slot_read];
+    double dt = __longlong_as_double((long long)slot.dt_bits);
+    if (!a.cfl_on) dt = a.dt_cap;
+    if (a.final_time > 0.0) {
+        double rem = a.final_time - slot.time;
+        if (rem < dt) dt = rem;
+        if (dt < 0.0) dt = 0.0;
+    }
+    if (a.last_stage && blockIdx.x == 0 && tid == 0) {
+        a.scal->slot[a.slot_write].time = slot.time + dt;
+        a.scal->dt_used = dt;
+        if (dt > 0.0) a.scal->steps += 1;
+        a.scal->slot[a.slot_reset].dt_bits = (unsigned long long)__double_as_longlong(a.dt_cap);
+        if (!a.cfl_on)
+            a.scal->slot[a.slot_write].dt_bits = (unsigned long long)__double_as_longlong(a.dt_cap);
+    }
+    const float qinf[4] = {(float)a.qinflow[0], (float)a.qinflow[1], (float)a.qinflow[2], (float)a.qinflow[3]};
+
+    double my_dt_min = a.dt_cap;
+    double my_norm = 0.0;
+    int my_flags = 0;
+
+    // Quads: each warp's first one by its index, then the next free one from
+    // a counter (work_next, reset to 0 by the last block), so that warps
+    // and SMs that finish early take more and the tail stays short.
+    const int nwarps = gridDim.x * WARPS;
+    int quad = blockIdx.x * WARPS + w;
+    while (quad < a.nquad) {
+        const QuadDesc &qd = a.quads[quad];
+        const double *g = qd.corner;
+        const double hx = (g[2] - g[0]) / (double)N, hy = (g[5] - g[1]) / (double)N;
+        const double vol = hx * hy, inv_vol = 1.0 / (hx * hy);
+        const float fhx = (float)hx, fhy = (float)hy;
+        const double *Qq = a.qin + (long long)quad * NN;
+        auto load_rec = [&](const double *base, int cell, float P[8], double q[4]) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) q[f] = base[f * stride + cell];
+            cell_prims_fp32(q, P);
+        };
+
+        // ---------------- edges: round 0 sides 0 / 1, round 1 sides 2 / 3
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+            const int s = 2 * round + h, m = i;
+            const SideDesc d = qd.side[s];
+            const int own = (s == 0) ? m * N : (s == 1) ? m * N + N - 1 : (s == 2) ? m : (N - 1) * N + m;
+            float Po[8], fl[4];
+            double qo[4];
+            load_rec(Qq, own, Po, qo);
+            const float hc = (float)cell_h_of(a.h_base, d.level, N);
+            double E[4];
+            if (d.kind == kSideBoundary) {
+                const float n0 = round == 0 ? (s == 0 ? -hc : hc) : 0.0f;
+                const float n1 = round == 0 ? 0.0f : (s == 2 ? -hc : hc);
+                bc_flux_rec_fp32(d.bc, Po, n0, n1, qinf, fl);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) E[f] = (s & 1) ? (double)fl[f] : -(double)fl[f];
+            } else {
+                // one flux site for a side's one or two neighbours: the
+                // neighbour quad computes the same face at the same site, so
+                // both see bit-identical values (conservation)
+                const int fc = facing_cell<N>(s, m);
+                const int nk = (d.kind == kSideCoarseHang) ? 2 : 1;
+#pragma unroll
+                for (int f = 0; f < 4; ++f) E[f] = 0.0;
+#pragma unroll 1
+                for (int k = 0; k < nk; ++k) {
+                    float Pn[8];
+                    double qn4[4];
+                    load_rec(a.qin + (long long)(k == 0 ? d.nbr0 : d.nbr1) * NN, fc, Pn, qn4);
+                    const float *L = (s & 1) ? Po : Pn;
+                    const float *R = (s & 1) ? Pn : Po;
+                    if (round == 0) roe_flux_axis_fp32<0>(L, R, hc, fl);
+                    else roe_flux_axis_fp32<1>(L, R, hc, fl);
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) E[f] = E[f] + (double)fl[f];
+                }
+            }
+#pragma unroll
+            for (int f = 0; f < 4; ++f) sedge[w][s][m][f] = E[f];
+        }
+        // ---------------- the faces between rows 7 and 8 (column i)
+        {
+            float P[8], O[8], fl[4];
+            double q4[4];
+            load_rec(Qq, (7 + h) * N + i, P, q4);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) O[k] = __shfl_xor_sync(FULL, P[k], 16);
+            if (h == 0) {
+                roe_flux_axis_fp32<1>(P, O, fhx, fl);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) sedge[w][4][i][f] = (double)fl[f];
+            }
+        }
+        __syncwarp();
+
+        // ---------------- sweep over the lane's 8 rows
+        float below[8];      // record of the row below (y-face partner)
+        double xpart[4];     // -F(x-1/2) + F(x+1/2) of the row below
+        double gbelow[4];    // F(y-1/2) of the row below
+        double qbelow[4];    // input state of the row below
+        double a0below[4] = {0.0, 0.0, 0.0, 0.0};  // first auxiliary input of the row below
+        double a0next[4] = {0.0, 0.0, 0.0, 0.0};   // ... of the current row, loaded a row ahead of its use
+        const bool has_a0 = a.a0 != nullptr;
+        auto finish = [&](int jr, const double gup[4]) {
+            const long long gi = (long long)quad * NN + jr * N + i;
+            double kv[4], qn[4];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                const double r = (xpart[f] - gbelow[f]) + gup[f];
+                kv[f] = -(r * inv_vol);
+            }
+            auto A0 = [&](int f) -> double { return a0below[f]; };
+            rk_update(a, dt, stride, gi, qbelow, kv, A0, qn);
+            if (a.last_stage) {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) my_norm += kv[f] * kv[f];
+                if (a.cfl_on) {
+                    const double cand = cfl_candidate_fp32(qn, vol, a.cfl);
+                    if (cand < my_dt_min) my_dt_min = cand;
+                }
+                const double rho = qn[0];
+                const double pe = qn[3] * rho - 0.5 * (qn[1] * qn[1] + qn[2] * qn[2]);
+                if (!(rho > 0.0) || !(pe > 0.0)) my_flags |= kFlagNegative;
+            }
+        };
+        double qnext[4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (8 * h) * N + i];
+#pragma unroll 1
+        for (int t = 0; t < 8; ++t) {
+            const int j = 8 * h + t;
+            double q4[4];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) q4[f] = qnext[f];
+            if (t < 7) {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (j + 1) * N + i];
+            }
+            // the auxiliary input of this row, used when the row is finished
+            // in the next step (its load latency is covered by the fluxes)
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                a0below[f] = a0next[f];
+                a0next[f] = has_a0 ? a.a0[f * stride + (long long)quad * NN + j * N + i] : 0.0;
+            }
+            float P[8];
+            cell_prims_fp32(q4, P);
+            // x-face at i-1/2 (lane 0's left face is an edge face)
+            float L[8], fx[4], fxr[4];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) L[k] = __shfl_up_sync(FULL, P[k], 1, 16);
+            roe_flux_axis_fp32<0>(L, P, fhy, fx);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) fxr[f] = __shfl_down_sync(FULL, fx[f], 1, 16);
+            double xp[4];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                const double fl = (i == 0) ? sedge[w][0][j][f] : (double)fx[f];
+                const double fr = (i == N - 1) ? sedge[w][1][j][f] : (double)fxr[f];
+                xp[f] = fr - fl;
+            }
+            // y-face at j-1/2 (the first row's is an edge or the row-7/8 face)
+            double gy[4];
+            if (t == 0) {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) gy[f] = h == 0 ? sedge[w][2][i][f] : sedge[w][4][i][f];
+            } else {
+                float fy[4];
+                roe_flux_axis_fp32<1>(below, P, fhx, fy);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) gy[f] = (double)fy[f];
+                finish(j - 1, gy);
+            }
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                xpart[f] = xp[f];
+                gbelow[f] = gy[f];
+                qbelow[f] = q4[f];
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) below[k] = P[k];
+        }
+        {
+            double gtop[4];
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                gtop[f] = h == 0 ? sedge[w][4][i][f] : sedge[w][3][i][f];
+                a0below[f] = a0next[f];
+            }
+            finish(8 * h + 7, gtop);
+        }
+        __syncwarp();  // the next quad rewrites this warp's edge table
+        unsigned nxt = 0;
+        if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);
+        quad = nwarps + (int)__shfl_sync(FULL, nxt, 0);
+    }
+
+    // ---------------- block reductions: CFL min (one atomic per block),
+    // norm partials summed by the last block in a fixed order, flags; the
+    // last block also resets the quad counter for the next launch
+    int wflags = __reduce_or_sync(FULL, my_flags);
+    if (wflags && lane == 0) atomicOr(&a.scal->flags, wflags);
+    if (a.last_stage) {
+        double wmin = warp_min(my_dt_min);
+        double wsum = warp_sum(my_norm);
+        if (lane == 0) { red[w] = wmin; red[32 + w] = wsum; }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (a.last_stage) {
+            double bmin = red[0], bsum = red[32];
+            for (int k = 1; k < WARPS; ++k) {
+                bmin = (red[k] < bmin) ? red[k] : bmin;
+                bsum += red[32 + k];
+            }
+            if (a.cfl_on)
+                atomicMin(&a.scal->slot[a.slot_write].dt_bits, (unsigned long long)__double_as_longlong(bmin));
+            a.partials[blockIdx.x] = bsum;
+        }
+        __threadfence();
+        const unsigned ticket = atomicAdd(&a.scal->done_blocks, 1u);
+        s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (a.last_stage) {
+        double part = 0.0;
+        for (int b = tid; b < (int)gridDim.x; b += WARPS * 32) part += __ldcg(a.partials + b);
+        part = warp_sum(part);
+        if (lane == 0) red[w] = part;
+        __syncthreads();
+        if (tid == 0) {
+            double tot = red[0];
+            for (int k = 1; k < WARPS; ++k) tot += red[k];
+            a.scal->norm_sq = tot;
+            if (!isfinite(tot)) atomicOr(&a.scal->flags, kFlagNonFinite);
+        }
+    }
+    if (tid == 0) {
+        a.scal->work_next = 0u;
+        a.scal->done_blocks = 0u;
+    }
+}
+
+}  // namespace amrgpu
