@@ -272,6 +272,13 @@ class Session:
     def set_form(self, form):
         check(lib().amrgpu_session_set_form(self._s, int(form)), "set_form")
 
+    def launch_variants(self):
+        """The compiled (quads per block, threads) launch shapes for this session."""
+        q = np.zeros(64, np.int32)
+        t = np.zeros(64, np.int32)
+        k = lib().amrgpu_session_launch_variants(self._s, ip(q), ip(t), 64)
+        return list(zip(q[:k].tolist(), t[:k].tolist()))
+
     def set_launch(self, qpb, threads):
         check(lib().amrgpu_session_set_launch(self._s, int(qpb), int(threads)), "set_launch")
 

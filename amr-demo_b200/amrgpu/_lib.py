@@ -104,6 +104,7 @@ PROTOTYPES = {
     "amrgpu_session_tag": (C.c_int, [C.c_void_p, i32p]),
     "amrgpu_session_remap": (C.c_int, [C.c_void_p, C.c_void_p, i32p, i32p]),
     "amrgpu_session_regrid": (C.c_int, [C.c_void_p, C.c_void_p, i32p, i32p]),
+    "amrgpu_session_launch_variants": (C.c_int, [C.c_void_p, i32p, i32p, C.c_int]),
     # forest
     "amrgpu_forest_new_brick": (C.c_void_p, [C.c_int] * 4 + [C.c_double] * 4 + [C.c_int]),
     "amrgpu_forest_destroy": (None, [C.c_void_p]),

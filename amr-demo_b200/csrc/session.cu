@@ -498,6 +498,23 @@ int amrgpu_session_set_launch(amrgpu_session_t *s, int qpb, int threads)
     return configure_launch(s, L);
 }
 
+int amrgpu_session_launch_variants(const amrgpu_session_t *s, int *qpb, int *threads, int cap)
+{
+    if (!s || cap < 0) return -AMRGPU_ERR_ARG;
+    const StageLaunch *tab;
+    const int cnt = (s->form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
+    int k = 0;
+    for (int i = 0; i < cnt; ++i) {
+        if (tab[i].n != s->n) continue;
+        if (k < cap && qpb && threads) {
+            qpb[k] = tab[i].qpb;
+            threads[k] = tab[i].threads;
+        }
+        ++k;
+    }
+    return k;
+}
+
 int amrgpu_session_upload(amrgpu_session_t *s, const double *soln)
 {
     if (!s || !soln) return AMRGPU_ERR_ARG;

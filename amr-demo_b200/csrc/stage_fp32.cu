@@ -83,14 +83,14 @@ const void *cfl_kernel_fp32(int n)
                 (const void *)stage_kernel<N, QPB, T, MINB, true, FluxOpsFP32>}
 
 // row-sweep kernel for 16x16 patches: one warp per quad, "quads per
-// block" = warps per block, no dynamic shared memory
+// block" = warps per block, no dynamic shared memory; all at 128
+// registers (16 resident warps per SM): fewer registers spill and run slower
 #define AMRGPU_SWEEP16(W, MINB) StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep16_kernel<W, MINB>}
 
 static const StageLaunch kTable32[] = {
-    AMRGPU_SWEEP16(4, 4),
-    AMRGPU_SWEEP16(8, 2),
-    AMRGPU_SWEEP16(4, 3),
+    AMRGPU_SWEEP16(4, 4),   // 128 registers, 16 warps per SM
     AMRGPU_SWEEP16(2, 8),
+    AMRGPU_SWEEP16(8, 2),
     AMRGPU_STAGE32(16, 1, 288, 3),
     AMRGPU_STAGE32(16, 1, 288, 2),
     AMRGPU_STAGE32(16, 2, 544, 1),

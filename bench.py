@@ -157,20 +157,19 @@ def autotune(ag, s, steps=6):
     from amrgpu._lib import lib
     st = torch.cuda.ExternalStream(s.stream())
     best = None
-    for qpb in (1, 2, 4, 8, 16):
-        for thr in (64, 128, 160, 192, 256, 288, 320, 384, 544, 576):
-            if lib().amrgpu_session_set_launch(s._s, qpb, thr) != 0:
-                ag.clear_error()
-                continue
-            s.step(3)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
-            s.step(steps)
-            e1.record(st)
-            e1.synchronize()
-            ms = e0.elapsed_time(e1)
-            if best is None or ms < best[0]:
-                best = (ms, qpb, thr)
+    for qpb, thr in s.launch_variants():
+        if lib().amrgpu_session_set_launch(s._s, qpb, thr) != 0:
+            ag.clear_error()
+            continue
+        s.step(3)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.step(steps)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if best is None or ms < best[0]:
+            best = (ms, qpb, thr)
     s.set_launch(best[1], best[2])
     return {"quads_per_block": best[1], "threads": best[2]}
 

@@ -195,6 +195,10 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *mesh,
 void amrgpu_session_destroy(amrgpu_session_t *s);
 int amrgpu_session_set_form(amrgpu_session_t *s, int form);
 int amrgpu_session_set_launch(amrgpu_session_t *s, int quads_per_block, int threads);
+/* The compiled stage-kernel launch shapes for the session's form and patch
+ * size (the autotuner's candidates): fills up to cap pairs, returns the count. */
+int amrgpu_session_launch_variants(const amrgpu_session_t *s, int *quads_per_block, int *threads,
+                                   int cap);
 /* Host AoS soln (reference layout, dof + ghost tail) <-> device SoA state. */
 int amrgpu_session_upload(amrgpu_session_t *s, const double *soln_aos);
 int amrgpu_session_download(amrgpu_session_t *s, double *soln_aos);
