@@ -286,8 +286,13 @@ class Session:
         a = np.ascontiguousarray(soln, dtype=np.float64)
         check(lib().amrgpu_session_upload(self._s, dp(a)), "upload")
 
-    def download(self):
-        out = np.empty(self.mesh.dof, np.float64)
+    def download(self, out=None):
+        """AoS state of the local quads; into ``out`` (e.g. pinned host
+        memory, dof doubles) when given."""
+        if out is None:
+            out = np.empty(self.mesh.dof, np.float64)
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size < self.mesh.dof:
+            raise ValueError("download: out must be a contiguous float64 array of at least dof values")
         check(lib().amrgpu_session_download(self._s, dp(out)), "download")
         return out
 

@@ -26,17 +26,20 @@ def riemann_64x64(seed=0, time_scheme=3, steps=200):
     return f, f.mesh(n), cfg, f.initialize(n)
 
 
-def vortex_1024(level=6, n=16, time_scheme=3, final_time=10.0, form=0, steps=100000):
+def vortex_1024(level=6, n=16, time_scheme=3, final_time=10.0, form=0, steps=100000, trees_x=1):
     """Isentropic vortex of strength 5 at (5,5) advected by the free stream
     (rho,u,v,p) = (1,1,1,1) on the periodic square [0,10]^2; level 6 with
-    16x16 patches = 1024^2 cells. CFL 0.5; one period is t = 10."""
+    16x16 patches = 1024^2 cells. CFL 0.5; one period is t = 10.
+    trees_x > 1 widens the periodic domain to [0,10*trees_x] x [0,10] with
+    one level-``level`` tree per 10 x 10 square (the weak-scaling mesh: one
+    tree per rank)."""
     mach = math.sqrt(2.0) / math.sqrt(1.4)
     cfg = Config.from_input(cfl=0.5, time_scheme=time_scheme, nelem_subgrid=n, coarse_grid_h=10.0,
                             initial_condition=4, time_steps=steps, dt=1.0, bc=[1] * 6, gamma=1.4,
                             density=1.0, pressure=1.0, mach=mach, alpha=45.0, beta=0.0,
                             ic_params=[5.0, 5.0, 5.0, 0.5], final_time=final_time, form=form)
     cfg.apply()
-    f = Forest(1, 1, periodic=(1, 1), lo=(0.0, 0.0, 0.0), scale=10.0, level=level)
+    f = Forest(int(trees_x), 1, periodic=(1, 1), lo=(0.0, 0.0, 0.0), scale=10.0, level=level)
     return f, f.mesh(n), cfg, f.initialize(n)
 
 

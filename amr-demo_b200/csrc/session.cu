@@ -26,6 +26,7 @@
 #include "amrgpu_internal.h"
 #include "device_common.cuh"
 #include "launch_table.h"
+#include "halo_kernels.h"
 #include "misc_kernels.h"
 #include "stage_kernel.cuh"
 
@@ -102,6 +103,8 @@ struct amrgpu_session {
     int *d_kind = nullptr;
     int *d_src = nullptr;
     void *d_scratch = nullptr;  // scratch of kernels outside this file (session_scratch)
+    int *d_send = nullptr;      // halo send list: local quads whose records go to other ranks
+    int nsend = 0;
     size_t scratch_bytes = 0;
     const void *occ_kernel = nullptr;  // launch whose occupancy occ_per_sm is
     int occ_per_sm = 0;
@@ -110,6 +113,7 @@ struct amrgpu_session {
     const StageLaunch *launch = nullptr;
     int grid = 0;
     long long step_index = 0;
+    int stage_pos = 0;  // stages of the current step enqueued by step_stage (0: at a step boundary)
     int64_t launches = 0;
     std::map<int, cudaGraphExec_t> graphs;
     bool primed = false;
@@ -319,7 +323,8 @@ int prime(amrgpu_session *s, bool keep_time = false)
     return AMRGPU_OK;
 }
 
-int enqueue_step(amrgpu_session *s)
+// Stage st (0-based) of the current step: its kernel arguments and launch.
+int enqueue_stage(amrgpu_session *s, size_t st)
 {
     int scheme = scheme_of(s);
     bool swap_xy = false;
@@ -346,22 +351,39 @@ int enqueue_step(amrgpu_session *s)
         double ms = s->cfg.ic_params[0] != 0.0 ? s->cfg.ic_params[0] : 2.0;
         shock_state(s->cfg.gamma, ms, 1.0, 1.0, a.qinflow);
     }
-    for (size_t st = 0; st < plan.size(); ++st) {
-        a.stage = int(st) + 1;
-        a.last_stage = (st + 1 == plan.size()) ? 1 : 0;
-        a.qin = rolebuf(s, plan[st].in);
-        a.a0 = rolebuf(s, plan[st].a0);
-        a.a1 = rolebuf(s, plan[st].a1);
-        a.out0 = rolebuf(s, plan[st].out0);
-        a.out1 = rolebuf(s, plan[st].out1);
-        void *args[] = {&a};
-        cudaError_t e = cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args,
-                                         s->launch->smem, s->stream);
-        if (!cuda_ok(e, "stage kernel")) return AMRGPU_ERR_CUDA;
-        s->launches++;
-    }
+    a.stage = int(st) + 1;
+    a.last_stage = (st + 1 == plan.size()) ? 1 : 0;
+    a.qin = rolebuf(s, plan[st].in);
+    a.a0 = rolebuf(s, plan[st].a0);
+    a.a1 = rolebuf(s, plan[st].a1);
+    a.out0 = rolebuf(s, plan[st].out0);
+    a.out1 = rolebuf(s, plan[st].out1);
+    void *args[] = {&a};
+    cudaError_t e = cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args,
+                                     s->launch->smem, s->stream);
+    if (!cuda_ok(e, "stage kernel")) return AMRGPU_ERR_CUDA;
+    s->launches++;
+    return AMRGPU_OK;
+}
+
+// After the last stage of a step: buffer roles and the step counter.
+void finish_step(amrgpu_session *s)
+{
+    bool swap_xy = false;
+    plan_of(scheme_of(s), swap_xy);
     if (swap_xy) std::swap(s->role[RX], s->role[RY]);
     s->step_index++;
+}
+
+int enqueue_step(amrgpu_session *s)
+{
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme_of(s), swap_xy);
+    for (size_t st = 0; st < plan.size(); ++st) {
+        int rc = enqueue_stage(s, st);
+        if (rc) return rc;
+    }
+    finish_step(s);
     return AMRGPU_OK;
 }
 
@@ -473,6 +495,7 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_kind);
     cudaFree(s->d_src);
     cudaFree(s->d_scratch);
+    cudaFree(s->d_send);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -545,9 +568,110 @@ int amrgpu_session_download(amrgpu_session_t *s, double *soln)
     return cuda_ok(cudaStreamSynchronize(s->stream), "sync") ? AMRGPU_OK : AMRGPU_ERR_CUDA;
 }
 
+int amrgpu_session_step_stage(amrgpu_session_t *s, int *stage, int *stages_per_step)
+{
+    if (!s) return AMRGPU_ERR_ARG;
+    if (!s->primed) {
+        int rc = prime(s);
+        if (rc) return rc;
+    }
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme_of(s), swap_xy);
+    if (stage) *stage = s->stage_pos + 1;
+    if (stages_per_step) *stages_per_step = int(plan.size());
+    if (s->nquad > 0) {
+        int rc = enqueue_stage(s, size_t(s->stage_pos));
+        if (rc) return rc;
+    }
+    if (++s->stage_pos == int(plan.size())) {
+        s->stage_pos = 0;
+        finish_step(s);
+    }
+    return AMRGPU_OK;
+}
+
+double *amrgpu_session_stage_input(amrgpu_session_t *s, long long *field_stride)
+{
+    if (!s) return nullptr;
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme_of(s), swap_xy);
+    if (field_stride) *field_stride = s->stride;
+    return rolebuf(s, plan[size_t(s->stage_pos)].in);
+}
+
+unsigned long long *amrgpu_session_dt_slot(amrgpu_session_t *s)
+{
+    if (!s) return nullptr;
+    return &s->d_scal->slot[s->step_index % 3].dt_bits;
+}
+
+int amrgpu_session_set_halo(amrgpu_session_t *s, const int *send_quads, int nsend)
+{
+    if (!s || nsend < 0 || (nsend > 0 && !send_quads)) return AMRGPU_ERR_ARG;
+    for (int k = 0; k < nsend; ++k)
+        if (send_quads[k] < 0 || send_quads[k] >= s->nquad) {
+            set_error(AMRGPU_ERR_ARG, "set_halo: send entry " + std::to_string(k) + " is not a local quad");
+            return AMRGPU_ERR_ARG;
+        }
+    if (nsend > s->nsend || !s->d_send) {
+        cudaFree(s->d_send);
+        s->d_send = nullptr;
+        s->nsend = 0;
+        if (!cuda_ok(cudaMalloc(&s->d_send, sizeof(int) * size_t(nsend > 0 ? nsend : 1)), "halo list"))
+            return AMRGPU_ERR_CUDA;
+    }
+    if (nsend > 0 &&
+        !cuda_ok(cudaMemcpyAsync(s->d_send, send_quads, sizeof(int) * size_t(nsend), cudaMemcpyHostToDevice,
+                                 s->stream),
+                 "H2D halo list"))
+        return AMRGPU_ERR_CUDA;
+    if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return AMRGPU_ERR_CUDA;
+    s->nsend = nsend;
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_halo_pack(amrgpu_session_t *s, int first, int count, double *d_out)
+{
+    if (!s || first < 0 || count < 0 || first + count > s->nsend || (count > 0 && !d_out)) return AMRGPU_ERR_ARG;
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme_of(s), swap_xy);
+    const double *q = rolebuf(s, plan[size_t(s->stage_pos)].in);
+    if (!cuda_ok(launch_halo_pack(q, s->stride, s->n, s->d_send + first, count, d_out, s->sms, s->stream),
+                 "halo pack"))
+        return AMRGPU_ERR_CUDA;
+    if (count > 0) s->launches++;
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_halo_unpack(amrgpu_session_t *s, int first_ghost, int count, const double *d_in)
+{
+    if (!s || first_ghost < 0 || count < 0 || first_ghost + count > s->nghost || (count > 0 && !d_in))
+        return AMRGPU_ERR_ARG;
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme_of(s), swap_xy);
+    double *q = rolebuf(s, plan[size_t(s->stage_pos)].in);
+    if (!cuda_ok(launch_halo_unpack(q, s->stride, s->n, s->nquad + first_ghost, count, d_in, s->sms, s->stream),
+                 "halo unpack"))
+        return AMRGPU_ERR_CUDA;
+    if (count > 0) s->launches++;
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_local_scalars(amrgpu_session_t *s, double *norm_sq, int *flags)
+{
+    if (!s) return AMRGPU_ERR_ARG;
+    if (norm_sq) *norm_sq = s->h_scal.norm_sq;
+    if (flags) *flags = s->h_scal.flags;
+    return AMRGPU_OK;
+}
+
 int amrgpu_session_step(amrgpu_session_t *s, int nsteps)
 {
     if (!s || nsteps < 0) return AMRGPU_ERR_ARG;
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_step: a step begun with step_stage is not finished");
+        return AMRGPU_ERR_ARG;
+    }
     if (!s->primed) {
         int rc = prime(s);
         if (rc) return rc;
@@ -563,6 +687,10 @@ int amrgpu_session_step(amrgpu_session_t *s, int nsteps)
 int amrgpu_session_step_graph(amrgpu_session_t *s, int nsteps, int graph_steps)
 {
     if (!s || nsteps < 0) return AMRGPU_ERR_ARG;
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_step_graph: a step begun with step_stage is not finished");
+        return AMRGPU_ERR_ARG;
+    }
     if (graph_steps < 6) graph_steps = 6;
     graph_steps -= graph_steps % 6;
     if (!s->primed) {
@@ -820,6 +948,10 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
     if (!s || !m || !kind || !src_index || !m->cell_info || !m->geom || (m->nface > 0 && !m->face_info) ||
         m->ncell < 0 || m->nghost < 0) {
         set_error(AMRGPU_ERR_ARG, "session_regrid: null or negative arguments");
+        return AMRGPU_ERR_ARG;
+    }
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_regrid: a step begun with step_stage is not finished");
         return AMRGPU_ERR_ARG;
     }
     if (m->nghost != 0) {

@@ -362,6 +362,142 @@ def amr_workload(args):
             "solve_ms_per_5_steps": 1e3 * solve / cycles}
 
 
+def time_sharded(ag, S, mesh, cfg, s0, form, steps, warmup, tune_on, world, rank):
+    """One rank of the sharded run: Morton-range shard of the global mesh,
+    per-stage ghost exchange and per-step CFL MIN over NCCL (amrgpu.shard);
+    every step timed with CUDA events on the rank's solver stream (exchange
+    included), L2 flushed between steps."""
+    import torch
+    import torch.distributed as dist
+    sh = S.make_shard(mesh, S.partition(mesh.ncell, world), rank)
+    cfg["form"] = form
+    r = S.GpuRank(sh, cfg)
+    local = sh.local_state(s0)
+    tune = None
+    if tune_on:
+        r.upload(local)
+        tune = autotune(ag, r.session)
+    drv = S.Distributed(r)
+    drv.start(local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    drv.step(warmup)
+    torch.cuda.synchronize()
+    dist.barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    l0 = r.session.launch_count()
+    for k in range(steps):
+        with torch.cuda.stream(r.stream):
+            flush.zero_()
+            evs[k][0].record(r.stream)
+        drv.step(1)
+        evs[k][1].record(r.stream)
+    rep = drv.report()
+    launches = r.session.launch_count() - l0
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    return r, drv, {"ms_steps": ms, "report": rep, "tune": tune, "launches": launches,
+                    "ghosts": int(len(sh.ghosts)), "sends": int(len(sh.send_quads)), "local_quads": sh.nlocal}
+
+
+def e2e_sharded(drv, local, steps, segment):
+    """Per rank: upload of the rank's state from pinned host memory, a
+    segment of steps, download of the state, wall-clock per segment."""
+    import torch
+    import torch.distributed as dist
+    host = torch.empty(len(local), dtype=torch.float64, pin_memory=True).numpy()
+    host[:] = local
+    calls = max(1, steps // segment)
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        drv.start(host)
+        drv.step(segment)
+        drv.download(host)
+    wall = time.perf_counter() - t0
+    t = torch.tensor([wall], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), calls
+
+
+def run_sharded(args, world, rank, local):
+    """--gpus N > 1: weak scaling, one 1024^2 tree per rank on a periodic
+    N x 1 brick, ranks exchange ghost quads before every stage."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import amrgpu as ag
+    from amrgpu import shard as S
+    from amrgpu import workloads as W
+    f, mesh, cfg, s0 = W.vortex_1024(level=args.level, final_time=0.0, steps=10 ** 9, trees_x=world)
+    hbm, peak_kind = peaks()
+    run_forms = (0, 1) if args.form < 0 else (args.form,)
+    res = {}
+    dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for form in run_forms:
+            res[form] = time_sharded(ag, S, mesh, cfg, s0, form, args.steps, args.warmup, not args.no_tune,
+                                     world, rank)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = clk.summary()
+    out = {}
+    for form, (r, drv, d) in res.items():
+        t = torch.tensor([sum(d["ms_steps"])], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+        cells = mesh.ncells  # all ranks
+        avg_ms = tot_ms / args.steps
+        per_rank_cells = d["local_quads"] * mesh.n * mesh.n
+        out[form] = {"value": cells * args.steps / (tot_ms * 1e-3), "ms_per_step": avg_ms,
+                     "achieved_gbs": per_rank_cells * B_ALG[form] / (avg_ms * 1e-3) / 1e9, **d}
+    e2e = None
+    if not args.no_e2e and 1 in res:
+        r, drv, d = res[1]
+        local_state = r.shard.local_state(s0)
+        wall, calls = e2e_sharded(drv, local_state, args.steps, args.segment)
+        e2e = {"value": mesh.ncells * calls * args.segment / wall, "unit": UNIT,
+               "h2d_bytes_per_step": len(local_state) * 8, "d2h_bytes_per_step": r.shard.mesh.dof * 8,
+               "step": f"per rank: upload + {args.segment} RK3 steps (sharded driver) + download, "
+                       "slowest rank's wall clock"}
+    for form, (r, drv, d) in res.items():
+        r.close()
+    if rank == 0:
+        head = out[1] if 1 in out else out[run_forms[0]]
+        hf = 1 if 1 in out else run_forms[0]
+        line = {
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 flux / f64 state" if hf == 1 else "f64",
+            "data": "synthetic (seeded analytic vortex; no dataset exists)",
+            "config": {"workload": f"isentropic vortex, periodic [0,{10 * world}]x[0,10] ({world}x1 trees), "
+                                   f"{mesh.ncell} quads x 16x16 = {mesh.ncells} cells, one 1024^2 tree per rank, "
+                                   "SSP-RK3, CFL 0.5",
+                       "cells": mesh.ncells, "quads": mesh.ncell, "patch": "16x16",
+                       "ghost_quads_per_rank": head["ghosts"], "send_quads_per_rank": head["sends"],
+                       "l2": "flushed between steps (256 MB write; per-step CUDA events exclude it)",
+                       "launch": head["tune"],
+                       "parallelism": f"dp{world}: Morton-range shards, NCCL ghost exchange before every "
+                                      "stage, MIN all-reduce of the CFL step every step"},
+            "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+                         "frac": head["achieved_gbs"] / hbm, "traffic": traffic_per_launch(hf),
+                         "peak_kind": peak_kind, "bytes_per_cell_update": B_ALG[hf],
+                         "note": "per rank; step time includes the ghost exchange"},
+            "forms": {("plain_fp64" if k == 0 else "fp32_flux"): {"value": v["value"],
+                                                                   "ms_per_step": v["ms_per_step"]}
+                      for k, v in out.items()},
+            "e2e": e2e,
+            "clocks": clocks,
+            "gpu_launches": int(sum(v["launches"] for v in out.values())),
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -371,11 +507,12 @@ def run_gpu(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
+    if world > 1 or args.shard:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        return run_sharded(args, world, rank, local)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if not args.no_cpu_baseline:
         cpu = cpu_baseline()
 
     import amrgpu as ag
@@ -385,27 +522,19 @@ def run_gpu(args):
     run_forms = (0, 1) if args.form < 0 else (args.form,)
 
     forms = {}
-    if world > 1:
-        dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         for form in run_forms:
             s, r = time_form(ag, mesh, cfg, s0, form, args.steps, args.warmup, not args.no_tune)
             forms[form] = (s, r)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     clocks = clk.summary()
 
     out = {}
     for form, (s, r) in forms.items():
         tot_ms = sum(r["ms_steps"])
-        if world > 1:
-            t = torch.tensor([tot_ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot_ms = float(t.item())
         cells = mesh.ncells
-        value = world * cells * args.steps / (tot_ms * 1e-3)
+        value = cells * args.steps / (tot_ms * 1e-3)
         avg_ms = tot_ms / args.steps
         achieved = cells * B_ALG[form] / (avg_ms * 1e-3) / 1e9
         out[form] = {"value": value, "ms_per_step": avg_ms, "achieved_gbs": achieved, "report": r["report"],
@@ -418,9 +547,6 @@ def run_gpu(args):
                               "level": args.level, "ms_per_step": r["ms_per_step"],
                               "achieved_gbs": r["achieved_gbs"], "launches": r["launches"],
                               "clocks": clocks}), flush=True)
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
         return
     # accuracy of the FP32 form against the FP64 form after the same steps
     q64 = forms[0][0].download().reshape(-1, 4)
@@ -431,14 +557,8 @@ def run_gpu(args):
     if not args.no_e2e:
         e2e = e2e_form(ag, mesh, cfg, s0, 1, args.steps, args.segment)
     amr = None
-    if not args.no_learned and rank == 0:
+    if not args.no_learned:
         amr = learned_amr(args)
-
-    if rank != 0:
-        if world > 1:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
     head = out[1]
     traffic = traffic_per_launch(1)
     line = {
@@ -449,7 +569,7 @@ def run_gpu(args):
         "config": {"workload": WORKLOAD, "cells": mesh.ncells, "quads": mesh.ncell, "patch": "16x16",
                    "form": "FP32 flux, FP64 state, Shu-Osher SSP-RK3", "l2": "flushed between steps "
                    "(256 MB write; per-step CUDA events exclude it)", "launch": head["tune"],
-                   "parallelism": "replicas" if world > 1 else "1 GPU"},
+                   "parallelism": "1 GPU"},
         "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": hbm, "unit": "GB/s",
                      "frac": head["achieved_gbs"] / hbm, "traffic": traffic,
                      "peak_kind": peak_kind, "bytes_per_cell_update": B_ALG[1]},
@@ -469,9 +589,6 @@ def run_gpu(args):
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
 
 
 def run_reference(args):
@@ -506,6 +623,8 @@ def main():
     ap.add_argument("--level", type=int, default=6, help="forest level (6: the 1024^2 workload)")
     ap.add_argument("--form", type=int, default=-1, help="time one form only (0 FP64, 1 FP32 flux)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
+    ap.add_argument("--shard", action="store_true",
+                    help="use the sharded multi-rank driver also at one rank (under torchrun)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator AMR comparison")
     ap.add_argument("--learned-only", action="store_true", help="run only the learned-indicator AMR comparison")
     ap.add_argument("--learned-seeds", type=int, default=32, help="seeded runs that make the training set")

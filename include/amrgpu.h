@@ -221,6 +221,39 @@ int64_t amrgpu_session_launch_count(const amrgpu_session_t *s);
 /* Conservation totals sum(vol*Q_f) for the 4 fields, in FP64. */
 int amrgpu_session_totals(amrgpu_session_t *s, double totals[4]);
 
+/* ---------------- sharded meshes (one session per rank) ----------------
+ * A rank's mesh holds its ncell local quads followed by nghost ghost quads,
+ * grouped by owning rank in ascending order (physics_mpi.c:54). The host
+ * driver refreshes the ghosts of every stage's input before the stage
+ * (physics_mpi_real_to_ghost, rk_time_integrators.c:227-262) and takes the
+ * cross-rank MIN of the CFL step before every step
+ * (physics_runge_kutta_interface.c:96,149,205,262,316) and the SUM of the
+ * squared residual norm (rk_time_integrators.c:74,162,274). One quad's
+ * halo record is 4 fields x n*n doubles. */
+/* Enqueues the next stage of the current step; reports its 1-based index
+ * and the stages of a step. A step begun here is finished here before
+ * amrgpu_session_step / step_graph / regrid. */
+int amrgpu_session_step_stage(amrgpu_session_t *s, int *stage, int *stages_per_step);
+/* Device buffer the next stage reads its own and its neighbours' cells
+ * from (SoA, field stride in cells), ghost quads included. */
+double *amrgpu_session_stage_input(amrgpu_session_t *s, long long *field_stride);
+/* Device address of the CFL step the next step uses, as the uint64 image
+ * of a positive double (MIN over ranks = MIN of the doubles). Written by
+ * the last stage of a step and by upload. */
+unsigned long long *amrgpu_session_dt_slot(amrgpu_session_t *s);
+/* Local quads (host array, each < ncell) whose records other ranks need,
+ * grouped by destination rank (the reference's send list). */
+int amrgpu_session_set_halo(amrgpu_session_t *s, const int *send_quads, int nsend);
+/* Records of send entries [first, first+count) of the next stage's input
+ * -> d_out (device, count * 4*n*n doubles), on the session stream. */
+int amrgpu_session_halo_pack(amrgpu_session_t *s, int first, int count, double *d_out);
+/* Records d_in (device) -> ghost quads first_ghost .. first_ghost+count-1
+ * of the next stage's input, on the session stream. */
+int amrgpu_session_halo_unpack(amrgpu_session_t *s, int first_ghost, int count, const double *d_in);
+/* This rank's squared residual norm and flag bits (1 non-finite, 2
+ * negative density or pressure) as of the last amrgpu_session_sync. */
+int amrgpu_session_local_scalars(amrgpu_session_t *s, double *norm_sq, int *flags);
+
 /* ---------------- host forest (stands in for p4est) ---------------- */
 typedef struct amrgpu_forest amrgpu_forest_t;
 amrgpu_forest_t *amrgpu_forest_new_brick(int nx, int ny, int periodic_x, int periodic_y,
