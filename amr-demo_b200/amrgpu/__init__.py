@@ -279,6 +279,12 @@ class Session:
         k = lib().amrgpu_session_launch_variants(self._s, ip(q), ip(t), 64)
         return list(zip(q[:k].tolist(), t[:k].tolist()))
 
+    def set_launch_variant(self, index):
+        check(lib().amrgpu_session_set_launch_variant(self._s, int(index)), "set_launch_variant")
+
+    def launch_variant(self):
+        return lib().amrgpu_session_launch_variant(self._s)
+
     def set_launch(self, qpb, threads):
         check(lib().amrgpu_session_set_launch(self._s, int(qpb), int(threads)), "set_launch")
 

@@ -521,6 +521,34 @@ int amrgpu_session_set_launch(amrgpu_session_t *s, int qpb, int threads)
     return configure_launch(s, L);
 }
 
+int amrgpu_session_set_launch_variant(amrgpu_session_t *s, int index)
+{
+    if (!s) return AMRGPU_ERR_ARG;
+    const StageLaunch *tab;
+    const int cnt = (s->form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
+    int k = 0;
+    for (int i = 0; i < cnt; ++i) {
+        if (tab[i].n != s->n) continue;
+        if (k++ == index) return configure_launch(s, &tab[i]);
+    }
+    set_error(AMRGPU_ERR_ARG, "no compiled variant with that index");
+    return AMRGPU_ERR_ARG;
+}
+
+int amrgpu_session_launch_variant(const amrgpu_session_t *s)
+{
+    if (!s || !s->launch) return -1;
+    const StageLaunch *tab;
+    const int cnt = (s->form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
+    int k = 0;
+    for (int i = 0; i < cnt; ++i) {
+        if (tab[i].n != s->n) continue;
+        if (&tab[i] == s->launch) return k;
+        ++k;
+    }
+    return -1;
+}
+
 int amrgpu_session_launch_variants(const amrgpu_session_t *s, int *qpb, int *threads, int cap)
 {
     if (!s || cap < 0) return -AMRGPU_ERR_ARG;

@@ -157,8 +157,8 @@ def autotune(ag, s, steps=6):
     from amrgpu._lib import lib
     st = torch.cuda.ExternalStream(s.stream())
     best = None
-    for qpb, thr in s.launch_variants():
-        if lib().amrgpu_session_set_launch(s._s, qpb, thr) != 0:
+    for idx, (qpb, thr) in enumerate(s.launch_variants()):
+        if lib().amrgpu_session_set_launch_variant(s._s, idx) != 0:
             ag.clear_error()
             continue
         s.step(3)
@@ -169,9 +169,9 @@ def autotune(ag, s, steps=6):
         e1.synchronize()
         ms = e0.elapsed_time(e1)
         if best is None or ms < best[0]:
-            best = (ms, qpb, thr)
-    s.set_launch(best[1], best[2])
-    return {"quads_per_block": best[1], "threads": best[2]}
+            best = (ms, qpb, thr, idx)
+    s.set_launch_variant(best[3])
+    return {"quads_per_block": best[1], "threads": best[2], "variant": best[3]}
 
 
 def time_form(ag, mesh, cfg, s0, form, steps, warmup, tune_on=True):

@@ -199,6 +199,11 @@ int amrgpu_session_set_launch(amrgpu_session_t *s, int quads_per_block, int thre
  * size (the autotuner's candidates): fills up to cap pairs, returns the count. */
 int amrgpu_session_launch_variants(const amrgpu_session_t *s, int *quads_per_block, int *threads,
                                    int cap);
+/* Selects variant `index` of that list (variants that share a shape are
+ * addressed this way); amrgpu_session_launch_variant returns the current
+ * index. */
+int amrgpu_session_set_launch_variant(amrgpu_session_t *s, int index);
+int amrgpu_session_launch_variant(const amrgpu_session_t *s);
 /* Host AoS soln (reference layout, dof + ghost tail) <-> device SoA state. */
 int amrgpu_session_upload(amrgpu_session_t *s, const double *soln_aos);
 int amrgpu_session_download(amrgpu_session_t *s, double *soln_aos);

@@ -20,7 +20,8 @@ pytestmark = pytest.mark.gpu
 os.environ.setdefault("AMRGPU_QUIET", "1")
 
 BLOCK = (1, 288)
-SWEEPS = [(4, 128), (8, 256), (2, 64)]
+# variant indices of the row sweep for 16x16 patches: (4,128), (2,64), (8,256)
+SWEEPS = [0, 1, 2]
 
 
 def case(ag, seed, scheme):
@@ -41,7 +42,11 @@ def case(ag, seed, scheme):
 
 def run(ag, m, cfg, s0, shape, steps):
     s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
-    s.set_launch(*shape)
+    if isinstance(shape, int):
+        s.set_launch_variant(shape)
+        assert s.launch_variant() == shape
+    else:
+        s.set_launch(*shape)
     s.upload(s0)
     s.step(steps)
     rep = s.sync()
@@ -75,7 +80,7 @@ def test_sweep_rhs_within_fp32_tolerance_of_oracle(ag, oracle, seed):
     f, m, cfg, s0 = case(ag, 400 + seed, 3)
     ref = oracle.rhs(m, s0, oracle.make_config(16, cfg)).reshape(-1, 4)
     s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
-    s.set_launch(*SWEEPS[0])
+    s.set_launch_variant(SWEEPS[0])
     s.upload(s0)
     got = s.rhs().reshape(-1, 4)
     s.close()
@@ -92,13 +97,22 @@ def test_sweep_conserves_on_periodic_hanging_mesh(ag):
     m = f.mesh(n)
     s0 = meshes.perturbed(f.initialize(n), 5, amp=1e-2)
     s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
-    s.set_launch(*SWEEPS[0])
+    s.set_launch_variant(SWEEPS[0])
     s.upload(s0)
     t0 = s.totals()
     s.step(40)
     t1 = s.totals()
     s.close()
     assert np.all(np.abs(t1 - t0) <= 1e-12 * np.abs(t0) + 1e-13), t1 - t0
+
+
+def test_sweep_variants_are_the_row_sweep_kernels(ag):
+    f, m, cfg, s0 = case(ag, 8, 3)
+    s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
+    v = s.launch_variants()
+    assert v[:3] == [(4, 128), (2, 64), (8, 256)]
+    assert s.launch_variant() == 0
+    s.close()
 
 
 def test_sweep_is_the_default_for_16x16_patches(ag):
