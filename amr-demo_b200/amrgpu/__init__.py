@@ -16,6 +16,9 @@ import numpy as np
 from ._lib import (AmrGpuError, ConfigStruct, MeshStruct, ReportStruct, check, lib, LIB_PATH,
                    PROTOTYPES)
 
+QUAD_DESC = np.dtype([("side", np.int32, (4, 6)), ("corner", np.float64, (8,))])
+assert QUAD_DESC.itemsize == 160
+
 FORM_FP64_EXACT = 0
 FORM_FP32_FLUX = 1
 
@@ -122,6 +125,39 @@ class Mesh:
         return self.cell_info[1::3][: self.ncell].copy()
 
 
+class ForestMesh:
+    """The mesh of a forest as a session built it on the device
+    (Session.regrid_forest): sizes at once, the host arrays (cell_info,
+    face_info, geom) from amrgpu_forest_external on first use -- valid while
+    the forest is unchanged."""
+
+    def __init__(self, forest, n, nface):
+        self.forest = forest
+        self.n = int(n)
+        self.ncell = forest.num_quads
+        self.nghost = 0
+        self.nface = int(nface)
+        self.dof = NFIELDS * self.n * self.n * self.ncell
+        self._version = forest.version
+        self._full = None
+
+    @property
+    def ncells(self):
+        return self.ncell * self.n * self.n
+
+    def full(self):
+        if self._full is None:
+            if self.forest.version != self._version:
+                raise RuntimeError("the forest changed since this mesh was built")
+            self._full = self.forest.mesh(self.n)
+        return self._full
+
+    def __getattr__(self, name):
+        if name in ("cell_info", "face_info", "geom", "struct", "levels"):
+            return getattr(self.full(), name)
+        raise AttributeError(name)
+
+
 class Forest:
     """Host quadtree forest on a brick of trees (stands in for p4est)."""
 
@@ -133,6 +169,7 @@ class Forest:
         if not self._f:
             raise AmrGpuError(L.amrgpu_last_error(), "forest_new_brick")
         self.scale = float(scale)
+        self.version = 0  # bumped by every change of the leaves
 
     def __del__(self):
         f = getattr(self, "_f", None)
@@ -170,6 +207,7 @@ class Forest:
         f = cls.__new__(cls)
         f._f = h.value
         f.scale = None
+        f.version = 0
         return f, n.value, soln, ist.value, t.value
 
     def quads(self):
@@ -187,14 +225,17 @@ class Forest:
     def refine(self, flags, max_level=30):
         fl = np.ascontiguousarray(flags, dtype=np.int32)
         assert len(fl) == self.num_quads
+        self.version += 1
         return lib().amrgpu_forest_refine(self._f, ip(fl), int(max_level))
 
     def coarsen(self, flags, min_level=0):
         fl = np.ascontiguousarray(flags, dtype=np.int32)
         assert len(fl) == self.num_quads
+        self.version += 1
         return lib().amrgpu_forest_coarsen(self._f, ip(fl), int(min_level))
 
     def balance(self):
+        self.version += 1
         r = lib().amrgpu_forest_balance(self._f)
         if r < 0:
             raise AmrGpuError(3, "forest_balance")
@@ -346,6 +387,23 @@ class Session:
         ms = mesh.struct()
         check(lib().amrgpu_session_regrid(self._s, C.byref(ms), ip(k), ip(s)), "regrid")
         self.mesh = mesh
+
+    def regrid_forest(self, forest):
+        """In place, from the forest after refine / coarsen / balance: quad
+        descriptors built on the device, state remapped by the forest's
+        remap table (amrgpu_session_regrid_forest)."""
+        check(lib().amrgpu_session_regrid_forest(self._s, C.c_void_p(forest._f)), "regrid_forest")
+        self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s))
+
+    def quad_descriptors(self):
+        """The device quad descriptors as a structured array (kind, nbr0,
+        nbr1, rank, level, bc per side; 8 corner doubles)."""
+        n = self.mesh.ncell
+        out = np.zeros(n, dtype=QUAD_DESC)
+        k = lib().amrgpu_session_quad_descriptors(self._s, out.ctypes.data_as(C.c_void_p), n)
+        if k < 0:
+            raise AmrGpuError(-k, "quad_descriptors")
+        return out
 
     def state_ptr(self, field):
         return lib().amrgpu_session_state_device(self._s, int(field))

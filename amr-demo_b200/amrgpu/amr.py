@@ -104,9 +104,11 @@ def host_tags(n, rho_tol, method=5):
     return tag
 
 
-def regrid(forest, session, n, min_level, max_level, config=None, form=None):
+def regrid(forest, session, n, min_level, max_level, config=None, form=None, device_mesh=True):
     """One regrid of the session in place (its mesh and state follow the
-    forest); returns the session."""
+    forest); returns the session. device_mesh: the quad descriptors are
+    built on the GPU from the forest (Session.regrid_forest); otherwise the
+    host lists the mesh arrays and the session decodes them."""
     tags = session.tag()
     _, lev, _, _ = forest.quads()
     forest.begin_regrid()
@@ -116,8 +118,11 @@ def regrid(forest, session, n, min_level, max_level, config=None, form=None):
     _, lev2, _, _ = forest.quads()
     forest.coarsen(((tags2 == 0) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
     forest.balance()
-    kind, src = forest.remap()
-    session.regrid(forest.mesh(n), kind, src)
+    if device_mesh:
+        session.regrid_forest(forest)
+    else:
+        kind, src = forest.remap()
+        session.regrid(forest.mesh(n), kind, src)
     return session
 
 

@@ -43,6 +43,14 @@ void forest_quad_corners(const Forest *f, const Leaf &q, double xyz[12]);
 std::vector<unsigned char> forest_save(const Forest *f);
 Forest *forest_load(const unsigned char *data, size_t size);
 double forest_quad_h(const Forest *f, const Leaf &q);
+// The brick a forest lives on: size, periodicity, origin and scale, tree id
+// -> brick position (tree_tx, tree_ty) and back (tree_at[ty*nx+tx]).
+struct BrickView {
+    int nx, ny, periodic[2];
+    double xlo[3], scale;
+    const int *tree_tx, *tree_ty, *tree_at;
+};
+void forest_brick(const Forest *f, BrickView *out);
 int forest_external(const Forest *f, int nelem_subgrid, int nfields, int *cell_info,
                     int *face_info, double *geom, int *nface_out, int *dof_out);
 

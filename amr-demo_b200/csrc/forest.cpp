@@ -433,6 +433,19 @@ bool forest_is_balanced(const Forest *f)
 
 // amr_p4est_utilities.c:15-81, 2D branch: corners of a quadrant through the
 // brick tree's vertices (vertex = integer brick position * scale + lo).
+void forest_brick(const Forest *f, BrickView *out)
+{
+    out->nx = f->nx;
+    out->ny = f->ny;
+    out->periodic[0] = f->periodic[0];
+    out->periodic[1] = f->periodic[1];
+    for (int k = 0; k < 3; ++k) out->xlo[k] = f->xlo[k];
+    out->scale = f->scale;
+    out->tree_tx = f->tree_tx.data();
+    out->tree_ty = f->tree_ty.data();
+    out->tree_at = f->tree_at.data();
+}
+
 void forest_quad_corners(const Forest *f, const Leaf &q, double xyz[12])
 {
     const double intsize = 1.0 / double(kRootLen);

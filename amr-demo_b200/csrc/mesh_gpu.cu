@@ -1,0 +1,264 @@
+// mesh_gpu.cu -- the quad descriptors of a forest's mesh built on the GPU.
+//
+// After a regrid the host forest has its new leaves (tree, level, x, y in
+// Morton order). The reference's driver then lists the mesh's faces
+// (amr_external.c:389-507) and the solver decodes them per quad
+// (physics_rhs_structured.c:73-262); the host path of this library does the
+// same (forest_external, then decode_mesh). Here the device does both in
+// one pass per (leaf, side), with the forest's rules of forest_external:
+//
+//   * the side's same-level neighbour region (across tree faces of the
+//     brick, periodic where the brick is) and the leaf holding it, found by
+//     binary search over the leaves' Morton keys within the tree;
+//   * the face type: boundary, full (same level), hanging with this leaf
+//     fine (coarser neighbour) or coarse (two finer neighbours);
+//   * the face's emitter, the participant with the smallest index, from
+//     its side (a leaf that is its own periodic neighbour emits from its
+//     even side): faces are numbered in emission order, leaf by leaf, sides
+//     0..3, so an exclusive scan of the per-(leaf, side) "emits" flags
+//     gives every face its index in the host's face list;
+//   * the side descriptor the host decode writes (kind, neighbours, the
+//     level that sizes the face, the boundary condition) and the face
+//     index as accumulation rank; the corners with the host's arithmetic
+//     (forest_quad_corners), each operation explicitly rounded.
+//
+// A 2:1 violation is reported through status[0]; status[1] gets the face
+// count. The result is byte-identical to decode_mesh(forest_external(...)).
+#include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
+
+#include "device_common.cuh"
+#include "mesh_gpu.h"
+
+namespace amrgpu {
+
+namespace {
+
+constexpr int kMaxLevelG = 30;
+constexpr long long kRootLenG = 1ll << kMaxLevelG;
+
+__device__ __forceinline__ long long qlen_d(int level) { return 1ll << (kMaxLevelG - level); }
+
+__device__ __forceinline__ unsigned long long spread_bits_d(unsigned long long v)
+{
+    v &= 0xffffffffULL;
+    v = (v | (v << 16)) & 0x0000ffff0000ffffULL;
+    v = (v | (v << 8)) & 0x00ff00ff00ff00ffULL;
+    v = (v | (v << 4)) & 0x0f0f0f0f0f0f0f0fULL;
+    v = (v | (v << 2)) & 0x3333333333333333ULL;
+    v = (v | (v << 1)) & 0x5555555555555555ULL;
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long morton_d(long long x, long long y)
+{
+    return spread_bits_d((unsigned long long)x) | (spread_bits_d((unsigned long long)y) << 1);
+}
+
+struct KeyD {
+    int tree;
+    long long x, y;
+};
+
+__device__ bool shifted_d(const ForestDev &F, int tree, int level, long long x, long long y, int dx, int dy,
+                          KeyD &out)
+{
+    const long long L = qlen_d(level);
+    long long nxq = x + dx * L, nyq = y + dy * L;
+    int tx = F.tree_tx[tree], ty = F.tree_ty[tree];
+    if (nxq < 0) { nxq += kRootLenG; tx -= 1; }
+    if (nxq >= kRootLenG) { nxq -= kRootLenG; tx += 1; }
+    if (nyq < 0) { nyq += kRootLenG; ty -= 1; }
+    if (nyq >= kRootLenG) { nyq -= kRootLenG; ty += 1; }
+    if (tx < 0 || tx >= F.nx) {
+        if (!F.px) return false;
+        tx = (tx + F.nx) % F.nx;
+    }
+    if (ty < 0 || ty >= F.ny) {
+        if (!F.py) return false;
+        ty = (ty + F.ny) % F.ny;
+    }
+    out.tree = F.tree_at[ty * F.nx + tx];
+    out.x = nxq;
+    out.y = nyq;
+    return true;
+}
+
+// last leaf of the tree whose corner precedes (x,y) on the Morton curve
+__device__ int locate_d(const ForestDev &F, int tree, long long x, long long y)
+{
+    const unsigned long long m = morton_d(x, y);
+    int lo = F.tree_begin[tree], hi = F.tree_begin[tree + 1];  // upper_bound in [lo, hi)
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (F.keys[mid] <= m) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo - 1;
+}
+
+__device__ int find_d(const ForestDev &F, int tree, int level, long long x, long long y)
+{
+    const int c = locate_d(F, tree, x, y);
+    if (c < 0) return -1;
+    const int4 l = F.leaves[c];
+    return (l.y == level && l.z == x && l.w == y) ? c : -1;
+}
+
+__global__ void keys_kernel(ForestDev F)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nq; i += gridDim.x * blockDim.x) {
+        const int4 l = F.leaves[i];
+        F.keys[i] = morton_d(l.z, l.w);
+    }
+}
+
+// One thread per (leaf, side): the side descriptor (rank filled later), the
+// emits flag and the emitter slot; the leaf's corners from side 0's thread.
+__global__ void sides_kernel(ForestDev F, QuadDesc *out, int *emits, int *emitter, int *status)
+{
+    const int total = 4 * F.nq;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int i = t >> 2, s = t & 3;
+        const int4 q = F.leaves[i];  // tree, level, x, y
+        const int dx = s == 0 ? -1 : (s == 1 ? 1 : 0);
+        const int dy = s == 2 ? -1 : (s == 3 ? 1 : 0);
+        const int opp = s ^ 1;
+        SideDesc d;
+        d.kind = kSideNone;
+        d.nbr0 = -1;
+        d.nbr1 = -1;
+        d.rank = -1;
+        d.level = q.y;
+        d.bc = 0;
+        int emit = 0, em = t;
+        KeyD k;
+        if (!shifted_d(F, q.x, q.y, q.z, q.w, dx, dy, k)) {
+            d.kind = kSideBoundary;
+            d.bc = F.bc[s];
+            emit = 1;
+        } else {
+            const int c0 = locate_d(F, k.tree, k.x, k.y);
+            const int lvl0 = c0 >= 0 ? F.leaves[c0].y : -1;
+            if (c0 < 0 || lvl0 < q.y - 1) {
+                atomicOr(status, 1);  // neighbour two or more levels coarser
+            } else if (lvl0 == q.y) {
+                const int j = c0;
+                d.kind = kSideFull;
+                d.nbr0 = j;
+                emit = (i < j) || (i == j && (s & 1) == 0);
+                em = (i < j) ? t : (i > j ? 4 * j + opp : 4 * i + (s & ~1));
+            } else if (lvl0 == q.y - 1) {
+                // this leaf is one of the two fine leaves of a hanging face
+                const int c = c0;
+                const long long Lp = qlen_d(q.y - 1), L = qlen_d(q.y);
+                const long long bx = ((long long)q.z / Lp) * Lp, by = ((long long)q.w / Lp) * Lp;
+                int fine[2];
+                for (int h = 0; h < 2; ++h)
+                    fine[h] = (s < 2) ? find_d(F, q.x, q.y, q.z, by + h * L) : find_d(F, q.x, q.y, bx + h * L, q.w);
+                if (fine[0] < 0 || fine[1] < 0) {
+                    atomicOr(status, 2);
+                } else {
+                    d.kind = kSideFineHang;
+                    d.nbr0 = c;
+                    const int mf = min(fine[0], fine[1]);
+                    const int mn = min(c, mf);
+                    emit = (i == mn);
+                    em = (mn == c) ? 4 * c + opp : 4 * mn + s;
+                }
+            } else {
+                // this leaf is the coarse side: two finer neighbours
+                const long long Lc = qlen_d(q.y + 1);
+                int fine[2];
+                for (int h = 0; h < 2; ++h) {
+                    if (s < 2) fine[h] = find_d(F, k.tree, q.y + 1, (s == 0) ? k.x + Lc : k.x, k.y + h * Lc);
+                    else fine[h] = find_d(F, k.tree, q.y + 1, k.x + h * Lc, (s == 2) ? k.y + Lc : k.y);
+                }
+                if (fine[0] < 0 || fine[1] < 0) {
+                    atomicOr(status, 2);
+                } else {
+                    d.kind = kSideCoarseHang;
+                    d.nbr0 = fine[0];
+                    d.nbr1 = fine[1];
+                    d.level = q.y + 1;
+                    const int mf = min(fine[0], fine[1]);
+                    emit = i < mf;
+                    em = emit ? t : 4 * mf + opp;
+                }
+            }
+        }
+        out[i].side[s] = d;
+        emits[t] = emit;
+        emitter[t] = em;
+        if (s == 0) {
+            // forest_quad_corners: bilinear map of the tree's brick square
+            const double intsize = 1.0 / double(kRootLenG);
+            const double h2 = __dmul_rn(__dmul_rn(0.5, intsize), double(qlen_d(q.y)));
+            const int tx = F.tree_tx[q.x], ty = F.tree_ty[q.x];
+            double v[4][2];
+            for (int c = 0; c < 4; ++c) {
+                const int vx = tx + (c & 1), vy = ty + ((c >> 1) & 1);
+                v[c][0] = __dadd_rn(__dmul_rn(double(vx), F.scale), F.xlo[0]);
+                v[c][1] = __dadd_rn(__dmul_rn(double(vy), F.scale), F.xlo[1]);
+            }
+            const double one_z = __dsub_rn(1.0, 0.0);  // (1 - eta_z), eta_z = 0
+            int kk = 0;
+            for (int yi = 0; yi < 2; ++yi) {
+                const double ey = __dadd_rn(__dmul_rn(intsize, double(q.w)), __dmul_rn(h2, 1.0 + (2 * yi - 1)));
+                for (int xi = 0; xi < 2; ++xi) {
+                    const double ex = __dadd_rn(__dmul_rn(intsize, double(q.z)), __dmul_rn(h2, 1.0 + (2 * xi - 1)));
+                    for (int j = 0; j < 2; ++j) {
+                        const double lo_ = __dadd_rn(__dmul_rn(__dsub_rn(1.0, ex), v[0][j]), __dmul_rn(ex, v[1][j]));
+                        const double hi_ = __dadd_rn(__dmul_rn(__dsub_rn(1.0, ex), v[2][j]), __dmul_rn(ex, v[3][j]));
+                        out[i].corner[2 * kk + j] =
+                            __dmul_rn(one_z, __dadd_rn(__dmul_rn(__dsub_rn(1.0, ey), lo_), __dmul_rn(ey, hi_)));
+                    }
+                    ++kk;
+                }
+            }
+        }
+    }
+}
+
+__global__ void rank_kernel(int nq, QuadDesc *out, const int *emits, const int *scan, const int *emitter,
+                            int *status)
+{
+    const int total = 4 * nq;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        out[t >> 2].side[t & 3].rank = scan[emitter[t]];
+        if (t == total - 1) status[1] = scan[t] + emits[t];
+    }
+}
+
+int grid_for(long long n, int sms)
+{
+    long long g = (n + 255) / 256;
+    const long long cap = (long long)sms * 16;
+    return int(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+}  // namespace
+
+size_t build_quads_scan_bytes(int nq)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int *)nullptr, (int *)nullptr, 4 * (nq > 0 ? nq : 1));
+    return bytes;
+}
+
+cudaError_t launch_build_quads(const ForestDev &F, QuadDesc *out, int *emits, int *scan, int *emitter,
+                               void *scan_tmp, size_t scan_bytes, int *status, int sms, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(status, 0, 2 * sizeof(int), st);
+    if (e != cudaSuccess || F.nq <= 0) return e;
+    keys_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F);
+    sides_kernel<<<grid_for(4ll * F.nq, sms), 256, 0, st>>>(F, out, emits, emitter, status);
+    size_t bytes = scan_bytes;
+    e = cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, emits, scan, 4 * F.nq, st);
+    if (e != cudaSuccess) return e;
+    rank_kernel<<<grid_for(4ll * F.nq, sms), 256, 0, st>>>(F.nq, out, emits, scan, emitter, status);
+    return cudaGetLastError();
+}
+
+}  // namespace amrgpu

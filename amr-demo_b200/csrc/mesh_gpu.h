@@ -1,0 +1,34 @@
+// mesh_gpu.h -- host launcher of mesh_gpu.cu (quad descriptors of a forest
+// built on the GPU).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace amrgpu {
+
+struct QuadDesc;
+
+// Device view of a forest's leaves and brick.
+struct ForestDev {
+    const int4 *leaves;        // (tree, level, x, y) per leaf, Morton order within trees
+    unsigned long long *keys;  // Morton key per leaf (written by the build)
+    const int *tree_begin;     // first leaf of each tree, ntrees + 1 entries
+    const int *tree_tx, *tree_ty, *tree_at;
+    int nx, ny, px, py;
+    double xlo[3];
+    double scale;
+    int bc[4];
+    int nq;
+};
+
+// Scratch of the face-numbering scan for nq leaves.
+size_t build_quads_scan_bytes(int nq);
+
+// out[0..nq): descriptors; emits / scan / emitter: 4*nq ints each;
+// status (device, 2 ints): [0] 2:1 violation bits, [1] face count.
+cudaError_t launch_build_quads(const ForestDev &F, QuadDesc *out, int *emits, int *scan, int *emitter,
+                               void *scan_tmp, size_t scan_bytes, int *status, int sms, cudaStream_t st);
+
+}  // namespace amrgpu

@@ -27,6 +27,7 @@
 #include "device_common.cuh"
 #include "launch_table.h"
 #include "halo_kernels.h"
+#include "mesh_gpu.h"
 #include "misc_kernels.h"
 #include "stage_kernel.cuh"
 
@@ -98,7 +99,15 @@ struct amrgpu_session {
     int partial_cap = 0;
     double *d_tot = nullptr;
     long long cap_stride = 0;  // cells per field the state buffers hold
-    int cap_quads = 0;         // quads the descriptor, tag and remap arrays hold
+    int cap_quads = 0;         // quads the tag and remap arrays hold
+    int cap_desc = 0;          // quads d_quads holds
+    QuadDesc *d_quads_alt = nullptr;  // build target of amrgpu_session_regrid_forest
+    int cap_desc_alt = 0;
+    void *h_stage = nullptr;          // pinned staging of a forest's leaves
+    size_t h_stage_bytes = 0;
+    void *d_mesh_scratch = nullptr;   // device scratch of the descriptor build
+    size_t mesh_scratch_bytes = 0;
+    bool rect = true;                 // every quad an axis-aligned rectangle
     int *d_tags = nullptr;
     int *d_kind = nullptr;
     int *d_src = nullptr;
@@ -245,7 +254,7 @@ int configure_launch(amrgpu_session *s, const StageLaunch *L)
         set_error(AMRGPU_ERR_UNSUPPORTED, "no stage kernel for this patch size");
         return AMRGPU_ERR_UNSUPPORTED;
     }
-    if (s->form == AMRGPU_FORM_FP32_FLUX && !quads_are_rectangles(s)) {
+    if (s->form == AMRGPU_FORM_FP32_FLUX && !s->rect) {
         set_error(AMRGPU_ERR_UNSUPPORTED, "the FP32-flux form needs axis-aligned rectangular quads");
         return AMRGPU_ERR_UNSUPPORTED;
     }
@@ -458,6 +467,8 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const 
     if (ok) ok = cuda_ok(cudaMalloc(&s->d_tot, sizeof(double) * 4 * size_t(totals_grid(std::max<long long>(s->ncells_total, 1)))), "cudaMalloc totals");
     s->cap_stride = s->stride;
     s->cap_quads = std::max(s->nquad, 1);
+    s->cap_desc = s->nquad;
+    s->rect = quads_are_rectangles(s);
     for (int **p : {&s->d_tags, &s->d_kind, &s->d_src})
         if (ok) ok = cuda_ok(cudaMalloc(p, sizeof(int) * size_t(s->cap_quads)), "cudaMalloc quad arrays");
     if (!ok) {
@@ -496,6 +507,9 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_src);
     cudaFree(s->d_scratch);
     cudaFree(s->d_send);
+    cudaFree(s->d_quads_alt);
+    cudaFree(s->d_mesh_scratch);
+    cudaFreeHost(s->h_stage);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -971,6 +985,129 @@ int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int
     return prime(dst);
 }
 
+}  // extern "C"
+
+namespace {
+
+// Per-quad tag and remap arrays for nq quads (grown by a quarter beyond the
+// need so that a slowly growing mesh reallocates rarely; cudaFree
+// synchronises the device).
+int ensure_quad_arrays(amrgpu_session *s, int nq)
+{
+    if (nq <= s->cap_quads) return AMRGPU_OK;
+    const int cap = nq + nq / 4;
+    int *arr[3] = {nullptr, nullptr, nullptr};
+    bool ok = true;
+    for (int k = 0; k < 3 && ok; ++k) ok = cuda_ok(cudaMalloc(&arr[k], sizeof(int) * size_t(cap)), "cudaMalloc quad arrays");
+    if (!ok) {
+        for (int *p : arr) cudaFree(p);
+        return AMRGPU_ERR_CUDA;
+    }
+    cudaStreamSynchronize(s->stream);
+    cudaFree(s->d_tags);
+    cudaFree(s->d_kind);
+    cudaFree(s->d_src);
+    s->d_tags = arr[0];
+    s->d_kind = arr[1];
+    s->d_src = arr[2];
+    s->cap_quads = cap;
+    return AMRGPU_OK;
+}
+
+// A descriptor buffer for at least nq quads (contents not kept).
+int ensure_desc(amrgpu_session *s, QuadDesc **buf, int *cap, int nq)
+{
+    if (nq <= *cap && *buf) return AMRGPU_OK;
+    const int c = std::max(nq + nq / 4, 1);
+    QuadDesc *d = nullptr;
+    if (!cuda_ok(cudaMalloc(&d, sizeof(QuadDesc) * size_t(c)), "cudaMalloc quads")) return AMRGPU_ERR_CUDA;
+    cudaStreamSynchronize(s->stream);
+    cudaFree(*buf);
+    *buf = d;
+    *cap = c;
+    return AMRGPU_OK;
+}
+
+// The state moves to the new mesh of nq quads (descriptors already in
+// d_quads, remap kind / source in d_kind / d_src): into the spare buffer Y
+// of the same capacity, or a fresh set when the mesh outgrew the capacity.
+int apply_regrid(amrgpu_session *s, int nq, int nface)
+{
+    const long long cells = (long long)nq * s->n * s->n;
+    const long long stride = std::max<long long>(((cells + 31) / 32) * 32, 32);
+    double *qold = rolebuf(s, RX);
+    const long long old_stride = s->stride;
+    double *fresh[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long cap = s->cap_stride;
+    bool ok = true;
+    if (stride > s->cap_stride) {
+        cap = ((stride + stride / 4 + 31) / 32) * 32;
+        for (int k = 0; k < 4 && ok; ++k)
+            ok = cuda_ok(cudaMalloc(&fresh[k], sizeof(double) * 4 * size_t(cap)), "cudaMalloc state");
+        double *aos = nullptr;
+        double *tot = nullptr;
+        if (ok) ok = cuda_ok(cudaMalloc(&aos, sizeof(double) * 4 * size_t(cap)), "cudaMalloc aos");
+        if (ok) ok = cuda_ok(cudaMalloc(&tot, sizeof(double) * 4 * size_t(totals_grid(cap))), "cudaMalloc totals");
+        if (!ok) {
+            for (double *p : fresh) cudaFree(p);
+            cudaFree(aos);
+            cudaFree(tot);
+            return AMRGPU_ERR_CUDA;
+        }
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->d_aos);
+        cudaFree(s->d_tot);
+        s->d_aos = aos;
+        s->d_tot = tot;
+    }
+    double *qnew = fresh[0] ? fresh[0] : rolebuf(s, RY);
+    if (nq > 0) {
+        ok = cuda_ok(launch_remap(s->n, qold, old_stride, qnew, stride, s->d_kind, s->d_src, nq, s->stream),
+                     "remap kernel");
+        s->launches++;
+    }
+    if (!ok) {
+        for (double *p : fresh) cudaFree(p);
+        return AMRGPU_ERR_CUDA;
+    }
+    if (fresh[0]) {
+        cudaStreamSynchronize(s->stream);
+        for (int k = 0; k < 4; ++k) {
+            cudaFree(s->buf[k]);
+            s->buf[k] = fresh[k];
+            s->role[k] = k;
+        }
+        s->cap_stride = cap;
+    } else {
+        std::swap(s->role[RX], s->role[RY]);
+    }
+    s->nquad = nq;
+    s->nghost = 0;
+    s->nface = nface;
+    s->dof = 4 * s->n * s->n * nq;
+    s->ncells_total = cells;
+    s->stride = stride;
+    int rc = configure_launch(s, s->launch);
+    if (rc != AMRGPU_OK) return rc;
+    return prime(s, s->primed);
+}
+
+bool check_remap(const amrgpu_session *s, int nq, const int *kind, const int *src_index)
+{
+    for (int q = 0; q < nq; ++q) {
+        const int lim = kind[q] == 0 ? s->nquad - 1 : s->nquad - 4;
+        if ((kind[q] != 0 && kind[q] != 1) || src_index[q] < 0 || src_index[q] > lim) {
+            set_error(AMRGPU_ERR_ARG, "remap kind or source index out of range");
+            return false;
+        }
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
 int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int *kind, const int *src_index)
 {
     if (!s || !m || !kind || !src_index || !m->cell_info || !m->geom || (m->nface > 0 && !m->face_info) ||
@@ -990,13 +1127,7 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
         set_error(AMRGPU_ERR_MESH, "dof != 4*n*n*ncell");
         return AMRGPU_ERR_MESH;
     }
-    for (int q = 0; q < m->ncell; ++q) {
-        int lim = kind[q] == 0 ? s->nquad - 1 : s->nquad - 4;
-        if ((kind[q] != 0 && kind[q] != 1) || src_index[q] < 0 || src_index[q] > lim) {
-            set_error(AMRGPU_ERR_ARG, "remap kind or source index out of range");
-            return AMRGPU_ERR_ARG;
-        }
-    }
+    if (!check_remap(s, m->ncell, kind, src_index)) return AMRGPU_ERR_ARG;
     std::vector<QuadDesc> old = std::move(s->h_quads);
     int rc = decode_mesh(s, m);
     if (rc == AMRGPU_OK && s->form == AMRGPU_FORM_FP32_FLUX && !quads_are_rectangles(s)) {
@@ -1008,100 +1139,161 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
         return rc;
     }
     const int nq = m->ncell;
-    const long long cells = (long long)nq * s->n * s->n;
-    const long long stride = std::max<long long>(((cells + 31) / 32) * 32, 32);
-    // per-quad arrays: grow by a quarter beyond the need so that a slowly
-    // growing mesh reallocates rarely (cudaFree synchronises the device)
-    if (nq > s->cap_quads) {
-        int cap = nq + nq / 4;
-        QuadDesc *dq = nullptr;
-        bool ok = cuda_ok(cudaMalloc(&dq, sizeof(QuadDesc) * size_t(cap)), "cudaMalloc quads");
-        int *arr[3] = {nullptr, nullptr, nullptr};
-        for (int k = 0; k < 3 && ok; ++k) ok = cuda_ok(cudaMalloc(&arr[k], sizeof(int) * size_t(cap)), "cudaMalloc quad arrays");
-        if (!ok) {
-            cudaFree(dq);
-            for (int *p : arr) cudaFree(p);
-            s->h_quads = std::move(old);
-            return AMRGPU_ERR_CUDA;
-        }
-        cudaStreamSynchronize(s->stream);
-        cudaFree(s->d_quads);
-        cudaFree(s->d_tags);
-        cudaFree(s->d_kind);
-        cudaFree(s->d_src);
-        s->d_quads = dq;
-        s->d_tags = arr[0];
-        s->d_kind = arr[1];
-        s->d_src = arr[2];
-        s->cap_quads = cap;
+    rc = ensure_quad_arrays(s, nq);
+    if (rc == AMRGPU_OK) rc = ensure_desc(s, &s->d_quads, &s->cap_desc, nq);
+    if (rc != AMRGPU_OK) {
+        s->h_quads = std::move(old);
+        return rc;
     }
     bool ok = cuda_ok(cudaMemcpyAsync(s->d_kind, kind, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, s->stream),
                       "H2D remap") &&
               cuda_ok(cudaMemcpyAsync(s->d_src, src_index, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice,
                                       s->stream),
                       "H2D remap");
-    // the new state goes to a buffer other than X: the spare Y of the same
-    // capacity, or a fresh set when the mesh outgrew the capacity
-    double *qold = rolebuf(s, RX);
-    const long long old_stride = s->stride;
-    double *fresh[4] = {nullptr, nullptr, nullptr, nullptr};
-    long long cap = s->cap_stride;
-    if (ok && stride > s->cap_stride) {
-        cap = ((stride + stride / 4 + 31) / 32) * 32;
-        for (int k = 0; k < 4 && ok; ++k)
-            ok = cuda_ok(cudaMalloc(&fresh[k], sizeof(double) * 4 * size_t(cap)), "cudaMalloc state");
-        double *aos = nullptr;
-        double *tot = nullptr;
-        if (ok) ok = cuda_ok(cudaMalloc(&aos, sizeof(double) * 4 * size_t(cap)), "cudaMalloc aos");
-        if (ok) ok = cuda_ok(cudaMalloc(&tot, sizeof(double) * 4 * size_t(totals_grid(cap))), "cudaMalloc totals");
-        if (!ok) {
-            for (double *p : fresh) cudaFree(p);
-            cudaFree(aos);
-            cudaFree(tot);
-            s->h_quads = std::move(old);
-            return AMRGPU_ERR_CUDA;
-        }
-        cudaStreamSynchronize(s->stream);
-        cudaFree(s->d_aos);
-        cudaFree(s->d_tot);
-        s->d_aos = aos;
-        s->d_tot = tot;
-    }
-    double *qnew = fresh[0] ? fresh[0] : rolebuf(s, RY);
-    if (ok && nq > 0) {
-        ok = cuda_ok(launch_remap(s->n, qold, old_stride, qnew, stride, s->d_kind, s->d_src, nq, s->stream),
-                     "remap kernel");
-        s->launches++;
-    }
     if (ok && nq > 0)
         ok = cuda_ok(cudaMemcpyAsync(s->d_quads, s->h_quads.data(), sizeof(QuadDesc) * size_t(nq),
                                      cudaMemcpyHostToDevice, s->stream),
                      "upload quads");
-    if (!ok) {
-        for (double *p : fresh) cudaFree(p);
-        return AMRGPU_ERR_CUDA;
-    }
-    if (fresh[0]) {
-        cudaStreamSynchronize(s->stream);
-        for (int k = 0; k < 4; ++k) {
-            cudaFree(s->buf[k]);
-            s->buf[k] = fresh[k];
-            s->role[k] = k;
-        }
-        s->cap_stride = cap;
-    } else {
-        std::swap(s->role[RX], s->role[RY]);
-    }
-    s->nquad = nq;
-    s->nghost = 0;
-    s->nface = m->nface;
-    s->dof = m->dof;
-    s->ncells_total = cells;
-    s->stride = stride;
-    rc = configure_launch(s, s->launch);
-    if (rc != AMRGPU_OK) return rc;
-    return prime(s, s->primed);
+    if (!ok) return AMRGPU_ERR_CUDA;
+    s->rect = (s->form != AMRGPU_FORM_FP32_FLUX) ? quads_are_rectangles(s) : true;
+    return apply_regrid(s, nq, m->nface);
 }
+
+int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f)
+{
+    if (!s || !f || !f->f) return AMRGPU_ERR_ARG;
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_regrid_forest: a step begun with step_stage is not finished");
+        return AMRGPU_ERR_ARG;
+    }
+    if (s->nghost != 0) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "session_regrid_forest: ghost quads need a ghost exchange after the remap");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    const std::vector<Leaf> &L = forest_leaves(f->f);
+    BrickView B;
+    forest_brick(f->f, &B);
+    const int nq = int(L.size());
+    const int ntrees = B.nx * B.ny;
+    // pinned staging: leaves (int4), kind, src, tree_begin, tree_tx, tree_ty, tree_at
+    const size_t n_int = 4 * size_t(nq) + 2 * size_t(nq) + size_t(ntrees + 1) + 3 * size_t(ntrees);
+    const size_t stage_bytes = sizeof(int) * n_int;
+    if (stage_bytes > s->h_stage_bytes) {
+        cudaStreamSynchronize(s->stream);
+        cudaFreeHost(s->h_stage);
+        s->h_stage = nullptr;
+        s->h_stage_bytes = 0;
+        const size_t want = stage_bytes + stage_bytes / 4;
+        if (!cuda_ok(cudaHostAlloc(&s->h_stage, want, cudaHostAllocDefault), "cudaHostAlloc staging"))
+            return AMRGPU_ERR_CUDA;
+        s->h_stage_bytes = want;
+    } else {
+        // the previous regrid's copies out of the staging buffer have finished
+        if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return AMRGPU_ERR_CUDA;
+    }
+    int *hs = static_cast<int *>(s->h_stage);
+    int *h_leaves = hs, *h_kind = hs + 4 * size_t(nq), *h_src = h_kind + nq, *h_tb = h_src + nq;
+    int *h_tx = h_tb + ntrees + 1, *h_ty = h_tx + ntrees, *h_at = h_ty + ntrees;
+    for (int t = 0; t <= ntrees; ++t) h_tb[t] = nq;
+    for (int i = nq - 1; i >= 0; --i) {
+        const Leaf &q = L[size_t(i)];
+        h_leaves[4 * i + 0] = q.tree;
+        h_leaves[4 * i + 1] = q.level;
+        h_leaves[4 * i + 2] = int(q.x);
+        h_leaves[4 * i + 3] = int(q.y);
+        h_kind[i] = q.src_kind;
+        h_src[i] = q.src;
+        h_tb[q.tree] = i;
+    }
+    for (int t = ntrees - 1; t >= 0; --t) h_tb[t] = std::min(h_tb[t], h_tb[t + 1]);
+    for (int t = 0; t < ntrees; ++t) {
+        h_tx[t] = B.tree_tx[t];
+        h_ty[t] = B.tree_ty[t];
+        h_at[t] = B.tree_at[t];
+    }
+    if (!check_remap(s, nq, h_kind, h_src)) return AMRGPU_ERR_ARG;
+    int rc = ensure_quad_arrays(s, nq);
+    if (rc == AMRGPU_OK) rc = ensure_desc(s, &s->d_quads_alt, &s->cap_desc_alt, nq);
+    if (rc != AMRGPU_OK) return rc;
+    // device scratch: staged ints, keys, emits / scan / emitter, scan temp, status
+    const size_t scan_bytes = build_quads_scan_bytes(nq);
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t o_keys = al(stage_bytes);
+    const size_t o_emit = o_keys + al(sizeof(unsigned long long) * size_t(std::max(nq, 1)));
+    const size_t o_scan = o_emit + al(sizeof(int) * 4 * size_t(std::max(nq, 1)));
+    const size_t o_emtr = o_scan + al(sizeof(int) * 4 * size_t(std::max(nq, 1)));
+    const size_t o_tmp = o_emtr + al(sizeof(int) * 4 * size_t(std::max(nq, 1)));
+    const size_t o_stat = o_tmp + al(scan_bytes);
+    const size_t need = o_stat + 256;
+    if (need > s->mesh_scratch_bytes) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->d_mesh_scratch);
+        s->d_mesh_scratch = nullptr;
+        s->mesh_scratch_bytes = 0;
+        const size_t want = need + need / 4;
+        if (!cuda_ok(cudaMalloc(&s->d_mesh_scratch, want), "cudaMalloc mesh scratch")) return AMRGPU_ERR_CUDA;
+        s->mesh_scratch_bytes = want;
+    }
+    char *base = static_cast<char *>(s->d_mesh_scratch);
+    int *d_stage = reinterpret_cast<int *>(base);
+    bool ok = cuda_ok(cudaMemcpyAsync(d_stage, hs, stage_bytes, cudaMemcpyHostToDevice, s->stream), "H2D forest") &&
+              cuda_ok(cudaMemcpyAsync(s->d_kind, h_kind, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice,
+                                      s->stream),
+                      "H2D remap") &&
+              cuda_ok(cudaMemcpyAsync(s->d_src, h_src, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, s->stream),
+                      "H2D remap");
+    if (!ok) return AMRGPU_ERR_CUDA;
+    ForestDev F;
+    F.leaves = reinterpret_cast<const int4 *>(d_stage);
+    F.keys = reinterpret_cast<unsigned long long *>(base + o_keys);
+    const int *d_tb = d_stage + (h_tb - hs);
+    F.tree_begin = d_tb;
+    F.tree_tx = d_stage + (h_tx - hs);
+    F.tree_ty = d_stage + (h_ty - hs);
+    F.tree_at = d_stage + (h_at - hs);
+    F.nx = B.nx;
+    F.ny = B.ny;
+    F.px = B.periodic[0];
+    F.py = B.periodic[1];
+    for (int k = 0; k < 3; ++k) F.xlo[k] = B.xlo[k];
+    F.scale = B.scale;
+    for (int k = 0; k < 4; ++k) F.bc[k] = s->cfg.bc[k];
+    F.nq = nq;
+    int *d_status = reinterpret_cast<int *>(base + o_stat);
+    if (!cuda_ok(launch_build_quads(F, s->d_quads_alt, reinterpret_cast<int *>(base + o_emit),
+                                    reinterpret_cast<int *>(base + o_scan), reinterpret_cast<int *>(base + o_emtr),
+                                    base + o_tmp, scan_bytes, d_status, s->sms, s->stream),
+                 "build quads"))
+        return AMRGPU_ERR_CUDA;
+    s->launches += nq > 0 ? 4 : 0;
+    int status[2] = {0, 0};
+    if (!cuda_ok(cudaMemcpyAsync(status, d_status, sizeof(status), cudaMemcpyDeviceToHost, s->stream), "D2H status") ||
+        !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
+        return AMRGPU_ERR_CUDA;
+    if (status[0]) {
+        set_error(AMRGPU_ERR_MESH, "session_regrid_forest: the forest is not 2:1 balanced");
+        return AMRGPU_ERR_MESH;
+    }
+    std::swap(s->d_quads, s->d_quads_alt);
+    std::swap(s->cap_desc, s->cap_desc_alt);
+    s->h_quads.clear();  // the live descriptors exist on the device only
+    s->rect = true;      // brick quads are axis-aligned rectangles
+    return apply_regrid(s, nq, nq > 0 ? status[1] : 0);
+}
+
+int amrgpu_session_quad_descriptors(amrgpu_session_t *s, void *out, int cap)
+{
+    if (!s || (cap > 0 && !out) || cap < 0) return -AMRGPU_ERR_ARG;
+    const int n = std::min(cap, s->nquad);
+    if (n > 0 && (!cuda_ok(cudaMemcpyAsync(out, s->d_quads, sizeof(QuadDesc) * size_t(n), cudaMemcpyDeviceToHost,
+                                           s->stream),
+                           "D2H quads") ||
+                  !cuda_ok(cudaStreamSynchronize(s->stream), "sync")))
+        return -AMRGPU_ERR_CUDA;
+    return s->nquad;
+}
+
+int amrgpu_session_face_count(const amrgpu_session_t *s) { return s ? s->nface : -1; }
 
 }  // extern "C"
 

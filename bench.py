@@ -319,7 +319,7 @@ def amr_workload(args):
     solve = reg = 0.0
     cu = steps = 0
     cells = []
-    parts = dict(tag=0.0, forest=0.0, balance=0.0, mesh=0.0, session_regrid=0.0)
+    parts = dict(tag=0.0, forest=0.0, balance=0.0, regrid_forest=0.0)
     cycles = max(1, args.steps // 5)
     for _ in range(cycles):
         # the regrid of amr.regrid, timed part by part
@@ -342,12 +342,9 @@ def amr_workload(args):
         d = time.perf_counter()
         f.balance()
         e = time.perf_counter()
-        kind, src = f.remap()
-        m2 = f.mesh(16)
-        g = time.perf_counter()
-        s.regrid(m2, kind, src)
+        s.regrid_forest(f)
         h = time.perf_counter()
-        for k, v in zip(parts, (c - b, d - c, e - d, g - e, h - g)):
+        for k, v in zip(parts, (c - b, d - c, e - d, h - e)):
             parts[k] += v
         solve += b - a
         reg += h - b

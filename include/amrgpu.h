@@ -304,6 +304,19 @@ int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int
  * amr_regrid.c:82-125 (new ghost layer, new face lists, new soln array). */
 int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int *kind,
                           const int *src_index);
+/* The same regrid straight from the forest after refine / coarsen / balance:
+ * the leaves and the remap table go to the device in one pinned copy and
+ * the quad descriptors (face types, neighbours, face order, corners) are
+ * built there -- byte-identical to decoding amrgpu_forest_external's
+ * arrays, without building them on the host. AMRGPU_ERR_MESH if the forest
+ * is not 2:1 balanced (the session keeps its mesh). */
+int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f);
+/* Copies up to cap quad descriptors (160 bytes each: 4 sides x {kind, nbr0,
+ * nbr1, face rank, level, bc} ints, then 8 corner doubles) to host memory;
+ * returns the session's quad count. */
+int amrgpu_session_quad_descriptors(amrgpu_session_t *s, void *out, int cap);
+/* Faces of the session's mesh. */
+int amrgpu_session_face_count(const amrgpu_session_t *s);
 
 /* ---------------- output: visualisation and checkpoint ---------------- */
 /* Unstructured VTK (.vtu, ASCII) of a forest and its AoS state (soln[f +

@@ -1,0 +1,123 @@
+"""Quad descriptors built on the GPU from the forest
+(amrgpu_session_regrid_forest) against the host path (amrgpu_forest_external
++ decode): byte-identical descriptors (face types, neighbours, face order,
+levels, boundary conditions, corners), the same face count, and the same
+states after the remap and after stepping, on bricks of several trees,
+periodic or not, with hanging faces at every level jump."""
+import os
+
+import numpy as np
+import pytest
+
+import meshes
+
+pytestmark = pytest.mark.gpu
+os.environ.setdefault("AMRGPU_QUIET", "1")
+
+
+def forest_case(ag, seed):
+    rng = np.random.default_rng(seed)
+    nx, ny = int(rng.integers(1, 4)), int(rng.integers(1, 3))
+    per = (int(rng.integers(2)), int(rng.integers(2)))
+    level = int(rng.integers(1, 3))
+    f = ag.Forest(nx, ny, periodic=per, lo=(-1.0, 0.5, 0.0), scale=1.5, level=level)
+    return f, rng
+
+
+def regrid_pair(ag, f, rng, n, form, cfg):
+    """Two sessions on the forest's current mesh; one random regrid of the
+    forest; one session follows through the host path, the other through
+    the device build."""
+    m0 = f.mesh(n)
+    s0 = meshes.perturbed(f.initialize(n), int(rng.integers(1 << 30)), amp=1e-2)
+    a = ag.Session(m0, cfg, form=form)
+    b = ag.Session(m0, cfg, form=form)
+    for s in (a, b):
+        s.upload(s0)
+        s.step(2)
+    _, lev, _, _ = f.quads()
+    f.begin_regrid()
+    f.refine((rng.random(f.num_quads) < 0.3).astype(np.int32), max_level=lev.max() + 2)
+    _, lev2, _, _ = f.quads()
+    f.coarsen((rng.random(f.num_quads) < 0.5).astype(np.int32), min_level=1)
+    f.balance()
+    kind, src = f.remap()
+    m1 = f.mesh(n)
+    a.regrid(m1, kind, src)
+    b.regrid_forest(f)
+    return a, b, m1
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_device_descriptors_equal_host_decode(ag, seed):
+    f, rng = forest_case(ag, 100 + seed)
+    n = 4
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.01,
+                             bc=tuple(int(x) for x in rng.integers(0, 3, 4)))
+    cfg.apply()
+    for rnd in range(3):
+        a, b, m1 = regrid_pair(ag, f, rng, n, ag.FORM_FP64_EXACT, cfg)
+        da, db = a.quad_descriptors(), b.quad_descriptors()
+        assert da.tobytes() == db.tobytes(), rnd
+        assert b.mesh.nface == m1.nface and b.mesh.ncell == m1.ncell
+        assert np.array_equal(a.download(), b.download())
+        a.step(4)
+        b.step(4)
+        assert np.array_equal(a.download(), b.download())
+        assert a.sync()["time"] == b.sync()["time"]
+        # the lazily built host mesh of the device path is the forest's
+        assert np.array_equal(b.mesh.face_info, m1.face_info)
+        a.close()
+        b.close()
+
+
+def test_fp32_form_and_hanging_ring(ag):
+    n = 16
+    f = meshes.two_level_ring(n, periodic=(1, 1))
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.01)
+    cfg.apply()
+    rng = np.random.default_rng(5)
+    a, b, m1 = regrid_pair(ag, f, rng, n, ag.FORM_FP32_FLUX, cfg)
+    assert a.quad_descriptors().tobytes() == b.quad_descriptors().tobytes()
+    a.step(5)
+    b.step(5)
+    assert np.array_equal(a.download(), b.download())
+
+
+def test_single_periodic_tree_is_its_own_neighbour(ag):
+    n = 4
+    f = ag.Forest(1, 1, periodic=(1, 1), level=0)
+    cfg = meshes.make_config(n)
+    cfg.apply()
+    m0 = f.mesh(n)
+    a = ag.Session(m0, cfg, form=0)
+    a.upload(f.initialize(n))
+    f.begin_regrid()
+    f.balance()
+    a.regrid_forest(f)
+    b = ag.Session(f.mesh(n), cfg, form=0)
+    assert a.quad_descriptors().tobytes() == b.quad_descriptors().tobytes()
+    assert a.mesh.nface == m0.nface == 2
+
+
+def test_unbalanced_forest_is_rejected_and_session_kept(ag):
+    n = 4
+    f = meshes.uniform(n, 2, periodic=(0, 0))
+    cfg = meshes.make_config(n)
+    cfg.apply()
+    s = ag.Session(f.mesh(n), cfg, form=0)
+    s.upload(f.initialize(n))
+    before = s.quad_descriptors()
+    f.begin_regrid()
+    fl = np.zeros(f.num_quads, np.int32)
+    fl[5] = 1
+    f.refine(fl)
+    fl = np.zeros(f.num_quads, np.int32)
+    fl[5] = 1
+    f.refine(fl)  # two levels finer next to level-2 quads, no balance
+    with pytest.raises(RuntimeError):
+        s.regrid_forest(f)
+    ag.clear_error()
+    assert s.quad_descriptors().tobytes() == before.tobytes()
+    s.step(1)
+    assert s.sync()["steps"] == 1
