@@ -234,8 +234,15 @@ class Forest:
         self.version += 1
         return lib().amrgpu_forest_coarsen(self._f, ip(fl), int(min_level))
 
-    def balance(self):
+    def balance(self, session=None):
+        """2:1 balance; with a session, each pass runs on its GPU
+        (amrgpu_forest_balance_device, same result)."""
         self.version += 1
+        if session is not None:
+            r = lib().amrgpu_forest_balance_device(self._f, session._s)
+            if r < 0:
+                raise AmrGpuError(-r, "forest_balance_device")
+            return r
         r = lib().amrgpu_forest_balance(self._f)
         if r < 0:
             raise AmrGpuError(3, "forest_balance")

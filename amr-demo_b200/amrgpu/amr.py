@@ -106,9 +106,10 @@ def host_tags(n, rho_tol, method=5):
 
 def regrid(forest, session, n, min_level, max_level, config=None, form=None, device_mesh=True):
     """One regrid of the session in place (its mesh and state follow the
-    forest); returns the session. device_mesh: the quad descriptors are
-    built on the GPU from the forest (Session.regrid_forest); otherwise the
-    host lists the mesh arrays and the session decodes them."""
+    forest); returns the session. device_mesh: the 2:1 balance passes and
+    the quad descriptors run on the GPU (Forest.balance(session=...),
+    Session.regrid_forest); otherwise the host balances, lists the mesh
+    arrays and the session decodes them."""
     tags = session.tag()
     _, lev, _, _ = forest.quads()
     forest.begin_regrid()
@@ -117,10 +118,11 @@ def regrid(forest, session, n, min_level, max_level, config=None, form=None, dev
     tags2 = forest.get_tags()
     _, lev2, _, _ = forest.quads()
     forest.coarsen(((tags2 == 0) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
-    forest.balance()
     if device_mesh:
+        forest.balance(session=session)
         session.regrid_forest(forest)
     else:
+        forest.balance()
         kind, src = forest.remap()
         session.regrid(forest.mesh(n), kind, src)
     return session

@@ -171,7 +171,7 @@ def regrid_by_classes(forest, session, n, classes, min_level, max_level):
     t2 = forest.get_tags()
     _, lev2, _, _ = forest.quads()
     forest.coarsen(((t2 == COARSEN) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
-    forest.balance()
+    forest.balance(session=session)
     session.regrid_forest(forest)
 
 

@@ -1,4 +1,15 @@
-// mesh_gpu.cu -- the quad descriptors of a forest's mesh built on the GPU.
+// mesh_gpu.cu -- a forest's 2:1 balance and its mesh's quad descriptors on
+// the GPU.
+//
+// Balance (forest_balance's passes, forest.cpp): every pass checks the
+// leaves created since the last pass (dirty), as the fine side of a
+// violation (a face or corner neighbour region held by a leaf two or more
+// levels coarser: that leaf is flagged) and as the coarse side (a leaf two
+// or more levels finer along an edge or at a corner: the leaf itself is
+// flagged); flagged leaves are replaced by their four z-ordered children,
+// which are the next pass's dirty set. One thread per leaf checks; the
+// refinement is a scan of 4-or-1 counts and a scatter, so Morton order is
+// kept. Same passes, same result as the host's.
 //
 // After a regrid the host forest has its new leaves (tree, level, x, y in
 // Morton order). The reference's driver then lists the mesh's faces
@@ -104,6 +115,115 @@ __device__ int find_d(const ForestDev &F, int tree, int level, long long x, long
     if (c < 0) return -1;
     const int4 l = F.leaves[c];
     return (l.y == level && l.z == x && l.w == y) ? c : -1;
+}
+
+__global__ void keys_kernel(ForestDev F);
+
+// One dirty leaf per thread: flags the leaves the pass refines.
+__global__ void balance_check_kernel(ForestDev F, const unsigned char *dirty, unsigned char *flags)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nq; i += gridDim.x * blockDim.x) {
+        if (!dirty[i]) continue;
+        const int4 q = F.leaves[i];
+        // fine side: neighbour regions (faces and corners) held by a leaf
+        // two or more levels coarser
+        if (q.y >= 2) {
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (!dx && !dy) continue;
+                    KeyD k;
+                    if (!shifted_d(F, q.x, q.y, q.z, q.w, dx, dy, k)) continue;
+                    const int c = locate_d(F, k.tree, k.x, k.y);
+                    if (c >= 0 && F.leaves[c].y < q.y - 1) flags[c] = 1;
+                }
+        }
+        // coarse side: a leaf two or more levels finer along an edge (walked
+        // leaf by leaf) or at a corner
+        if (q.y + 2 <= kMaxLevelG) {
+            const long long L = qlen_d(q.y);
+            const int lim = q.y + 2;
+            bool fine = false;
+            for (int s = 0; s < 4 && !fine; ++s) {
+                // a leaf of level < lim spans at least L/2 of the edge: the
+                // walk takes a few steps; the guard only bounds a malformed forest
+                int guard = 0;
+                for (long long t = 0; t < L && guard < 64; ++guard) {
+                    long long px = q.z, py = q.w;
+                    int dx = 0, dy = 0;
+                    if (s == 0) { py += t; dx = -1; }
+                    if (s == 1) { px += L - 1; py += t; dx = 1; }
+                    if (s == 2) { px += t; dy = -1; }
+                    if (s == 3) { px += t; py += L - 1; dy = 1; }
+                    KeyD k;
+                    if (!shifted_d(F, q.x, kMaxLevelG, px, py, dx, dy, k)) break;
+                    const int c = locate_d(F, k.tree, k.x, k.y);
+                    if (c < 0) break;
+                    const int4 cl = F.leaves[c];
+                    if (cl.y >= lim) {
+                        fine = true;
+                        break;
+                    }
+                    const long long len = qlen_d(cl.y);
+                    const long long adv = (s < 2) ? ((long long)cl.w + len - k.y) : ((long long)cl.z + len - k.x);
+                    if (adv <= 0) break;
+                    t += adv;
+                }
+            }
+            for (int dy = -1; dy <= 1 && !fine; dy += 2)
+                for (int dx = -1; dx <= 1 && !fine; dx += 2) {
+                    KeyD k;
+                    const long long px = dx < 0 ? q.z : q.z + L - 1, py = dy < 0 ? q.w : q.w + L - 1;
+                    if (!shifted_d(F, q.x, kMaxLevelG, px, py, dx, dy, k)) continue;
+                    const int c = locate_d(F, k.tree, k.x, k.y);
+                    if (c >= 0 && F.leaves[c].y >= lim) fine = true;
+                }
+            if (fine) flags[i] = 1;
+        }
+    }
+}
+
+__global__ void balance_counts_kernel(int nq, const unsigned char *flags, int *cnt)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x)
+        cnt[i] = flags[i] ? 4 : 1;
+}
+
+// flagged leaves -> four z-ordered children at pos[i]..pos[i]+3 (dirty),
+// others copied (clean); origin: the leaf of the pass's input it came from
+__global__ void balance_refine_kernel(int nq, const int4 *in, const int *orig_in, const unsigned char *flags,
+                                      const int *pos, int4 *out, int *orig_out, unsigned char *dirty_out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+        const int4 p = in[i];
+        const int o = orig_in[i];
+        const int at = pos[i];
+        if (flags[i]) {
+            const int h = int(qlen_d(p.y + 1));
+            for (int c = 0; c < 4; ++c) {
+                out[at + c] = make_int4(p.x, p.y + 1, p.z + (c & 1) * h, p.w + ((c >> 1) & 1) * h);
+                orig_out[at + c] = o;
+                dirty_out[at + c] = 1;
+            }
+        } else {
+            out[at] = p;
+            orig_out[at] = o;
+            dirty_out[at] = 0;
+        }
+    }
+}
+
+__global__ void tree_begin_kernel(int nq, int ntrees, const int4 *leaves, int *tb)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nq; i += gridDim.x * blockDim.x) {
+        if (i == nq) {
+            const int last = nq == 0 ? -1 : leaves[nq - 1].x;
+            for (int u = last + 1; u <= ntrees; ++u) tb[u] = nq;
+        } else {
+            const int t = leaves[i].x;
+            const int prev = i == 0 ? -1 : leaves[i - 1].x;
+            for (int u = prev + 1; u <= t; ++u) tb[u] = i;  // trees without leaves start here too
+        }
+    }
 }
 
 __global__ void keys_kernel(ForestDev F)
@@ -239,6 +359,39 @@ int grid_for(long long n, int sms)
 }
 
 }  // namespace
+
+size_t balance_scan_bytes(int nq)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int *)nullptr, (int *)nullptr, nq > 0 ? nq : 1);
+    return bytes;
+}
+
+cudaError_t launch_balance_pass(const ForestDev &F, int ntrees, int *tree_begin, const unsigned char *dirty,
+                                unsigned char *flags, int *cnt, int *pos, void *scan_tmp, size_t scan_bytes,
+                                int sms, cudaStream_t st)
+{
+    if (F.nq <= 0) return cudaSuccess;
+    tree_begin_kernel<<<grid_for(F.nq + 1ll, sms), 256, 0, st>>>(F.nq, ntrees, F.leaves, tree_begin);
+    keys_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F);
+    cudaError_t e = cudaMemsetAsync(flags, 0, size_t(F.nq), st);
+    if (e != cudaSuccess) return e;
+    balance_check_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F, dirty, flags);
+    balance_counts_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F.nq, flags, cnt);
+    size_t bytes = scan_bytes;
+    e = cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, cnt, pos, F.nq, st);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_balance_refine(int nq, const int4 *in, const int *orig_in, const unsigned char *flags,
+                                  const int *pos, int4 *out, int *orig_out, unsigned char *dirty_out, int sms,
+                                  cudaStream_t st)
+{
+    if (nq <= 0) return cudaSuccess;
+    balance_refine_kernel<<<grid_for(nq, sms), 256, 0, st>>>(nq, in, orig_in, flags, pos, out, orig_out, dirty_out);
+    return cudaGetLastError();
+}
 
 size_t build_quads_scan_bytes(int nq)
 {

@@ -107,6 +107,10 @@ struct amrgpu_session {
     size_t h_stage_bytes = 0;
     void *d_mesh_scratch = nullptr;   // device scratch of the descriptor build
     size_t mesh_scratch_bytes = 0;
+    void *d_bal[2] = {nullptr, nullptr};  // balance: leaves / origin / dirty, double-buffered
+    void *d_bal_work = nullptr;           // balance: flags, counts, positions, keys, trees, scan temp
+    int bal_cap = 0;                      // leaves the balance buffers hold
+    int bal_trees = 0;                    // trees the balance work area holds tables for
     bool rect = true;                 // every quad an axis-aligned rectangle
     int *d_tags = nullptr;
     int *d_kind = nullptr;
@@ -509,6 +513,9 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_send);
     cudaFree(s->d_quads_alt);
     cudaFree(s->d_mesh_scratch);
+    cudaFree(s->d_bal[0]);
+    cudaFree(s->d_bal[1]);
+    cudaFree(s->d_bal_work);
     cudaFreeHost(s->h_stage);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -1279,6 +1286,255 @@ int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f)
     s->h_quads.clear();  // the live descriptors exist on the device only
     s->rect = true;      // brick quads are axis-aligned rectangles
     return apply_regrid(s, nq, nq > 0 ? status[1] : 0);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Balance buffers for cap leaves: per buffer int4 leaves, int origin,
+// uint8 dirty; work: flags (uint8), counts, positions, keys, tree begin,
+// brick tables, scan temp.
+struct BalLayout {
+    size_t o_orig, o_dirty, buf;
+    size_t o_flags, o_cnt, o_pos, o_keys, o_tb, o_tx, o_ty, o_at, o_tmp, work;
+    size_t scan_bytes;
+};
+
+BalLayout bal_layout(int cap, int ntrees)
+{
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    BalLayout L;
+    const size_t c = size_t(std::max(cap, 1));
+    L.o_orig = al(16 * c);
+    L.o_dirty = L.o_orig + al(4 * c);
+    L.buf = L.o_dirty + al(c);
+    L.scan_bytes = balance_scan_bytes(int(c));
+    L.o_flags = 0;
+    L.o_cnt = al(c);
+    L.o_pos = L.o_cnt + al(4 * c);
+    L.o_keys = L.o_pos + al(4 * c);
+    L.o_tb = L.o_keys + al(8 * c);
+    L.o_tx = L.o_tb + al(4 * size_t(ntrees + 1));
+    L.o_ty = L.o_tx + al(4 * size_t(ntrees));
+    L.o_at = L.o_ty + al(4 * size_t(ntrees));
+    L.o_tmp = L.o_at + al(4 * size_t(ntrees));
+    L.work = L.o_tmp + al(L.scan_bytes);
+    return L;
+}
+
+// Grows the balance buffers to cap leaves, keeping the first keep leaves of
+// buffer `live` (leaves, origin, dirty).
+int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
+{
+    const BalLayout L = bal_layout(cap, ntrees);
+    const BalLayout O = bal_layout(s->bal_cap, s->bal_trees);
+    void *nb[2] = {nullptr, nullptr};
+    void *nw = nullptr;
+    bool ok = cuda_ok(cudaMalloc(&nb[0], L.buf), "cudaMalloc balance") &&
+              cuda_ok(cudaMalloc(&nb[1], L.buf), "cudaMalloc balance") &&
+              cuda_ok(cudaMalloc(&nw, L.work), "cudaMalloc balance");
+    if (ok && keep > 0 && s->d_bal[live]) {
+        char *src = static_cast<char *>(s->d_bal[live]);
+        char *dst = static_cast<char *>(nb[0]);
+        ok = cuda_ok(cudaMemcpyAsync(dst, src, 16 * size_t(keep), cudaMemcpyDeviceToDevice, s->stream), "balance copy") &&
+             cuda_ok(cudaMemcpyAsync(dst + L.o_orig, src + O.o_orig, 4 * size_t(keep), cudaMemcpyDeviceToDevice,
+                                     s->stream),
+                     "balance copy") &&
+             cuda_ok(cudaMemcpyAsync(dst + L.o_dirty, src + O.o_dirty, size_t(keep), cudaMemcpyDeviceToDevice,
+                                     s->stream),
+                     "balance copy");
+        // brick tables live in the work area (same forest: same tree count)
+        if (ok && s->d_bal_work && s->bal_trees == ntrees)
+            ok = cuda_ok(cudaMemcpyAsync(static_cast<char *>(nw) + L.o_tx, static_cast<char *>(s->d_bal_work) + O.o_tx,
+                                         L.o_tmp - L.o_tx, cudaMemcpyDeviceToDevice, s->stream),
+                         "balance copy");
+    }
+    if (ok) ok = cuda_ok(cudaStreamSynchronize(s->stream), "sync");
+    if (!ok) {
+        cudaFree(nb[0]);
+        cudaFree(nb[1]);
+        cudaFree(nw);
+        return AMRGPU_ERR_CUDA;
+    }
+    cudaFree(s->d_bal[0]);
+    cudaFree(s->d_bal[1]);
+    cudaFree(s->d_bal_work);
+    s->d_bal[0] = nb[0];
+    s->d_bal[1] = nb[1];
+    s->d_bal_work = nw;
+    s->bal_cap = cap;
+    s->bal_trees = ntrees;
+    return AMRGPU_OK;
+}
+
+int ensure_stage(amrgpu_session *s, size_t bytes)
+{
+    if (bytes <= s->h_stage_bytes) return cuda_ok(cudaStreamSynchronize(s->stream), "sync") ? AMRGPU_OK : AMRGPU_ERR_CUDA;
+    cudaStreamSynchronize(s->stream);
+    cudaFreeHost(s->h_stage);
+    s->h_stage = nullptr;
+    s->h_stage_bytes = 0;
+    const size_t want = bytes + bytes / 4;
+    if (!cuda_ok(cudaHostAlloc(&s->h_stage, want, cudaHostAllocDefault), "cudaHostAlloc staging")) return AMRGPU_ERR_CUDA;
+    s->h_stage_bytes = want;
+    return AMRGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
+{
+    if (!f || !f->f || !s) return -AMRGPU_ERR_ARG;
+    std::vector<Leaf> &leaves = forest_leaves_mut(f->f);
+    BrickView B;
+    forest_brick(f->f, &B);
+    const int ntrees = B.nx * B.ny;
+    int nl = int(leaves.size());
+    // staging: leaves (int4), origin, dirty bytes, brick tables
+    size_t sb = 16 * size_t(nl) + 4 * size_t(nl) + size_t(nl) + 12 * size_t(ntrees) + 64;
+    int rc = ensure_stage(s, sb);
+    if (rc) return -rc;
+    {
+        int *h = static_cast<int *>(s->h_stage);
+        int *h_orig = h + 4 * size_t(nl);
+        unsigned char *h_dirty = reinterpret_cast<unsigned char *>(h_orig + nl);
+        for (int i = 0; i < nl; ++i) {
+            const Leaf &q = leaves[size_t(i)];
+            h[4 * i + 0] = q.tree;
+            h[4 * i + 1] = q.level;
+            h[4 * i + 2] = int(q.x);
+            h[4 * i + 3] = int(q.y);
+            h_orig[i] = i;
+            h_dirty[i] = q.dirty ? 1 : 0;
+        }
+        int *h_tab = reinterpret_cast<int *>(h_dirty + ((size_t(nl) + 15) & ~size_t(15)));
+        for (int t = 0; t < ntrees; ++t) {
+            h_tab[t] = B.tree_tx[t];
+            h_tab[ntrees + t] = B.tree_ty[t];
+            h_tab[2 * ntrees + t] = B.tree_at[t];
+        }
+        const int cap = std::max(4 * nl, 64);
+        if (cap > s->bal_cap || ntrees != s->bal_trees) {
+            rc = bal_grow(s, std::max(cap, s->bal_cap), ntrees, 0, 0);
+            if (rc) return -rc;
+        }
+        const BalLayout L = bal_layout(s->bal_cap, ntrees);
+        char *b0 = static_cast<char *>(s->d_bal[0]);
+        char *w = static_cast<char *>(s->d_bal_work);
+        bool ok = cuda_ok(cudaMemcpyAsync(b0, h, 16 * size_t(nl), cudaMemcpyHostToDevice, s->stream), "H2D balance") &&
+                  cuda_ok(cudaMemcpyAsync(b0 + L.o_orig, h_orig, 4 * size_t(nl), cudaMemcpyHostToDevice, s->stream),
+                          "H2D balance") &&
+                  cuda_ok(cudaMemcpyAsync(b0 + L.o_dirty, h_dirty, size_t(nl), cudaMemcpyHostToDevice, s->stream),
+                          "H2D balance") &&
+                  cuda_ok(cudaMemcpyAsync(w + L.o_tx, h_tab, 4 * size_t(ntrees), cudaMemcpyHostToDevice, s->stream),
+                          "H2D balance") &&
+                  cuda_ok(cudaMemcpyAsync(w + L.o_ty, h_tab + ntrees, 4 * size_t(ntrees), cudaMemcpyHostToDevice,
+                                          s->stream),
+                          "H2D balance") &&
+                  cuda_ok(cudaMemcpyAsync(w + L.o_at, h_tab + 2 * ntrees, 4 * size_t(ntrees), cudaMemcpyHostToDevice,
+                                          s->stream),
+                          "H2D balance");
+        if (!ok) return -AMRGPU_ERR_CUDA;
+    }
+    int live = 0;
+    bool done = false;
+    for (int pass = 0; pass < 64 && !done; ++pass) {
+        const BalLayout L = bal_layout(s->bal_cap, ntrees);
+        char *in = static_cast<char *>(s->d_bal[live]);
+        char *w = static_cast<char *>(s->d_bal_work);
+        ForestDev F;
+        F.leaves = reinterpret_cast<const int4 *>(in);
+        F.keys = reinterpret_cast<unsigned long long *>(w + L.o_keys);
+        F.tree_begin = reinterpret_cast<const int *>(w + L.o_tb);
+        F.tree_tx = reinterpret_cast<const int *>(w + L.o_tx);
+        F.tree_ty = reinterpret_cast<const int *>(w + L.o_ty);
+        F.tree_at = reinterpret_cast<const int *>(w + L.o_at);
+        F.nx = B.nx;
+        F.ny = B.ny;
+        F.px = B.periodic[0];
+        F.py = B.periodic[1];
+        for (int k = 0; k < 3; ++k) F.xlo[k] = B.xlo[k];
+        F.scale = B.scale;
+        for (int k = 0; k < 4; ++k) F.bc[k] = 0;
+        F.nq = nl;
+        unsigned char *flags = reinterpret_cast<unsigned char *>(w + L.o_flags);
+        int *cnt = reinterpret_cast<int *>(w + L.o_cnt);
+        int *pos = reinterpret_cast<int *>(w + L.o_pos);
+        if (!cuda_ok(launch_balance_pass(F, ntrees, reinterpret_cast<int *>(w + L.o_tb),
+                                         reinterpret_cast<const unsigned char *>(in + L.o_dirty), flags, cnt, pos,
+                                         w + L.o_tmp, L.scan_bytes, s->sms, s->stream),
+                     "balance pass"))
+            return -AMRGPU_ERR_CUDA;
+        s->launches += 5;
+        int tail[2] = {0, 0};
+        int *ht = static_cast<int *>(s->h_stage);  // staging is free: the uploads above have completed by now
+        if (nl > 0) {
+            if (!cuda_ok(cudaMemcpyAsync(ht, pos + nl - 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
+                !cuda_ok(cudaMemcpyAsync(ht + 1, cnt + nl - 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
+                !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
+                return -AMRGPU_ERR_CUDA;
+            tail[0] = ht[0];
+            tail[1] = ht[1];
+        }
+        const int total = nl > 0 ? tail[0] + tail[1] : 0;
+        if (total == nl) {
+            done = true;
+            break;
+        }
+        if (total > s->bal_cap) {
+            rc = bal_grow(s, 2 * total, ntrees, live, nl);
+            if (rc) return -rc;
+            live = 0;
+            // flags and positions were in the old work area: redo the pass
+            continue;
+        }
+        const BalLayout L2 = bal_layout(s->bal_cap, ntrees);
+        char *out = static_cast<char *>(s->d_bal[1 - live]);
+        if (!cuda_ok(launch_balance_refine(nl, reinterpret_cast<const int4 *>(in),
+                                           reinterpret_cast<const int *>(in + L2.o_orig), flags, pos,
+                                           reinterpret_cast<int4 *>(out), reinterpret_cast<int *>(out + L2.o_orig),
+                                           reinterpret_cast<unsigned char *>(out + L2.o_dirty), s->sms, s->stream),
+                     "balance refine"))
+            return -AMRGPU_ERR_CUDA;
+        s->launches++;
+        live = 1 - live;
+        nl = total;
+    }
+    if (!done) {
+        set_error(AMRGPU_ERR_MESH, "forest_balance_device: no balance after 64 passes");
+        return -AMRGPU_ERR_MESH;
+    }
+    // the balanced leaves back to the host: coordinates and origin
+    rc = ensure_stage(s, 20 * size_t(nl) + 64);
+    if (rc) return -rc;
+    const BalLayout L = bal_layout(s->bal_cap, ntrees);
+    char *in = static_cast<char *>(s->d_bal[live]);
+    int *h = static_cast<int *>(s->h_stage);
+    int *h_orig = h + 4 * size_t(nl);
+    if (nl > 0 &&
+        (!cuda_ok(cudaMemcpyAsync(h, in, 16 * size_t(nl), cudaMemcpyDeviceToHost, s->stream), "D2H balance") ||
+         !cuda_ok(cudaMemcpyAsync(h_orig, in + L.o_orig, 4 * size_t(nl), cudaMemcpyDeviceToHost, s->stream),
+                  "D2H balance") ||
+         !cuda_ok(cudaStreamSynchronize(s->stream), "sync")))
+        return -AMRGPU_ERR_CUDA;
+    if (nl != int(leaves.size())) {
+        std::vector<Leaf> out((size_t)nl);
+        for (int k = 0; k < nl; ++k) {
+            Leaf q = leaves[size_t(h_orig[k])];
+            q.level = h[4 * k + 1];
+            q.x = h[4 * k + 2];
+            q.y = h[4 * k + 3];
+            q.dirty = 0;
+            out[size_t(k)] = q;
+        }
+        leaves.swap(out);
+    } else {
+        for (Leaf &q : leaves) q.dirty = 0;
+    }
+    return nl;
 }
 
 int amrgpu_session_quad_descriptors(amrgpu_session_t *s, void *out, int cap)

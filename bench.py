@@ -340,7 +340,7 @@ def amr_workload(args):
         _, lev2, _, _ = f.quads()
         f.coarsen(((t2 == 0) & (lev2 > lo)).astype(np.int32), min_level=lo)
         d = time.perf_counter()
-        f.balance()
+        f.balance(session=s)
         e = time.perf_counter()
         s.regrid_forest(f)
         h = time.perf_counter()

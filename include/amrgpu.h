@@ -311,6 +311,10 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
  * arrays, without building them on the host. AMRGPU_ERR_MESH if the forest
  * is not 2:1 balanced (the session keeps its mesh). */
 int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f);
+/* amrgpu_forest_balance with the checks and the refinement of every pass
+ * on the session's GPU (same passes, same leaves, tags and remap table);
+ * returns the leaf count, or -error. */
+int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s);
 /* Copies up to cap quad descriptors (160 bytes each: 4 sides x {kind, nbr0,
  * nbr1, face rank, level, bc} ints, then 8 corner doubles) to host memory;
  * returns the session's quad count. */

@@ -121,3 +121,41 @@ def test_unbalanced_forest_is_rejected_and_session_kept(ag):
     assert s.quad_descriptors().tobytes() == before.tobytes()
     s.step(1)
     assert s.sync()["steps"] == 1
+
+
+def leaves_of(f):
+    tree, lev, x, y = f.quads()
+    kind, src = f.remap()
+    return tree, lev, x, y, f.get_tags(), kind, src
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_device_balance_equals_host_balance(ag, seed):
+    """Two identical forests through the same random refine / coarsen, one
+    balanced on the host, one with every pass on the GPU: the same leaves,
+    tags and remap tables; then a few more regrid rounds."""
+    n = 4
+    rng = np.random.default_rng(700 + seed)
+    nx, ny = int(rng.integers(1, 4)), int(rng.integers(1, 3))
+    per = (int(rng.integers(2)), int(rng.integers(2)))
+    fa = ag.Forest(nx, ny, periodic=per, level=2)
+    fb = ag.Forest(nx, ny, periodic=per, level=2)
+    cfg = meshes.make_config(n)
+    cfg.apply()
+    s = ag.Session(fa.mesh(n), cfg, form=0)
+    for rnd in range(4):
+        _, lev, _, _ = fa.quads()
+        rf = (rng.random(fa.num_quads) < 0.15).astype(np.int32)
+        for f in (fa, fb):
+            f.begin_regrid()
+            f.set_tags(rf)
+            f.refine(rf, max_level=7)
+        cf = (rng.random(fa.num_quads) < 0.6).astype(np.int32)
+        for f in (fa, fb):
+            f.coarsen(cf, min_level=1)
+        fa.balance()
+        nb = fb.balance(session=s)
+        assert nb == fa.num_quads == fb.num_quads
+        assert fb.is_balanced()
+        for u, v in zip(leaves_of(fa), leaves_of(fb)):
+            assert np.array_equal(u, v), rnd
