@@ -86,6 +86,7 @@ const void *cfl_kernel_fp32(int n)
 // block" = warps per block, no dynamic shared memory; all at 128
 // registers (16 resident warps per SM): fewer registers spill and run slower
 #define AMRGPU_SWEEP16(W, MINB) StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep16_kernel<W, MINB>}
+#define AMRGPU_SWEEP8(W, MINB) StageLaunch{8, 2 * (W), 32 * (W), MINB, 0, (const void *)sweep8_kernel<W, MINB>}
 
 static const StageLaunch kTable32[] = {
     AMRGPU_SWEEP16(4, 4),   // 128 registers, 16 warps per SM
@@ -96,6 +97,9 @@ static const StageLaunch kTable32[] = {
     AMRGPU_STAGE32(16, 2, 544, 1),
     AMRGPU_STAGE32(16, 2, 576, 1),
     AMRGPU_STAGE32(16, 1, 544, 2),
+    AMRGPU_SWEEP8(4, 4),    // two 8x8 quads per warp
+    AMRGPU_SWEEP8(2, 8),
+    AMRGPU_SWEEP8(8, 2),
     AMRGPU_STAGE32(8, 4, 288, 3),
     AMRGPU_STAGE32(8, 2, 160, 4),
     AMRGPU_STAGE32(8, 8, 576, 1),

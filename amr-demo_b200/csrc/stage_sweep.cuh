@@ -1,21 +1,23 @@
-// stage_sweep.cuh -- the FP32-flux form's RK stage for 16x16 patches as a
-// row sweep: one warp per quadrant, no shared-memory records and no
-// block-wide barriers between phases.
+// stage_sweep.cuh -- the FP32-flux form's RK stage for 16x16 and 8x8
+// patches as a row sweep: one warp per 16x16 quadrant (two per warp for
+// 8x8), no shared-memory records and no block-wide barriers between phases.
 //
 // Same arithmetic as stage_kernel<16, ..., FP32> (the reference's
 // flux_roe_2d, flux_2d_module.F90:63-182, and boundary flux, bc_2d_module.F90,
 // in FP32 on per-cell records; FP64 residual sums, stage update, norm and
 // conservation; FP32 CFL candidate), reorganised for the register file:
 //
-//   lane = (i, h): column i = lane & 15 of the patch, rows 8h .. 8h+7.
+//   lane = (sub, h, i): quad sub of the warp's 32/(2N) quads, column
+//        i < N of the patch, rows R*h .. R*h+R-1 with R = N/2 (for 16x16:
+//        one quad, i = lane & 15, rows 8h .. 8h+7).
 //   edges   per quad, the 4 x 16 edge faces (each lane one per round: the
 //           own edge cell's record, the neighbour cell(s) the reference
 //           pairs it with, the Roe or boundary flux, a coarse hanging edge's
-//           two fluxes summed in FP64) and the 16 faces between rows 7 and 8
+//           two fluxes summed in FP64) and the N faces between rows R-1 and R
 //           go to a small per-warp table, in the interior sign convention
 //           (a cell adds -F at its low face and +F at its high face);
-//   sweep   8 steps; at step t lane (i, h) loads cell (i, 8h+t) straight
-//           from HBM (16 lanes read 128 contiguous bytes per field), builds
+//   sweep   R steps; at step t lane (i, h) loads cell (i, Rh+t) straight
+//           from HBM (N lanes read 8N contiguous bytes per field), builds
 //           its record in registers, computes the x-face flux at i-1/2 with
 //           the left neighbour's record taken by a warp shuffle, hands that
 //           flux to lane i-1 (which needs it as its i+1/2 face) by a second
@@ -34,18 +36,23 @@
 
 namespace amrgpu {
 
-template <int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageArgs a)
+template <int N, int WARPS>
+__device__ __forceinline__ void sweep_body(const StageArgs &a)
 {
-    constexpr int N = 16, NN = N * N;
+    static_assert(N == 16 || N == 8, "row sweep for 16x16 and 8x8 patches");
+    constexpr int NN = N * N;
+    constexpr int QPW = 32 / (2 * N);  // quads per warp
+    constexpr int R = N / 2;           // rows per half-patch
     constexpr unsigned FULL = 0xffffffffu;
-    // edge fluxes per warp: [side 0..3, 4 = faces between rows 7 and 8][position][field]
-    __shared__ double sedge[WARPS][5][N][4];
+    // edge fluxes per warp and quad: [side 0..3, 4 = faces between rows R-1
+    // and R][position][field]
+    __shared__ double sedge[WARPS][QPW][5][N][4];
     __shared__ double red[64];
     __shared__ int s_last;
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int i = lane & 15, h = lane >> 4;
+    const int sub = lane / (2 * N), l = lane % (2 * N);
+    const int i = l % N, h = l / N;
     const long long stride = a.stride;
 
     // step scalars (as stage_kernel)
@@ -71,12 +78,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageAr
     double my_norm = 0.0;
     int my_flags = 0;
 
-    // Quads: each warp's first one by its index, then the next free one from
-    // a counter (work_next, reset to 0 by the last block), so that warps
-    // and SMs that finish early take more and the tail stays short.
+    // Work items (QPW consecutive quads each): each warp's first one by its
+    // index, then the next free one from a counter (work_next, reset to 0 by
+    // the last block), so that warps and SMs that finish early take more and
+    // the tail stays short. A quad past the end (odd count, 8x8) is computed
+    // on its item's first quad and neither stored nor reduced.
     const int nwarps = gridDim.x * WARPS;
-    int quad = blockIdx.x * WARPS + w;
-    while (quad < a.nquad) {
+    const int nitems = (a.nquad + QPW - 1) / QPW;
+    int item = blockIdx.x * WARPS + w;
+    while (item < nitems) {
+        const bool valid = item * QPW + sub < a.nquad;
+        const int quad = valid ? item * QPW + sub : item * QPW;
         const QuadDesc &qd = a.quads[quad];
         const double *g = qd.corner;
         const double hx = (g[2] - g[0]) / (double)N, hy = (g[5] - g[1]) / (double)N;
@@ -128,24 +140,24 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageAr
                 }
             }
 #pragma unroll
-            for (int f = 0; f < 4; ++f) sedge[w][s][m][f] = E[f];
+            for (int f = 0; f < 4; ++f) sedge[w][sub][s][m][f] = E[f];
         }
-        // ---------------- the faces between rows 7 and 8 (column i)
+        // ---------------- the faces between rows R-1 and R (column i)
         {
             float P[8], O[8], fl[4];
             double q4[4];
-            load_rec(Qq, (7 + h) * N + i, P, q4);
+            load_rec(Qq, (R - 1 + h) * N + i, P, q4);
 #pragma unroll
-            for (int k = 0; k < 8; ++k) O[k] = __shfl_xor_sync(FULL, P[k], 16);
+            for (int k = 0; k < 8; ++k) O[k] = __shfl_xor_sync(FULL, P[k], N);
             if (h == 0) {
                 roe_flux_axis_fp32<1>(P, O, fhx, fl);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) sedge[w][4][i][f] = (double)fl[f];
+                for (int f = 0; f < 4; ++f) sedge[w][sub][4][i][f] = (double)fl[f];
             }
         }
         __syncwarp();
 
-        // ---------------- sweep over the lane's 8 rows
+        // ---------------- sweep over the lane's R rows
         float below[8];      // record of the row below (y-face partner)
         double xpart[4];     // -F(x-1/2) + F(x+1/2) of the row below
         double gbelow[4];    // F(y-1/2) of the row below
@@ -161,6 +173,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageAr
                 const double r = (xpart[f] - gbelow[f]) + gup[f];
                 kv[f] = -(r * inv_vol);
             }
+            if (!valid) return;
             auto A0 = [&](int f) -> double { return a0below[f]; };
             rk_update(a, dt, stride, gi, qbelow, kv, A0, qn);
             if (a.last_stage) {
@@ -177,14 +190,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageAr
         };
         double qnext[4];
 #pragma unroll
-        for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (8 * h) * N + i];
+        for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (R * h) * N + i];
 #pragma unroll 1
-        for (int t = 0; t < 8; ++t) {
-            const int j = 8 * h + t;
+        for (int t = 0; t < R; ++t) {
+            const int j = R * h + t;
             double q4[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) q4[f] = qnext[f];
-            if (t < 7) {
+            if (t < R - 1) {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (j + 1) * N + i];
             }
@@ -200,22 +213,22 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageAr
             // x-face at i-1/2 (lane 0's left face is an edge face)
             float L[8], fx[4], fxr[4];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) L[k] = __shfl_up_sync(FULL, P[k], 1, 16);
+            for (int k = 0; k < 8; ++k) L[k] = __shfl_up_sync(FULL, P[k], 1, N);
             roe_flux_axis_fp32<0>(L, P, fhy, fx);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) fxr[f] = __shfl_down_sync(FULL, fx[f], 1, 16);
+            for (int f = 0; f < 4; ++f) fxr[f] = __shfl_down_sync(FULL, fx[f], 1, N);
             double xp[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                const double fl = (i == 0) ? sedge[w][0][j][f] : (double)fx[f];
-                const double fr = (i == N - 1) ? sedge[w][1][j][f] : (double)fxr[f];
+                const double fl = (i == 0) ? sedge[w][sub][0][j][f] : (double)fx[f];
+                const double fr = (i == N - 1) ? sedge[w][sub][1][j][f] : (double)fxr[f];
                 xp[f] = fr - fl;
             }
-            // y-face at j-1/2 (the first row's is an edge or the row-7/8 face)
+            // y-face at j-1/2 (the first row's is an edge or the row R-1/R face)
             double gy[4];
             if (t == 0) {
 #pragma unroll
-                for (int f = 0; f < 4; ++f) gy[f] = h == 0 ? sedge[w][2][i][f] : sedge[w][4][i][f];
+                for (int f = 0; f < 4; ++f) gy[f] = h == 0 ? sedge[w][sub][2][i][f] : sedge[w][sub][4][i][f];
             } else {
                 float fy[4];
                 roe_flux_axis_fp32<1>(below, P, fhx, fy);
@@ -236,15 +249,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageAr
             double gtop[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                gtop[f] = h == 0 ? sedge[w][4][i][f] : sedge[w][3][i][f];
+                gtop[f] = h == 0 ? sedge[w][sub][4][i][f] : sedge[w][sub][3][i][f];
                 a0below[f] = a0next[f];
             }
-            finish(8 * h + 7, gtop);
+            finish(R * h + R - 1, gtop);
         }
-        __syncwarp();  // the next quad rewrites this warp's edge table
+        __syncwarp();  // the next item rewrites this warp's edge table
         unsigned nxt = 0;
         if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);
-        quad = nwarps + (int)__shfl_sync(FULL, nxt, 0);
+        item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
     }
 
     // ---------------- block reductions: CFL min (one atomic per block),
@@ -293,6 +306,18 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageAr
         a.scal->work_next = 0u;
         a.scal->done_blocks = 0u;
     }
+}
+
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageArgs a)
+{
+    sweep_body<16, WARPS>(a);
+}
+
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) sweep8_kernel(const StageArgs a)
+{
+    sweep_body<8, WARPS>(a);
 }
 
 }  // namespace amrgpu

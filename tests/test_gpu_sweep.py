@@ -1,4 +1,4 @@
-"""The FP32-flux form's row-sweep stage kernel for 16x16 patches
+"""The FP32-flux form's row-sweep stage kernels for 16x16 and 8x8 patches
 (csrc/stage_sweep.cuh) against the block-phase FP32 kernel it replaces as
 the default and against the FP64 oracle.
 
@@ -19,14 +19,15 @@ import meshes
 pytestmark = pytest.mark.gpu
 os.environ.setdefault("AMRGPU_QUIET", "1")
 
-BLOCK = (1, 288)
-# variant indices of the row sweep for 16x16 patches: (4,128), (2,64), (8,256)
+# the first block-phase FP32 variant per patch size
+BLOCK = {16: (1, 288), 8: (4, 288)}
+# variant indices of the row sweep, the first three of each list:
+# 16x16 (4,128), (2,64), (8,256); 8x8 (8,128), (4,64), (16,256)
 SWEEPS = [0, 1, 2]
 
 
-def case(ag, seed, scheme):
+def case(ag, seed, scheme, n=16):
     rng = np.random.default_rng(seed)
-    n = 16
     per = (int(rng.integers(2)), int(rng.integers(2)))
     f = meshes.uniform(n, 2, periodic=per)
     fl = (rng.random(f.num_quads) < 0.4).astype(np.int32)
@@ -55,10 +56,11 @@ def run(ag, m, cfg, s0, shape, steps):
     return q, rep
 
 
+@pytest.mark.parametrize("n", [16, 8])
 @pytest.mark.parametrize("seed,scheme", [(0, 3), (1, 1), (2, 2), (3, 4), (4, 5), (5, 3), (6, 3)])
-def test_sweep_matches_block_kernel(ag, seed, scheme):
-    f, m, cfg, s0 = case(ag, 300 + seed, scheme)
-    ref, rep0 = run(ag, m, cfg, s0, BLOCK, 6)
+def test_sweep_matches_block_kernel(ag, seed, scheme, n):
+    f, m, cfg, s0 = case(ag, 300 + seed, scheme, n)
+    ref, rep0 = run(ag, m, cfg, s0, BLOCK[n], 6)
     ref = ref.reshape(-1, 4)
     first = None
     for shape in SWEEPS:
@@ -76,9 +78,10 @@ def test_sweep_matches_block_kernel(ag, seed, scheme):
 
 
 @pytest.mark.parametrize("seed", range(3))
-def test_sweep_rhs_within_fp32_tolerance_of_oracle(ag, oracle, seed):
-    f, m, cfg, s0 = case(ag, 400 + seed, 3)
-    ref = oracle.rhs(m, s0, oracle.make_config(16, cfg)).reshape(-1, 4)
+@pytest.mark.parametrize("n", [16, 8])
+def test_sweep_rhs_within_fp32_tolerance_of_oracle(ag, oracle, seed, n):
+    f, m, cfg, s0 = case(ag, 400 + seed, 3, n)
+    ref = oracle.rhs(m, s0, oracle.make_config(n, cfg)).reshape(-1, 4)
     s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
     s.set_launch_variant(SWEEPS[0])
     s.upload(s0)
@@ -89,8 +92,8 @@ def test_sweep_rhs_within_fp32_tolerance_of_oracle(ag, oracle, seed):
         assert np.abs(got[:, k] - ref[:, k]).max() <= 2e-5 * scale, k
 
 
-def test_sweep_conserves_on_periodic_hanging_mesh(ag):
-    n = 16
+@pytest.mark.parametrize("n", [16, 8])
+def test_sweep_conserves_on_periodic_hanging_mesh(ag, n):
     f = meshes.two_level_ring(n, periodic=(1, 1))
     cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.01)
     cfg.apply()
@@ -106,17 +109,43 @@ def test_sweep_conserves_on_periodic_hanging_mesh(ag):
     assert np.all(np.abs(t1 - t0) <= 1e-12 * np.abs(t0) + 1e-13), t1 - t0
 
 
-def test_sweep_variants_are_the_row_sweep_kernels(ag):
-    f, m, cfg, s0 = case(ag, 8, 3)
+@pytest.mark.parametrize("n,shapes", [(16, [(4, 128), (2, 64), (8, 256)]), (8, [(8, 128), (4, 64), (16, 256)])])
+def test_sweep_variants_are_the_row_sweep_kernels(ag, n, shapes):
+    f, m, cfg, s0 = case(ag, 8, 3, n)
     s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
     v = s.launch_variants()
-    assert v[:3] == [(4, 128), (2, 64), (8, 256)]
+    assert v[:3] == shapes
     assert s.launch_variant() == 0
     s.close()
 
 
-def test_sweep_is_the_default_for_16x16_patches(ag):
-    f, m, cfg, s0 = case(ag, 7, 3)
+def test_sweep8_with_an_odd_quad_count(ag):
+    """Two 8x8 quads per warp: with an odd count the last warp's second
+    quad is absent; the result still matches the block kernel and nothing
+    is written past the last quad (the state of every quad is finite)."""
+    n = 8
+    f = meshes.uniform(n, 2, periodic=(1, 1))
+    fl = np.zeros(f.num_quads, np.int32)
+    fl[5] = 1
+    f.refine(fl)
+    f.balance()
+    assert f.num_quads % 2 == 1
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.01)
+    cfg.apply()
+    m = f.mesh(n)
+    s0 = meshes.perturbed(f.initialize(n), 17, amp=2e-2)
+    ref, _ = run(ag, m, cfg, s0, BLOCK[n], 5)
+    for v in SWEEPS:
+        got, rep = run(ag, m, cfg, s0, v, 5)
+        assert rep["error"] == 0 and np.isfinite(got).all()
+        for k in range(4):
+            scale = np.abs(ref[k::4]).max()
+            assert np.abs(got[k::4] - ref[k::4]).max() <= 1e-6 * scale, (v, k)
+
+
+@pytest.mark.parametrize("n", [16, 8])
+def test_sweep_is_the_default(ag, n):
+    f, m, cfg, s0 = case(ag, 7, 3, n)
     a, _ = run(ag, m, cfg, s0, SWEEPS[0], 3)
     s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
     s.upload(s0)
