@@ -402,6 +402,14 @@ class Session:
         check(lib().amrgpu_session_regrid_forest(self._s, C.c_void_p(forest._f)), "regrid_forest")
         self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s))
 
+    def balance_regrid(self, forest):
+        """forest.balance(session=self) and self.regrid_forest(forest) in one
+        call: the descriptors are built from the balanced leaves on the
+        device (amrgpu_session_balance_regrid)."""
+        forest.version += 1
+        check(lib().amrgpu_session_balance_regrid(self._s, C.c_void_p(forest._f)), "balance_regrid")
+        self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s))
+
     def quad_descriptors(self):
         """The device quad descriptors as a structured array (kind, nbr0,
         nbr1, rank, level, bc per side; 8 corner doubles)."""

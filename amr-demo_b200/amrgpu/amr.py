@@ -119,8 +119,7 @@ def regrid(forest, session, n, min_level, max_level, config=None, form=None, dev
     _, lev2, _, _ = forest.quads()
     forest.coarsen(((tags2 == 0) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
     if device_mesh:
-        forest.balance(session=session)
-        session.regrid_forest(forest)
+        session.balance_regrid(forest)
     else:
         forest.balance()
         kind, src = forest.remap()

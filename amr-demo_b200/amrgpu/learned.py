@@ -171,8 +171,7 @@ def regrid_by_classes(forest, session, n, classes, min_level, max_level):
     t2 = forest.get_tags()
     _, lev2, _, _ = forest.quads()
     forest.coarsen(((t2 == COARSEN) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
-    forest.balance(session=session)
-    session.regrid_forest(forest)
+    session.balance_regrid(forest)
 
 
 def vortex_amr(seed=0, n=8, min_level=3, max_level=6, tol=0.02, lo_frac=0.25, form=1, beta=None, center=None):

@@ -107,6 +107,8 @@ struct amrgpu_session {
     size_t h_stage_bytes = 0;
     void *d_mesh_scratch = nullptr;   // device scratch of the descriptor build
     size_t mesh_scratch_bytes = 0;
+    void *d_fstage = nullptr;         // device copy of a staged forest and its keys
+    size_t fstage_bytes = 0;
     void *d_bal[2] = {nullptr, nullptr};  // balance: leaves / origin / dirty, double-buffered
     void *d_bal_work = nullptr;           // balance: flags, counts, positions, keys, trees, scan temp
     int bal_cap = 0;                      // leaves the balance buffers hold
@@ -513,6 +515,7 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_send);
     cudaFree(s->d_quads_alt);
     cudaFree(s->d_mesh_scratch);
+    cudaFree(s->d_fstage);
     cudaFree(s->d_bal[0]);
     cudaFree(s->d_bal[1]);
     cudaFree(s->d_bal_work);
@@ -1002,7 +1005,7 @@ namespace {
 int ensure_quad_arrays(amrgpu_session *s, int nq)
 {
     if (nq <= s->cap_quads) return AMRGPU_OK;
-    const int cap = nq + nq / 4;
+    const int cap = nq + nq / 2;
     int *arr[3] = {nullptr, nullptr, nullptr};
     bool ok = true;
     for (int k = 0; k < 3 && ok; ++k) ok = cuda_ok(cudaMalloc(&arr[k], sizeof(int) * size_t(cap)), "cudaMalloc quad arrays");
@@ -1025,7 +1028,7 @@ int ensure_quad_arrays(amrgpu_session *s, int nq)
 int ensure_desc(amrgpu_session *s, QuadDesc **buf, int *cap, int nq)
 {
     if (nq <= *cap && *buf) return AMRGPU_OK;
-    const int c = std::max(nq + nq / 4, 1);
+    const int c = std::max(nq + nq / 2, 1);
     QuadDesc *d = nullptr;
     if (!cuda_ok(cudaMalloc(&d, sizeof(QuadDesc) * size_t(c)), "cudaMalloc quads")) return AMRGPU_ERR_CUDA;
     cudaStreamSynchronize(s->stream);
@@ -1048,7 +1051,7 @@ int apply_regrid(amrgpu_session *s, int nq, int nface)
     long long cap = s->cap_stride;
     bool ok = true;
     if (stride > s->cap_stride) {
-        cap = ((stride + stride / 4 + 31) / 32) * 32;
+        cap = ((stride + stride / 2 + 31) / 32) * 32;
         for (int k = 0; k < 4 && ok; ++k)
             ok = cuda_ok(cudaMalloc(&fresh[k], sizeof(double) * 4 * size_t(cap)), "cudaMalloc state");
         double *aos = nullptr;
@@ -1097,6 +1100,87 @@ int apply_regrid(amrgpu_session *s, int nq, int nface)
     int rc = configure_launch(s, s->launch);
     if (rc != AMRGPU_OK) return rc;
     return prime(s, s->primed);
+}
+
+// A device buffer of at least `need` bytes (contents not kept; grown by half
+// beyond the need so that a fluctuating mesh reallocates rarely).
+int ensure_dev(amrgpu_session *s, void **buf, size_t *bytes, size_t need)
+{
+    if (need <= *bytes && *buf) return AMRGPU_OK;
+    cudaStreamSynchronize(s->stream);
+    cudaFree(*buf);
+    *buf = nullptr;
+    *bytes = 0;
+    const size_t want = need + need / 2;
+    if (!cuda_ok(cudaMalloc(buf, want), "cudaMalloc scratch")) return AMRGPU_ERR_CUDA;
+    *bytes = want;
+    return AMRGPU_OK;
+}
+
+// Pinned host staging of at least `bytes`; when the buffer is kept, waits
+// for the copies still reading or writing it.
+int ensure_stage(amrgpu_session *s, size_t bytes)
+{
+    if (bytes <= s->h_stage_bytes) return cuda_ok(cudaStreamSynchronize(s->stream), "sync") ? AMRGPU_OK : AMRGPU_ERR_CUDA;
+    cudaStreamSynchronize(s->stream);
+    cudaFreeHost(s->h_stage);
+    s->h_stage = nullptr;
+    s->h_stage_bytes = 0;
+    const size_t want = bytes + bytes / 2;
+    if (!cuda_ok(cudaHostAlloc(&s->h_stage, want, cudaHostAllocDefault), "cudaHostAlloc staging")) return AMRGPU_ERR_CUDA;
+    s->h_stage_bytes = want;
+    return AMRGPU_OK;
+}
+
+void set_brick(ForestDev &F, const BrickView &B, const int *bc)
+{
+    F.nx = B.nx;
+    F.ny = B.ny;
+    F.px = B.periodic[0];
+    F.py = B.periodic[1];
+    for (int k = 0; k < 3; ++k) F.xlo[k] = B.xlo[k];
+    F.scale = B.scale;
+    for (int k = 0; k < 4; ++k) F.bc[k] = bc ? bc[k] : 0;
+}
+
+// Descriptors of the device forest F (leaves, tree tables and key buffer on
+// the device; remap table already queued into d_kind / d_src) into the spare
+// descriptor buffer; on success it becomes the live one and the state is
+// remapped. A 2:1 violation leaves the session as it was.
+int build_and_apply(amrgpu_session *s, const ForestDev &F)
+{
+    const int nq = F.nq;
+    int rc = ensure_desc(s, &s->d_quads_alt, &s->cap_desc_alt, nq);
+    if (rc) return rc;
+    const size_t scan_bytes = build_quads_scan_bytes(nq);
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t q4 = al(sizeof(int) * 4 * size_t(std::max(nq, 1)));
+    const size_t o_emit = 0, o_scan = q4, o_emtr = 2 * q4, o_tmp = 3 * q4;
+    const size_t o_stat = o_tmp + al(scan_bytes);
+    rc = ensure_dev(s, &s->d_mesh_scratch, &s->mesh_scratch_bytes, o_stat + 256);
+    if (rc) return rc;
+    char *base = static_cast<char *>(s->d_mesh_scratch);
+    int *d_status = reinterpret_cast<int *>(base + o_stat);
+    if (!cuda_ok(launch_build_quads(F, s->d_quads_alt, reinterpret_cast<int *>(base + o_emit),
+                                    reinterpret_cast<int *>(base + o_scan), reinterpret_cast<int *>(base + o_emtr),
+                                    base + o_tmp, scan_bytes, d_status, s->sms, s->stream),
+                 "build quads"))
+        return AMRGPU_ERR_CUDA;
+    s->launches += nq > 0 ? 4 : 0;
+    int *status = reinterpret_cast<int *>(s->h_stage);  // staging is at least 64 bytes
+    if (!cuda_ok(cudaMemcpyAsync(status, d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H status") ||
+        !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
+        return AMRGPU_ERR_CUDA;
+    if (status[0]) {
+        set_error(AMRGPU_ERR_MESH, "session regrid from a forest: the forest is not 2:1 balanced");
+        return AMRGPU_ERR_MESH;
+    }
+    const int nface = nq > 0 ? status[1] : 0;
+    std::swap(s->d_quads, s->d_quads_alt);
+    std::swap(s->cap_desc, s->cap_desc_alt);
+    s->h_quads.clear();  // the live descriptors exist on the device only
+    s->rect = true;      // brick quads are axis-aligned rectangles
+    return apply_regrid(s, nq, nface);
 }
 
 bool check_remap(const amrgpu_session *s, int nq, const int *kind, const int *src_index)
@@ -1185,19 +1269,8 @@ int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f)
     // pinned staging: leaves (int4), kind, src, tree_begin, tree_tx, tree_ty, tree_at
     const size_t n_int = 4 * size_t(nq) + 2 * size_t(nq) + size_t(ntrees + 1) + 3 * size_t(ntrees);
     const size_t stage_bytes = sizeof(int) * n_int;
-    if (stage_bytes > s->h_stage_bytes) {
-        cudaStreamSynchronize(s->stream);
-        cudaFreeHost(s->h_stage);
-        s->h_stage = nullptr;
-        s->h_stage_bytes = 0;
-        const size_t want = stage_bytes + stage_bytes / 4;
-        if (!cuda_ok(cudaHostAlloc(&s->h_stage, want, cudaHostAllocDefault), "cudaHostAlloc staging"))
-            return AMRGPU_ERR_CUDA;
-        s->h_stage_bytes = want;
-    } else {
-        // the previous regrid's copies out of the staging buffer have finished
-        if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return AMRGPU_ERR_CUDA;
-    }
+    int rc = ensure_stage(s, stage_bytes);
+    if (rc) return rc;
     int *hs = static_cast<int *>(s->h_stage);
     int *h_leaves = hs, *h_kind = hs + 4 * size_t(nq), *h_src = h_kind + nq, *h_tb = h_src + nq;
     int *h_tx = h_tb + ntrees + 1, *h_ty = h_tx + ntrees, *h_at = h_ty + ntrees;
@@ -1219,29 +1292,14 @@ int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f)
         h_at[t] = B.tree_at[t];
     }
     if (!check_remap(s, nq, h_kind, h_src)) return AMRGPU_ERR_ARG;
-    int rc = ensure_quad_arrays(s, nq);
-    if (rc == AMRGPU_OK) rc = ensure_desc(s, &s->d_quads_alt, &s->cap_desc_alt, nq);
-    if (rc != AMRGPU_OK) return rc;
-    // device scratch: staged ints, keys, emits / scan / emitter, scan temp, status
-    const size_t scan_bytes = build_quads_scan_bytes(nq);
+    rc = ensure_quad_arrays(s, nq);
+    if (rc) return rc;
+    // device copy of the staged ints, then the leaves' Morton keys
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t o_keys = al(stage_bytes);
-    const size_t o_emit = o_keys + al(sizeof(unsigned long long) * size_t(std::max(nq, 1)));
-    const size_t o_scan = o_emit + al(sizeof(int) * 4 * size_t(std::max(nq, 1)));
-    const size_t o_emtr = o_scan + al(sizeof(int) * 4 * size_t(std::max(nq, 1)));
-    const size_t o_tmp = o_emtr + al(sizeof(int) * 4 * size_t(std::max(nq, 1)));
-    const size_t o_stat = o_tmp + al(scan_bytes);
-    const size_t need = o_stat + 256;
-    if (need > s->mesh_scratch_bytes) {
-        cudaStreamSynchronize(s->stream);
-        cudaFree(s->d_mesh_scratch);
-        s->d_mesh_scratch = nullptr;
-        s->mesh_scratch_bytes = 0;
-        const size_t want = need + need / 4;
-        if (!cuda_ok(cudaMalloc(&s->d_mesh_scratch, want), "cudaMalloc mesh scratch")) return AMRGPU_ERR_CUDA;
-        s->mesh_scratch_bytes = want;
-    }
-    char *base = static_cast<char *>(s->d_mesh_scratch);
+    rc = ensure_dev(s, &s->d_fstage, &s->fstage_bytes, o_keys + sizeof(unsigned long long) * size_t(std::max(nq, 1)));
+    if (rc) return rc;
+    char *base = static_cast<char *>(s->d_fstage);
     int *d_stage = reinterpret_cast<int *>(base);
     bool ok = cuda_ok(cudaMemcpyAsync(d_stage, hs, stage_bytes, cudaMemcpyHostToDevice, s->stream), "H2D forest") &&
               cuda_ok(cudaMemcpyAsync(s->d_kind, h_kind, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice,
@@ -1253,39 +1311,13 @@ int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f)
     ForestDev F;
     F.leaves = reinterpret_cast<const int4 *>(d_stage);
     F.keys = reinterpret_cast<unsigned long long *>(base + o_keys);
-    const int *d_tb = d_stage + (h_tb - hs);
-    F.tree_begin = d_tb;
+    F.tree_begin = d_stage + (h_tb - hs);
     F.tree_tx = d_stage + (h_tx - hs);
     F.tree_ty = d_stage + (h_ty - hs);
     F.tree_at = d_stage + (h_at - hs);
-    F.nx = B.nx;
-    F.ny = B.ny;
-    F.px = B.periodic[0];
-    F.py = B.periodic[1];
-    for (int k = 0; k < 3; ++k) F.xlo[k] = B.xlo[k];
-    F.scale = B.scale;
-    for (int k = 0; k < 4; ++k) F.bc[k] = s->cfg.bc[k];
+    set_brick(F, B, s->cfg.bc);
     F.nq = nq;
-    int *d_status = reinterpret_cast<int *>(base + o_stat);
-    if (!cuda_ok(launch_build_quads(F, s->d_quads_alt, reinterpret_cast<int *>(base + o_emit),
-                                    reinterpret_cast<int *>(base + o_scan), reinterpret_cast<int *>(base + o_emtr),
-                                    base + o_tmp, scan_bytes, d_status, s->sms, s->stream),
-                 "build quads"))
-        return AMRGPU_ERR_CUDA;
-    s->launches += nq > 0 ? 4 : 0;
-    int status[2] = {0, 0};
-    if (!cuda_ok(cudaMemcpyAsync(status, d_status, sizeof(status), cudaMemcpyDeviceToHost, s->stream), "D2H status") ||
-        !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
-        return AMRGPU_ERR_CUDA;
-    if (status[0]) {
-        set_error(AMRGPU_ERR_MESH, "session_regrid_forest: the forest is not 2:1 balanced");
-        return AMRGPU_ERR_MESH;
-    }
-    std::swap(s->d_quads, s->d_quads_alt);
-    std::swap(s->cap_desc, s->cap_desc_alt);
-    s->h_quads.clear();  // the live descriptors exist on the device only
-    s->rect = true;      // brick quads are axis-aligned rectangles
-    return apply_regrid(s, nq, nq > 0 ? status[1] : 0);
+    return build_and_apply(s, F);
 }
 
 }  // extern "C"
@@ -1368,29 +1400,15 @@ int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
     return AMRGPU_OK;
 }
 
-int ensure_stage(amrgpu_session *s, size_t bytes)
+// 2:1 balance of forest fo with every pass on the session's GPU; the
+// balanced leaves stay in d_bal[*live_out] (with the last pass's keys and
+// tree starts in the work area) and are copied back into the host forest.
+// Returns the leaf count or -error.
+int balance_impl(amrgpu_session *s, Forest *fo, int *live_out)
 {
-    if (bytes <= s->h_stage_bytes) return cuda_ok(cudaStreamSynchronize(s->stream), "sync") ? AMRGPU_OK : AMRGPU_ERR_CUDA;
-    cudaStreamSynchronize(s->stream);
-    cudaFreeHost(s->h_stage);
-    s->h_stage = nullptr;
-    s->h_stage_bytes = 0;
-    const size_t want = bytes + bytes / 4;
-    if (!cuda_ok(cudaHostAlloc(&s->h_stage, want, cudaHostAllocDefault), "cudaHostAlloc staging")) return AMRGPU_ERR_CUDA;
-    s->h_stage_bytes = want;
-    return AMRGPU_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
-{
-    if (!f || !f->f || !s) return -AMRGPU_ERR_ARG;
-    std::vector<Leaf> &leaves = forest_leaves_mut(f->f);
+    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
     BrickView B;
-    forest_brick(f->f, &B);
+    forest_brick(fo, &B);
     const int ntrees = B.nx * B.ny;
     int nl = int(leaves.size());
     // staging: leaves (int4), origin, dirty bytes, brick tables
@@ -1440,7 +1458,7 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
         if (!ok) return -AMRGPU_ERR_CUDA;
     }
     int live = 0;
-    bool done = false;
+    bool done = false, refined = false;
     for (int pass = 0; pass < 64 && !done; ++pass) {
         const BalLayout L = bal_layout(s->bal_cap, ntrees);
         char *in = static_cast<char *>(s->d_bal[live]);
@@ -1502,10 +1520,16 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
         s->launches++;
         live = 1 - live;
         nl = total;
+        refined = true;
     }
     if (!done) {
         set_error(AMRGPU_ERR_MESH, "forest_balance_device: no balance after 64 passes");
         return -AMRGPU_ERR_MESH;
+    }
+    *live_out = live;
+    if (!refined) {
+        for (Leaf &q : leaves) q.dirty = 0;
+        return nl;
     }
     // the balanced leaves back to the host: coordinates and origin
     rc = ensure_stage(s, 20 * size_t(nl) + 64);
@@ -1535,6 +1559,67 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
         for (Leaf &q : leaves) q.dirty = 0;
     }
     return nl;
+}
+
+}  // namespace
+
+extern "C" {
+
+int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
+{
+    if (!f || !f->f || !s) return -AMRGPU_ERR_ARG;
+    int live = 0;
+    return balance_impl(s, f->f, &live);
+}
+
+int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f)
+{
+    if (!s || !f || !f->f) return AMRGPU_ERR_ARG;
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_balance_regrid: a step begun with step_stage is not finished");
+        return AMRGPU_ERR_ARG;
+    }
+    if (s->nghost != 0) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "session_balance_regrid: ghost quads need a ghost exchange after the remap");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    int live = 0;
+    const int nq = balance_impl(s, f->f, &live);
+    if (nq < 0) return -nq;
+    // remap table of the balanced leaves (host forest now holds them)
+    const std::vector<Leaf> &L = forest_leaves(f->f);
+    BrickView B;
+    forest_brick(f->f, &B);
+    const int ntrees = B.nx * B.ny;
+    int rc = ensure_stage(s, 8 * size_t(nq) + 64);
+    if (rc) return rc;
+    int *h_kind = static_cast<int *>(s->h_stage) + 16, *h_src = h_kind + nq;  // ints 0..15: status
+    for (int i = 0; i < nq; ++i) {
+        h_kind[i] = L[size_t(i)].src_kind;
+        h_src[i] = L[size_t(i)].src;
+    }
+    if (!check_remap(s, nq, h_kind, h_src)) return AMRGPU_ERR_ARG;
+    rc = ensure_quad_arrays(s, nq);
+    if (rc) return rc;
+    if (!cuda_ok(cudaMemcpyAsync(s->d_kind, h_kind, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, s->stream),
+                 "H2D remap") ||
+        !cuda_ok(cudaMemcpyAsync(s->d_src, h_src, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, s->stream),
+                 "H2D remap"))
+        return AMRGPU_ERR_CUDA;
+    // the descriptors straight from the balanced leaves on the device
+    const BalLayout BL = bal_layout(s->bal_cap, ntrees);
+    char *in = static_cast<char *>(s->d_bal[live]);
+    char *w = static_cast<char *>(s->d_bal_work);
+    ForestDev F;
+    F.leaves = reinterpret_cast<const int4 *>(in);
+    F.keys = reinterpret_cast<unsigned long long *>(w + BL.o_keys);
+    F.tree_begin = reinterpret_cast<const int *>(w + BL.o_tb);
+    F.tree_tx = reinterpret_cast<const int *>(w + BL.o_tx);
+    F.tree_ty = reinterpret_cast<const int *>(w + BL.o_ty);
+    F.tree_at = reinterpret_cast<const int *>(w + BL.o_at);
+    set_brick(F, B, s->cfg.bc);
+    F.nq = nq;
+    return build_and_apply(s, F);
 }
 
 int amrgpu_session_quad_descriptors(amrgpu_session_t *s, void *out, int cap)

@@ -239,23 +239,24 @@ def learned_amr(args):
     indicator with the FP32-flux form (regrid every 10 steps, the model
     trained on look-ahead labels 10 steps ahead) against the plain
     indicator with the plain FP64 form (regrid every 5 steps), on unseen
-    seeds of the vortex family under AMR (levels 3-6, 8x8 patches,
+    seeds of the vortex family under AMR (levels 3 to --learned-max-level (7: 1024^2 at the finest), 8x8 patches,
     relative density-jump tolerance 0.02, t = 3). Rates include the regrid
     time; L1(rho) is measured against the exact translated vortex and
     between the two runs on the level-6 uniform grid."""
     import numpy as np
     from amrgpu import learned as L
-    n, lo, hi, tol = 8, 3, 6, 0.02
+    n, lo, hi, tol = 8, 3, args.learned_max_level, 0.02
     t0 = time.perf_counter()
     m = L.Mlp(seed=0)
     rows = L.collect(m, range(args.learned_seeds), n, lo, hi, tol, regrid_interval=10, regrids=25, lookahead=True)
     t1 = time.perf_counter()
-    hist, _ = L.train(m, epochs=20, batch=4096, lr=1e-3, seed=0)
+    hist, _ = L.train(m, epochs=20, batch=8192, lr=1e-3, seed=0)
     t2 = time.perf_counter()
-    out = {"workload": "isentropic vortex family under AMR, periodic [0,10]^2, levels 3-6, 8x8 patches, "
+    out = {"workload": f"isentropic vortex family under AMR, periodic [0,10]^2, levels 3-{hi}, 8x8 patches, "
                        "density-jump tol 0.02, SSP-RK3 CFL 0.5, t = 3, unseen seeds 5000-5002",
-           "training": {"rows": rows, "epochs": 20, "batch": 4096, "lr": 1e-3, "collect_s": t1 - t0,
-                        "train_s": t2 - t1, "final_loss": hist[-1][0], "final_accuracy": hist[-1][1]}}
+           "training": {"rows": rows, "epochs": 20, "batch": 8192, "lr": 1e-3, "collect_s": t1 - t0,
+                        "train_s": t2 - t1, "final_loss": hist[-1][0], "final_accuracy": hist[-1][1],
+                        "seeds": args.learned_seeds}}
     runs = {"plain_fp64": [], "learned_fp32": []}
     for seed in (5000, 5001, 5002):
         ends = {}
@@ -319,7 +320,7 @@ def amr_workload(args):
     solve = reg = 0.0
     cu = steps = 0
     cells = []
-    parts = dict(tag=0.0, forest=0.0, balance=0.0, regrid_forest=0.0)
+    parts = dict(tag=0.0, forest=0.0, balance_regrid=0.0)
     cycles = max(1, args.steps // 5)
     for _ in range(cycles):
         # the regrid of amr.regrid, timed part by part
@@ -340,11 +341,9 @@ def amr_workload(args):
         _, lev2, _, _ = f.quads()
         f.coarsen(((t2 == 0) & (lev2 > lo)).astype(np.int32), min_level=lo)
         d = time.perf_counter()
-        f.balance(session=s)
-        e = time.perf_counter()
-        s.regrid_forest(f)
+        s.balance_regrid(f)
         h = time.perf_counter()
-        for k, v in zip(parts, (c - b, d - c, e - d, h - e)):
+        for k, v in zip(parts, (c - b, d - c, h - d)):
             parts[k] += v
         solve += b - a
         reg += h - b
@@ -624,7 +623,9 @@ def main():
                     help="use the sharded multi-rank driver also at one rank (under torchrun)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator AMR comparison")
     ap.add_argument("--learned-only", action="store_true", help="run only the learned-indicator AMR comparison")
-    ap.add_argument("--learned-seeds", type=int, default=32, help="seeded runs that make the training set")
+    ap.add_argument("--learned-seeds", type=int, default=64, help="seeded runs that make the training set")
+    ap.add_argument("--learned-max-level", type=int, default=7,
+                    help="finest level of the learned-indicator workload (8x8 patches; 7 = 1024^2 at the finest)")
     ap.add_argument("--workload", choices=["vortex", "four_quadrant", "shock_bubble"], default="vortex",
                     help="vortex: the headline line; the others time one adaptive workload")
     ap.add_argument("--amr-form", type=int, default=1, help="form of the adaptive workloads (0 FP64, 1 FP32 flux)")

@@ -315,6 +315,10 @@ int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f);
  * on the session's GPU (same passes, same leaves, tags and remap table);
  * returns the leaf count, or -error. */
 int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s);
+/* amrgpu_forest_balance_device then amrgpu_session_regrid_forest, with the
+ * descriptors built from the balanced leaves already on the device (one
+ * upload of the forest per regrid instead of two). */
+int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f);
 /* Copies up to cap quad descriptors (160 bytes each: 4 sides x {kind, nbr0,
  * nbr1, face rank, level, bc} ints, then 8 corner doubles) to host memory;
  * returns the session's quad count. */

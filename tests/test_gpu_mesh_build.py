@@ -159,3 +159,47 @@ def test_device_balance_equals_host_balance(ag, seed):
         assert fb.is_balanced()
         for u, v in zip(leaves_of(fa), leaves_of(fb)):
             assert np.array_equal(u, v), rnd
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_fused_balance_regrid_equals_host_path(ag, seed):
+    """balance_regrid (balance passes and descriptors from the balanced
+    leaves on the device) against the host balance + host mesh + decode."""
+    n = 8
+    rng = np.random.default_rng(900 + seed)
+    nx, ny = int(rng.integers(1, 3)), int(rng.integers(1, 3))
+    per = (int(rng.integers(2)), int(rng.integers(2)))
+    fa = ag.Forest(nx, ny, periodic=per, level=2)
+    fb = ag.Forest(nx, ny, periodic=per, level=2)
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.005, h=1.0)  # trees of side 1
+    cfg.apply()
+    s0 = meshes.perturbed(fa.initialize(n), seed, amp=1e-2)
+    a = ag.Session(fa.mesh(n), cfg, form=1)
+    b = ag.Session(fb.mesh(n), cfg, form=1)
+    for s in (a, b):
+        s.upload(s0)
+    for rnd in range(4):
+        for s in (a, b):
+            s.step(3)
+        rf = (rng.random(fa.num_quads) < 0.2).astype(np.int32)
+        cf = None
+        for f in (fa, fb):
+            f.begin_regrid()
+            f.set_tags(rf)
+            f.refine(rf, max_level=6)
+        cf = (rng.random(fa.num_quads) < 0.5).astype(np.int32)
+        for f in (fa, fb):
+            f.coarsen(cf, min_level=1)
+        fa.balance()
+        kind, src = fa.remap()
+        a.regrid(fa.mesh(n), kind, src)
+        b.balance_regrid(fb)
+        for u, v in zip(leaves_of(fa), leaves_of(fb)):
+            assert np.array_equal(u, v), rnd
+        assert a.quad_descriptors().tobytes() == b.quad_descriptors().tobytes(), rnd
+        qa = a.download()
+        assert np.isfinite(qa).all() and np.array_equal(qa, b.download()), rnd
+    a.step(4)
+    b.step(4)
+    qa = a.download()
+    assert np.isfinite(qa).all() and np.array_equal(qa, b.download())
