@@ -38,6 +38,14 @@ os.environ.setdefault("AMRGPU_QUIET", "1")
 METRIC = "RK cell-updates/s on 1 B200: learned+FP32 form vs plain FP64, at equal L1(rho)"
 UNIT = "cell-updates/s"
 WORKLOAD = "isentropic vortex, periodic [0,10]^2, 4096 quads x 16x16 = 1024^2 cells, SSP-RK3, CFL 0.5"
+
+
+def workload_name(mesh, n):
+    if n == 16 and mesh.ncell == 4096:
+        return WORKLOAD
+    side = int(round(mesh.ncells ** 0.5))
+    return (f"isentropic vortex, periodic [0,10]^2, {mesh.ncell} quads x {n}x{n} = {side}^2 cells, "
+            "SSP-RK3, CFL 0.5")
 # Algorithmic HBM bytes per cell-update (one RK step of one cell, summed over
 # its stages). FP64 exact SSP-RK3: stage 1 reads X, writes Y and K (96 B);
 # stage 2 reads Y, X, K, writes X, K (160 B); stage 3 reads X, K, writes Y
@@ -513,7 +521,7 @@ def run_gpu(args):
 
     import amrgpu as ag
     from amrgpu import workloads as W
-    f, mesh, cfg, s0 = W.vortex_1024(level=args.level, final_time=0.0, steps=10 ** 9)
+    f, mesh, cfg, s0 = W.vortex_1024(level=args.level, n=args.patch, final_time=0.0, steps=10 ** 9)
     hbm, peak_kind = peaks()
     run_forms = (0, 1) if args.form < 0 else (args.form,)
 
@@ -556,13 +564,15 @@ def run_gpu(args):
     if not args.no_learned:
         amr = learned_amr(args)
     head = out[1]
-    traffic = traffic_per_launch(1)
+    # the committed ncu traffic figure is for the default workload (16x16, level 6)
+    traffic = traffic_per_launch(1) if (args.patch == 16 and args.level == 6) else None
     line = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 flux / f64 state",
         "data": "synthetic (seeded analytic vortex; no dataset exists)",
-        "config": {"workload": WORKLOAD, "cells": mesh.ncells, "quads": mesh.ncell, "patch": "16x16",
+        "config": {"workload": workload_name(mesh, args.patch), "cells": mesh.ncells, "quads": mesh.ncell,
+                   "patch": f"{args.patch}x{args.patch}",
                    "form": "FP32 flux, FP64 state, Shu-Osher SSP-RK3", "l2": "flushed between steps "
                    "(256 MB write; per-step CUDA events exclude it)", "launch": head["tune"],
                    "parallelism": "1 GPU"},
@@ -617,6 +627,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--level", type=int, default=6, help="forest level (6: the 1024^2 workload)")
+    ap.add_argument("--patch", type=int, default=16, choices=[8, 16],
+                    help="subgrid patch size of the vortex workload (16: the 1024^2 workload at level 6)")
     ap.add_argument("--form", type=int, default=-1, help="time one form only (0 FP64, 1 FP32 flux)")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape")
     ap.add_argument("--shard", action="store_true",
