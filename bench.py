@@ -244,19 +244,22 @@ def traffic_per_launch(form):
 
 def learned_amr(args):
     """The metric's comparison on an adaptive workload: the learned
-    indicator with the FP32-flux form (regrid every 10 steps, the model
-    trained on look-ahead labels 10 steps ahead) against the plain
+    indicator with the FP32-flux form (regrid every --learned-interval
+    steps, default 20, the model trained on look-ahead labels that many
+    steps ahead) against the plain
     indicator with the plain FP64 form (regrid every 5 steps), on unseen
-    seeds of the vortex family under AMR (levels 3 to --learned-max-level (7: 1024^2 at the finest), 8x8 patches,
-    relative density-jump tolerance 0.02, t = 3). Rates include the regrid
-    time; L1(rho) is measured against the exact translated vortex and
-    between the two runs on the level-6 uniform grid."""
+    seeds of the vortex family under AMR (levels 3 to --learned-max-level,
+    default 7 = 1024^2 at the finest, 8x8 patches, relative density-jump
+    tolerance 0.02, t = 3). Rates include the regrid time; L1(rho) is
+    measured against the exact translated vortex and between the two runs
+    on the finest level's uniform grid."""
     import numpy as np
     from amrgpu import learned as L
     n, lo, hi, tol = 8, 3, args.learned_max_level, 0.02
     t0 = time.perf_counter()
     m = L.Mlp(seed=0)
-    rows = L.collect(m, range(args.learned_seeds), n, lo, hi, tol, regrid_interval=10, regrids=25, lookahead=True)
+    rows = L.collect(m, range(args.learned_seeds), n, lo, hi, tol, regrid_interval=args.learned_interval,
+                     regrids=25, lookahead=True)
     t1 = time.perf_counter()
     hist, _ = L.train(m, epochs=20, batch=8192, lr=1e-3, seed=0)
     t2 = time.perf_counter()
@@ -268,7 +271,7 @@ def learned_amr(args):
     runs = {"plain_fp64": [], "learned_fp32": []}
     for seed in (5000, 5001, 5002):
         ends = {}
-        for key, mlp, form, ri in (("plain_fp64", None, 0, 5), ("learned_fp32", m, 1, 10)):
+        for key, mlp, form, ri in (("plain_fp64", None, 0, 5), ("learned_fp32", m, 1, args.learned_interval)):
             f, cfg, soln, par = L.vortex_amr(seed, n, lo, hi, tol, form=form)
             s, r = L.run(f, soln, n, cfg, final_time=3.0, regrid_interval=ri, min_level=lo, max_level=hi, tol=tol,
                          mlp=mlp, form=form, seed=seed)
@@ -282,7 +285,7 @@ def learned_amr(args):
     for key, rs in runs.items():
         cu = sum(r["cell_updates"] for r in rs)
         secs = sum(r["solve_s"] + r["regrid_s"] for r in rs)
-        out[key] = {"value": cu / secs, "unit": UNIT, "regrid_interval": 5 if key == "plain_fp64" else 10,
+        out[key] = {"value": cu / secs, "unit": UNIT, "regrid_interval": 5 if key == "plain_fp64" else args.learned_interval,
                     "mean_cells": float(np.mean([r["mean_cells"] for r in rs])),
                     "l1_rho_vs_exact": float(np.mean([r["l1_rho_vs_exact"] for r in rs])),
                     "regrids": int(sum(r["regrids"] for r in rs)),
@@ -636,6 +639,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator AMR comparison")
     ap.add_argument("--learned-only", action="store_true", help="run only the learned-indicator AMR comparison")
     ap.add_argument("--learned-seeds", type=int, default=64, help="seeded runs that make the training set")
+    ap.add_argument("--learned-interval", type=int, default=20,
+                    help="regrid interval of the learned run (its model predicts the plain class that many steps ahead)")
     ap.add_argument("--learned-max-level", type=int, default=7,
                     help="finest level of the learned-indicator workload (8x8 patches; 7 = 1024^2 at the finest)")
     ap.add_argument("--workload", choices=["vortex", "four_quadrant", "shock_bubble"], default="vortex",
