@@ -82,6 +82,37 @@ uint64_t fnv1a(const void *p, size_t bytes, uint64_t h = 1469598103934665603ULL)
     return h;
 }
 
+// Hash of a large array (the mesh arrays the reference passes on every
+// evolve call): 8-byte words into four independent multiply-xorshift lanes,
+// so that a call hashes ~1 MB in tens of microseconds instead of the byte
+// loop's milliseconds. Only used to notice that the mesh changed.
+uint64_t hash_words(const void *p, size_t bytes, uint64_t seed)
+{
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    const uint64_t k = 0x9E3779B97F4A7C15ULL;
+    uint64_t h[4] = {seed ^ 0x243F6A8885A308D3ULL, seed ^ 0x13198A2E03707344ULL, seed ^ 0xA4093822299F31D0ULL,
+                     seed ^ 0x082EFA98EC4E6C89ULL};
+    size_t nw = bytes / 8, i = 0;
+    for (; i + 4 <= nw; i += 4)
+        for (int l = 0; l < 4; ++l) {
+            uint64_t w;
+            std::memcpy(&w, b + 8 * (i + size_t(l)), 8);
+            h[l] = (h[l] ^ w) * k;
+            h[l] ^= h[l] >> 29;
+        }
+    for (; i < nw; ++i) {
+        uint64_t w;
+        std::memcpy(&w, b + 8 * i, 8);
+        h[0] = ((h[0] ^ w) * k) ^ (h[0] >> 31);
+    }
+    uint64_t t = 0;
+    std::memcpy(&t, b + 8 * nw, bytes - 8 * nw);
+    h[1] = ((h[1] ^ t ^ (uint64_t)bytes) * k);
+    uint64_t r = h[0];
+    for (int l = 1; l < 4; ++l) r = ((r ^ (h[l] + (r << 6) + (r >> 2))) * k) ^ (r >> 33);
+    return r;
+}
+
 }  // namespace
 
 struct amrgpu_session {
@@ -1700,10 +1731,10 @@ void evolve(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *
 
     auto wall0 = std::chrono::steady_clock::now();
     EvolveCache &ec = cache();
-    uint64_t mh = fnv1a(cell_info, sizeof(int) * 3 * size_t(*ncell + *nghost));
-    mh = fnv1a(face_info, sizeof(int) * 11 * size_t(*nface), mh);
-    mh = fnv1a(geom, sizeof(double) * 12 * size_t(*ncell + *nghost), mh);
-    mh = fnv1a(ncell, sizeof(int), mh);
+    uint64_t mh = hash_words(cell_info, sizeof(int) * 3 * size_t(*ncell + *nghost), 1469598103934665603ULL);
+    mh = hash_words(face_info, sizeof(int) * 11 * size_t(*nface), mh);
+    mh = hash_words(geom, sizeof(double) * 12 * size_t(*ncell + *nghost), mh);
+    mh = hash_words(ncell, sizeof(int), mh);
     uint64_t ch = cfg_hash(c);
     if (!ec.s || ec.mesh_hash != mh || ec.cfg_hash != ch) {
         if (ec.s) amrgpu_session_destroy(ec.s);
