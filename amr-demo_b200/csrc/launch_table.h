@@ -17,6 +17,7 @@ struct StageLaunch {
     int min_blocks;
     size_t smem;
     const void *kernel;  // __global__ void(StageArgs)
+    int sweep = 0;       // 1: a row-sweep kernel (one warp per qpb*32/threads quads)
 };
 
 int stage_table_fp64(const StageLaunch **out);

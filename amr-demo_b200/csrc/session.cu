@@ -145,6 +145,7 @@ struct amrgpu_session {
     int bal_cap = 0;                      // leaves the balance buffers hold
     int bal_trees = 0;                    // trees the balance work area holds tables for
     bool rect = true;                 // every quad an axis-aligned rectangle
+    bool launch_pinned = false;       // the stage launch was chosen by the caller
     int *d_tags = nullptr;
     int *d_kind = nullptr;
     int *d_src = nullptr;
@@ -273,6 +274,30 @@ bool quads_are_rectangles(const amrgpu_session *s)
             return false;
     }
     return true;
+}
+
+// The launch a session uses unless one was chosen: the first compiled entry
+// for its patch size, except that a row sweep (one warp per quad or quad
+// pair, each running a serial sweep) gives way to the first block kernel
+// when the mesh has too few quads to occupy the GPU with sweep warps
+// (fewer than 1024 warps: measured slower on 256-1024 quads, faster from
+// 2048 warps on).
+const StageLaunch *default_launch(int form, int n, int nquad)
+{
+    const StageLaunch *tab;
+    const int cnt = (form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
+    const StageLaunch *first = nullptr, *block = nullptr;
+    for (int i = 0; i < cnt; ++i) {
+        if (tab[i].n != n) continue;
+        if (!first) first = &tab[i];
+        if (!block && !tab[i].sweep) block = &tab[i];
+    }
+    if (first && first->sweep && block) {
+        const int qpw = first->qpb / (first->threads / 32);
+        const long long warps = (nquad + qpw - 1) / qpw;
+        if (warps < 1024) return block;
+    }
+    return first;
 }
 
 const StageLaunch *find_launch(int form, int n, int qpb, int threads)
@@ -512,12 +537,15 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const 
         amrgpu_session_destroy(s);
         return AMRGPU_ERR_CUDA;
     }
-    const StageLaunch *L = find_launch(s->form, s->n, 0, 0);
+    const StageLaunch *L = default_launch(s->form, s->n, s->nquad);
     const char *env_q = std::getenv("AMRGPU_QPB");
     const char *env_t = std::getenv("AMRGPU_THREADS");
     if (env_q || env_t) {
         const StageLaunch *L2 = find_launch(s->form, s->n, env_q ? std::atoi(env_q) : 0, env_t ? std::atoi(env_t) : 0);
-        if (L2) L = L2;
+        if (L2) {
+            L = L2;
+            s->launch_pinned = true;
+        }
     }
     rc = configure_launch(s, L);
     if (rc != AMRGPU_OK) {
@@ -562,7 +590,8 @@ int amrgpu_session_set_form(amrgpu_session_t *s, int form)
     // keep the current state where the canonical X role points
     s->form = form;
     s->cfg.form = form;
-    return configure_launch(s, find_launch(form, s->n, 0, 0));
+    s->launch_pinned = false;
+    return configure_launch(s, default_launch(form, s->n, s->nquad));
 }
 
 int amrgpu_session_set_launch(amrgpu_session_t *s, int qpb, int threads)
@@ -573,6 +602,7 @@ int amrgpu_session_set_launch(amrgpu_session_t *s, int qpb, int threads)
         set_error(AMRGPU_ERR_ARG, "no compiled variant with that shape");
         return AMRGPU_ERR_ARG;
     }
+    s->launch_pinned = true;
     return configure_launch(s, L);
 }
 
@@ -584,7 +614,10 @@ int amrgpu_session_set_launch_variant(amrgpu_session_t *s, int index)
     int k = 0;
     for (int i = 0; i < cnt; ++i) {
         if (tab[i].n != s->n) continue;
-        if (k++ == index) return configure_launch(s, &tab[i]);
+        if (k++ == index) {
+            s->launch_pinned = true;
+            return configure_launch(s, &tab[i]);
+        }
     }
     set_error(AMRGPU_ERR_ARG, "no compiled variant with that index");
     return AMRGPU_ERR_ARG;
@@ -1128,7 +1161,8 @@ int apply_regrid(amrgpu_session *s, int nq, int nface)
     s->dof = 4 * s->n * s->n * nq;
     s->ncells_total = cells;
     s->stride = stride;
-    int rc = configure_launch(s, s->launch);
+    // a launch chosen by the caller stays; the default follows the mesh size
+    int rc = configure_launch(s, s->launch_pinned ? s->launch : default_launch(s->form, s->n, nq));
     if (rc != AMRGPU_OK) return rc;
     return prime(s, s->primed);
 }

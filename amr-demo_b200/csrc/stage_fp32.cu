@@ -85,8 +85,8 @@ const void *cfl_kernel_fp32(int n)
 // row-sweep kernel for 16x16 patches: one warp per quad, "quads per
 // block" = warps per block, no dynamic shared memory; all at 128
 // registers (16 resident warps per SM): fewer registers spill and run slower
-#define AMRGPU_SWEEP16(W, MINB) StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep16_kernel<W, MINB>}
-#define AMRGPU_SWEEP8(W, MINB) StageLaunch{8, 2 * (W), 32 * (W), MINB, 0, (const void *)sweep8_kernel<W, MINB>}
+#define AMRGPU_SWEEP16(W, MINB) StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep16_kernel<W, MINB>, 1}
+#define AMRGPU_SWEEP8(W, MINB) StageLaunch{8, 2 * (W), 32 * (W), MINB, 0, (const void *)sweep8_kernel<W, MINB>, 1}
 
 static const StageLaunch kTable32[] = {
     AMRGPU_SWEEP16(4, 4),   // 128 registers, 16 warps per SM

@@ -113,9 +113,7 @@ def test_sweep_conserves_on_periodic_hanging_mesh(ag, n):
 def test_sweep_variants_are_the_row_sweep_kernels(ag, n, shapes):
     f, m, cfg, s0 = case(ag, 8, 3, n)
     s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
-    v = s.launch_variants()
-    assert v[:3] == shapes
-    assert s.launch_variant() == 0
+    assert s.launch_variants()[:3] == shapes
     s.close()
 
 
@@ -143,13 +141,25 @@ def test_sweep8_with_an_odd_quad_count(ag):
             assert np.abs(got[k::4] - ref[k::4]).max() <= 1e-6 * scale, (v, k)
 
 
-@pytest.mark.parametrize("n", [16, 8])
-def test_sweep_is_the_default(ag, n):
-    f, m, cfg, s0 = case(ag, 7, 3, n)
-    a, _ = run(ag, m, cfg, s0, SWEEPS[0], 3)
-    s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
-    s.upload(s0)
-    s.step(3)
-    b = s.download()
+@pytest.mark.parametrize("n,level,default", [(16, 5, 0), (16, 3, 3), (8, 6, 0), (8, 5, 3)])
+def test_default_launch_follows_the_mesh_size(ag, n, level, default):
+    """The row sweep is the default from 1024 sweep warps on (1024 quads of
+    16x16, 2048 of 8x8); smaller meshes take the first block kernel. A
+    regrid re-chooses unless the caller set a launch."""
+    f = meshes.uniform(n, level, periodic=(1, 1))
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.01)
+    cfg.apply()
+    s = ag.Session(f.mesh(n), cfg, form=ag.FORM_FP32_FLUX)
+    assert s.launch_variant() == default
+    s.upload(f.initialize(n))
+    # coarsen everything once: far fewer quads -> the block kernel
+    f.begin_regrid()
+    f.coarsen(np.ones(f.num_quads, np.int32), min_level=0)
+    f.balance()
+    kind, src = f.remap()
+    s.regrid(f.mesh(n), kind, src)
+    assert s.launch_variant() == 3
+    s.set_launch_variant(1)
+    s.step(1)
+    assert s.launch_variant() == 1
     s.close()
-    assert np.array_equal(a, b)
