@@ -285,16 +285,25 @@ class Distributed:
         if self.nranks != rank_obj.shard.nranks:
             raise ValueError("the shard's partition and the process group differ in size")
 
+    def _ops(self):
+        """The per-stage send/recv descriptors, built once: the buffers and
+        lists do not change while the mesh does not."""
+        ops = getattr(self, "_p2p", None)
+        if ops is None:
+            r, dist = self.r, self.dist
+            rec = r.shard.record
+            ops = []
+            for peer, first, count in r.shard.recv:
+                ops.append(dist.P2POp(dist.irecv, r.recvbuf[first * rec:(first + count) * rec], peer, self.group))
+            for peer, first, count in r.shard.send:
+                ops.append(dist.P2POp(dist.isend, r.sendbuf[first * rec:(first + count) * rec], peer, self.group))
+            self._p2p = ops
+        return ops
+
     def _exchange(self):
-        r, dist = self.r, self.dist
-        rec = r.shard.record
-        ops = []
-        for peer, first, count in r.shard.recv:
-            ops.append(dist.P2POp(dist.irecv, r.recvbuf[first * rec:(first + count) * rec], peer, self.group))
-        for peer, first, count in r.shard.send:
-            ops.append(dist.P2POp(dist.isend, r.sendbuf[first * rec:(first + count) * rec], peer, self.group))
+        ops = self._ops()
         if ops:
-            for w in dist.batch_isend_irecv(ops):
+            for w in self.dist.batch_isend_irecv(ops):
                 w.wait()
 
     def _in_stream(self, fn):
