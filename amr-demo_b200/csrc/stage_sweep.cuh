@@ -159,8 +159,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
 
         // ---------------- sweep over the lane's R rows
         float below[8];      // record of the row below (y-face partner)
-        double xpart[4];     // -F(x-1/2) + F(x+1/2) of the row below
-        double gbelow[4];    // F(y-1/2) of the row below
+        double part[4];      // (-F(x-1/2) + F(x+1/2)) - F(y-1/2) of the row below
         double qbelow[4];    // input state of the row below
         double a0below[4] = {0.0, 0.0, 0.0, 0.0};  // first auxiliary input of the row below
         double a0next[4] = {0.0, 0.0, 0.0, 0.0};   // ... of the current row, loaded a row ahead of its use
@@ -170,7 +169,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
             double kv[4], qn[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                const double r = (xpart[f] - gbelow[f]) + gup[f];
+                const double r = part[f] + gup[f];
                 kv[f] = -(r * inv_vol);
             }
             if (!valid) return;
@@ -238,8 +237,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
             }
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                xpart[f] = xp[f];
-                gbelow[f] = gy[f];
+                part[f] = xp[f] - gy[f];
                 qbelow[f] = q4[f];
             }
 #pragma unroll
