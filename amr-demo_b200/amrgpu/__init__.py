@@ -234,6 +234,20 @@ class Forest:
         self.version += 1
         return lib().amrgpu_forest_coarsen(self._f, ip(fl), int(min_level))
 
+    def adapt(self, tags, refine_value, coarsen_value, min_level, max_level):
+        """begin_regrid, store the tags, refine the quads tagged refine_value
+        below max_level (children keep tag 1), coarsen the complete families
+        tagged coarsen_value above min_level -- in one call
+        (amrgpu_forest_adapt)."""
+        t = np.ascontiguousarray(tags, dtype=np.int32)
+        assert len(t) == self.num_quads
+        self.version += 1
+        r = lib().amrgpu_forest_adapt(self._f, ip(t), int(refine_value), int(coarsen_value), int(min_level),
+                                      int(max_level))
+        if r < 0:
+            raise AmrGpuError(-r, "forest_adapt")
+        return r
+
     def balance(self, session=None):
         """2:1 balance; with a session, each pass runs on its GPU
         (amrgpu_forest_balance_device, same result)."""

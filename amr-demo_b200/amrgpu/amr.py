@@ -111,16 +111,17 @@ def regrid(forest, session, n, min_level, max_level, config=None, form=None, dev
     Session.regrid_forest); otherwise the host balances, lists the mesh
     arrays and the session decodes them."""
     tags = session.tag()
-    _, lev, _, _ = forest.quads()
-    forest.begin_regrid()
-    forest.set_tags(tags)
-    forest.refine(((tags > 0) & (lev < max_level)).astype(np.int32), max_level=max_level)
-    tags2 = forest.get_tags()
-    _, lev2, _, _ = forest.quads()
-    forest.coarsen(((tags2 == 0) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
     if device_mesh:
+        forest.adapt(tags, 1, 0, min_level, max_level)
         session.balance_regrid(forest)
     else:
+        _, lev, _, _ = forest.quads()
+        forest.begin_regrid()
+        forest.set_tags(tags)
+        forest.refine(((tags > 0) & (lev < max_level)).astype(np.int32), max_level=max_level)
+        tags2 = forest.get_tags()
+        _, lev2, _, _ = forest.quads()
+        forest.coarsen(((tags2 == 0) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
         forest.balance()
         kind, src = forest.remap()
         session.regrid(forest.mesh(n), kind, src)

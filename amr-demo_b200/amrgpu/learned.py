@@ -164,13 +164,7 @@ def regrid_by_classes(forest, session, n, classes, min_level, max_level):
     coarsen complete families whose children are all class 0 above
     min_level (a refined child inherits its parent's refine tag), 2:1
     balance, remap in place."""
-    _, lev, _, _ = forest.quads()
-    forest.begin_regrid()
-    forest.set_tags(classes)
-    forest.refine(((classes == REFINE) & (lev < max_level)).astype(np.int32), max_level=max_level)
-    t2 = forest.get_tags()
-    _, lev2, _, _ = forest.quads()
-    forest.coarsen(((t2 == COARSEN) & (lev2 > min_level)).astype(np.int32), min_level=min_level)
+    forest.adapt(classes, REFINE, COARSEN, min_level, max_level)
     session.balance_regrid(forest)
 
 

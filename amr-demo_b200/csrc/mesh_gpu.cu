@@ -119,66 +119,73 @@ __device__ int find_d(const ForestDev &F, int tree, int level, long long x, long
 
 __global__ void keys_kernel(ForestDev F);
 
-// One dirty leaf per thread: flags the leaves the pass refines.
+// One thread per (dirty leaf, check): checks 0-7 look at the eight face
+// and corner neighbour regions for a leaf two or more levels coarser (that
+// leaf is flagged), checks 8-11 walk the four edges leaf by leaf and 12-15
+// look at the four corners for a leaf two or more levels finer (the dirty
+// leaf itself is flagged). Splitting a leaf's checks over threads shortens
+// each thread's chain of dependent binary searches; the flags are the same.
 __global__ void balance_check_kernel(ForestDev F, const unsigned char *dirty, unsigned char *flags)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nq; i += gridDim.x * blockDim.x) {
+    const long long total = 16ll * F.nq;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = int(t >> 4), item = int(t & 15);
         if (!dirty[i]) continue;
         const int4 q = F.leaves[i];
-        // fine side: neighbour regions (faces and corners) held by a leaf
-        // two or more levels coarser
-        if (q.y >= 2) {
-            for (int dy = -1; dy <= 1; ++dy)
-                for (int dx = -1; dx <= 1; ++dx) {
-                    if (!dx && !dy) continue;
-                    KeyD k;
-                    if (!shifted_d(F, q.x, q.y, q.z, q.w, dx, dy, k)) continue;
-                    const int c = locate_d(F, k.tree, k.x, k.y);
-                    if (c >= 0 && F.leaves[c].y < q.y - 1) flags[c] = 1;
-                }
+        if (item < 8) {
+            // fine side: the neighbour region across a face or a corner
+            if (q.y < 2) continue;
+            const int d = item < 4 ? item : item + 1;  // 0..8 without the centre 4
+            const int dx = d % 3 - 1, dy = d / 3 - 1;
+            KeyD k;
+            if (!shifted_d(F, q.x, q.y, q.z, q.w, dx, dy, k)) continue;
+            const int c = locate_d(F, k.tree, k.x, k.y);
+            if (c >= 0 && F.leaves[c].y < q.y - 1) flags[c] = 1;
+            continue;
         }
-        // coarse side: a leaf two or more levels finer along an edge (walked
-        // leaf by leaf) or at a corner
-        if (q.y + 2 <= kMaxLevelG) {
-            const long long L = qlen_d(q.y);
-            const int lim = q.y + 2;
-            bool fine = false;
-            for (int s = 0; s < 4 && !fine; ++s) {
-                // a leaf of level < lim spans at least L/2 of the edge: the
-                // walk takes a few steps; the guard only bounds a malformed forest
-                int guard = 0;
-                for (long long t = 0; t < L && guard < 64; ++guard) {
-                    long long px = q.z, py = q.w;
-                    int dx = 0, dy = 0;
-                    if (s == 0) { py += t; dx = -1; }
-                    if (s == 1) { px += L - 1; py += t; dx = 1; }
-                    if (s == 2) { px += t; dy = -1; }
-                    if (s == 3) { px += t; py += L - 1; dy = 1; }
-                    KeyD k;
-                    if (!shifted_d(F, q.x, kMaxLevelG, px, py, dx, dy, k)) break;
-                    const int c = locate_d(F, k.tree, k.x, k.y);
-                    if (c < 0) break;
-                    const int4 cl = F.leaves[c];
-                    if (cl.y >= lim) {
-                        fine = true;
-                        break;
-                    }
-                    const long long len = qlen_d(cl.y);
-                    const long long adv = (s < 2) ? ((long long)cl.w + len - k.y) : ((long long)cl.z + len - k.x);
-                    if (adv <= 0) break;
-                    t += adv;
+        // coarse side
+        if (q.y + 2 > kMaxLevelG) continue;
+        const long long L = qlen_d(q.y);
+        const int lim = q.y + 2;
+        bool fine = false;
+        if (item < 12) {
+            const int s = item - 8;
+            // a leaf of level < lim spans at least L/2 of the edge: the walk
+            // takes a few steps; the guard only bounds a malformed forest
+            int guard = 0;
+            for (long long tt = 0; tt < L && guard < 64; ++guard) {
+                long long px = q.z, py = q.w;
+                int dx = 0, dy = 0;
+                if (s == 0) { py += tt; dx = -1; }
+                if (s == 1) { px += L - 1; py += tt; dx = 1; }
+                if (s == 2) { px += tt; dy = -1; }
+                if (s == 3) { px += tt; py += L - 1; dy = 1; }
+                KeyD k;
+                if (!shifted_d(F, q.x, kMaxLevelG, px, py, dx, dy, k)) break;
+                const int c = locate_d(F, k.tree, k.x, k.y);
+                if (c < 0) break;
+                const int4 cl = F.leaves[c];
+                if (cl.y >= lim) {
+                    fine = true;
+                    break;
                 }
+                const long long len = qlen_d(cl.y);
+                const long long adv = (s < 2) ? ((long long)cl.w + len - k.y) : ((long long)cl.z + len - k.x);
+                if (adv <= 0) break;
+                tt += adv;
             }
-            for (int dy = -1; dy <= 1 && !fine; dy += 2)
-                for (int dx = -1; dx <= 1 && !fine; dx += 2) {
-                    KeyD k;
-                    const long long px = dx < 0 ? q.z : q.z + L - 1, py = dy < 0 ? q.w : q.w + L - 1;
-                    if (!shifted_d(F, q.x, kMaxLevelG, px, py, dx, dy, k)) continue;
-                    const int c = locate_d(F, k.tree, k.x, k.y);
-                    if (c >= 0 && F.leaves[c].y >= lim) fine = true;
-                }
-            if (fine) flags[i] = 1;
+        } else {
+            const int cidx = item - 12;
+            const int dx = (cidx & 1) ? 1 : -1, dy = (cidx & 2) ? 1 : -1;
+            KeyD k;
+            const long long px = dx < 0 ? q.z : q.z + L - 1, py = dy < 0 ? q.w : q.w + L - 1;
+            if (shifted_d(F, q.x, kMaxLevelG, px, py, dx, dy, k)) {
+                const int c = locate_d(F, k.tree, k.x, k.y);
+                if (c >= 0 && F.leaves[c].y >= lim) fine = true;
+            }
         }
+        if (fine) flags[i] = 1;
     }
 }
 
@@ -376,7 +383,7 @@ cudaError_t launch_balance_pass(const ForestDev &F, int ntrees, int *tree_begin,
     keys_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F);
     cudaError_t e = cudaMemsetAsync(flags, 0, size_t(F.nq), st);
     if (e != cudaSuccess) return e;
-    balance_check_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F, dirty, flags);
+    balance_check_kernel<<<grid_for(16ll * F.nq, sms), 256, 0, st>>>(F, dirty, flags);
     balance_counts_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F.nq, flags, cnt);
     size_t bytes = scan_bytes;
     e = cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, cnt, pos, F.nq, st);

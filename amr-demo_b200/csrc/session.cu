@@ -512,12 +512,17 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const 
     s->ncells_total = (long long)(m->ncell + m->nghost) * s->n * s->n;
     s->stride = ((s->ncells_total + 31) / 32) * 32;
     if (s->stride == 0) s->stride = 32;
+    // state buffers hold a quarter more cells than the mesh, so that a regrid
+    // that grows the mesh a little reuses them; the AoS staging and the
+    // totals partials are sized for the same capacity
+    s->cap_stride = ((s->stride + s->stride / 4 + 31) / 32) * 32;
     bool ok = cuda_ok(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
     for (int k = 0; k < 4 && ok; ++k) {
-        ok = cuda_ok(cudaMalloc(&s->buf[k], sizeof(double) * 4 * size_t(s->stride)), "cudaMalloc state");
-        if (ok) ok = cuda_ok(cudaMemsetAsync(s->buf[k], 0, sizeof(double) * 4 * size_t(s->stride), s->stream), "memset");
+        ok = cuda_ok(cudaMalloc(&s->buf[k], sizeof(double) * 4 * size_t(s->cap_stride)), "cudaMalloc state");
+        if (ok)
+            ok = cuda_ok(cudaMemsetAsync(s->buf[k], 0, sizeof(double) * 4 * size_t(s->cap_stride), s->stream), "memset");
     }
-    if (ok) ok = cuda_ok(cudaMalloc(&s->d_aos, sizeof(double) * 4 * size_t(std::max<long long>(s->ncells_total, 1))), "cudaMalloc aos");
+    if (ok) ok = cuda_ok(cudaMalloc(&s->d_aos, sizeof(double) * 4 * size_t(s->cap_stride)), "cudaMalloc aos");
     if (ok) ok = cuda_ok(cudaMalloc(&s->d_scal, sizeof(DeviceScalars)), "cudaMalloc scalars");
     if (ok && s->nquad > 0) {
         ok = cuda_ok(cudaMalloc(&s->d_quads, sizeof(QuadDesc) * size_t(s->nquad)), "cudaMalloc quads");
@@ -526,8 +531,7 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const 
                                     cudaMemcpyHostToDevice),
                          "upload quads");
     }
-    if (ok) ok = cuda_ok(cudaMalloc(&s->d_tot, sizeof(double) * 4 * size_t(totals_grid(std::max<long long>(s->ncells_total, 1)))), "cudaMalloc totals");
-    s->cap_stride = s->stride;
+    if (ok) ok = cuda_ok(cudaMalloc(&s->d_tot, sizeof(double) * 4 * size_t(totals_grid(s->cap_stride))), "cudaMalloc totals");
     s->cap_quads = std::max(s->nquad, 1);
     s->cap_desc = s->nquad;
     s->rect = quads_are_rectangles(s);
@@ -1167,8 +1171,8 @@ int apply_regrid(amrgpu_session *s, int nq, int nface)
     return prime(s, s->primed);
 }
 
-// A device buffer of at least `need` bytes (contents not kept; grown by half
-// beyond the need so that a fluctuating mesh reallocates rarely).
+// A device buffer of at least `need` bytes (contents not kept; grown to twice
+// the need, at least 1 MB, so that a fluctuating mesh reallocates rarely).
 int ensure_dev(amrgpu_session *s, void **buf, size_t *bytes, size_t need)
 {
     if (need <= *bytes && *buf) return AMRGPU_OK;
@@ -1176,7 +1180,7 @@ int ensure_dev(amrgpu_session *s, void **buf, size_t *bytes, size_t need)
     cudaFree(*buf);
     *buf = nullptr;
     *bytes = 0;
-    const size_t want = need + need / 2;
+    const size_t want = std::max<size_t>(2 * need, size_t(1) << 20);
     if (!cuda_ok(cudaMalloc(buf, want), "cudaMalloc scratch")) return AMRGPU_ERR_CUDA;
     *bytes = want;
     return AMRGPU_OK;
@@ -1191,7 +1195,8 @@ int ensure_stage(amrgpu_session *s, size_t bytes)
     cudaFreeHost(s->h_stage);
     s->h_stage = nullptr;
     s->h_stage_bytes = 0;
-    const size_t want = bytes + bytes / 2;
+    // pinning host pages is slow: grow by 2x, at least 1 MB
+    const size_t want = std::max<size_t>(2 * bytes, size_t(1) << 20);
     if (!cuda_ok(cudaHostAlloc(&s->h_stage, want, cudaHostAllocDefault), "cudaHostAlloc staging")) return AMRGPU_ERR_CUDA;
     s->h_stage_bytes = want;
     return AMRGPU_OK;
@@ -1499,7 +1504,7 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out)
             h_tab[ntrees + t] = B.tree_ty[t];
             h_tab[2 * ntrees + t] = B.tree_at[t];
         }
-        const int cap = std::max(4 * nl, 64);
+        const int cap = std::max(nl + nl / 2, 64);  // passes that outgrow it grow it (2x)
         if (cap > s->bal_cap || ntrees != s->bal_trees) {
             rc = bal_grow(s, std::max(cap, s->bal_cap), ntrees, 0, 0);
             if (rc) return -rc;

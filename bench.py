@@ -344,13 +344,7 @@ def amr_workload(args):
         cells.append(s.mesh.ncells)
         tags = s.tag()
         c = time.perf_counter()
-        _, lev, _, _ = f.quads()
-        f.begin_regrid()
-        f.set_tags(tags)
-        f.refine(((tags > 0) & (lev < hi)).astype(np.int32), max_level=hi)
-        t2 = f.get_tags()
-        _, lev2, _, _ = f.quads()
-        f.coarsen(((t2 == 0) & (lev2 > lo)).astype(np.int32), min_level=lo)
+        f.adapt(tags, 1, 0, lo, hi)
         d = time.perf_counter()
         s.balance_regrid(f)
         h = time.perf_counter()

@@ -274,6 +274,14 @@ void amrgpu_forest_begin_regrid(amrgpu_forest_t *f);
 int amrgpu_forest_refine(amrgpu_forest_t *f, const int *flags, int max_level);
 int amrgpu_forest_coarsen(amrgpu_forest_t *f, const int *flags, int min_level);
 int amrgpu_forest_balance(amrgpu_forest_t *f);
+/* One regrid's refine and coarsen from per-quad tags in a single call (the
+ * reference's amr_regrid.c:15-81 steps without the balance): begin_regrid,
+ * tags stored on the quads, every quad tagged refine_value below
+ * max_level refined (children keep tag 1), then every complete family of
+ * quads tagged coarsen_value above min_level coarsened. Returns the quad
+ * count, or -error. */
+int amrgpu_forest_adapt(amrgpu_forest_t *f, const int *tags, int refine_value, int coarsen_value, int min_level,
+                        int max_level);
 int amrgpu_forest_is_balanced(const amrgpu_forest_t *f);
 /* For every quad after the last begin_regrid: kind 0 = copy (injection)
  * from old quad src, kind 1 = average of old quads src..src+3. */

@@ -206,3 +206,27 @@ def test_host_tag_feature_matches_restated_fortran(ag, oracle):
             rho = soln[0::4]
             expect = int((rho <= tol).any()) if meth == 1 else int((rho >= tol).any())
             assert tag.value == expect
+
+
+def test_adapt_equals_the_step_by_step_regrid(ag):
+    """Forest.adapt (begin_regrid, tags, refine, coarsen in one call) gives
+    the same leaves, tags and remap table as the separate calls."""
+    import numpy as np
+    rng = np.random.default_rng(3)
+    fa = ag.Forest(2, 1, periodic=(1, 0), level=3)
+    fb = ag.Forest(2, 1, periodic=(1, 0), level=3)
+    for rnd in range(5):
+        tags = rng.integers(0, 3, fa.num_quads).astype(np.int32)
+        _, lev, _, _ = fa.quads()
+        fa.begin_regrid()
+        fa.set_tags(tags)
+        fa.refine(((tags == 1) & (lev < 6)).astype(np.int32), max_level=6)
+        t2 = fa.get_tags()
+        _, lev2, _, _ = fa.quads()
+        fa.coarsen(((t2 == 0) & (lev2 > 1)).astype(np.int32), min_level=1)
+        nb = fb.adapt(tags, 1, 0, 1, 6)
+        assert nb == fa.num_quads == fb.num_quads
+        for u, v in zip(fa.quads() + fa.remap() + (fa.get_tags(),), fb.quads() + fb.remap() + (fb.get_tags(),)):
+            assert np.array_equal(u, v), rnd
+        fa.balance()
+        fb.balance()
