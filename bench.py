@@ -299,6 +299,45 @@ def learned_amr(args):
     return out
 
 
+def vortex_period(args):
+    """Config 2 to its end: the 1024^2 vortex (16x16 patches, level 6) run to
+    t = 10, one period, in both forms on the device (CUDA graphs of 60 steps,
+    the last step clipped at t = 10). Reports steps, wall time and rate, the
+    relative L1(rho) of each form against the exact translated vortex and
+    between the forms."""
+    import numpy as np
+    import torch
+    import amrgpu as ag
+    from amrgpu import learned as L, workloads as W
+    out = {"workload": "isentropic vortex, periodic [0,10]^2, 4096 quads x 16x16 = 1024^2 cells, SSP-RK3, "
+                       "CFL 0.5, run to t = 10 (one period)"}
+    ends = {}
+    for form, key in ((1, "fp32_flux"), (0, "plain_fp64")):
+        f, mesh, cfg, s0 = W.vortex_1024(level=args.level, n=args.patch, final_time=10.0, steps=10 ** 9)
+        s = ag.Session(mesh, cfg, form=form)
+        s.upload(s0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        steps = 0
+        while True:
+            s.step(600, graph_steps=60)
+            rep = s.sync()
+            if rep["time"] >= 10.0 or rep["error"] or rep["steps"] == steps:
+                break
+            steps = rep["steps"]
+        wall = time.perf_counter() - t0
+        q = s.download()
+        s.close()
+        ends[key] = q
+        out[key] = {"steps": rep["steps"], "time": rep["time"], "wall_s": wall,
+                    "value": mesh.ncells * rep["steps"] / wall, "unit": UNIT, "error": rep["error"],
+                    "l1_rho_vs_exact": L.l1_rho_vs_exact(mesh, q, args.patch, rep["time"], (5.0, 5.0, 5.0))}
+    a = ends["fp32_flux"].reshape(-1, 4)[:, 0]
+    b = ends["plain_fp64"].reshape(-1, 4)[:, 0]
+    out["l1_rho_rel_fp32_vs_fp64"] = float(np.abs(a - b).sum() / np.abs(b).sum())
+    return out
+
+
 def amr_workload(args):
     """One adaptive workload through the library's AMR loop (regrid every 5
     steps: GPU tagging by the density jump, host forest refine / coarsen /
@@ -637,8 +676,10 @@ def main():
                     help="regrid interval of the learned run (its model predicts the plain class that many steps ahead)")
     ap.add_argument("--learned-max-level", type=int, default=7,
                     help="finest level of the learned-indicator workload (8x8 patches; 7 = 1024^2 at the finest)")
-    ap.add_argument("--workload", choices=["vortex", "four_quadrant", "shock_bubble"], default="vortex",
-                    help="vortex: the headline line; the others time one adaptive workload")
+    ap.add_argument("--workload", choices=["vortex", "vortex_period", "four_quadrant", "shock_bubble"],
+                    default="vortex",
+                    help="vortex: the headline line; vortex_period: both forms to t = 10 with their errors; "
+                         "the others time one adaptive workload")
     ap.add_argument("--amr-form", type=int, default=1, help="form of the adaptive workloads (0 FP64, 1 FP32 flux)")
     ap.add_argument("--max-level", type=int, default=11, help="finest level of the shock-bubble workload")
     args = ap.parse_args()
@@ -646,6 +687,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "vortex_period":
+        sys.path[:0] = [ROOT, os.path.join(ROOT, "amr-demo_b200")]
+        print(json.dumps({"metric": METRIC, "vortex_period": vortex_period(args)}), flush=True)
     elif args.workload != "vortex":
         sys.path[:0] = [ROOT, os.path.join(ROOT, "amr-demo_b200")]
         print(json.dumps(amr_workload(args)), flush=True)
