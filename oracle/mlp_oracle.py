@@ -1,6 +1,6 @@
 """CPU restatement of the learned refinement indicator -- TEST INFRASTRUCTURE.
 
-Only tests/ use this module, as the checker of the GPU indicator
+Only tests/ use this module, to verify the GPU indicator
 (amr-demo_b200/csrc/mlp.cu); the product path never calls it. The indicator
 has no reference counterpart; what it stands in for is the reference's
 plain tagger (solver_tag_feature.F90:9-52), and its labels come from the

@@ -1,7 +1,7 @@
 """ctypes access to the CPU oracle -- TEST INFRASTRUCTURE.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
-this module, and only as the checker / the timed CPU baseline; the product
+this module, and only to verify GPU results / as the timed CPU baseline; the product
 path (libamrgpu) never calls it.
 
 Two libraries, both built by oracle/Makefile:
