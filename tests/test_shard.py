@@ -121,7 +121,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _gloo_rank(rank, world, port, seed, steps, outdir):
+def _gloo_rank(rank, world, port, seed, steps, outdir, scheme=3, fail_rank=-1, timeout_s=60):
     import sys
     here = os.path.dirname(os.path.abspath(__file__))
     for p in (os.path.dirname(here), os.path.join(os.path.dirname(here), "amr-demo_b200"), here):
@@ -132,9 +132,11 @@ def _gloo_rank(rank, world, port, seed, steps, outdir):
     from amrgpu import shard as S
     from shard_oracle import OracleRank as OR
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
-                            timeout=datetime.timedelta(seconds=60))
+                            timeout=datetime.timedelta(seconds=timeout_s))
     try:
-        m, cfg, s0 = build(seed)
+        if rank == fail_rank:
+            raise RuntimeError("rank failed before its first exchange")
+        m, cfg, s0 = build(seed, scheme=scheme)
         off = S.partition(m.ncell, world)
         drv = S.Distributed(OR(S.make_shard(m, off, rank), cfg))
         drv.start(drv.r.shard.local_state(s0))
@@ -146,18 +148,18 @@ def _gloo_rank(rank, world, port, seed, steps, outdir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2])
-def test_gloo_ranks_equal_unsharded(ag, oracle, tmp_path, world):
+@pytest.mark.parametrize("world,scheme", [(2, 3), (3, 4)])
+def test_gloo_ranks_equal_unsharded(ag, oracle, tmp_path, world, scheme):
     import torch.multiprocessing as mp
     seed, steps = 21, 5
-    m, cfg, s0 = build(seed)
+    m, cfg, s0 = build(seed, scheme=scheme)
     ref = s0.copy()
     oc = oracle.make_config(m.n, cfg)
     oc.time_steps = steps
     out = oracle.evolve(m, ref, oc)
     assert out["steps"] == steps
     port = _free_port()
-    mp.start_processes(_gloo_rank, args=(world, port, seed, steps, str(tmp_path)), nprocs=world,
+    mp.start_processes(_gloo_rank, args=(world, port, seed, steps, str(tmp_path), scheme), nprocs=world,
                        start_method="spawn", join=True)
     parts = [np.load(tmp_path / f"rank{r}.npz") for r in range(world)]
     got = np.concatenate([p["q"] for p in parts])
@@ -165,3 +167,20 @@ def test_gloo_ranks_equal_unsharded(ag, oracle, tmp_path, world):
     for p in parts:
         assert int(p["steps"]) == steps and float(p["time"]) == out["time"]
         assert abs(float(p["norm"]) - out["residual_norm"]) <= 1e-12 * out["residual_norm"]
+
+
+def test_a_failed_rank_ends_the_others_with_an_error(ag, tmp_path):
+    """Failure detection without a GPU: one of two gloo ranks raises before
+    its first exchange. The launcher reports the failure and ends the run
+    (the other rank, stuck in its first collective, has a 5 s process-group
+    timeout as the last bound); nothing waits for good and no result is
+    written."""
+    import time
+    import torch.multiprocessing as mp
+    port = _free_port()
+    t0 = time.perf_counter()
+    with pytest.raises(Exception):
+        mp.start_processes(_gloo_rank, args=(2, port, 21, 3, str(tmp_path), 3, 1, 5), nprocs=2,
+                           start_method="spawn", join=True)
+    assert time.perf_counter() - t0 < 120
+    assert not (tmp_path / "rank0.npz").exists()
