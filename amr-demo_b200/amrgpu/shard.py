@@ -272,9 +272,9 @@ class Distributed:
 
     ``rank_obj`` is a :class:`GpuRank` (or any object with its stage
     protocol and tensors on the process group's device). Every rank issues
-    the same collectives in the same order: per stage one grouped
-    send/recv batch with its face neighbours, per step one MIN all-reduce of
-    the CFL step image, per report two all-reduces."""
+    the same collectives in the same order: per stage one all-to-all of
+    ghost records (non-zero only between face neighbours), per step one MIN
+    all-reduce of the CFL step image, per report two all-reduces."""
 
     def __init__(self, rank_obj, group=None):
         import torch.distributed as dist
@@ -285,26 +285,33 @@ class Distributed:
         if self.nranks != rank_obj.shard.nranks:
             raise ValueError("the shard's partition and the process group differ in size")
 
-    def _ops(self):
-        """The per-stage send/recv descriptors, built once: the buffers and
-        lists do not change while the mesh does not."""
-        ops = getattr(self, "_p2p", None)
-        if ops is None:
-            r, dist = self.r, self.dist
+    def _plan(self):
+        """The per-stage exchange as one all-to-all, built once: send records
+        are grouped by destination rank and ghosts by owner, both ascending,
+        so the buffers are already in rank order; ranks that share no face
+        get zero-length slices."""
+        plan = getattr(self, "_a2a", None)
+        if plan is None:
+            r = self.r
             rec = r.shard.record
-            ops = []
-            for peer, first, count in r.shard.recv:
-                ops.append(dist.P2POp(dist.irecv, r.recvbuf[first * rec:(first + count) * rec], peer, self.group))
-            for peer, first, count in r.shard.send:
-                ops.append(dist.P2POp(dist.isend, r.sendbuf[first * rec:(first + count) * rec], peer, self.group))
-            self._p2p = ops
-        return ops
+            out_split = [0] * self.nranks
+            in_split = [0] * self.nranks
+            for peer, _, count in r.shard.send:
+                in_split[peer] = count * rec
+            for peer, _, count in r.shard.recv:
+                out_split[peer] = count * rec
+            nin, nout = sum(in_split), sum(out_split)
+            plan = (r.sendbuf[:nin], r.recvbuf[:nout], in_split, out_split)
+            self._a2a = plan
+        return plan
 
     def _exchange(self):
-        ops = self._ops()
-        if ops:
-            for w in self.dist.batch_isend_irecv(ops):
-                w.wait()
+        # a collective: every rank calls it, also one with nothing to send
+        if self.nranks < 2:
+            return
+        send, recv, in_split, out_split = self._plan()
+        self.dist.all_to_all_single(recv, send, output_split_sizes=out_split, input_split_sizes=in_split,
+                                    group=self.group)
 
     def _in_stream(self, fn):
         s = getattr(self.r, "stream", None)
