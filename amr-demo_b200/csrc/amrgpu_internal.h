@@ -31,6 +31,9 @@ void forest_destroy(Forest *f);
 int forest_num_quads(const Forest *f);
 const std::vector<Leaf> &forest_leaves(const Forest *f);
 std::vector<Leaf> &forest_leaves_mut(Forest *f);
+// Resizes the forest's leaves to n, reserving a quarter more when the
+// capacity runs out (a regrid then rarely touches freshly allocated pages).
+void forest_grow_leaves(Forest *f, size_t n);
 void forest_begin_regrid(Forest *f);
 int forest_refine(Forest *f, const int *flags, int max_level);
 int forest_coarsen(Forest *f, const int *flags, int min_level);
@@ -129,4 +132,5 @@ void tag_feature_host(const PhysicsConfig &cfg, int nfields, int n, const double
 // The C ABI's forest handle (amrgpu_forest_t of include/amrgpu.h).
 struct amrgpu_forest {
     amrgpu::Forest *f;
+    std::vector<int> flags;  // refine / coarsen flags of amrgpu_forest_adapt (capacity kept)
 };

@@ -271,6 +271,64 @@ int forest_num_quads(const Forest *f) { return int(f->leaves.size()); }
 const std::vector<Leaf> &forest_leaves(const Forest *f) { return f->leaves; }
 std::vector<Leaf> &forest_leaves_mut(Forest *f) { return f->leaves; }
 
+void forest_grow_leaves(Forest *f, size_t n)
+{
+    std::vector<Leaf> &L = f->leaves;
+    if (L.capacity() < n) L.reserve(n + n / 4);
+    L.resize(n);
+}
+
+namespace {
+
+// Replaces every leaf i with refine(i) true by its four z-ordered children,
+// in place: the output index of a leaf is never below its input index, so
+// the leaves are rewritten from the end backwards and the unchanged prefix
+// before the first refined leaf is not touched. Children take the parent's
+// fields with child_tag (or the parent's tag when child_tag < 0) and
+// dirty = 1; other leaves keep theirs, with dirty = keep_dirty (or as they
+// are when keep_dirty < 0). The leaves are written field by field: copying
+// a whole struct right after overwriting some of its fields stalls on
+// store forwarding.
+template <class Pred>
+void refine_in_place(Forest *f, Pred refine, int child_tag, int keep_dirty)
+{
+    std::vector<Leaf> &L = f->leaves;
+    const size_t n = L.size();
+    size_t nout = n, first = n;
+    for (size_t i = 0; i < n; ++i)
+        if (refine(i)) {
+            nout += 3;
+            if (first == n) first = i;
+        }
+    if (keep_dirty >= 0)
+        for (size_t i = 0; i < first; ++i) L[i].dirty = keep_dirty;
+    if (nout == n) return;
+    forest_grow_leaves(f, nout);
+    size_t k = nout;
+    for (size_t i = n; i-- > first;) {
+        const bool r = refine(i);  // reads leaf i before anything at or below k-1 >= i is written
+        const Leaf p = L[i];
+        if (r) {
+            const int64_t h = qlen(p.level + 1);
+            for (int c = 3; c >= 0; --c) {
+                Leaf &ch = L[--k];
+                ch = p;
+                ch.level = p.level + 1;
+                ch.x = p.x + (c & 1) * h;
+                ch.y = p.y + ((c >> 1) & 1) * h;
+                if (child_tag >= 0) ch.tag = child_tag;
+                ch.dirty = 1;
+            }
+        } else {
+            Leaf &d = L[--k];
+            d = p;
+            if (keep_dirty >= 0) d.dirty = keep_dirty;
+        }
+    }
+}
+
+}  // namespace
+
 void forest_begin_regrid(Forest *f)
 {
     for (size_t i = 0; i < f->leaves.size(); ++i) {
@@ -281,48 +339,33 @@ void forest_begin_regrid(Forest *f)
 
 int forest_refine(Forest *f, const int *flags, int max_level)
 {
-    std::vector<Leaf> out;
-    out.reserve(f->leaves.size() + 3 * f->leaves.size() / 4);
-    for (size_t i = 0; i < f->leaves.size(); ++i) {
-        const Leaf &p = f->leaves[i];
-        if (flags[i] && p.level < max_level && p.level < kMaxLevel) {
-            int64_t h = qlen(p.level + 1);
-            for (int c = 0; c < 4; ++c) {
-                Leaf ch = p;
-                ch.level = p.level + 1;
-                ch.x = p.x + (c & 1) * h;
-                ch.y = p.y + ((c >> 1) & 1) * h;
-                ch.tag = 1;  // children inherit the refine tag
-                ch.dirty = 1;
-                out.push_back(ch);
-            }
-        } else {
-            out.push_back(p);
-        }
-    }
-    f->leaves.swap(out);
+    const std::vector<Leaf> &L = f->leaves;
+    // children inherit the refine tag
+    refine_in_place(f, [&](size_t i) { return flags[i] && L[i].level < max_level && L[i].level < kMaxLevel; }, 1,
+                    -1);
     return int(f->leaves.size());
 }
 
 int forest_coarsen(Forest *f, const int *flags, int min_level)
 {
-    std::vector<Leaf> out;
-    out.reserve(f->leaves.size());
-    size_t i = 0, n = f->leaves.size();
+    // in place, forwards: a leaf's output index never exceeds its input
+    // index, and each family is read before its parent is written
+    std::vector<Leaf> &L = f->leaves;
+    size_t i = 0, w = 0, n = L.size();
     while (i < n) {
-        const Leaf &a = f->leaves[i];
+        const Leaf &a = L[i];
         bool family = false;
         if (a.level > 0 && a.level > min_level && i + 3 < n) {
-            int64_t L = qlen(a.level - 1);
-            int64_t px = (a.x / L) * L, py = (a.y / L) * L;
+            int64_t P = qlen(a.level - 1);
+            int64_t px = (a.x / P) * P, py = (a.y / P) * P;
             if (a.x == px && a.y == py) {
                 family = true;
                 for (int c = 0; c < 4 && family; ++c) {
-                    const Leaf &b = f->leaves[i + c];
+                    const Leaf &b = L[i + c];
                     int64_t h = qlen(a.level);
                     if (b.tree != a.tree || b.level != a.level || b.x != px + (c & 1) * h ||
                         b.y != py + ((c >> 1) & 1) * h || !flags[i + c] ||
-                        b.src_kind != kRemapCopy || b.src != f->leaves[i].src + c)
+                        b.src_kind != kRemapCopy || b.src != L[i].src + c)
                         family = false;
                 }
             }
@@ -330,23 +373,24 @@ int forest_coarsen(Forest *f, const int *flags, int min_level)
         if (family) {
             Leaf p = a;
             p.level = a.level - 1;
-            int64_t L = qlen(p.level);
-            p.x = (a.x / L) * L;
-            p.y = (a.y / L) * L;
-            p.type = f->leaves[i + 3].type;  // the reference keeps the last child's type
+            int64_t P = qlen(p.level);
+            p.x = (a.x / P) * P;
+            p.y = (a.y / P) * P;
+            p.type = L[i + 3].type;  // the reference keeps the last child's type
             p.tag = 0;
             p.src = a.src;
             p.src_kind = kRemapAverage;
             p.dirty = 1;
-            out.push_back(p);
+            L[w++] = p;
             i += 4;
         } else {
-            out.push_back(a);
+            if (w != i) L[w] = L[i];
+            ++w;
             ++i;
         }
     }
-    f->leaves.swap(out);
-    return int(f->leaves.size());
+    L.resize(w);
+    return int(L.size());
 }
 
 int forest_balance(Forest *f)
@@ -395,26 +439,7 @@ int forest_balance(Forest *f)
             return int(f->leaves.size());
         }
         // balance refinement keeps the refined quad's own tag on its children
-        std::vector<Leaf> out;
-        out.reserve(nl + 3 * nl / 8);
-        for (size_t i = 0; i < nl; ++i) {
-            const Leaf &p = f->leaves[i];
-            if (flags[i]) {
-                int64_t h = qlen(p.level + 1);
-                for (int c = 0; c < 4; ++c) {
-                    Leaf ch = p;
-                    ch.level = p.level + 1;
-                    ch.x = p.x + (c & 1) * h;
-                    ch.y = p.y + ((c >> 1) & 1) * h;
-                    ch.dirty = 1;
-                    out.push_back(ch);
-                }
-            } else {
-                out.push_back(p);
-                out.back().dirty = 0;
-            }
-        }
-        f->leaves.swap(out);
+        refine_in_place(f, [&](size_t i) { return flags[i] != 0; }, -1, 0);
     }
     return -1;
 }

@@ -688,7 +688,8 @@ int amrgpu_forest_adapt(amrgpu_forest_t *f, const int *tags, int refine_value, i
     forest_begin_regrid(f->f);
     auto &L = forest_leaves_mut(f->f);
     const size_t n0 = L.size();
-    std::vector<int> flags(n0);
+    std::vector<int> &flags = f->flags;
+    flags.resize(n0);
     for (size_t i = 0; i < n0; ++i) {
         L[i].tag = tags[i];
         flags[i] = (tags[i] == refine_value && L[i].level < max_level) ? 1 : 0;

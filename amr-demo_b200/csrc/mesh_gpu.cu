@@ -38,6 +38,8 @@
 #include <cuda_runtime.h>
 
 #include <cub/device/device_scan.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 
 #include "device_common.cuh"
 #include "mesh_gpu.h"
@@ -189,11 +191,14 @@ __global__ void balance_check_kernel(ForestDev F, const unsigned char *dirty, un
     }
 }
 
-__global__ void balance_counts_kernel(int nq, const unsigned char *flags, int *cnt)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x)
-        cnt[i] = flags[i] ? 4 : 1;
-}
+// Leaves after a balance pass per leaf: 4 if flagged for refinement, else
+// 1, and 0 past the last leaf (the scan's extra entry holds the total).
+struct BalanceCount {
+    const unsigned char *flags;
+    int nq;
+    __host__ __device__ int operator()(int i) const { return i < nq ? (flags[i] ? 4 : 1) : 0; }
+};
+using BalanceCountIt = thrust::transform_iterator<BalanceCount, thrust::counting_iterator<int>, int>;
 
 // flagged leaves -> four z-ordered children at pos[i]..pos[i]+3 (dirty),
 // others copied (clean); origin: the leaf of the pass's input it came from
@@ -219,25 +224,31 @@ __global__ void balance_refine_kernel(int nq, const int4 *in, const int *orig_in
     }
 }
 
-__global__ void tree_begin_kernel(int nq, int ntrees, const int4 *leaves, int *tb)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nq; i += gridDim.x * blockDim.x) {
-        if (i == nq) {
-            const int last = nq == 0 ? -1 : leaves[nq - 1].x;
-            for (int u = last + 1; u <= ntrees; ++u) tb[u] = nq;
-        } else {
-            const int t = leaves[i].x;
-            const int prev = i == 0 ? -1 : leaves[i - 1].x;
-            for (int u = prev + 1; u <= t; ++u) tb[u] = i;  // trees without leaves start here too
-        }
-    }
-}
-
 __global__ void keys_kernel(ForestDev F)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nq; i += gridDim.x * blockDim.x) {
         const int4 l = F.leaves[i];
         F.keys[i] = morton_d(l.z, l.w);
+    }
+}
+
+// Start of a balance pass in one launch: each leaf's Morton key, a cleared
+// refine flag and the first leaf of each tree (tb[t] = first leaf of tree t
+// or of a later tree when t has none; tb[ntrees] = nq).
+__global__ void pass_prep_kernel(ForestDev F, int ntrees, int *tb, unsigned char *flags)
+{
+    const int nq = F.nq;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nq; i += gridDim.x * blockDim.x) {
+        if (i == nq) {
+            const int last = nq == 0 ? -1 : F.leaves[nq - 1].x;
+            for (int u = last + 1; u <= ntrees; ++u) tb[u] = nq;
+        } else {
+            const int4 l = F.leaves[i];
+            F.keys[i] = morton_d(l.z, l.w);
+            flags[i] = 0;
+            const int prev = i == 0 ? -1 : F.leaves[i - 1].x;
+            for (int u = prev + 1; u <= l.x; ++u) tb[u] = i;  // trees without leaves start here too
+        }
     }
 }
 
@@ -370,23 +381,21 @@ int grid_for(long long n, int sms)
 size_t balance_scan_bytes(int nq)
 {
     size_t bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int *)nullptr, (int *)nullptr, nq > 0 ? nq : 1);
+    const BalanceCountIt it(thrust::counting_iterator<int>(0), BalanceCount{nullptr, 0});
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, it, (int *)nullptr, (nq > 0 ? nq : 1) + 1);
     return bytes;
 }
 
 cudaError_t launch_balance_pass(const ForestDev &F, int ntrees, int *tree_begin, const unsigned char *dirty,
-                                unsigned char *flags, int *cnt, int *pos, void *scan_tmp, size_t scan_bytes,
-                                int sms, cudaStream_t st)
+                                unsigned char *flags, int *pos, void *scan_tmp, size_t scan_bytes, int sms,
+                                cudaStream_t st)
 {
     if (F.nq <= 0) return cudaSuccess;
-    tree_begin_kernel<<<grid_for(F.nq + 1ll, sms), 256, 0, st>>>(F.nq, ntrees, F.leaves, tree_begin);
-    keys_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F);
-    cudaError_t e = cudaMemsetAsync(flags, 0, size_t(F.nq), st);
-    if (e != cudaSuccess) return e;
+    pass_prep_kernel<<<grid_for(F.nq + 1ll, sms), 256, 0, st>>>(F, ntrees, tree_begin, flags);
     balance_check_kernel<<<grid_for(16ll * F.nq, sms), 256, 0, st>>>(F, dirty, flags);
-    balance_counts_kernel<<<grid_for(F.nq, sms), 256, 0, st>>>(F.nq, flags, cnt);
     size_t bytes = scan_bytes;
-    e = cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, cnt, pos, F.nq, st);
+    const BalanceCountIt it(thrust::counting_iterator<int>(0), BalanceCount{flags, F.nq});
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, it, pos, F.nq + 1, st);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }

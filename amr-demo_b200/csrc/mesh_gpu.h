@@ -23,14 +23,14 @@ struct ForestDev {
     int nq;
 };
 
-// One 2:1 balance pass over F's leaves (F.keys written, F.tree_begin
-// rebuilt into tree_begin): flags[i] = 1 for leaves to refine, cnt / pos
-// the 4-or-1 counts and their exclusive scan; the new leaf count is
-// pos[nq-1] + cnt[nq-1].
+// One 2:1 balance pass over F's leaves in three launches (F.keys written,
+// F.tree_begin rebuilt into tree_begin, flags cleared; the checks; the
+// scan): flags[i] = 1 for leaves to refine, pos (nq + 1 entries) the
+// exclusive scan of the 4-or-1 counts, so pos[nq] is the new leaf count.
 size_t balance_scan_bytes(int nq);
 cudaError_t launch_balance_pass(const ForestDev &F, int ntrees, int *tree_begin, const unsigned char *dirty,
-                                unsigned char *flags, int *cnt, int *pos, void *scan_tmp, size_t scan_bytes,
-                                int sms, cudaStream_t st);
+                                unsigned char *flags, int *pos, void *scan_tmp, size_t scan_bytes, int sms,
+                                cudaStream_t st);
 // The pass's refinement: out / orig_out / dirty_out at the scanned positions.
 cudaError_t launch_balance_refine(int nq, const int4 *in, const int *orig_in, const unsigned char *flags,
                                   const int *pos, int4 *out, int *orig_out, unsigned char *dirty_out, int sms,

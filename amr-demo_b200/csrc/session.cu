@@ -1395,11 +1395,11 @@ int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f)
 namespace {
 
 // Balance buffers for cap leaves: per buffer int4 leaves, int origin,
-// uint8 dirty; work: flags (uint8), counts, positions, keys, tree begin,
-// brick tables, scan temp.
+// uint8 dirty; work: flags (uint8), positions (cap + 1: the last is the
+// total), keys, tree begin, brick tables, scan temp.
 struct BalLayout {
     size_t o_orig, o_dirty, buf;
-    size_t o_flags, o_cnt, o_pos, o_keys, o_tb, o_tx, o_ty, o_at, o_tmp, work;
+    size_t o_flags, o_pos, o_keys, o_tb, o_tx, o_ty, o_at, o_tmp, work;
     size_t scan_bytes;
 };
 
@@ -1413,9 +1413,8 @@ BalLayout bal_layout(int cap, int ntrees)
     L.buf = L.o_dirty + al(c);
     L.scan_bytes = balance_scan_bytes(int(c));
     L.o_flags = 0;
-    L.o_cnt = al(c);
-    L.o_pos = L.o_cnt + al(4 * c);
-    L.o_keys = L.o_pos + al(4 * c);
+    L.o_pos = al(c);
+    L.o_keys = L.o_pos + al(4 * (c + 1));
     L.o_tb = L.o_keys + al(8 * c);
     L.o_tx = L.o_tb + al(4 * size_t(ntrees + 1));
     L.o_ty = L.o_tx + al(4 * size_t(ntrees));
@@ -1549,25 +1548,21 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out)
         for (int k = 0; k < 4; ++k) F.bc[k] = 0;
         F.nq = nl;
         unsigned char *flags = reinterpret_cast<unsigned char *>(w + L.o_flags);
-        int *cnt = reinterpret_cast<int *>(w + L.o_cnt);
         int *pos = reinterpret_cast<int *>(w + L.o_pos);
         if (!cuda_ok(launch_balance_pass(F, ntrees, reinterpret_cast<int *>(w + L.o_tb),
-                                         reinterpret_cast<const unsigned char *>(in + L.o_dirty), flags, cnt, pos,
+                                         reinterpret_cast<const unsigned char *>(in + L.o_dirty), flags, pos,
                                          w + L.o_tmp, L.scan_bytes, s->sms, s->stream),
                      "balance pass"))
             return -AMRGPU_ERR_CUDA;
-        s->launches += 5;
-        int tail[2] = {0, 0};
+        s->launches += 4;
+        int total = 0;
         int *ht = static_cast<int *>(s->h_stage);  // staging is free: the uploads above have completed by now
         if (nl > 0) {
-            if (!cuda_ok(cudaMemcpyAsync(ht, pos + nl - 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
-                !cuda_ok(cudaMemcpyAsync(ht + 1, cnt + nl - 1, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
+            if (!cuda_ok(cudaMemcpyAsync(ht, pos + nl, sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
                 !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
                 return -AMRGPU_ERR_CUDA;
-            tail[0] = ht[0];
-            tail[1] = ht[1];
+            total = ht[0];
         }
-        const int total = nl > 0 ? tail[0] + tail[1] : 0;
         if (total == nl) {
             done = true;
             break;
@@ -1615,16 +1610,30 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out)
          !cuda_ok(cudaStreamSynchronize(s->stream), "sync")))
         return -AMRGPU_ERR_CUDA;
     if (nl != int(leaves.size())) {
-        std::vector<Leaf> out((size_t)nl);
-        for (int k = 0; k < nl; ++k) {
-            Leaf q = leaves[size_t(h_orig[k])];
-            q.level = h[4 * k + 1];
-            q.x = h[4 * k + 2];
-            q.y = h[4 * k + 3];
-            q.dirty = 0;
-            out[size_t(k)] = q;
+        // in place, from the end backwards: balance only refines, so leaf k
+        // comes from input leaf h_orig[k] <= k (non-decreasing in k), which
+        // is read before anything at or below it is overwritten; the prefix
+        // of leaves the balance left alone is not touched. Field by field:
+        // copying a whole leaf right after overwriting some of its fields
+        // stalls on store forwarding.
+        const int n0 = int(leaves.size());
+        int first = 0;
+        while (first < n0 && h_orig[first] == first && h[4 * first + 1] == leaves[size_t(first)].level)
+            leaves[size_t(first++)].dirty = 0;
+        forest_grow_leaves(fo, size_t(nl));
+        for (int k = nl - 1; k >= first; --k) {
+            const Leaf &p = leaves[size_t(h_orig[k])];
+            Leaf &d = leaves[size_t(k)];
+            d.tree = p.tree;
+            d.tag = p.tag;
+            d.type = p.type;
+            d.src = p.src;
+            d.src_kind = p.src_kind;
+            d.level = h[4 * k + 1];
+            d.x = h[4 * k + 2];
+            d.y = h[4 * k + 3];
+            d.dirty = 0;
         }
-        leaves.swap(out);
     } else {
         for (Leaf &q : leaves) q.dirty = 0;
     }

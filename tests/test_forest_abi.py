@@ -230,3 +230,76 @@ def test_adapt_equals_the_step_by_step_regrid(ag):
             assert np.array_equal(u, v), rnd
         fa.balance()
         fb.balance()
+
+
+def _py_refine(leaves, flags, max_level):
+    """Refinement as the reference's regrid does it (amr_regrid.c:239-244):
+    a flagged leaf below max_level becomes its four z-ordered children,
+    which carry the refine tag; other leaves are kept. Leaves are tuples
+    (tree, level, x, y, tag, kind, src)."""
+    out = []
+    for leaf, f in zip(leaves, flags):
+        tree, lev, x, y, tag, kind, src = leaf
+        if f and lev < max_level:
+            h = 1 << (30 - (lev + 1))
+            out += [(tree, lev + 1, x + (c & 1) * h, y + ((c >> 1) & 1) * h, 1, kind, src) for c in range(4)]
+        else:
+            out.append(leaf)
+    return out
+
+
+def _py_coarsen(leaves, flags, min_level):
+    """Coarsening of complete families (amr_tag.c:202-220): four flagged
+    siblings above min_level, untouched since the regrid began (copies of
+    consecutive old leaves), become their parent (tag 0, averaged from the
+    first sibling's source)."""
+    out, i, n = [], 0, len(leaves)
+    while i < n:
+        tree, lev, x, y, tag, kind, src = leaves[i]
+        fam = False
+        if lev > 0 and lev > min_level and i + 3 < n:
+            P, h = 1 << (30 - (lev - 1)), 1 << (30 - lev)
+            px, py = (x // P) * P, (y // P) * P
+            if (x, y) == (px, py):
+                fam = all(leaves[i + c][:4] == (tree, lev, px + (c & 1) * h, py + ((c >> 1) & 1) * h)
+                          and flags[i + c] and leaves[i + c][5] == 0 and leaves[i + c][6] == src + c
+                          for c in range(4))
+        if fam:
+            out.append((tree, lev - 1, px, py, 0, 1, src))
+            i += 4
+        else:
+            out.append(leaves[i])
+            i += 1
+    return out
+
+
+def _lib_leaves(f):
+    tree, lev, x, y = f.quads()
+    kind, src = f.remap()
+    tags = f.get_tags()
+    return [tuple(int(v) for v in t) for t in zip(tree, lev, x, y, tags, kind, src)]
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_forest_edits_match_a_list_restatement(ag, seed):
+    """The forest's refine and coarsen (rewritten in place in the leaf
+    array) give the same leaves, tags and remap table as a plain list
+    restatement, over random rounds of refine, coarsen and 2:1 balance on a
+    periodic 2x1 brick."""
+    rng = np.random.default_rng(seed)
+    f = ag.Forest(2, 1, periodic=(1, 1), level=2)
+    for rnd in range(8):
+        f.begin_regrid()
+        tags = rng.integers(0, 3, f.num_quads).astype(np.int32)
+        f.set_tags(tags)
+        ref = _lib_leaves(f)
+        flags = (rng.random(f.num_quads) < 0.3).astype(np.int32)
+        f.refine(flags, max_level=7)
+        ref = _py_refine(ref, flags, 7)
+        assert _lib_leaves(f) == ref, rnd
+        flags = (rng.random(f.num_quads) < 0.7).astype(np.int32)
+        f.coarsen(flags, min_level=1)
+        ref = _py_coarsen(ref, flags, 1)
+        assert _lib_leaves(f) == ref, rnd
+        f.balance()
+        assert f.is_balanced()
