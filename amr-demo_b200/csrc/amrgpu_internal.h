@@ -37,6 +37,11 @@ void forest_grow_leaves(Forest *f, size_t n);
 void forest_begin_regrid(Forest *f);
 int forest_refine(Forest *f, const int *flags, int max_level);
 int forest_coarsen(Forest *f, const int *flags, int min_level);
+// begin_regrid, the tags, refinement of the quads tagged refine_value below
+// max_level (children tagged 1), coarsening of complete families tagged
+// coarsen_value above min_level: forest_begin_regrid + forest_refine +
+// forest_coarsen in three passes over the leaves; returns the leaf count.
+int forest_adapt(Forest *f, const int *tags, int refine_value, int coarsen_value, int min_level, int max_level);
 int forest_balance(Forest *f);
 bool forest_is_balanced(const Forest *f);
 void forest_quad_corners(const Forest *f, const Leaf &q, double xyz[12]);
@@ -132,5 +137,4 @@ void tag_feature_host(const PhysicsConfig &cfg, int nfields, int n, const double
 // The C ABI's forest handle (amrgpu_forest_t of include/amrgpu.h).
 struct amrgpu_forest {
     amrgpu::Forest *f;
-    std::vector<int> flags;  // refine / coarsen flags of amrgpu_forest_adapt (capacity kept)
 };

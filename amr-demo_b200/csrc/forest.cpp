@@ -282,26 +282,19 @@ namespace {
 
 // Replaces every leaf i with refine(i) true by its four z-ordered children,
 // in place: the output index of a leaf is never below its input index, so
-// the leaves are rewritten from the end backwards and the unchanged prefix
-// before the first refined leaf is not touched. Children take the parent's
-// fields with child_tag (or the parent's tag when child_tag < 0) and
-// dirty = 1; other leaves keep theirs, with dirty = keep_dirty (or as they
-// are when keep_dirty < 0). The leaves are written field by field: copying
-// a whole struct right after overwriting some of its fields stalls on
-// store forwarding.
+// the leaves are rewritten from the end backwards, down to the first
+// refined leaf `first` (nout leaves in all); the prefix before it is not
+// touched. Children take the parent's fields with child_tag (or the
+// parent's tag when child_tag < 0) and dirty = 1; other leaves keep
+// theirs, with dirty = keep_dirty (or as they are when keep_dirty < 0).
+// Leaves are written field by field or whole, never copied whole right
+// after some of their fields were overwritten (that stalls on store
+// forwarding).
 template <class Pred>
-void refine_in_place(Forest *f, Pred refine, int child_tag, int keep_dirty)
+void refine_rewrite(Forest *f, size_t first, size_t nout, Pred refine, int child_tag, int keep_dirty)
 {
     std::vector<Leaf> &L = f->leaves;
     const size_t n = L.size();
-    size_t nout = n, first = n;
-    for (size_t i = 0; i < n; ++i)
-        if (refine(i)) {
-            nout += 3;
-            if (first == n) first = i;
-        }
-    if (keep_dirty >= 0)
-        for (size_t i = 0; i < first; ++i) L[i].dirty = keep_dirty;
     if (nout == n) return;
     forest_grow_leaves(f, nout);
     size_t k = nout;
@@ -327,29 +320,29 @@ void refine_in_place(Forest *f, Pred refine, int child_tag, int keep_dirty)
     }
 }
 
-}  // namespace
-
-void forest_begin_regrid(Forest *f)
+template <class Pred>
+void refine_in_place(Forest *f, Pred refine, int child_tag, int keep_dirty)
 {
-    for (size_t i = 0; i < f->leaves.size(); ++i) {
-        f->leaves[i].src = int(i);
-        f->leaves[i].src_kind = kRemapCopy;
-    }
+    std::vector<Leaf> &L = f->leaves;
+    const size_t n = L.size();
+    size_t nout = n, first = n;
+    for (size_t i = 0; i < n; ++i)
+        if (refine(i)) {
+            nout += 3;
+            if (first == n) first = i;
+        }
+    if (keep_dirty >= 0)
+        for (size_t i = 0; i < first; ++i) L[i].dirty = keep_dirty;
+    refine_rewrite(f, first, nout, refine, child_tag, keep_dirty);
 }
 
-int forest_refine(Forest *f, const int *flags, int max_level)
+// Coarsening of complete families, in place and forwards: a leaf's output
+// index never exceeds its input index, and each family (flag(i) per input
+// index i, read before anything at it is written) is read before its parent
+// is written.
+template <class Flag>
+void coarsen_in_place(Forest *f, Flag flag, int min_level)
 {
-    const std::vector<Leaf> &L = f->leaves;
-    // children inherit the refine tag
-    refine_in_place(f, [&](size_t i) { return flags[i] && L[i].level < max_level && L[i].level < kMaxLevel; }, 1,
-                    -1);
-    return int(f->leaves.size());
-}
-
-int forest_coarsen(Forest *f, const int *flags, int min_level)
-{
-    // in place, forwards: a leaf's output index never exceeds its input
-    // index, and each family is read before its parent is written
     std::vector<Leaf> &L = f->leaves;
     size_t i = 0, w = 0, n = L.size();
     while (i < n) {
@@ -364,7 +357,7 @@ int forest_coarsen(Forest *f, const int *flags, int min_level)
                     const Leaf &b = L[i + c];
                     int64_t h = qlen(a.level);
                     if (b.tree != a.tree || b.level != a.level || b.x != px + (c & 1) * h ||
-                        b.y != py + ((c >> 1) & 1) * h || !flags[i + c] ||
+                        b.y != py + ((c >> 1) & 1) * h || !flag(i + c) ||
                         b.src_kind != kRemapCopy || b.src != L[i].src + c)
                         family = false;
                 }
@@ -390,6 +383,55 @@ int forest_coarsen(Forest *f, const int *flags, int min_level)
         }
     }
     L.resize(w);
+}
+
+}  // namespace
+
+void forest_begin_regrid(Forest *f)
+{
+    for (size_t i = 0; i < f->leaves.size(); ++i) {
+        f->leaves[i].src = int(i);
+        f->leaves[i].src_kind = kRemapCopy;
+    }
+}
+
+int forest_refine(Forest *f, const int *flags, int max_level)
+{
+    const std::vector<Leaf> &L = f->leaves;
+    // children inherit the refine tag
+    refine_in_place(f, [&](size_t i) { return flags[i] && L[i].level < max_level && L[i].level < kMaxLevel; }, 1,
+                    -1);
+    return int(f->leaves.size());
+}
+
+int forest_coarsen(Forest *f, const int *flags, int min_level)
+{
+    coarsen_in_place(f, [&](size_t i) { return flags[i] != 0; }, min_level);
+    return int(f->leaves.size());
+}
+
+int forest_adapt(Forest *f, const int *tags, int refine_value, int coarsen_value, int min_level, int max_level)
+{
+    std::vector<Leaf> &L = f->leaves;
+    const size_t n = L.size();
+    auto refines = [&](size_t i) {
+        return tags[i] == refine_value && L[i].level < max_level && L[i].level < kMaxLevel;
+    };
+    // begin the regrid, store the tags and count the refinement in one pass
+    size_t nout = n, first = n;
+    for (size_t i = 0; i < n; ++i) {
+        Leaf &q = L[i];
+        q.src = int(i);
+        q.src_kind = kRemapCopy;
+        q.tag = tags[i];
+        if (refines(i)) {
+            nout += 3;
+            if (first == n) first = i;
+        }
+    }
+    refine_rewrite(f, first, nout, refines, 1, -1);  // children carry the refine tag
+    coarsen_in_place(
+        f, [&](size_t i) { return L[i].tag == coarsen_value && L[i].level > min_level; }, min_level);
     return int(L.size());
 }
 

@@ -685,20 +685,7 @@ int amrgpu_forest_adapt(amrgpu_forest_t *f, const int *tags, int refine_value, i
                         int max_level)
 {
     if (!f || !tags) return -AMRGPU_ERR_ARG;
-    forest_begin_regrid(f->f);
-    auto &L = forest_leaves_mut(f->f);
-    const size_t n0 = L.size();
-    std::vector<int> &flags = f->flags;
-    flags.resize(n0);
-    for (size_t i = 0; i < n0; ++i) {
-        L[i].tag = tags[i];
-        flags[i] = (tags[i] == refine_value && L[i].level < max_level) ? 1 : 0;
-    }
-    forest_refine(f->f, flags.data(), max_level);
-    const auto &L1 = forest_leaves(f->f);
-    flags.assign(L1.size(), 0);
-    for (size_t i = 0; i < L1.size(); ++i) flags[i] = (L1[i].tag == coarsen_value && L1[i].level > min_level) ? 1 : 0;
-    return forest_coarsen(f->f, flags.data(), min_level);
+    return forest_adapt(f->f, tags, refine_value, coarsen_value, min_level, max_level);
 }
 
 int amrgpu_forest_balance(amrgpu_forest_t *f)

@@ -224,6 +224,17 @@ __global__ void balance_refine_kernel(int nq, const int4 *in, const int *orig_in
     }
 }
 
+// Remap table of the balanced leaves: leaf k descends from pre-balance leaf
+// orig[k] and inherits its kind / source.
+__global__ void remap_gather_kernel(int n, const int *orig, const int *kind0, const int *src0, int *kind, int *src)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int o = orig[k];
+        kind[k] = kind0[o];
+        src[k] = src0[o];
+    }
+}
+
 __global__ void keys_kernel(ForestDev F)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nq; i += gridDim.x * blockDim.x) {
@@ -397,6 +408,14 @@ cudaError_t launch_balance_pass(const ForestDev &F, int ntrees, int *tree_begin,
     const BalanceCountIt it(thrust::counting_iterator<int>(0), BalanceCount{flags, F.nq});
     cudaError_t e = cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, it, pos, F.nq + 1, st);
     if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_remap_gather(int n, const int *orig, const int *kind0, const int *src0, int *kind, int *src,
+                                int sms, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    remap_gather_kernel<<<grid_for(n, sms), 256, 0, st>>>(n, orig, kind0, src0, kind, src);
     return cudaGetLastError();
 }
 

@@ -31,6 +31,10 @@ size_t balance_scan_bytes(int nq);
 cudaError_t launch_balance_pass(const ForestDev &F, int ntrees, int *tree_begin, const unsigned char *dirty,
                                 unsigned char *flags, int *pos, void *scan_tmp, size_t scan_bytes, int sms,
                                 cudaStream_t st);
+// kind[k] = kind0[orig[k]], src[k] = src0[orig[k]] for k < n: the remap
+// table of balanced leaves from that of the leaves they descend from.
+cudaError_t launch_remap_gather(int n, const int *orig, const int *kind0, const int *src0, int *kind, int *src,
+                                int sms, cudaStream_t st);
 // The pass's refinement: out / orig_out / dirty_out at the scanned positions.
 cudaError_t launch_balance_refine(int nq, const int4 *in, const int *orig_in, const unsigned char *flags,
                                   const int *pos, int4 *out, int *orig_out, unsigned char *dirty_out, int sms,

@@ -142,6 +142,8 @@ struct amrgpu_session {
     size_t fstage_bytes = 0;
     void *d_bal[2] = {nullptr, nullptr};  // balance: leaves / origin / dirty, double-buffered
     void *d_bal_work = nullptr;           // balance: flags, counts, positions, keys, trees, scan temp
+    void *d_remap0 = nullptr;             // balance + regrid: remap kind / source of the pre-balance leaves
+    size_t remap0_bytes = 0;
     int bal_cap = 0;                      // leaves the balance buffers hold
     int bal_trees = 0;                    // trees the balance work area holds tables for
     bool rect = true;                 // every quad an axis-aligned rectangle
@@ -581,6 +583,7 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_fstage);
     cudaFree(s->d_bal[0]);
     cudaFree(s->d_bal[1]);
+    cudaFree(s->d_remap0);
     cudaFree(s->d_bal_work);
     cudaFreeHost(s->h_stage);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1073,7 +1076,7 @@ namespace {
 int ensure_quad_arrays(amrgpu_session *s, int nq)
 {
     if (nq <= s->cap_quads) return AMRGPU_OK;
-    const int cap = nq + nq / 2;
+    const int cap = 2 * nq;
     int *arr[3] = {nullptr, nullptr, nullptr};
     bool ok = true;
     for (int k = 0; k < 3 && ok; ++k) ok = cuda_ok(cudaMalloc(&arr[k], sizeof(int) * size_t(cap)), "cudaMalloc quad arrays");
@@ -1096,7 +1099,7 @@ int ensure_quad_arrays(amrgpu_session *s, int nq)
 int ensure_desc(amrgpu_session *s, QuadDesc **buf, int *cap, int nq)
 {
     if (nq <= *cap && *buf) return AMRGPU_OK;
-    const int c = std::max(nq + nq / 2, 1);
+    const int c = std::max(2 * nq, 1);
     QuadDesc *d = nullptr;
     if (!cuda_ok(cudaMalloc(&d, sizeof(QuadDesc) * size_t(c)), "cudaMalloc quads")) return AMRGPU_ERR_CUDA;
     cudaStreamSynchronize(s->stream);
@@ -1119,7 +1122,10 @@ int apply_regrid(amrgpu_session *s, int nq, int nface)
     long long cap = s->cap_stride;
     bool ok = true;
     if (stride > s->cap_stride) {
-        cap = ((stride + stride / 2 + 31) / 32) * 32;
+        // twice the need: large device allocations and frees cost
+        // milliseconds each (tens on some hosts), so an adaptive run that
+        // keeps growing should meet them rarely
+        cap = ((2 * stride + 31) / 32) * 32;
         for (int k = 0; k < 4 && ok; ++k)
             ok = cuda_ok(cudaMalloc(&fresh[k], sizeof(double) * 4 * size_t(cap)), "cudaMalloc state");
         double *aos = nullptr;
@@ -1472,22 +1478,33 @@ int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
 // 2:1 balance of forest fo with every pass on the session's GPU; the
 // balanced leaves stay in d_bal[*live_out] (with the last pass's keys and
 // tree starts in the work area) and are copied back into the host forest.
+// With remap, the remap table of the balanced leaves (kind / source of the
+// pre-balance leaf each one descends from, validated against the session's
+// current quad count) is gathered into d_kind / d_src on the device.
 // Returns the leaf count or -error.
-int balance_impl(amrgpu_session *s, Forest *fo, int *live_out)
+int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
 {
     std::vector<Leaf> &leaves = forest_leaves_mut(fo);
     BrickView B;
     forest_brick(fo, &B);
     const int ntrees = B.nx * B.ny;
     int nl = int(leaves.size());
-    // staging: leaves (int4), origin, dirty bytes, brick tables
-    size_t sb = 16 * size_t(nl) + 4 * size_t(nl) + size_t(nl) + 12 * size_t(ntrees) + 64;
+    // staging: leaves (int4), origin, remap kind / source (with remap),
+    // dirty bytes, brick tables
+    const size_t nrm = remap ? 2 * size_t(nl) : 0;
+    size_t sb = 16 * size_t(nl) + 4 * size_t(nl) + 4 * nrm + size_t(nl) + 12 * size_t(ntrees) + 64;
     int rc = ensure_stage(s, sb);
     if (rc) return -rc;
+    if (remap) {
+        rc = ensure_dev(s, &s->d_remap0, &s->remap0_bytes, 4 * nrm + 16);
+        if (rc) return -rc;
+    }
     {
         int *h = static_cast<int *>(s->h_stage);
         int *h_orig = h + 4 * size_t(nl);
-        unsigned char *h_dirty = reinterpret_cast<unsigned char *>(h_orig + nl);
+        int *h_rm = h_orig + nl;  // kind[nl], source[nl]
+        unsigned char *h_dirty = reinterpret_cast<unsigned char *>(h_rm + nrm);
+        bool bad = false;
         for (int i = 0; i < nl; ++i) {
             const Leaf &q = leaves[size_t(i)];
             h[4 * i + 0] = q.tree;
@@ -1496,6 +1513,18 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out)
             h[4 * i + 3] = int(q.y);
             h_orig[i] = i;
             h_dirty[i] = q.dirty ? 1 : 0;
+            if (remap) {
+                // balance children inherit these, so the pre-balance range
+                // check covers the balanced table
+                const int lim = q.src_kind == 0 ? s->nquad - 1 : s->nquad - 4;
+                bad |= (q.src_kind != 0 && q.src_kind != 1) || q.src < 0 || q.src > lim;
+                h_rm[i] = q.src_kind;
+                h_rm[nl + i] = q.src;
+            }
+        }
+        if (bad) {
+            set_error(AMRGPU_ERR_ARG, "remap kind or source index out of range");
+            return -AMRGPU_ERR_ARG;
         }
         int *h_tab = reinterpret_cast<int *>(h_dirty + ((size_t(nl) + 15) & ~size_t(15)));
         for (int t = 0; t < ntrees; ++t) {
@@ -1524,6 +1553,8 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out)
                   cuda_ok(cudaMemcpyAsync(w + L.o_at, h_tab + 2 * ntrees, 4 * size_t(ntrees), cudaMemcpyHostToDevice,
                                           s->stream),
                           "H2D balance");
+        if (ok && remap && nl > 0)
+            ok = cuda_ok(cudaMemcpyAsync(s->d_remap0, h_rm, 4 * nrm, cudaMemcpyHostToDevice, s->stream), "H2D remap");
         if (!ok) return -AMRGPU_ERR_CUDA;
     }
     int live = 0;
@@ -1592,6 +1623,18 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out)
         return -AMRGPU_ERR_MESH;
     }
     *live_out = live;
+    if (remap && nl > 0) {
+        rc = ensure_quad_arrays(s, nl);
+        if (rc) return -rc;
+        const BalLayout L = bal_layout(s->bal_cap, ntrees);
+        const int *rm = static_cast<const int *>(s->d_remap0);
+        const int n0 = int(leaves.size());
+        if (!cuda_ok(launch_remap_gather(nl, reinterpret_cast<const int *>(static_cast<char *>(s->d_bal[live]) + L.o_orig),
+                                         rm, rm + n0, s->d_kind, s->d_src, s->sms, s->stream),
+                     "remap gather"))
+            return -AMRGPU_ERR_CUDA;
+        s->launches++;
+    }
     if (!refined) {
         for (Leaf &q : leaves) q.dirty = 0;
         return nl;
@@ -1648,7 +1691,7 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
 {
     if (!f || !f->f || !s) return -AMRGPU_ERR_ARG;
     int live = 0;
-    return balance_impl(s, f->f, &live);
+    return balance_impl(s, f->f, &live, false);
 }
 
 int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f)
@@ -1663,28 +1706,11 @@ int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f)
         return AMRGPU_ERR_UNSUPPORTED;
     }
     int live = 0;
-    const int nq = balance_impl(s, f->f, &live);
+    const int nq = balance_impl(s, f->f, &live, true);  // remap table into d_kind / d_src
     if (nq < 0) return -nq;
-    // remap table of the balanced leaves (host forest now holds them)
-    const std::vector<Leaf> &L = forest_leaves(f->f);
     BrickView B;
     forest_brick(f->f, &B);
     const int ntrees = B.nx * B.ny;
-    int rc = ensure_stage(s, 8 * size_t(nq) + 64);
-    if (rc) return rc;
-    int *h_kind = static_cast<int *>(s->h_stage) + 16, *h_src = h_kind + nq;  // ints 0..15: status
-    for (int i = 0; i < nq; ++i) {
-        h_kind[i] = L[size_t(i)].src_kind;
-        h_src[i] = L[size_t(i)].src;
-    }
-    if (!check_remap(s, nq, h_kind, h_src)) return AMRGPU_ERR_ARG;
-    rc = ensure_quad_arrays(s, nq);
-    if (rc) return rc;
-    if (!cuda_ok(cudaMemcpyAsync(s->d_kind, h_kind, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, s->stream),
-                 "H2D remap") ||
-        !cuda_ok(cudaMemcpyAsync(s->d_src, h_src, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, s->stream),
-                 "H2D remap"))
-        return AMRGPU_ERR_CUDA;
     // the descriptors straight from the balanced leaves on the device
     const BalLayout BL = bal_layout(s->bal_cap, ntrees);
     char *in = static_cast<char *>(s->d_bal[live]);
