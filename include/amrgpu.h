@@ -306,7 +306,7 @@ int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int
 /* In-place regrid: the session takes the new mesh m (no ghost quads) and
  * its state is remapped by kind/src (amrgpu_forest_remap) into the spare
  * state buffer; device arrays are reused while they are large enough and
- * grow by a quarter beyond the need otherwise. Simulated time and the step
+ * grow to twice the need otherwise. Simulated time and the step
  * counter carry over on the device; the first step's CFL minimum is folded
  * for the new mesh. Replaces the per-regrid rebuild of the reference's
  * amr_regrid.c:82-125 (new ghost layer, new face lists, new soln array). */
@@ -325,7 +325,10 @@ int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f);
 int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s);
 /* amrgpu_forest_balance_device then amrgpu_session_regrid_forest, with the
  * descriptors built from the balanced leaves already on the device (one
- * upload of the forest per regrid instead of two). */
+ * upload of the forest per regrid instead of two) and the remap table of
+ * the balanced leaves gathered there from the pre-balance leaves they
+ * descend from (no remap table built or uploaded by the host after the
+ * balance). */
 int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f);
 /* Copies up to cap quad descriptors (160 bytes each: 4 sides x {kind, nbr0,
  * nbr1, face rank, level, bc} ints, then 8 corner doubles) to host memory;
