@@ -103,6 +103,9 @@ struct Forest {
     std::vector<int> tree_tx, tree_ty;
     std::vector<int> tree_at;  // [ty*nx+tx] -> tree id
     std::vector<Leaf> leaves;
+    // output buffer of forest_adapt's single pass, swapped with `leaves`
+    // afterwards; its capacity is kept from regrid to regrid
+    std::vector<Leaf> spare;
 
     int tree_of(int tx, int ty) const { return tree_at[size_t(ty) * nx + tx]; }
 
@@ -412,26 +415,77 @@ int forest_coarsen(Forest *f, const int *flags, int min_level)
 
 int forest_adapt(Forest *f, const int *tags, int refine_value, int coarsen_value, int min_level, int max_level)
 {
+    // One pass over the leaves into the spare buffer, equal to begin_regrid,
+    // storing the tags, forest_refine and then forest_coarsen: the children
+    // of a refined leaf all carry their parent's source index, so they never
+    // form a coarsenable family, and a family is four consecutive unrefined
+    // leaves (siblings, all tagged coarsen_value above min_level).
     std::vector<Leaf> &L = f->leaves;
+    std::vector<Leaf> &out = f->spare;
     const size_t n = L.size();
     auto refines = [&](size_t i) {
         return tags[i] == refine_value && L[i].level < max_level && L[i].level < kMaxLevel;
     };
-    // begin the regrid, store the tags and count the refinement in one pass
-    size_t nout = n, first = n;
-    for (size_t i = 0; i < n; ++i) {
-        Leaf &q = L[i];
-        q.src = int(i);
-        q.src_kind = kRemapCopy;
-        q.tag = tags[i];
+    auto coarsens = [&](size_t i) { return tags[i] == coarsen_value && L[i].level > min_level; };
+    size_t nref = 0;
+    for (size_t i = 0; i < n; ++i) nref += refines(i) ? 1 : 0;
+    if (out.capacity() < n + 3 * nref) out.reserve(std::max(n + 3 * nref + (n + 3 * nref) / 4, L.capacity()));
+    out.resize(n + 3 * nref);
+    size_t w = 0, i = 0;
+    while (i < n) {
+        const Leaf &a = L[i];
         if (refines(i)) {
-            nout += 3;
-            if (first == n) first = i;
+            const int64_t h = qlen(a.level + 1);
+            for (int c = 0; c < 4; ++c) {
+                Leaf &ch = out[w++];
+                ch = a;
+                ch.level = a.level + 1;
+                ch.x = a.x + (c & 1) * h;
+                ch.y = a.y + ((c >> 1) & 1) * h;
+                ch.tag = 1;  // children carry the refine tag
+                ch.src = int(i);
+                ch.src_kind = kRemapCopy;
+                ch.dirty = 1;
+            }
+            ++i;
+            continue;
+        }
+        bool family = false;
+        int64_t px = 0, py = 0;
+        if (a.level > 0 && a.level > min_level && i + 3 < n) {
+            const int64_t P = qlen(a.level - 1), h = qlen(a.level);
+            px = (a.x / P) * P;
+            py = (a.y / P) * P;
+            if (a.x == px && a.y == py) {
+                family = true;
+                for (int c = 0; c < 4 && family; ++c) {
+                    const Leaf &b = L[i + c];
+                    if (b.tree != a.tree || b.level != a.level || b.x != px + (c & 1) * h ||
+                        b.y != py + ((c >> 1) & 1) * h || refines(i + c) || !coarsens(i + c))
+                        family = false;
+                }
+            }
+        }
+        Leaf &d = out[w++];
+        d = a;
+        d.src = int(i);
+        if (family) {
+            d.level = a.level - 1;
+            d.x = px;
+            d.y = py;
+            d.type = L[i + 3].type;  // the reference keeps the last child's type
+            d.tag = 0;
+            d.src_kind = kRemapAverage;
+            d.dirty = 1;
+            i += 4;
+        } else {
+            d.tag = tags[i];
+            d.src_kind = kRemapCopy;
+            ++i;
         }
     }
-    refine_rewrite(f, first, nout, refines, 1, -1);  // children carry the refine tag
-    coarsen_in_place(
-        f, [&](size_t i) { return L[i].tag == coarsen_value && L[i].level > min_level; }, min_level);
+    out.resize(w);
+    L.swap(out);
     return int(L.size());
 }
 
