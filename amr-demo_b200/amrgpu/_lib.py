@@ -77,6 +77,7 @@ PROTOTYPES = {
     "physics_go_gpu": (None, [i32p] * 15 + [f64p] * 2 + [i32p] * 5 + [C.c_ssize_t] + [f64p] * 3),
     # Part 2: errors and configuration
     "amrgpu_last_error": (C.c_int, []),
+    "amrgpu_evolve_config": (C.c_int, [C.c_int, C.POINTER(ConfigStruct)]),
     "amrgpu_error_string": (C.c_char_p, [C.c_int]),
     "amrgpu_last_error_message": (C.c_char_p, []),
     "amrgpu_clear_error": (None, []),

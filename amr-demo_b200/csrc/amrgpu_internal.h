@@ -102,7 +102,12 @@ struct PhysicsConfig {
 };
 
 PhysicsConfig &global_config();
+// True once hpc_amr_initialize_solver read input.physics or
+// amrgpu_config_set was called; evolve refuses to run on bare defaults.
+bool config_initialized();
+void set_config_initialized(bool v);
 int parse_physics_file(const char *path, PhysicsConfig &cfg);
+void config_to_public(const PhysicsConfig &c, amrgpu_config_t *o);
 
 // ---------------------------------------------------------------- errors
 void set_error(int code, const std::string &msg);

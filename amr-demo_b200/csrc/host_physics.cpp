@@ -34,6 +34,12 @@ PhysicsConfig &global_config()
     return cfg;
 }
 
+// Set once the library's configuration came from a successful
+// hpc_amr_initialize_solver (input.physics read) or amrgpu_config_set.
+static bool g_configured = false;
+bool config_initialized() { return g_configured; }
+void set_config_initialized(bool v) { g_configured = v; }
+
 // physics_utilities.c: a line containing the keyword is parsed from
 // offset strlen(keyword) of the line (not from the match position).
 static bool find_line(const char *path, const char *kw, std::string &rest)
@@ -514,6 +520,7 @@ int amrgpu_config_set(const amrgpu_config_t *cfg)
 {
     if (!cfg) return AMRGPU_ERR_ARG;
     from_public(cfg, global_config());
+    set_config_initialized(true);
     return AMRGPU_OK;
 }
 
@@ -545,8 +552,13 @@ void hpc_amr_initialize_solver(int *rank, int *dim, double *mesh_scale, int *nle
     }
     int rc = parse_physics_file("input.physics", c);
     if (rc != AMRGPU_OK) {
+        // the reference exits here (physics_initialize.c); this library
+        // stays loaded but refuses to evolve until it is configured
         if (*rank == 0) std::printf("[physics] The physics input file does not exist!\n");
-        set_error(rc, "input.physics not found; defaults kept");
+        set_error(rc, "input.physics not found; the library is not configured");
+        set_config_initialized(false);
+    } else {
+        set_config_initialized(true);
     }
 }
 
@@ -746,3 +758,7 @@ int amrgpu_forest_initialize(const amrgpu_forest_t *f, int nelem_subgrid, double
 }
 
 }  // extern "C"
+
+namespace amrgpu {
+void config_to_public(const PhysicsConfig &c, amrgpu_config_t *o) { to_public(c, o); }
+}  // namespace amrgpu

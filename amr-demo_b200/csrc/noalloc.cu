@@ -17,6 +17,7 @@
 // or different host threads on one device) race on it.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 
 #include "amrgpu_internal.h"
@@ -26,9 +27,10 @@ namespace amrgpu {
 
 static __device__ __align__(256) double g_totals_scratch[(AMRGPU_NOALLOC_MAX_QUADS + 1) * 4];
 
-// device address of g_totals_scratch per device, found once per device
-static double *g_scratch_addr[64];
-static bool g_scratch_ready[64];
+// device address of g_totals_scratch per device, found once per device;
+// atomic so that two host threads making their first call on one device at
+// the same time both publish (the same) address without a data race
+static std::atomic<double *> g_scratch_addr[64];
 
 // one block per quad group: sum of vol * Q_f over each quad's cells, in
 // cell order, written to the quad's own scratch slot
@@ -96,23 +98,28 @@ extern "C" int amrgpu_totals_noalloc(const double *q_device, long long field_str
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    if (e != cudaSuccess) {
         set_error(AMRGPU_ERR_CUDA, std::string("totals_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
         return AMRGPU_ERR_CUDA;
     }
+    if (dev < 0 || dev >= 64) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "totals_noalloc: device index " + std::to_string(dev) +
+                                              " is outside the 64 devices this entry point tracks");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
     // set-up, once per device, with that device current: the host-side name
     // g_totals_scratch is only a stand-in, the kernels need the device address
-    if (!g_scratch_ready[dev]) {
+    double *scratch = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!scratch) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_totals_scratch);
         if (e != cudaSuccess || !p) {
             set_error(AMRGPU_ERR_CUDA, std::string("totals_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             return AMRGPU_ERR_CUDA;
         }
-        g_scratch_addr[dev] = static_cast<double *>(p);
-        g_scratch_ready[dev] = true;
+        scratch = static_cast<double *>(p);
+        g_scratch_addr[dev].store(scratch, std::memory_order_release);
     }
-    double *scratch = g_scratch_addr[dev];
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (nquad > 0) {
         const int per_block = 4;  // warps (quads) per 128-thread block

@@ -82,37 +82,6 @@ uint64_t fnv1a(const void *p, size_t bytes, uint64_t h = 1469598103934665603ULL)
     return h;
 }
 
-// Hash of a large array (the mesh arrays the reference passes on every
-// evolve call): 8-byte words into four independent multiply-xorshift lanes,
-// so that a call hashes ~1 MB in tens of microseconds instead of the byte
-// loop's milliseconds. Only used to notice that the mesh changed.
-uint64_t hash_words(const void *p, size_t bytes, uint64_t seed)
-{
-    const unsigned char *b = static_cast<const unsigned char *>(p);
-    const uint64_t k = 0x9E3779B97F4A7C15ULL;
-    uint64_t h[4] = {seed ^ 0x243F6A8885A308D3ULL, seed ^ 0x13198A2E03707344ULL, seed ^ 0xA4093822299F31D0ULL,
-                     seed ^ 0x082EFA98EC4E6C89ULL};
-    size_t nw = bytes / 8, i = 0;
-    for (; i + 4 <= nw; i += 4)
-        for (int l = 0; l < 4; ++l) {
-            uint64_t w;
-            std::memcpy(&w, b + 8 * (i + size_t(l)), 8);
-            h[l] = (h[l] ^ w) * k;
-            h[l] ^= h[l] >> 29;
-        }
-    for (; i < nw; ++i) {
-        uint64_t w;
-        std::memcpy(&w, b + 8 * i, 8);
-        h[0] = ((h[0] ^ w) * k) ^ (h[0] >> 31);
-    }
-    uint64_t t = 0;
-    std::memcpy(&t, b + 8 * nw, bytes - 8 * nw);
-    h[1] = ((h[1] ^ t ^ (uint64_t)bytes) * k);
-    uint64_t r = h[0];
-    for (int l = 1; l < 4; ++l) r = ((r ^ (h[l] + (r << 6) + (r >> 2))) * k) ^ (r >> 33);
-    return r;
-}
-
 }  // namespace
 
 struct amrgpu_session {
@@ -462,9 +431,22 @@ int enqueue_step(amrgpu_session *s)
 
 }  // namespace
 
+int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const PhysicsConfig &c);
+
 extern "C" {
 
 int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const amrgpu_config_t *cfg)
+{
+    if (cfg) amrgpu_config_set(cfg);  // keeps global and session in step
+    return session_create_cfg(out, m, global_config());
+}
+
+}  // extern "C"
+
+// A session on mesh m with configuration c (the public create passes the
+// library's global configuration; the evolve entry points pass the one
+// they resolved).
+int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const PhysicsConfig &c)
 {
     if (!out || !m || !m->cell_info || !m->geom || (m->nface > 0 && !m->face_info) || m->ncell < 0 ||
         m->nghost < 0) {
@@ -478,10 +460,7 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const 
         return AMRGPU_ERR_NO_DEVICE;
     }
     amrgpu_session *s = new amrgpu_session;
-    if (cfg) {
-        amrgpu_config_set(cfg);  // keeps global and session in step
-    }
-    s->cfg = global_config();
+    s->cfg = c;
     s->n = s->cfg.nelem_subgrid;
     s->form = s->cfg.form;
     if (s->cfg.dim != 2 || s->cfg.nfields != 4) {
@@ -561,6 +540,8 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *m, const 
     *out = s;
     return AMRGPU_OK;
 }
+
+extern "C" {
 
 void amrgpu_session_destroy(amrgpu_session_t *s)
 {
@@ -1746,13 +1727,126 @@ int amrgpu_session_face_count(const amrgpu_session_t *s) { return s ? s->nface :
 // ======================================================================
 // The reference's evolve entry points
 // ======================================================================
+// The reference's configuration globals (physics_var_interface.h:20-39,
+// physics_var_physics.h:21-49, physics_var_simulation.h:20-37), declared
+// weak: when the reference's physics layer is built with -D_GPU_ and linked
+// against this library, they resolve to its definitions (filled by its own
+// hpc_amr_initialize_solver -> physics_initialize); otherwise they stay
+// unresolved (null address). Layouts are the reference's, field for field.
+extern "C" {
+struct RefPhysicsInterface {
+    int dim, nfringe, nfields, nelem_subgrid;
+    int extern_cell_size, extern_face_size, extern_edge_size, extern_node_size, extern_mpi_comm_size;
+    int nlevels;
+    double coarse_grid_h;
+};
+struct RefPhysicsFluid {
+    int initial_condition;
+    int bc[6];
+    int amr_ntag_methods;
+    int *amr_tag_methods;
+    double *amr_tag_tolerances;
+    double cfl, mach, alpha, beta, gamma, density, pressure;
+};
+struct RefPhysicsSimulation {
+    int checkpoint_interval, visualization_interval, regrid_interval;
+    int time_scheme, time_steps;
+    double dt;
+};
+extern RefPhysicsInterface d_physics_interface __attribute__((weak));
+extern RefPhysicsFluid d_physics_fluid __attribute__((weak));
+extern RefPhysicsSimulation d_physics_simulation __attribute__((weak));
+}
+static_assert(sizeof(RefPhysicsInterface) == 48, "physics_interface_t layout");
+static_assert(sizeof(RefPhysicsFluid) == 104, "physics_fluid_t layout");
+static_assert(sizeof(RefPhysicsSimulation) == 32, "physics_simulation_t layout");
+
 namespace {
+
+// The reference's physics layer is in this process and its
+// physics_initialize has run (it stores nfields from the driver, > 0).
+bool reference_config_present()
+{
+    return &d_physics_interface != nullptr && &d_physics_fluid != nullptr && &d_physics_simulation != nullptr &&
+           d_physics_interface.nfields > 0;
+}
+
+// PhysicsConfig from the reference's globals; the extensions this library
+// adds (form, final time, NaN abort, IC parameters) come from its own
+// configuration.
+PhysicsConfig config_from_reference()
+{
+    PhysicsConfig c = global_config();
+    const RefPhysicsInterface &I = d_physics_interface;
+    const RefPhysicsFluid &F = d_physics_fluid;
+    const RefPhysicsSimulation &S = d_physics_simulation;
+    c.dim = I.dim;
+    c.nfringe = I.nfringe;
+    c.nfields = I.nfields;
+    c.nelem_subgrid = I.nelem_subgrid;
+    c.extern_cell_size = I.extern_cell_size;
+    c.extern_face_size = I.extern_face_size;
+    c.extern_mpi_comm_size = I.extern_mpi_comm_size;
+    c.nlevels = I.nlevels;
+    c.coarse_grid_h = I.coarse_grid_h;
+    c.initial_condition = F.initial_condition;
+    for (int k = 0; k < 6; ++k) c.bc[k] = F.bc[k];
+    c.amr_ntag_methods = F.amr_ntag_methods;
+    c.amr_tag_methods.clear();
+    c.amr_tag_tolerances.clear();
+    for (int k = 0; k < F.amr_ntag_methods && F.amr_tag_methods && F.amr_tag_tolerances; ++k) {
+        c.amr_tag_methods.push_back(F.amr_tag_methods[k]);
+        c.amr_tag_tolerances.push_back(F.amr_tag_tolerances[k]);
+    }
+    c.cfl = F.cfl;  // already 0.25*cfl*time_scheme (physics_initialize.c)
+    c.mach = F.mach;
+    c.alpha = F.alpha;
+    c.beta = F.beta;
+    c.gamma = F.gamma;
+    c.density = F.density;
+    c.pressure = F.pressure;
+    auto interval = [](int v) { return v > 0 ? v : 2147483647; };
+    c.checkpoint_interval = interval(S.checkpoint_interval);
+    c.visualization_interval = interval(S.visualization_interval);
+    c.regrid_interval = interval(S.regrid_interval);
+    c.time_scheme = S.time_scheme;
+    c.time_steps = S.time_steps;
+    c.dt = S.dt;
+    return c;
+}
+
+// The configuration an evolve call runs with. physics_go_gpu is called by
+// the reference's physics layer (physics_evolve_interface.c:42-46), so the
+// reference's globals come first there; hpc_amr_evolve_solver replaces that
+// layer, so this library's own configuration comes first. Either falls back
+// to the other; with neither initialised the call is refused.
+bool resolve_config(bool from_reference_layer, PhysicsConfig &out)
+{
+    const bool ref = reference_config_present();
+    const bool own = config_initialized();
+    if (from_reference_layer ? ref : (ref && !own)) {
+        out = config_from_reference();
+        return true;
+    }
+    if (own) {
+        out = global_config();
+        return true;
+    }
+    set_error(AMRGPU_ERR_CONFIG,
+              "no configuration: neither this library's hpc_amr_initialize_solver / amrgpu_config_set nor the "
+              "reference's physics_initialize has run");
+    return false;
+}
 
 struct EvolveCache {
     amrgpu_session *s = nullptr;
-    uint64_t mesh_hash = 0;
+    // the mesh the session was built from, kept to compare byte for byte
+    std::vector<int> cell_info, face_info;
+    std::vector<double> geom;
+    int ncell = -1, nghost = -1, nface = -1, dof = -1;
     uint64_t cfg_hash = 0;
     double sim_time = 0.0;
+    int end_istep = -1;  // *istep at the end of the last call
 };
 
 EvolveCache &cache()
@@ -1776,13 +1870,30 @@ uint64_t cfg_hash(const PhysicsConfig &c)
     return h;
 }
 
-void evolve(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *ncell, int *nghost, int *nface,
-            int *dof, int *cell_info, int *face_info, int *nsend, int *nrecv, int *sizes, double *geom, double *soln,
-            int *istep, int *regrid, int *visualize, int *checkpoint, int *evolve_solution, double *total_time,
-            double *compute_time, double *residual_time)
+// True when (cell_info, face_info, geom) and the counts equal the cached
+// mesh's, compared byte for byte (a hash alone could collide and reuse the
+// wrong quad descriptors).
+bool same_mesh(const EvolveCache &ec, int ncell, int nghost, int nface, int dof, const int *cell_info,
+               const int *face_info, const double *geom)
+{
+    if (!ec.s || ec.ncell != ncell || ec.nghost != nghost || ec.nface != nface || ec.dof != dof) return false;
+    const size_t nc = size_t(ncell + nghost);
+    return std::memcmp(ec.cell_info.data(), cell_info, sizeof(int) * 3 * nc) == 0 &&
+           std::memcmp(ec.face_info.data(), face_info, sizeof(int) * 11 * size_t(nface)) == 0 &&
+           std::memcmp(ec.geom.data(), geom, sizeof(double) * 12 * nc) == 0;
+}
+
+void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *ncell,
+            int *nghost, int *nface, int *dof, int *cell_info, int *face_info, int *nsend, int *nrecv, int *sizes,
+            double *geom, double *soln, int *istep, int *regrid, int *visualize, int *checkpoint,
+            int *evolve_solution, double *total_time, double *compute_time, double *residual_time)
 {
     (void)sizes;
-    PhysicsConfig &c = global_config();
+    PhysicsConfig c;
+    if (!resolve_config(from_reference_layer, c)) {
+        *evolve_solution = 0;
+        return;
+    }
     // physics_go.c:66-69
     if (*istep >= c.time_steps) {
         *evolve_solution = 0;
@@ -1805,22 +1916,31 @@ void evolve(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *
 
     auto wall0 = std::chrono::steady_clock::now();
     EvolveCache &ec = cache();
-    uint64_t mh = hash_words(cell_info, sizeof(int) * 3 * size_t(*ncell + *nghost), 1469598103934665603ULL);
-    mh = hash_words(face_info, sizeof(int) * 11 * size_t(*nface), mh);
-    mh = hash_words(geom, sizeof(double) * 12 * size_t(*ncell + *nghost), mh);
-    mh = hash_words(ncell, sizeof(int), mh);
-    uint64_t ch = cfg_hash(c);
-    if (!ec.s || ec.mesh_hash != mh || ec.cfg_hash != ch) {
+    const uint64_t ch = cfg_hash(c);
+    // simulated time (for the final-time stop) continues only when this call
+    // picks up where the last one ended: same configuration, *istep equal
+    // to the istep the last call returned, and not a fresh start at 0
+    const bool continuing = ec.s && ec.cfg_hash == ch && *istep > 0 && *istep == ec.end_istep;
+    if (!continuing) ec.sim_time = 0.0;
+    if (ec.cfg_hash != ch || !same_mesh(ec, *ncell, *nghost, *nface, *dof, cell_info, face_info, geom)) {
         if (ec.s) amrgpu_session_destroy(ec.s);
         ec.s = nullptr;
         amrgpu_mesh_t m{*ncell, *nghost, *nface, *dof, cell_info, face_info, geom};
         amrgpu_session *s = nullptr;
-        if (amrgpu_session_create(&s, &m, nullptr) != AMRGPU_OK) {
+        const int rc = session_create_cfg(&s, &m, c);
+        if (rc != AMRGPU_OK) {
             *evolve_solution = 0;
             return;
         }
+        const size_t nc = size_t(*ncell + *nghost);
         ec.s = s;
-        ec.mesh_hash = mh;
+        ec.cell_info.assign(cell_info, cell_info + 3 * nc);
+        ec.face_info.assign(face_info, face_info + 11 * size_t(*nface));
+        ec.geom.assign(geom, geom + 12 * nc);
+        ec.ncell = *ncell;
+        ec.nghost = *nghost;
+        ec.nface = *nface;
+        ec.dof = *dof;
         ec.cfg_hash = ch;
     }
     amrgpu_session *s = ec.s;
@@ -1830,6 +1950,7 @@ void evolve(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *
     s->role[0] = 0; s->role[1] = 1; s->role[2] = 2; s->role[3] = 3;
     if (amrgpu_session_upload(s, soln) != AMRGPU_OK) {
         *evolve_solution = 0;
+        ec.end_istep = -1;
         return;
     }
     cudaEvent_t e0, e1;
@@ -1877,6 +1998,7 @@ void evolve(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *
     cudaEventDestroy(e1);
     ec.sim_time = rep.time;
     *istep += steps;
+    ec.end_istep = *istep;
     if (*istep % c.regrid_interval == 0) *regrid = 1;
     if (*istep % c.checkpoint_interval == 0) *checkpoint = 1;
     if (*istep % c.visualization_interval == 0) *visualize = 1;
@@ -1908,6 +2030,15 @@ void evolve(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *
 
 extern "C" {
 
+int amrgpu_evolve_config(int from_reference_layer, amrgpu_config_t *out)
+{
+    if (!out) return AMRGPU_ERR_ARG;
+    PhysicsConfig c;
+    if (!resolve_config(from_reference_layer != 0, c)) return AMRGPU_ERR_CONFIG;
+    config_to_public(c, out);
+    return AMRGPU_OK;
+}
+
 void hpc_amr_evolve_solver(int *dim, int *unstructured, int *nfields, int *nsub_elem, int *ncell, int *nghost,
                            int *nface, int *dof, int *cell_info, int *face_info, int *nsend, int *nrecv, int *send,
                            int *recv, int *sizes, double *geom, double *soln, int *istep, int *regrid,
@@ -1917,7 +2048,7 @@ void hpc_amr_evolve_solver(int *dim, int *unstructured, int *nfields, int *nsub_
     (void)send;
     (void)recv;
     (void)mpicomm_ext;
-    evolve(dim, unstructured, nfields, nsub_elem, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
+    evolve(false, dim, unstructured, nfields, nsub_elem, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
            sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, total_time, compute_time,
            residual_time);
 }
@@ -1931,7 +2062,7 @@ void physics_go_gpu(int *dim, int *unstructured, int *nfields, int *nelem_subgri
     (void)send;
     (void)recv;
     (void)mpicomm_ext;
-    evolve(dim, unstructured, nfields, nelem_subgrid, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
+    evolve(true, dim, unstructured, nfields, nelem_subgrid, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
            sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, total_time, compute_time,
            residual_time);
 }

@@ -169,6 +169,20 @@ int amrgpu_config_read(const char *path, amrgpu_config_t *cfg);
 int amrgpu_config_get(amrgpu_config_t *cfg);
 int amrgpu_config_set(const amrgpu_config_t *cfg);
 
+/* The configuration the next evolve call runs with: from_reference_layer = 1
+ * for physics_go_gpu, 0 for hpc_amr_evolve_solver. physics_go_gpu is called by
+ * the reference's own physics layer built with -D_GPU_
+ * (physics_evolve_interface.c:42-46), so it takes the reference's globals
+ * d_physics_interface / d_physics_fluid / d_physics_simulation
+ * (physics_var_*.h) when that layer is loaded and its physics_initialize has
+ * run, else this library's configuration; hpc_amr_evolve_solver takes this
+ * library's configuration (hpc_amr_initialize_solver above, or
+ * amrgpu_config_set) first and the reference's second. With neither the
+ * evolve entry points refuse to run (AMRGPU_ERR_CONFIG, *evolve_solution = 0)
+ * and so does this call. The library's extensions (form, final_time, IC
+ * parameters) always come from its own configuration. */
+int amrgpu_evolve_config(int from_reference_layer, amrgpu_config_t *out);
+
 /* ---------------- device-resident sessions ---------------- */
 typedef struct amrgpu_session amrgpu_session_t;
 

@@ -1,0 +1,163 @@
+"""Parity at the benchmark workloads' own sizes, on their default launches.
+
+* 1024^2 isentropic vortex (4096 quads of 16x16, the benchmark's mesh):
+  plain FP64 form -- one residual bit for bit against the reference's own C
+  driver (physics_rhs_structured.c:19-283 over the restated Fortran kernels)
+  and 3 SSP-RK3 steps bit for bit against the oracle
+  (rk_time_integrators.c:169-277); FP32-flux form -- one residual within
+  2e-5 of max|R| per field and L1(rho) after 20 steps within 1e-5 relative
+  of the oracle's FP64 run (the north-star bound is 1e-3).
+* shock-bubble interaction, levels 5-11 (28.6k quads, 7.3M cells, hanging
+  faces at every level jump) after two GPU regrids (tagging, refine /
+  coarsen, 2:1 balance and quad descriptors on the device): 5 FP64 steps
+  bit for bit against the oracle on the forest's own mesh arrays.
+* the learned-indicator family (8x8 patches, levels 3-7): FP64 residual bit
+  for bit, and the FP32 8x8 row sweep within 2e-5 of max|R|.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+os.environ.setdefault("AMRGPU_QUIET", "1")
+
+
+def _rel_by_field(r, rr):
+    r = r.reshape(-1, 4)
+    rr = rr.reshape(-1, 4)
+    return max(float(np.abs(r[:, k] - rr[:, k]).max() / (np.abs(rr[:, k]).max() + 1e-300)) for k in range(4))
+
+
+@pytest.fixture(scope="module")
+def vortex(ag):
+    from amrgpu import workloads as W
+    f, m, cfg, s0 = W.vortex_1024(form=0)
+    assert m.ncell == 4096 and m.ncells == 1024 * 1024
+    return f, m, cfg, s0
+
+
+def test_vortex1024_fp64_rhs_bitwise_vs_reference_driver(ag, oracle, vortex):
+    _, m, cfg, s0 = vortex
+    s = ag.Session(m, cfg, form=ag.FORM_FP64_EXACT)
+    s.upload(s0)
+    r = s.rhs()
+    s.close()
+    if oracle.reference_available():
+        ref = oracle.reference_rhs(m, s0, 16, cfg)
+    else:
+        ref = oracle.rhs(m, s0, oracle.make_config(16, cfg))
+    assert np.array_equal(r, ref), np.abs(r - ref).max()
+
+
+def test_vortex1024_fp64_three_rk3_steps_bitwise(ag, oracle, vortex):
+    _, m, cfg, s0 = vortex
+    s = ag.Session(m, cfg, form=ag.FORM_FP64_EXACT)
+    s.upload(s0)
+    s.step(3)
+    rep = s.sync()
+    got = s.download()
+    s.close()
+    oc = oracle.make_config(16, cfg)
+    oc.time_steps = 3
+    ref = s0.copy()
+    out = oracle.evolve(m, ref, oc)
+    assert out["steps"] == 3 and rep["steps"] == 3
+    assert rep["time"] == out["time"]
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
+
+
+@pytest.fixture(scope="module")
+def vortex_oracle_20(oracle, vortex):
+    _, m, cfg, s0 = vortex
+    oc = oracle.make_config(16, cfg)
+    oc.time_steps = 20
+    ref = s0.copy()
+    oracle.evolve(m, ref, oc)
+    return ref
+
+
+def test_vortex1024_fp32_default_launch(ag, oracle, vortex, vortex_oracle_20):
+    """The FP32-flux form as the library launches it by default at this
+    size: one residual within 2e-5 of max|R| per field, then L1(rho) after
+    20 steps against the oracle's FP64 run."""
+    _, m, cfg, s0 = vortex
+    s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
+    s.upload(s0)
+    r = s.rhs()
+    ref = oracle.rhs(m, s0, oracle.make_config(16, cfg))
+    worst = _rel_by_field(r, ref)
+    assert worst <= 2e-5, worst
+    s.upload(s0)
+    s.step(20)
+    s.sync()
+    got = s.download()
+    s.close()
+    rho, rho_ref = got[0::4], vortex_oracle_20[0::4]
+    l1 = float(np.abs(rho - rho_ref).sum() / np.abs(rho_ref).sum())
+    assert l1 <= 1e-5, l1
+    # conservation: periodic domain, every face flux added and subtracted
+    # with identical bits
+    assert abs(got[0::4].sum() - s0[0::4].sum()) <= 1e-12 * abs(s0[0::4].sum())
+
+
+def test_vortex1024_every_fp32_launch_agrees(ag, oracle, vortex):
+    """Every compiled FP32 launch shape at 16x16 gives a residual within
+    2e-5 of max|R| of the oracle on the full mesh."""
+    _, m, cfg, s0 = vortex
+    ref = oracle.rhs(m, s0, oracle.make_config(16, cfg))
+    s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
+    for k in range(len(s.launch_variants())):
+        s.set_launch_variant(k)
+        s.upload(s0)
+        worst = _rel_by_field(s.rhs(), ref)
+        assert worst <= 2e-5, (k, worst)
+    s.close()
+
+
+def test_shock_bubble_after_two_gpu_regrids_fp64_bitwise(ag, oracle):
+    from amrgpu import amr, workloads as W
+    n, lo, hi = 16, 5, 11
+    f, m, cfg, s0 = W.shock_bubble(form=0)
+    s = ag.Session(m, cfg, form=ag.FORM_FP64_EXACT)
+    s.upload(s0)
+    for _ in range(2):
+        s.step(5)
+        assert s.sync()["error"] == 0
+        amr.regrid(f, s, n, lo, hi)  # tags, adapt, 2:1 balance + descriptors on the GPU
+    m2 = f.mesh(n)  # forest_external of the regridded forest
+    assert m2.ncell == s.mesh.ncell and m2.ncell > 20000
+    lev = f.quads()[1]
+    assert lev.min() == lo and lev.max() == hi
+    q = s.download()
+    s.step(5)
+    assert s.sync()["error"] == 0
+    got = s.download()
+    s.close()
+    oc = oracle.make_config(n, cfg)
+    oc.time_steps = 5
+    ref = q.copy()
+    out = oracle.evolve(m2, ref, oc)
+    assert out["steps"] == 5
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
+
+
+def test_learned_family_8x8_levels_3_to_7(ag, oracle):
+    from amrgpu import learned as L
+    f, cfg, soln, _ = L.vortex_amr(seed=101, n=8, min_level=3, max_level=7, form=0)
+    m = f.mesh(8)
+    lev = f.quads()[1]
+    assert lev.max() == 7 and lev.min() == 3
+    ref = oracle.rhs(m, soln, oracle.make_config(8, cfg))
+    s = ag.Session(m, cfg, form=ag.FORM_FP64_EXACT)
+    s.upload(soln)
+    r = s.rhs()
+    s.close()
+    assert np.array_equal(r, ref), np.abs(r - ref).max()
+    s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
+    s.set_launch_variant(0)  # sweep8_kernel: two 8x8 quads per warp
+    s.upload(soln)
+    worst = _rel_by_field(s.rhs(), ref)
+    s.close()
+    assert worst <= 2e-5, worst
