@@ -8,6 +8,7 @@
 #include "flux_fp64.cuh"
 #include "launch_table.h"
 #include "stage_kernel.cuh"
+#include "stage_sweep64.cuh"
 
 namespace amrgpu {
 
@@ -92,6 +93,10 @@ const void *cfl_kernel_fp64(int n)
     StageLaunch{N, QPB, T, MINB, StageSmem<N, QPB, false>::total,                              \
                 (const void *)stage_kernel<N, QPB, T, MINB, false, FluxOpsFP64>}
 
+// row-sweep kernels: one warp per 16x16 quad or per two 8x8 quads
+#define AMRGPU_SWEEP64_16(W, MINB) StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep64_16_kernel<W, MINB>, 1}
+#define AMRGPU_SWEEP64_8(W, MINB) StageLaunch{8, 2 * (W), 32 * (W), MINB, 0, (const void *)sweep64_8_kernel<W, MINB>, 1}
+
 static const StageLaunch kTable64[] = {
     AMRGPU_STAGE64(16, 1, 288, 1),
     AMRGPU_STAGE64(16, 1, 288, 2),
@@ -104,6 +109,11 @@ static const StageLaunch kTable64[] = {
     AMRGPU_STAGE64(4, 16, 320, 2),
     AMRGPU_STAGE64(2, 16, 96, 4),
     AMRGPU_STAGE64(2, 32, 192, 2),
+    AMRGPU_SWEEP64_16(4, 3),
+    AMRGPU_SWEEP64_16(4, 4),
+    AMRGPU_SWEEP64_16(2, 6),
+    AMRGPU_SWEEP64_8(4, 3),
+    AMRGPU_SWEEP64_8(4, 4),
 };
 
 int stage_table_fp64(const StageLaunch **out)

@@ -33,6 +33,7 @@
 
 #include "flux_fp32.cuh"
 #include "stage_kernel.cuh"
+#include "sweep_common.cuh"
 
 namespace amrgpu {
 
@@ -55,23 +56,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
     const int i = l % N, h = l / N;
     const long long stride = a.stride;
 
-    // step scalars (as stage_kernel)
-    const StepSlot slot = a.scal->slot[a.slot_read];
-    double dt = __longlong_as_double((long long)slot.dt_bits);
-    if (!a.cfl_on) dt = a.dt_cap;
-    if (a.final_time > 0.0) {
-        double rem = a.final_time - slot.time;
-        if (rem < dt) dt = rem;
-        if (dt < 0.0) dt = 0.0;
-    }
-    if (a.last_stage && blockIdx.x == 0 && tid == 0) {
-        a.scal->slot[a.slot_write].time = slot.time + dt;
-        a.scal->dt_used = dt;
-        if (dt > 0.0) a.scal->steps += 1;
-        a.scal->slot[a.slot_reset].dt_bits = (unsigned long long)__double_as_longlong(a.dt_cap);
-        if (!a.cfl_on)
-            a.scal->slot[a.slot_write].dt_bits = (unsigned long long)__double_as_longlong(a.dt_cap);
-    }
+    const double dt = sweep_step_dt(a);
     const float qinf[4] = {(float)a.qinflow[0], (float)a.qinflow[1], (float)a.qinflow[2], (float)a.qinflow[3]};
 
     double my_dt_min = a.dt_cap;
@@ -258,52 +243,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
         item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
     }
 
-    // ---------------- block reductions: CFL min (one atomic per block),
-    // norm partials summed by the last block in a fixed order, flags; the
-    // last block also resets the quad counter for the next launch
-    int wflags = __reduce_or_sync(FULL, my_flags);
-    if (wflags && lane == 0) atomicOr(&a.scal->flags, wflags);
-    if (a.last_stage) {
-        double wmin = warp_min(my_dt_min);
-        double wsum = warp_sum(my_norm);
-        if (lane == 0) { red[w] = wmin; red[32 + w] = wsum; }
-    }
-    __syncthreads();
-    if (tid == 0) {
-        if (a.last_stage) {
-            double bmin = red[0], bsum = red[32];
-            for (int k = 1; k < WARPS; ++k) {
-                bmin = (red[k] < bmin) ? red[k] : bmin;
-                bsum += red[32 + k];
-            }
-            if (a.cfl_on)
-                atomicMin(&a.scal->slot[a.slot_write].dt_bits, (unsigned long long)__double_as_longlong(bmin));
-            a.partials[blockIdx.x] = bsum;
-        }
-        __threadfence();
-        const unsigned ticket = atomicAdd(&a.scal->done_blocks, 1u);
-        s_last = (ticket == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    if (a.last_stage) {
-        double part = 0.0;
-        for (int b = tid; b < (int)gridDim.x; b += WARPS * 32) part += __ldcg(a.partials + b);
-        part = warp_sum(part);
-        if (lane == 0) red[w] = part;
-        __syncthreads();
-        if (tid == 0) {
-            double tot = red[0];
-            for (int k = 1; k < WARPS; ++k) tot += red[k];
-            a.scal->norm_sq = tot;
-            if (!isfinite(tot)) atomicOr(&a.scal->flags, kFlagNonFinite);
-        }
-    }
-    if (tid == 0) {
-        a.scal->work_next = 0u;
-        a.scal->done_blocks = 0u;
-    }
+    sweep_reduce<WARPS>(a, my_dt_min, my_norm, my_flags, red, &s_last);
 }
 
 template <int WARPS, int MINB>

@@ -61,6 +61,10 @@ def restatement():
         L.oracle_evolve.restype = C.c_int
         L.oracle_flux_roe_2d.argtypes = [f64p, f64p, f64p, f64p]
         L.oracle_flux_roe_2d.restype = None
+        L.oracle_set_inflow.argtypes = [f64p]
+        L.oracle_set_inflow.restype = None
+        L.oracle_shock_state.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, f64p]
+        L.oracle_shock_state.restype = None
         _cache["r"] = L
     return _cache["r"]
 
@@ -69,8 +73,24 @@ def reference_available():
     return os.path.exists(REFERENCE)
 
 
+def set_inflow(cfg):
+    """bc 3 (extension): the shock-bubble workload's inflow state, the
+    post-shock state of its Mach ic_params[0] (default 2) shock into (1, 1)."""
+    L = restatement()
+    out = np.zeros(4, np.float64)
+    if cfg["initial_condition"] == 5:
+        ms = cfg["ic_params"][0] or 2.0
+        L.oracle_shock_state(cfg["gamma"], ms, 1.0, 1.0, dp(out))
+    L.oracle_set_inflow(dp(out))
+    if reference_available():
+        reference().oracle_set_inflow(dp(out))
+    return out
+
+
 def make_config(n, cfg):
-    """OracleConfig from an amrgpu.Config-like mapping."""
+    """OracleConfig from an amrgpu.Config-like mapping (also sets the
+    inflow state of bc 3)."""
+    set_inflow(cfg)
     c = OracleConfig()
     c.nelem_subgrid = n
     c.time_scheme = cfg["time_scheme"]
@@ -167,6 +187,8 @@ def reference():
         L.physics_go.argtypes = [i32p] * 15 + [f64p] * 2 + [i32p] * 5 + [C.c_int] + [f64p] * 3
         L.oracle_mpi_take_abort_code.restype = C.c_int
         L.oracle_mpi_take_abort_code.argtypes = []
+        L.oracle_set_inflow.argtypes = [f64p]
+        L.oracle_set_inflow.restype = None
         _cache["ref"] = L
     return _cache["ref"]
 

@@ -147,7 +147,34 @@ void oracle_flux_roe_2d(const double ql[4], const double qr[4],
         flux[k] = flux[k] * mag;
 }
 
-/* bc_2d_module.F90:14-75  bc_2d (0: extrapolate, 1: slip wall, 2: no-slip) */
+/* Extension with no reference counterpart: bc 3, a prescribed boundary
+ * state (the supersonic inflow of the shock-bubble workload), set by
+ * oracle_set_inflow. */
+static double oracle_inflow[4];
+
+void oracle_set_inflow(const double q[4])
+{
+    for (int k = 0; k < 4; k++) oracle_inflow[k] = q[k];
+}
+
+/* The post-shock state of a planar shock of Mach ms running into gas at
+ * rest (rho1, p1), by the Rankine-Hugoniot relations: the inflow state of
+ * the shock-bubble workload (an extension, restated from the relations). */
+void oracle_shock_state(double gamma, double ms, double rho1, double p1, double out[4])
+{
+    double c1 = sqrt(gamma * p1 / rho1);
+    double m2 = ms * ms;
+    double rho2 = rho1 * (gamma + 1.0) * m2 / ((gamma - 1.0) * m2 + 2.0);
+    double p2 = p1 * (1.0 + 2.0 * gamma / (gamma + 1.0) * (m2 - 1.0));
+    double u2 = ms * c1 * (1.0 - rho1 / rho2);
+    out[0] = rho2;
+    out[1] = rho2 * u2;
+    out[2] = 0.0;
+    out[3] = p2 / (gamma - 1.0) + 0.5 * rho2 * u2 * u2;
+}
+
+/* bc_2d_module.F90:14-75  bc_2d (0: extrapolate, 1: slip wall, 2: no-slip;
+ * 3: the prescribed state above, an extension) */
 static void bc_2d(int bc_type, const double normal[2], const double Q[4], double Q_bc[4])
 {
     const double gamma = 1.4;
@@ -180,6 +207,9 @@ static void bc_2d(int bc_type, const double normal[2], const double Q[4], double
         Q_bc[1] = 0.0;
         Q_bc[2] = 0.0;
         Q_bc[3] = Q[3] - 0.5 * rho * (u * u + v * v);
+        break;
+    case 3:
+        for (int k = 0; k < 4; k++) Q_bc[k] = oracle_inflow[k];
         break;
     default:
         /* The Fortran leaves Q_bc undefined for other types; the oracle

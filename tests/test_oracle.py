@@ -205,3 +205,19 @@ def test_product_ic_matches_oracle_ic(ag, oracle):
                                          oracle.dp(out), *[C.byref(d) for d in dv])
             ref[256 * q:256 * q + 256] = out
         assert np.array_equal(s, ref)
+
+
+def test_oracle_inflow_state_matches_the_library_ic(ag, oracle):
+    """bc 3 (extension): the oracle's inflow state is the post-shock state
+    the library's shock-bubble IC puts left of the shock, bit for bit."""
+    cfg = ag.Config.from_input(cfl=0.5, time_scheme=3, nelem_subgrid=4, coarse_grid_h=1.0, initial_condition=5,
+                               time_steps=1, dt=1.0, bc=[3, 0, 1, 1, 1, 1], gamma=1.4,
+                               ic_params=[2.0, 0.1, 0.1375, 0.2])
+    cfg.apply()
+    f = ag.Forest(2, 1, periodic=(0, 0), lo=(0.0, 0.0, 0.0), scale=1.0, level=5)
+    s = f.initialize(4).reshape(-1, 4, 4, 4)
+    m = f.mesh(4)
+    g = m.geom.reshape(-1, 12)
+    left = int(np.argmin(g[:, 0] + g[:, 1]))  # the quad at the lower-left corner, behind the shock
+    q = oracle.set_inflow(cfg)
+    assert np.array_equal(s[left, 0, 0], q)
