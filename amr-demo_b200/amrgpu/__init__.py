@@ -347,6 +347,21 @@ class Session:
     def launch_variant(self):
         return lib().amrgpu_session_launch_variant(self._s)
 
+    def launch_variant_info(self, index):
+        """(quads per block, threads, min blocks per SM, is_sweep) of a variant."""
+        v = [C.c_int() for _ in range(4)]
+        check(lib().amrgpu_session_launch_variant_info(self._s, int(index), *[C.byref(x) for x in v]),
+              "launch_variant_info")
+        return tuple(x.value for x in v)
+
+    def autotune(self, retime=False):
+        """Runs the library's stage-launch autotuner now (see
+        amrgpu_session_autotune); returns the chosen variant index and shape."""
+        check(lib().amrgpu_session_autotune(self._s, int(bool(retime))), "autotune")
+        k = self.launch_variant()
+        qpb, thr = self.launch_variants()[k]
+        return {"variant": k, "quads_per_block": qpb, "threads": thr}
+
     def set_launch(self, qpb, threads):
         check(lib().amrgpu_session_set_launch(self._s, int(qpb), int(threads)), "set_launch")
 

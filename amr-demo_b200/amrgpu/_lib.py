@@ -78,6 +78,12 @@ PROTOTYPES = {
     # Part 2: errors and configuration
     "amrgpu_last_error": (C.c_int, []),
     "amrgpu_evolve_config": (C.c_int, [C.c_int, C.POINTER(ConfigStruct)]),
+    "amrgpu_session_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "amrgpu_session_launch_variant_info": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, i32p, i32p]),
+    "amrgpu_tune_cache_get": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, i32p, i32p, i32p, f64p]),
+    "amrgpu_tune_cache_put": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_double]),
+    "amrgpu_tune_cache_reload": (None, []),
     "amrgpu_error_string": (C.c_char_p, [C.c_int]),
     "amrgpu_last_error_message": (C.c_char_p, []),
     "amrgpu_clear_error": (None, []),

@@ -109,6 +109,38 @@ void set_config_initialized(bool v);
 int parse_physics_file(const char *path, PhysicsConfig &cfg);
 void config_to_public(const PhysicsConfig &c, amrgpu_config_t *o);
 
+// ---------------------------------------------------------------- autotuner
+// One tuned choice: the key (GPU name, SM count, form, patch size,
+// floor(log2(quads))) and the launch shape picked, with its residual-stage
+// time in ms. tune_cache.cpp keeps them in memory and in a JSON file.
+struct TuneEntry {
+    std::string gpu;
+    int sms = 0, form = 0, n = 0, bucket = 0;
+    int qpb = 0, threads = 0, min_blocks = 0;
+    double ms = 0.0;
+};
+std::string tune_cache_path();
+bool tune_lookup(const TuneEntry &key, TuneEntry *out);
+void tune_store(const TuneEntry &e);
+void tune_forget();  // drops the in-memory table; the file is read again on next use
+
+// ---------------------------------------------------------------- staging
+// Two pinned chunks and their events (staging.cu): pageable host arrays move
+// to and from the device through them, host copies overlapping the DMA.
+struct PinnedRing {
+    static constexpr size_t kChunk = size_t(8) << 20;
+    void *buf[2] = {nullptr, nullptr};
+    void *ev[2] = {nullptr, nullptr};  // cudaEvent_t
+    bool ensure();
+    void release();
+};
+bool host_is_pinned(const void *p);
+// dst/src device arrays, stream a cudaStream_t. ring_h2d returns once the
+// last chunk is queued (the caller's array may be reused after that);
+// ring_d2h returns after the data has landed in dst.
+bool ring_h2d(PinnedRing &r, void *dst, const void *src, size_t bytes, void *stream);
+bool ring_d2h(PinnedRing &r, void *dst, const void *src, size_t bytes, void *stream);
+
 // ---------------------------------------------------------------- errors
 void set_error(int code, const std::string &msg);
 

@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -72,6 +73,22 @@ bool cuda_ok(cudaError_t e, const char *what)
     return false;
 }
 
+// The device's name (cudaDeviceProp::name), looked up once per device.
+std::string device_name(int dev)
+{
+    static std::mutex mu;
+    static std::map<int, std::string> names;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = names.find(dev);
+    if (it != names.end()) return it->second;
+    cudaDeviceProp prop;
+    std::string name = cudaGetDeviceProperties(&prop, dev) == cudaSuccess ? std::string(prop.name) : "unknown";
+    for (char &c : name)
+        if (c == '"' || c == '\\') c = '_';
+    names[dev] = name;
+    return name;
+}
+
 uint64_t fnv1a(const void *p, size_t bytes, uint64_t h = 1469598103934665603ULL)
 {
     const unsigned char *b = static_cast<const unsigned char *>(p);
@@ -103,6 +120,7 @@ struct amrgpu_session {
     int cap_desc = 0;          // quads d_quads holds
     QuadDesc *d_quads_alt = nullptr;  // build target of amrgpu_session_regrid_forest
     int cap_desc_alt = 0;
+    PinnedRing ring;                  // pinned chunks for pageable state transfers
     void *h_stage = nullptr;          // pinned staging of a forest's leaves
     size_t h_stage_bytes = 0;
     void *d_mesh_scratch = nullptr;   // device scratch of the descriptor build
@@ -117,6 +135,8 @@ struct amrgpu_session {
     int bal_trees = 0;                    // trees the balance work area holds tables for
     bool rect = true;                 // every quad an axis-aligned rectangle
     bool launch_pinned = false;       // the stage launch was chosen by the caller
+    bool tune_pending = false;        // the autotuner runs before the next step
+    std::string gpu_name;             // key of the autotuner's choices
     int *d_tags = nullptr;
     int *d_kind = nullptr;
     int *d_src = nullptr;
@@ -431,6 +451,145 @@ int enqueue_step(amrgpu_session *s)
 
 }  // namespace
 
+namespace {
+
+// A residual-only stage of the current launch: reads the state (role X)
+// and writes the residual into role Z, which no scheme carries across a
+// step boundary. Used by amrgpu_session_rhs and by the autotuner.
+bool launch_rhs_stage(amrgpu_session *s)
+{
+    StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.quads = s->d_quads;
+    a.qin = rolebuf(s, RX);
+    a.out0 = rolebuf(s, RZ);
+    a.partials = s->d_partials;
+    a.scal = s->d_scal;
+    a.stride = s->stride;
+    a.nquad = s->nquad;
+    a.scheme = kSchemeRhsOnly;
+    a.stage = 1;
+    a.last_stage = 0;
+    a.cfl_on = 0;
+    a.slot_read = int(s->step_index % 3);
+    a.slot_write = (a.slot_read + 1) % 3;
+    a.slot_reset = (a.slot_read + 2) % 3;
+    a.h_base = s->cfg.coarse_grid_h;
+    a.cfl = s->cfg.cfl;
+    a.dt_cap = s->cfg.dt;
+    if (s->cfg.initial_condition == 5) {
+        double ms = s->cfg.ic_params[0] != 0.0 ? s->cfg.ic_params[0] : 2.0;
+        amrgpu::shock_state(s->cfg.gamma, ms, 1.0, 1.0, a.qinflow);
+    }
+    void *args[] = {&a};
+    if (!cuda_ok(cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args, s->launch->smem,
+                                  s->stream),
+                 "rhs kernel"))
+        return false;
+    s->launches++;
+    return true;
+}
+
+constexpr int kTuneMinQuads = 256;
+
+int quad_bucket(int nquad)
+{
+    int b = 0;
+    while ((2LL << b) <= (long long)nquad) ++b;
+    return b;
+}
+
+// Launches that may replace the default: all of the patch size for the FP64
+// form (every shape gives the same bits); for the FP32-flux form only the
+// shapes of the default's family (row sweep or block kernel), which agree
+// bit for bit among themselves.
+bool tune_candidate(const amrgpu_session *s, const StageLaunch &L, const StageLaunch *def)
+{
+    if (L.n != s->n) return false;
+    if (s->form == AMRGPU_FORM_FP32_FLUX && def && L.sweep != def->sweep) return false;
+    return true;
+}
+
+// Chooses the session's stage launch: the stored choice for its key when
+// there is one (and retime is false), else the fastest candidate, timed
+// with residual-only stages on the session's current state.
+int autotune_session(amrgpu_session *s, bool retime)
+{
+    s->tune_pending = false;
+    if (s->nquad == 0) return AMRGPU_OK;
+    const StageLaunch *tab;
+    const int cnt = (s->form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
+    const StageLaunch *def = default_launch(s->form, s->n, s->nquad);
+    TuneEntry key;
+    key.gpu = s->gpu_name;
+    key.sms = s->sms;
+    key.form = s->form;
+    key.n = s->n;
+    key.bucket = quad_bucket(s->nquad);
+    TuneEntry hit;
+    if (!retime && tune_lookup(key, &hit)) {
+        for (int i = 0; i < cnt; ++i)
+            if (tune_candidate(s, tab[i], def) && tab[i].qpb == hit.qpb && tab[i].threads == hit.threads &&
+                tab[i].min_blocks == hit.min_blocks)
+                return configure_launch(s, &tab[i]);
+    }
+    cudaEvent_t e0, e1;
+    if (!cuda_ok(cudaEventCreate(&e0), "tune event")) return AMRGPU_ERR_CUDA;
+    if (!cuda_ok(cudaEventCreate(&e1), "tune event")) {
+        cudaEventDestroy(e0);
+        return AMRGPU_ERR_CUDA;
+    }
+    const StageLaunch *best = nullptr;
+    float best_ms = 0.f;
+    constexpr int kReps = 3;
+    for (int i = 0; i < cnt; ++i) {
+        if (!tune_candidate(s, tab[i], def)) continue;
+        if (configure_launch(s, &tab[i]) != AMRGPU_OK) {
+            set_error(AMRGPU_OK, "");
+            continue;
+        }
+        bool ok = launch_rhs_stage(s);  // warm-up (first launch of a kernel)
+        ok = ok && cuda_ok(cudaEventRecord(e0, s->stream), "tune record");
+        for (int r = 0; r < kReps && ok; ++r) ok = launch_rhs_stage(s);
+        ok = ok && cuda_ok(cudaEventRecord(e1, s->stream), "tune record");
+        ok = ok && cuda_ok(cudaEventSynchronize(e1), "tune sync");
+        float ms = 0.f;
+        if (ok) ok = cuda_ok(cudaEventElapsedTime(&ms, e0, e1), "tune elapsed");
+        if (!ok) break;
+        ms /= kReps;
+        if (!best || ms < best_ms) {
+            best = &tab[i];
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!best) return configure_launch(s, def);
+    int rc = configure_launch(s, best);
+    if (rc == AMRGPU_OK) {
+        TuneEntry e = key;
+        e.qpb = best->qpb;
+        e.threads = best->threads;
+        e.min_blocks = best->min_blocks;
+        e.ms = best_ms;
+        tune_store(e);
+    }
+    return rc;
+}
+
+// The autotuner, when a step is about to run on a default launch: sessions
+// of at least kTuneMinQuads quads, unless AMRGPU_AUTOTUNE=0.
+int maybe_autotune(amrgpu_session *s)
+{
+    if (!s->tune_pending) return AMRGPU_OK;
+    s->tune_pending = false;
+    if (s->launch_pinned || s->nquad < kTuneMinQuads) return AMRGPU_OK;
+    if (const char *e = std::getenv("AMRGPU_AUTOTUNE"); e && std::atoi(e) == 0) return AMRGPU_OK;
+    return autotune_session(s, false);
+}
+
+}  // namespace
+
 int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const PhysicsConfig &c);
 
 extern "C" {
@@ -537,6 +696,8 @@ int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const Phy
         amrgpu_session_destroy(s);
         return rc;
     }
+    s->gpu_name = device_name(dev);
+    s->tune_pending = !s->launch_pinned;
     *out = s;
     return AMRGPU_OK;
 }
@@ -567,6 +728,7 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_remap0);
     cudaFree(s->d_bal_work);
     cudaFreeHost(s->h_stage);
+    s->ring.release();
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -579,6 +741,7 @@ int amrgpu_session_set_form(amrgpu_session_t *s, int form)
     s->form = form;
     s->cfg.form = form;
     s->launch_pinned = false;
+    s->tune_pending = true;
     return configure_launch(s, default_launch(form, s->n, s->nquad));
 }
 
@@ -642,13 +805,34 @@ int amrgpu_session_launch_variants(const amrgpu_session_t *s, int *qpb, int *thr
     return k;
 }
 
+int amrgpu_session_launch_variant_info(const amrgpu_session_t *s, int index, int *qpb, int *threads,
+                                       int *min_blocks, int *sweep)
+{
+    if (!s) return AMRGPU_ERR_ARG;
+    const StageLaunch *tab;
+    const int cnt = (s->form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
+    int k = 0;
+    for (int i = 0; i < cnt; ++i) {
+        if (tab[i].n != s->n) continue;
+        if (k++ != index) continue;
+        if (qpb) *qpb = tab[i].qpb;
+        if (threads) *threads = tab[i].threads;
+        if (min_blocks) *min_blocks = tab[i].min_blocks;
+        if (sweep) *sweep = tab[i].sweep;
+        return AMRGPU_OK;
+    }
+    set_error(AMRGPU_ERR_ARG, "no compiled variant with that index");
+    return AMRGPU_ERR_ARG;
+}
+
 int amrgpu_session_upload(amrgpu_session_t *s, const double *soln)
 {
     if (!s || !soln) return AMRGPU_ERR_ARG;
     size_t bytes = sizeof(double) * 4 * size_t(s->ncells_total);
     if (bytes) {
-        if (!cuda_ok(cudaMemcpyAsync(s->d_aos, soln, bytes, cudaMemcpyHostToDevice, s->stream), "H2D soln"))
-            return AMRGPU_ERR_CUDA;
+        // pinned caller arrays go straight to the device; pageable ones
+        // through the session's pinned chunks (staging.cu)
+        if (!ring_h2d(s->ring, s->d_aos, soln, bytes, s->stream)) return AMRGPU_ERR_CUDA;
         if (!cuda_ok(launch_aos_to_soa(s->d_aos, rolebuf(s, RX), s->ncells_total, s->stride, s->stream), "aos_to_soa"))
             return AMRGPU_ERR_CUDA;
         s->launches++;
@@ -664,9 +848,7 @@ int amrgpu_session_download(amrgpu_session_t *s, double *soln)
         if (!cuda_ok(launch_soa_to_aos(rolebuf(s, RX), s->d_aos, cells, s->stride, s->stream), "soa_to_aos"))
             return AMRGPU_ERR_CUDA;
         s->launches++;
-        if (!cuda_ok(cudaMemcpyAsync(soln, s->d_aos, sizeof(double) * 4 * size_t(cells), cudaMemcpyDeviceToHost,
-                                     s->stream),
-                     "D2H soln"))
+        if (!ring_d2h(s->ring, soln, s->d_aos, sizeof(double) * 4 * size_t(cells), s->stream))
             return AMRGPU_ERR_CUDA;
     }
     return cuda_ok(cudaStreamSynchronize(s->stream), "sync") ? AMRGPU_OK : AMRGPU_ERR_CUDA;
@@ -678,6 +860,9 @@ int amrgpu_session_step_stage(amrgpu_session_t *s, int *stage, int *stages_per_s
     if (!s->primed) {
         int rc = prime(s);
         if (rc) return rc;
+    }
+    if (s->stage_pos == 0 && s->nquad > 0) {
+        if (int rc = maybe_autotune(s)) return rc;
     }
     bool swap_xy = false;
     const auto &plan = plan_of(scheme_of(s), swap_xy);
@@ -781,6 +966,7 @@ int amrgpu_session_step(amrgpu_session_t *s, int nsteps)
         if (rc) return rc;
     }
     if (s->nquad == 0) return AMRGPU_OK;
+    if (int rc = maybe_autotune(s)) return rc;
     for (int k = 0; k < nsteps; ++k) {
         int rc = enqueue_step(s);
         if (rc) return rc;
@@ -802,6 +988,7 @@ int amrgpu_session_step_graph(amrgpu_session_t *s, int nsteps, int graph_steps)
         if (rc) return rc;
     }
     if (s->nquad == 0) return AMRGPU_OK;
+    if (int rc = maybe_autotune(s)) return rc;
     int done = 0;
     // align to a 6-step boundary: slot phase (3) and buffer-role parity (2)
     while (done < nsteps && (s->step_index % 6) != 0) {
@@ -871,34 +1058,7 @@ int amrgpu_session_rhs(amrgpu_session_t *s, double *rhs)
 {
     if (!s || !rhs) return AMRGPU_ERR_ARG;
     if (s->nquad == 0) return AMRGPU_OK;
-    StageArgs a;
-    std::memset(&a, 0, sizeof(a));
-    a.quads = s->d_quads;
-    a.qin = rolebuf(s, RX);
-    a.out0 = rolebuf(s, RZ);
-    a.partials = s->d_partials;
-    a.scal = s->d_scal;
-    a.stride = s->stride;
-    a.nquad = s->nquad;
-    a.scheme = kSchemeRhsOnly;
-    a.stage = 1;
-    a.last_stage = 0;
-    a.cfl_on = 0;
-    a.slot_read = int(s->step_index % 3);
-    a.slot_write = (a.slot_read + 1) % 3;
-    a.slot_reset = (a.slot_read + 2) % 3;
-    a.h_base = s->cfg.coarse_grid_h;
-    a.cfl = s->cfg.cfl;
-    a.dt_cap = s->cfg.dt;
-    if (s->cfg.initial_condition == 5) {
-        double ms = s->cfg.ic_params[0] != 0.0 ? s->cfg.ic_params[0] : 2.0;
-        amrgpu::shock_state(s->cfg.gamma, ms, 1.0, 1.0, a.qinflow);
-    }
-    void *args[] = {&a};
-    if (!cuda_ok(cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args, s->launch->smem,
-                                  s->stream),
-                 "rhs kernel"))
-        return AMRGPU_ERR_CUDA;
+    if (!launch_rhs_stage(s)) return AMRGPU_ERR_CUDA;
     s->launches++;
     long long cells = (long long)s->nquad * s->n * s->n;
     if (!cuda_ok(launch_soa_to_aos(rolebuf(s, RZ), s->d_aos, cells, s->stride, s->stream), "soa_to_aos"))
@@ -935,6 +1095,61 @@ int amrgpu_session_cells(const amrgpu_session_t *s) { return s ? int((long long)
 void *amrgpu_session_stream(amrgpu_session_t *s) { return s ? (void *)s->stream : nullptr; }
 
 int64_t amrgpu_session_launch_count(const amrgpu_session_t *s) { return s ? s->launches : 0; }
+
+int amrgpu_session_autotune(amrgpu_session_t *s, int retime)
+{
+    if (!s) return AMRGPU_ERR_ARG;
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_autotune: a step begun with step_stage is not finished");
+        return AMRGPU_ERR_ARG;
+    }
+    if (!s->primed) {
+        set_error(AMRGPU_ERR_ARG, "session_autotune: no state uploaded");
+        return AMRGPU_ERR_ARG;
+    }
+    s->launch_pinned = false;
+    return autotune_session(s, retime != 0);
+}
+
+int amrgpu_tune_cache_get(const char *gpu, int sms, int form, int n, int nquad, int *qpb, int *threads,
+                          int *min_blocks, double *ms)
+{
+    if (!gpu) return 0;
+    TuneEntry key, hit;
+    key.gpu = gpu;
+    key.sms = sms;
+    key.form = form;
+    key.n = n;
+    key.bucket = quad_bucket(nquad);
+    if (!tune_lookup(key, &hit)) return 0;
+    if (qpb) *qpb = hit.qpb;
+    if (threads) *threads = hit.threads;
+    if (min_blocks) *min_blocks = hit.min_blocks;
+    if (ms) *ms = hit.ms;
+    return 1;
+}
+
+int amrgpu_tune_cache_put(const char *gpu, int sms, int form, int n, int nquad, int qpb, int threads,
+                          int min_blocks, double ms)
+{
+    if (!gpu || nquad < 1) return AMRGPU_ERR_ARG;
+    TuneEntry e;
+    e.gpu = gpu;
+    for (char &c : e.gpu)
+        if (c == '"' || c == '\\') c = '_';
+    e.sms = sms;
+    e.form = form;
+    e.n = n;
+    e.bucket = quad_bucket(nquad);
+    e.qpb = qpb;
+    e.threads = threads;
+    e.min_blocks = min_blocks;
+    e.ms = ms;
+    tune_store(e);
+    return AMRGPU_OK;
+}
+
+void amrgpu_tune_cache_reload(void) { tune_forget(); }
 
 }  // extern "C"
 
@@ -1154,6 +1369,7 @@ int apply_regrid(amrgpu_session *s, int nq, int nface)
     s->stride = stride;
     // a launch chosen by the caller stays; the default follows the mesh size
     int rc = configure_launch(s, s->launch_pinned ? s->launch : default_launch(s->form, s->n, nq));
+    if (!s->launch_pinned) s->tune_pending = true;
     if (rc != AMRGPU_OK) return rc;
     return prime(s, s->primed);
 }

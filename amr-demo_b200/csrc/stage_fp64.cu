@@ -94,14 +94,24 @@ const void *cfl_kernel_fp64(int n)
                 (const void *)stage_kernel<N, QPB, T, MINB, false, FluxOpsFP64>}
 
 // row-sweep kernels: one warp per 16x16 quad or per two 8x8 quads
-#define AMRGPU_SWEEP64_16(W, MINB) StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep64_16_kernel<W, MINB>, 1}
-#define AMRGPU_SWEEP64_8(W, MINB) StageLaunch{8, 2 * (W), 32 * (W), MINB, 0, (const void *)sweep64_8_kernel<W, MINB>, 1}
+#define AMRGPU_SWEEP64_16(W, MINB)                                                             \
+    StageLaunch{16, W, 32 * (W), MINB, Sweep64Smem<16>::bytes(W), (const void *)sweep64_16_kernel<W, MINB>, 1}
+#define AMRGPU_SWEEP64_8(W, MINB)                                                              \
+    StageLaunch{8, 2 * (W), 32 * (W), MINB, Sweep64Smem<8>::bytes(W), (const void *)sweep64_8_kernel<W, MINB>, 1}
 
+// Per patch size the first entry is the default launch (a row sweep gives
+// way to the size's first block kernel on meshes too small to fill the GPU
+// with sweep warps); the autotuner picks among all entries of the size.
 static const StageLaunch kTable64[] = {
-    AMRGPU_STAGE64(16, 1, 288, 1),
+    AMRGPU_SWEEP64_16(4, 4),  // 128 registers, 16 warps per SM
+    AMRGPU_SWEEP64_16(2, 8),
+    AMRGPU_SWEEP64_16(4, 3),
     AMRGPU_STAGE64(16, 1, 288, 2),
+    AMRGPU_STAGE64(16, 1, 288, 1),
     AMRGPU_STAGE64(16, 2, 576, 1),
     AMRGPU_STAGE64(16, 1, 256, 2),
+    AMRGPU_SWEEP64_8(4, 4),   // two 8x8 quads per warp
+    AMRGPU_SWEEP64_8(4, 3),
     AMRGPU_STAGE64(8, 4, 288, 2),
     AMRGPU_STAGE64(8, 2, 160, 3),
     AMRGPU_STAGE64(8, 4, 576, 1),
@@ -109,11 +119,6 @@ static const StageLaunch kTable64[] = {
     AMRGPU_STAGE64(4, 16, 320, 2),
     AMRGPU_STAGE64(2, 16, 96, 4),
     AMRGPU_STAGE64(2, 32, 192, 2),
-    AMRGPU_SWEEP64_16(4, 3),
-    AMRGPU_SWEEP64_16(4, 4),
-    AMRGPU_SWEEP64_16(2, 6),
-    AMRGPU_SWEEP64_8(4, 3),
-    AMRGPU_SWEEP64_8(4, 4),
 };
 
 int stage_table_fp64(const StageLaunch **out)

@@ -259,11 +259,11 @@ __device__ __forceinline__ int facing_cell(int s, int m)
 // The stage update of one cell for every scheme, with the reference's
 // coefficients and summation order (rk_time_integrators.c:22-540; the
 // Shu-Osher RK3 of the FP32-flux form is the extension). kv is the cell's
-// residual, q0v its input state, A0(f) the first auxiliary input; writes
-// the outputs at gi and returns the new state in qn.
-template <typename A0F>
+// residual, q0v its input state, A0(f) / A1(f) the first / second auxiliary
+// inputs; writes the outputs at gi and returns the new state in qn.
+template <typename A0F, typename A1F>
 __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long long stride, long long gi,
-                                          const double q0v[4], const double kv[4], A0F A0, double qn[4])
+                                          const double q0v[4], const double kv[4], A0F A0, A1F A1, double qn[4])
 {
     switch (a.scheme) {
     case kSchemeRhsOnly:
@@ -308,7 +308,7 @@ __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long lo
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 double Q0 = A0(f);
-                double k1 = a.a1[f * stride + gi];
+                double k1 = A1(f);
                 qn[f] = Q0 + alpha21 * k1 + alpha22 * kv[f];
                 double C = Q0 + beta1 * k1 + beta2 * kv[f];
                 a.out0[f * stride + gi] = qn[f];
@@ -337,7 +337,7 @@ __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long lo
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 double Q0 = A0(f);
-                double K = a.a1[f * stride + gi];
+                double K = A1(f);
                 qn[f] = Q0 + al * kv[f];
                 a.out0[f * stride + gi] = qn[f];
                 a.out1[f * stride + gi] = K + 2.0 * kv[f];
@@ -346,7 +346,7 @@ __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long lo
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 double Q0 = A0(f);
-                double K = a.a1[f * stride + gi];
+                double K = A1(f);
                 qn[f] = Q0 + beta1 * (K + kv[f]);
                 a.out0[f * stride + gi] = qn[f];
             }
@@ -859,7 +859,8 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
 #pragma unroll
             for (int f = 0; f < 4; ++f) q0v[f] = raw[(ql * 4 + f) * NN + c];
 
-            rk_update(a, dt, stride, gi, q0v, kv, A0, qn);
+            auto A1 = [&](int f) -> double { return a.a1[f * stride + gi]; };
+            rk_update(a, dt, stride, gi, q0v, kv, A0, A1, qn);
 
             if (a.last_stage) {
 #pragma unroll

@@ -159,7 +159,8 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
             }
             if (!valid) return;
             auto A0 = [&](int f) -> double { return a0below[f]; };
-            rk_update(a, dt, stride, gi, qbelow, kv, A0, qn);
+            auto A1 = [&](int f) -> double { return a.a1[f * stride + gi]; };
+            rk_update(a, dt, stride, gi, qbelow, kv, A0, A1, qn);
             if (a.last_stage) {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) my_norm += kv[f] * kv[f];

@@ -1,6 +1,6 @@
 // stage_sweep64.cuh -- the plain FP64 form's RK stage for 16x16 and 8x8
 // patches as a row sweep: one warp per 16x16 quadrant (two per warp for
-// 8x8), per-cell records in registers, no block-wide barriers.
+// 8x8), no block-wide barriers.
 //
 // It produces the same bits as stage_kernel<n, ..., FP64> and therefore as
 // the reference: the same flux code (flux_roe_2d, flux_2d_module.F90:63-182,
@@ -21,36 +21,56 @@
 //   edges   each lane evaluates one edge face per round (sides 0/1, then
 //           2/3; a coarse hanging edge also its second, index-paired flux)
 //           into a per-warp table, and the faces between rows R-1 and R;
-//   sweep   at step t lane (i, h) loads cell (i, j = Rh+t) and builds its
-//           record; it first completes row j-1 (the y-face flux at j-1/2
-//           with the record it kept of row j-1, then that row's update),
-//           then computes the bilinear nodes of row j+1 at columns i and i+1
-//           (row j's came from the step before), the x-face flux at i-1/2
-//           with the left neighbour's record taken by a warp shuffle, and
-//           hands it to lane i-1 (its i+1/2 face) by a second shuffle. The
-//           two flux evaluations of a step thus never hold their operands at
-//           the same time (168 registers, 12 warps per SM).
+//   sweep   at step t lane (i, h) takes cell (i, j = Rh+t): its record, the
+//           bilinear nodes of row j+1 at columns i and i+1 (row j's came
+//           from the step before), then two flux evaluations through one
+//           call site -- the x-face at i-1/2 with the left neighbour's record
+//           taken by a warp shuffle (its value goes to lane i-1, which needs
+//           it as its i+1/2 face, by a second shuffle), then the y-face at
+//           j-1/2 with the record of row j-1, which completes row j-1 (its
+//           update is written).
+//
+// Registers are the limit of an FP64 flux kernel (a flux evaluation holds
+// about 60 live doubles), so what a lane carries from one row to the next --
+// row j-1's record, partial residual, input state and volume -- waits in
+// shared memory, and the row's own-cell inputs (the next row's state, the
+// stage's auxiliary inputs) arrive there by cp.async one step ahead of use.
 #pragma once
 
+#include "async_copy.cuh"
 #include "flux_fp64.cuh"
 #include "stage_kernel.cuh"
 #include "sweep_common.cuh"
 
 namespace amrgpu {
 
+// Dynamic shared memory of the FP64 sweep, in doubles per warp.
+template <int N>
+struct Sweep64Smem {
+    static constexpr int QPW = 32 / (2 * N);
+    static constexpr int RS = 9;                      // record: rho, rho u, rho v, rho E, u, v, p, H, sqrt(rho)
+    static constexpr int edge = QPW * 4 * 2 * N * 4;  // [quad][side][first/second flux][position][field]
+    static constexpr int mid = QPW * N * 4;           // [quad][column][field]: faces between rows R-1 and R
+    static constexpr int carry = (RS + 4 + 4 + 1) * 32;  // [record, partial, input state, volume][lane]
+    static constexpr int qbuf = 4 * 32;                  // next row's state [field][lane]
+    static constexpr int abuf = 8 * 32;                  // auxiliary inputs a0, a1 [field][lane]
+    static constexpr int o_edge = 0, o_mid = o_edge + edge, o_carry = o_mid + mid, o_q = o_carry + carry,
+                         o_a = o_q + qbuf;
+    static constexpr int per_warp = o_a + abuf;
+    static constexpr size_t bytes(int warps) { return sizeof(double) * (size_t)per_warp * (size_t)warps; }
+};
+
 template <int N, int WARPS>
 __device__ __forceinline__ void sweep64_body(const StageArgs &a)
 {
     static_assert(N == 16 || N == 8, "row sweep for 16x16 and 8x8 patches");
+    using S = Sweep64Smem<N>;
     constexpr int NN = N * N;
-    constexpr int QPW = 32 / (2 * N);  // quads per warp
-    constexpr int R = N / 2;           // rows per half-patch
-    constexpr int RS = 9;              // record: rho, rho u, rho v, rho E, u, v, p, H, sqrt(rho)
+    constexpr int QPW = S::QPW;
+    constexpr int R = N / 2;  // rows per half-patch
+    constexpr int RS = S::RS;
     constexpr unsigned FULL = 0xffffffffu;
-    // per warp and quad: edge fluxes [side][first / second (coarse hanging
-    // edge) flux][position][field] and the faces between rows R-1 and R
-    __shared__ double sedge[WARPS][QPW][4][2][N][4];
-    __shared__ double smid[WARPS][QPW][N][4];
+    extern __shared__ __align__(16) double sm64[];
     __shared__ double red[64];
     __shared__ int s_last;
 
@@ -62,10 +82,19 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
     const double xi0 = scale_factor * (double)i - 1.0;        // nodes at column i
     const double xi1 = scale_factor * (double)(i + 1) - 1.0;  // ... and i+1
 
+    double *wsm = sm64 + (size_t)w * S::per_warp;
+    double(*sedge)[4][2][N][4] = reinterpret_cast<double(*)[4][2][N][4]>(wsm + S::o_edge);
+    double(*smid)[N][4] = reinterpret_cast<double(*)[N][4]>(wsm + S::o_mid);
+    double *car = wsm + S::o_carry + lane;  // slot c at car[32 c]
+    double *qb = wsm + S::o_q + lane;       // field f at qb[32 f]
+    double *ab = wsm + S::o_a + lane;       // a0 field f at ab[32 f], a1 at ab[32 (4 + f)]
+    enum { kPart = RS, kQ = RS + 4, kVol = RS + 8 };
+
     const double dt = sweep_step_dt(a);
     double my_dt_min = a.dt_cap;
     double my_norm = 0.0;
     int my_flags = 0;
+    const bool has_a0 = a.a0 != nullptr, has_a1 = a.a1 != nullptr;
 
     // work items as in the FP32 sweep: first by warp index, then from the
     // quad counter; a quad past the end is computed on the item's first
@@ -85,9 +114,14 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
             for (int f = 0; f < 4; ++f) q[f] = base[f * stride + cell];
             cell_prims_fp64(q, P);
         };
+        // the first row's state, on its way while the edges are computed
+#pragma unroll
+        for (int f = 0; f < 4; ++f) cp_async8(qb + 32 * f, Qq + f * stride + (R * h) * N + i);
+        cp_async_commit();
+        cp_async_commit();  // (no auxiliary group before the first row)
 
         // ---------------- edges: round 0 sides 0 / 1, round 1 sides 2 / 3
-#pragma unroll
+#pragma unroll 1
         for (int round = 0; round < 2; ++round) {
             const int s = 2 * round + h, m = i;
             const bool xd = round == 0;
@@ -101,7 +135,7 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
                 const double n1 = xd ? 0.0 : ((s & 1) ? hc : -hc);
                 bc_flux_fp64(d.bc, Po, n0, n1, a.qinflow, fl);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) sedge[w][sub][s][0][m][f] = fl[f];
+                for (int f = 0; f < 4; ++f) sedge[sub][s][0][m][f] = fl[f];
             } else {
                 // the neighbour's facing cell at the same position (a coarse
                 // hanging edge pairs it with both fine quads)
@@ -119,7 +153,7 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
                     }
                     roe_flux_prim_fp64(Lr, Rr, n0, n1, fl);
 #pragma unroll
-                    for (int f = 0; f < 4; ++f) sedge[w][sub][s][k][m][f] = fl[f];
+                    for (int f = 0; f < 4; ++f) sedge[sub][s][k][m][f] = fl[f];
                 }
             }
         }
@@ -137,7 +171,7 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
                 bilinear_node(g, xi0, eta, x2, y2);
                 roe_flux_prim_fp64(P, O, y2 - y1, x1 - x2, fl);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) smid[w][sub][i][f] = fl[f];
+                for (int f = 0; f < 4; ++f) smid[sub][i][f] = fl[f];
             }
         }
         __syncwarp();
@@ -149,7 +183,10 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
             const int sy = (j == 0) ? 2 : (j == N - 1) ? 3 : -1;
             if (sx < 0 && sy < 0) return;
             int first = sx, second = sy;
-            if (sx >= 0 && sy >= 0 && qd.side[sy].rank < qd.side[sx].rank) { first = sy; second = sx; }
+            if (sx >= 0 && sy >= 0 && qd.side[sy].rank < qd.side[sx].rank) {
+                first = sy;
+                second = sx;
+            }
 #pragma unroll
             for (int pass = 0; pass < 2; ++pass) {
                 const int s = pass == 0 ? first : second;
@@ -157,8 +194,8 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
                 const int kind = qd.side[s].kind;
                 const int m = (s < 2) ? j : i;
                 const bool hang = kind == kSideCoarseHang;
-                const double *F = sedge[w][sub][s][0][m];
-                const double *F2 = sedge[w][sub][s][1][m];
+                const double *F = sedge[sub][s][0][m];
+                const double *F2 = sedge[sub][s][1][m];
                 if (kind == kSideBoundary || (s & 1)) {
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
@@ -174,35 +211,29 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
                 }
             }
         };
-
-        // ---------------- sweep over the lane's R rows
-        // A step first completes the row below (its y-face flux, then the
-        // update) and only then evaluates its own x-face flux, so that the
-        // two flux evaluations never hold their operands at the same time.
-        double below[RS];  // record of the row below (partner of the y-face)
-        double part[4];    // residual of the row below without its face at j+1/2
-        double qbelow[4];  // input state of the row below
-        double volbelow = 0.0;
-        const bool has_a0 = a.a0 != nullptr;
-        // finishes row jr: + F(y+1/2) when that face is interior, / volume,
-        // x -1, stage update, last-stage reductions; a0 is the row's first
-        // auxiliary input
-        auto finish = [&](int jr, const double *gup, const double a0r[4]) {
+        // finishes row jr from the carried state: + F(y+1/2) when that face
+        // is interior, / volume, x -1, stage update with the auxiliary
+        // inputs in ab, last-stage reductions
+        auto finish = [&](int jr, const double *gup) {
             const long long gi = (long long)quad * NN + jr * N + i;
-            double kv[4], qn[4];
+            const double vol = car[32 * kVol];
+            double kv[4], qn[4], q0v[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                const double r = gup ? part[f] + gup[f] : part[f];
-                kv[f] = (r / volbelow) * -1.0;
+                const double p = car[32 * (kPart + f)];
+                const double r = gup ? p + gup[f] : p;
+                kv[f] = (r / vol) * -1.0;
+                q0v[f] = car[32 * (kQ + f)];
             }
             if (!valid) return;
-            auto A0 = [&](int f) -> double { return a0r[f]; };
-            rk_update(a, dt, stride, gi, qbelow, kv, A0, qn);
+            auto A0 = [&](int f) -> double { return ab[32 * f]; };
+            auto A1 = [&](int f) -> double { return ab[32 * (4 + f)]; };
+            rk_update(a, dt, stride, gi, q0v, kv, A0, A1, qn);
             if (a.last_stage) {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) my_norm += kv[f] * kv[f];
                 if (a.cfl_on) {
-                    const double cand = cfl_candidate_fp64(qn, volbelow, a.cfl);
+                    const double cand = cfl_candidate_fp64(qn, vol, a.cfl);
                     if (cand < my_dt_min) my_dt_min = cand;
                 }
                 const double rho = qn[0];
@@ -210,84 +241,118 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
                 if (!(rho > 0.0) || !(pe > 0.0)) my_flags |= kFlagNegative;
             }
         };
-        auto load_a0 = [&](int jr, double a0r[4]) {
+        // the auxiliary inputs of row jr into ab (one cp.async group)
+        auto fetch_aux = [&](int jr) {
+            const long long gi = (long long)quad * NN + jr * N + i;
+            if (has_a0) {
 #pragma unroll
-            for (int f = 0; f < 4; ++f)
-                a0r[f] = has_a0 ? a.a0[f * stride + (long long)quad * NN + jr * N + i] : 0.0;
+                for (int f = 0; f < 4; ++f) cp_async8(ab + 32 * f, a.a0 + f * stride + gi);
+            }
+            if (has_a1) {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) cp_async8(ab + 32 * (4 + f), a.a1 + f * stride + gi);
+            }
+            cp_async_commit();
         };
-        // nodes (i, j) and (i+1, j) of the current row
-        double xa, ya, xb, yb;
+
+        // ---------------- sweep over the lane's R rows. cp.async groups in
+        // flight at the start of step t: the state of row j (issued one step
+        // earlier) and the auxiliary inputs of row j-1.
+        double xa, ya, xb, yb;  // nodes (i, j) and (i+1, j) of the current row
         {
             const double eta = scale_factor * (double)(R * h) - 1.0;
             bilinear_node(g, xi0, eta, xa, ya);
             bilinear_node(g, xi1, eta, xb, yb);
         }
-        double qnext[4];
-#pragma unroll
-        for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (R * h) * N + i];
 #pragma unroll 1
         for (int t = 0; t < R; ++t) {
             const int j = R * h + t;
+            cp_async_wait_group<1>();  // row j's state has landed
             double q4[4];
 #pragma unroll
-            for (int f = 0; f < 4; ++f) q4[f] = qnext[f];
-            if (t < R - 1) {
-#pragma unroll
-                for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (j + 1) * N + i];
-            }
+            for (int f = 0; f < 4; ++f) q4[f] = qb[32 * f];
             double P[RS];
             cell_prims_fp64(q4, P);
-            // y-face at j-1/2: nodes (i+1, j) -> (i, j); completes row j-1
-            double fy[4];
-            const bool has_fy = j > 0;
-            if (t == 0) {
-                if (h == 1) {
+            // the next row's state into the buffer just read (the record
+            // above consumed it)
+            if (t < R - 1) {
 #pragma unroll
-                    for (int f = 0; f < 4; ++f) fy[f] = smid[w][sub][i][f];
-                }
-            } else {
-                double a0r[4];
-                load_a0(j - 1, a0r);
-                roe_flux_prim_fp64(below, P, ya - yb, xb - xa, fy);
-                finish(j - 1, fy, a0r);
+                for (int f = 0; f < 4; ++f) cp_async8(qb + 32 * f, Qq + f * stride + (j + 1) * N + i);
             }
-            // nodes (i, j+1), (i+1, j+1) and the cell's volume
+            cp_async_commit();
+            // nodes (i, j+1), (i+1, j+1), the cell's volume and x-face normal
             double xc, yc, xd, yd;
             {
                 const double eta = scale_factor * (double)(j + 1) - 1.0;
                 bilinear_node(g, xi0, eta, xc, yc);
                 bilinear_node(g, xi1, eta, xd, yd);
             }
-            const double n0x = yc - ya, n1x = xa - xc;
-            volbelow = subcell_volume(xa, ya, xb, yb, xc, yc, xd, yd);
-            xa = xc; ya = yc; xb = xd; yb = yd;
-            // x-face at i-1/2: nodes (i, j) -> (i, j+1); lane i = 0's is an edge face
-            double L[RS], fx[4], fxr[4];
+            const double vol = subcell_volume(xa, ya, xb, yb, xc, yc, xd, yd);
+            double r[4];
+            // k = 0: x-face at i-1/2, nodes (i, j) -> (i, j+1), the left
+            //        neighbour's record (lane i = 0's is an edge face);
+            // k = 1: y-face at j-1/2, nodes (i+1, j) -> (i, j), row j-1's
+            //        record, which completes row j-1
+            const int nk = (t > 0) ? 2 : 1;
+#pragma unroll 1
+            for (int k = 0; k < nk; ++k) {
+                double A[RS];
+                double n0, n1;
+                if (k == 0) {
 #pragma unroll
-            for (int c = 0; c < RS; ++c) L[c] = __shfl_up_sync(FULL, P[c], 1, N);
-            roe_flux_prim_fp64(L, P, n0x, n1x, fx);
+                    for (int c = 0; c < RS; ++c) A[c] = __shfl_up_sync(FULL, P[c], 1, N);
+                    n0 = yc - ya;
+                    n1 = xa - xc;
+                } else {
 #pragma unroll
-            for (int f = 0; f < 4; ++f) fxr[f] = __shfl_down_sync(FULL, fx[f], 1, N);
-            double r[4] = {0.0, 0.0, 0.0, 0.0};
-            edge_sum(j, r);
+                    for (int c = 0; c < RS; ++c) A[c] = car[32 * c];
+                    n0 = ya - yb;
+                    n1 = xb - xa;
+                }
+                double F[4];
+                roe_flux_prim_fp64(A, P, n0, n1, F);
+                if (k == 0) {
+                    double Fr[4];
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) Fr[f] = __shfl_down_sync(FULL, F[f], 1, N);
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) r[f] = 0.0;
+                    edge_sum(j, r);
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) {
+                        if (i > 0) r[f] = r[f] - F[f];
+                        if (i < N - 1) r[f] = r[f] + Fr[f];
+                    }
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) r[f] = r[f] - F[f];
+                    cp_async_wait_group<1>();  // row j-1's auxiliary inputs
+                    finish(j - 1, F);
+                }
+            }
+            if (t == 0 && h == 1) {
+#pragma unroll
+                for (int f = 0; f < 4; ++f) r[f] = r[f] - smid[sub][i][f];
+            }
+            fetch_aux(j);
+            // carry row j to the next step
+#pragma unroll
+            for (int c = 0; c < RS; ++c) car[32 * c] = P[c];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                if (i > 0) r[f] = r[f] - fx[f];
-                if (i < N - 1) r[f] = r[f] + fxr[f];
-                if (has_fy) r[f] = r[f] - fy[f];
-                part[f] = r[f];
-                qbelow[f] = q4[f];
+                car[32 * (kPart + f)] = r[f];
+                car[32 * (kQ + f)] = q4[f];
             }
-#pragma unroll
-            for (int c = 0; c < RS; ++c) below[c] = P[c];
+            car[32 * kVol] = vol;
+            xa = xc;
+            ya = yc;
+            xb = xd;
+            yb = yd;
         }
-        {
-            // the half's top row: the face between rows R-1 and R (h = 0) or
-            // the patch's top edge, already summed (h = 1)
-            double a0r[4];
-            load_a0(R * h + R - 1, a0r);
-            finish(R * h + R - 1, h == 0 ? smid[w][sub][i] : nullptr, a0r);
-        }
+        // the half's top row: the face between rows R-1 and R (h = 0) or the
+        // patch's top edge, already summed (h = 1)
+        cp_async_wait_group<0>();
+        finish(R * h + R - 1, h == 0 ? smid[sub][i] : nullptr);
         __syncwarp();  // the next item rewrites this warp's tables
         unsigned nxt = 0;
         if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);

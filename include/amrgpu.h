@@ -209,6 +209,33 @@ int amrgpu_session_create(amrgpu_session_t **out, const amrgpu_mesh_t *mesh,
 void amrgpu_session_destroy(amrgpu_session_t *s);
 int amrgpu_session_set_form(amrgpu_session_t *s, int form);
 int amrgpu_session_set_launch(amrgpu_session_t *s, int quads_per_block, int threads);
+/* Stage-launch autotuner (SURVEY build plan step 5; no reference
+ * counterpart: the reference has one CPU code path). A session whose launch
+ * was not set by the caller tunes on its first step after an upload or a
+ * regrid, when it has at least 256 quads and AMRGPU_AUTOTUNE is not 0: each
+ * compiled launch shape of its patch size runs a residual-only stage on the
+ * session's own state (into a scratch buffer; the solution is untouched) and
+ * the fastest is kept. Only shapes that give bits identical to the default
+ * launch compete (every FP64 shape; for the FP32-flux form, the row sweeps
+ * among themselves and the block kernels among themselves). The choice is
+ * stored per (GPU name, SM count, form, patch size, floor(log2(quads))) in
+ * memory and in a JSON file -- AMRGPU_TUNE_CACHE (empty: memory only), else
+ * $XDG_CACHE_HOME/amrgpu/tune.json or $HOME/.cache/amrgpu/tune.json -- and
+ * later sessions with the same key use it without timing. hpc_amr_evolve_solver,
+ * physics_go_gpu and every regrid go through the same path.
+ * amrgpu_session_autotune tunes now (retime = 1: ignore the stored choice
+ * and time again); the chosen shape is then amrgpu_session_launch_variant. */
+int amrgpu_session_autotune(amrgpu_session_t *s, int retime);
+/* The stored choice for a key (nquad picks the bucket): 1 and the shape
+ * when present, 0 when not. */
+int amrgpu_tune_cache_get(const char *gpu, int sms, int form, int n, int nquad, int *quads_per_block,
+                          int *threads, int *min_blocks, double *ms);
+/* Stores a choice (replacing the key's previous one) and rewrites the file. */
+int amrgpu_tune_cache_put(const char *gpu, int sms, int form, int n, int nquad, int quads_per_block,
+                          int threads, int min_blocks, double ms);
+/* Forgets the in-memory choices (the file is read again on next use). */
+void amrgpu_tune_cache_reload(void);
+
 /* The compiled stage-kernel launch shapes for the session's form and patch
  * size (the autotuner's candidates): fills up to cap pairs, returns the count. */
 int amrgpu_session_launch_variants(const amrgpu_session_t *s, int *quads_per_block, int *threads,
@@ -218,6 +245,10 @@ int amrgpu_session_launch_variants(const amrgpu_session_t *s, int *quads_per_blo
  * index. */
 int amrgpu_session_set_launch_variant(amrgpu_session_t *s, int index);
 int amrgpu_session_launch_variant(const amrgpu_session_t *s);
+/* Shape of variant `index`: quads per CTA, threads, the minimum resident CTAs
+ * per SM it was compiled for, and 1 for a row sweep / 0 for a block kernel. */
+int amrgpu_session_launch_variant_info(const amrgpu_session_t *s, int index, int *quads_per_block,
+                                       int *threads, int *min_blocks, int *sweep);
 /* Host AoS soln (reference layout, dof + ghost tail) <-> device SoA state. */
 int amrgpu_session_upload(amrgpu_session_t *s, const double *soln_aos);
 int amrgpu_session_download(amrgpu_session_t *s, double *soln_aos);

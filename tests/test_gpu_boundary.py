@@ -91,3 +91,28 @@ def test_final_time_carries_over_a_continuing_run(ag, oracle):
             break
     assert r["evolve_solution"] == 0 and istep > 6
     assert np.array_equal(got, ref), np.abs(got - ref).max()
+
+
+def test_pageable_and_pinned_transfers_agree(ag):
+    """The 1024^2 state (33.5 MB: four 8 MB chunks of the session's pinned
+    ring and a partial fifth) makes the same round trip from pageable numpy
+    memory as from page-locked memory."""
+    import torch
+    from amrgpu import workloads as W
+    f, m, cfg, s0 = W.vortex_1024(form=0)
+    rng = np.random.default_rng(5)
+    q = s0 * (1.0 + 1e-3 * rng.uniform(-1, 1, s0.shape))
+    s = ag.Session(m, cfg, form=ag.FORM_FP64_EXACT)
+    s.upload(q)
+    assert np.array_equal(s.download(), q)
+    pin = torch.empty(m.dof, dtype=torch.float64, pin_memory=True).numpy()
+    pin[:] = q[::-1]
+    s.upload(pin)
+    back = torch.empty(m.dof, dtype=torch.float64, pin_memory=True).numpy()
+    s.download(back)
+    assert np.array_equal(back, q[::-1])
+    s.upload(q)
+    r_pageable = s.rhs()
+    s.upload(pin[::-1].copy())
+    assert np.array_equal(s.rhs(), r_pageable)
+    s.close()
