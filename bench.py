@@ -20,11 +20,12 @@ fused stage kernels, the next step's CFL minimum folded into the last one).
           included; the model is trained on the GPU in the same run
 
 `--impl reference` times the reference's own CPU path (its C driver over
-the restated Fortran kernels, oracle/_ref) on all host cores instead.
+the restated Fortran kernels, oracle/_ref, compiled -O3) on the same 1024^2
+mesh on all host cores instead: one MPI rank per core (threads over a
+multi-rank MPI stand-in, the reference's ghost exchange every stage).
 """
 import argparse
 import json
-import multiprocessing as mp
 import os
 import statistics
 import subprocess
@@ -63,51 +64,64 @@ def peaks():
 
 
 # ------------------------------------------------------------------ CPU baseline
-def _cpu_worker(args):
-    level, steps, use_ref = args
-    import numpy as np  # noqa: F401
-    sys.path[:0] = [ROOT, os.path.join(ROOT, "amr-demo_b200")]
-    os.environ["AMRGPU_QUIET"] = "1"
-    from amrgpu import workloads as W
-    from oracle import oracle as O
-    f, m, cfg, s0 = W.vortex_1024(level=level, steps=steps, final_time=0.0)
-    s = s0.copy()
+def _quiet(fn):
+    """Runs fn() with the process's stdout (fd 1) sent to /dev/null: the
+    reference's driver prints a report every call."""
+    sys.stdout.flush()
     devnull = os.open(os.devnull, os.O_WRONLY)
     saved = os.dup(1)
     os.dup2(devnull, 1)
-    t0 = time.perf_counter()
     try:
-        if use_ref:
-            O.reference_go(m, s, 16, cfg)
-        else:
-            O.evolve(m, s, O.make_config(16, cfg))
+        return fn()
     finally:
-        t1 = time.perf_counter()
         os.dup2(saved, 1)
         os.close(devnull)
-    return m.ncells * steps, t1 - t0
+        os.close(saved)
 
 
-def cpu_baseline(level=5, steps=16):
-    """All host cores, one process each (the reference's own MPI-rank model
-    without its exchange), each advancing its own copy of the vortex problem
-    at level `level` for `steps` RK3 steps."""
-    from oracle import oracle as O
-    use_ref = O.reference_available()
-    procs = max(1, min(os.cpu_count() or 1, 128))
-    ctx = mp.get_context("spawn")
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(steps=10, one_rank_steps=2, level=6):
+    """The reference's own CPU path on this host, on the benchmark's own
+    workload (the 1024^2 vortex mesh, built in NumPy by oracle/workload.py:
+    no product library is loaded): its C driver (physics_go over the
+    restated Fortran kernels) compiled -O3 for this CPU, run as P MPI ranks
+    = P threads (one per host core) over the multi-rank MPI stand-in, each
+    rank holding a Morton range of quads plus its ghost quads and
+    exchanging them every stage as physics_mpi_real_to_ghost does. value =
+    cells x steps / the slowest rank's time in physics_go. A one-rank run of
+    the same mesh is reported beside it."""
+    from oracle import oracle as O, workload as WL
+    from amrgpu import shard as S  # NumPy partitioning only; the library is not loaded
+    n = 16
+    mesh = WL.uniform_periodic_mesh(level, n)
+    s0 = WL.vortex_state(mesh)
+    procs = max(1, min(host_cores(), 128, mesh.ncell))
+    mt_path, flags = O.timing_build("libref_physics_mt")
+    one_path, _ = O.timing_build("libref_physics")
+    offs = S.partition(mesh.ncell, procs)
+    shards = [S.make_shard(mesh, offs, r) for r in range(procs)]
+    cfg = WL.vortex_config(n, steps=steps)
+    states = [sh.local_state(s0) for sh in shards]
+    out = _quiet(lambda: O.reference_mt_go(shards, states, n, cfg, path=mt_path))
+    value = mesh.ncells * steps / out["wall"]
+    cfg1 = WL.vortex_config(n, steps=one_rank_steps)
+    q = s0.copy()
     t0 = time.perf_counter()
-    with ctx.Pool(procs) as pool:
-        res = pool.map(_cpu_worker, [(level, steps, use_ref)] * procs)
-    wall = time.perf_counter() - t0
-    updates = sum(r[0] for r in res)
-    slowest = max(r[1] for r in res)
-    value = updates / slowest
-    cells = (4 ** level) * 256
-    return {"value": value, "unit": UNIT, "cores": procs, "kind": "reference" if use_ref else "port",
-            "sample": f"{procs} processes x {steps} RK3 steps of the same vortex at {cells} cells "
-                      f"(level {level}, 16x16 patches); rate = all updates / slowest process "
-                      f"({slowest:.2f} s; pool wall {wall:.2f} s)"}
+    _quiet(lambda: O.reference_go(mesh, q, n, cfg1, path=one_path))
+    one = mesh.ncells * one_rank_steps / (time.perf_counter() - t0)
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"the reference's physics_go ({flags}) on the {int(round(mesh.ncells ** 0.5))}^2 vortex mesh "
+                      f"({mesh.ncell} quads of 16x16), {steps} RK3 steps, {procs} MPI ranks as threads with the "
+                      f"reference's ghost exchange every stage; slowest rank {out['wall']:.2f} s",
+            "one_rank": {"value": one, "unit": UNIT, "cores": 1, "steps": one_rank_steps,
+                         "sample": f"one rank, the same mesh, {one_rank_steps} RK3 steps"},
+            "same_config": True}
 
 
 # ------------------------------------------------------------------ clocks
@@ -663,20 +677,21 @@ def run_gpu(args):
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU path (cpu_baseline) on the
+    benchmark's mesh, --warmup untimed steps then --steps timed steps on all
+    host cores; rank 0 of a torchrun launch alone runs it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    vals = []
-    cb = None
-    for _ in range(max(1, args.steps // 10)):
-        cb = cpu_baseline()
-        vals.append(cb["value"])
-    value = statistics.median(vals)
-    cb["value"] = value
+    from oracle import oracle as O, workload as WL  # noqa: F401
+    cpu_baseline(steps=max(1, args.warmup), one_rank_steps=1)  # warm-up: page in, first touch
+    cb = cpu_baseline(steps=args.steps, one_rank_steps=2)
+    value = cb["value"]
+    ms = 1e3 * (1024 * 1024) / value
     line = {"metric": METRIC, "impl": "reference", "value": value, "unit": UNIT, "n_gpus": 0,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded analytic vortex)",
-            "config": {"workload": WORKLOAD + " (CPU sample, see cpu_baseline.sample)"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded analytic vortex)",
+            "config": {"workload": WORKLOAD, "parallelism": f"{cb['cores']} MPI ranks (threads) on host cores"},
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

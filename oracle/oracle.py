@@ -19,6 +19,28 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT = os.path.join(HERE, "_build", "liboracle.so")
 REFERENCE = os.path.join(HERE, "_ref", "libref_physics.so")
+REFERENCE_MT = os.path.join(HERE, "_ref", "libref_physics_mt.so")
+
+
+def _host_has_avx512():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("flags"):
+                    return " avx512f " in line + " "
+    except OSError:
+        pass
+    return False
+
+
+def timing_build(base):
+    """The -O3 timing build of a reference library (x86-64-v4 on AVX-512
+    hosts, else x86-64-v3); the parity build when neither was built."""
+    for arch in (("v4", "v3") if _host_has_avx512() else ("v3",)):
+        p = os.path.join(HERE, "_ref", f"{base}_fast_{arch}.so")
+        if os.path.exists(p):
+            return p, f"-O3 -march=x86-64-{arch}"
+    return os.path.join(HERE, "_ref", f"{base}.so"), "-O2 -ffp-contract=off (parity build)"
 
 i32p = C.POINTER(C.c_int)
 f64p = C.POINTER(C.c_double)
@@ -175,12 +197,15 @@ class _Simulation(C.Structure):  # physics_var_simulation.h:20-30
                 ("dt", C.c_double)]
 
 
-def reference():
-    """The reference's own C driver (oracle/_ref), with its globals."""
-    if "ref" not in _cache:
-        if not reference_available():
-            raise RuntimeError(f"{REFERENCE} missing: run `make -C oracle ref` where the reference tree exists")
-        L = C.CDLL(REFERENCE)
+def reference(path=None):
+    """The reference's own C driver (oracle/_ref), with its globals; path
+    selects another build of it (a timing build, the multi-rank build)."""
+    path = path or REFERENCE
+    key = ("ref", path)
+    if key not in _cache:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: run `make -C oracle ref` where the reference tree exists")
+        L = C.CDLL(path)
         L.physics_rhs_structured.restype = None
         L.physics_rhs_structured.argtypes = [i32p, i32p, i32p, i32p, i32p, f64p, i32p, i32p, i32p, f64p, f64p]
         L.physics_go.restype = None
@@ -189,8 +214,22 @@ def reference():
         L.oracle_mpi_take_abort_code.argtypes = []
         L.oracle_set_inflow.argtypes = [f64p]
         L.oracle_set_inflow.restype = None
-        _cache["ref"] = L
-    return _cache["ref"]
+        if hasattr(L, "oracle_mt_go"):
+            L.oracle_mt_go.restype = C.c_int
+            L.oracle_mt_go.argtypes = [C.c_int, C.c_int, C.POINTER(MtRank)]
+        _cache[key] = L
+    return _cache[key]
+
+
+class MtRank(C.Structure):
+    """oracle_mt_rank_t of mt_driver.c: one rank's arrays and results."""
+
+    _fields_ = [("ncell", C.c_int), ("nghost", C.c_int), ("nface", C.c_int), ("dof", C.c_int), ("nsend", C.c_int),
+                ("nrecv", C.c_int), ("cell_info", i32p), ("face_info", i32p), ("send", i32p), ("recv", i32p),
+                ("sizes", i32p), ("geom", f64p), ("soln", f64p), ("istep", C.c_int), ("regrid", C.c_int),
+                ("visualize", C.c_int), ("checkpoint", C.c_int), ("evolve_solution", C.c_int),
+                ("total_time", C.c_double), ("compute_time", C.c_double), ("residual_time", C.c_double),
+                ("wall", C.c_double)]
 
 
 def _pad_int(a, pad=16):
@@ -201,8 +240,8 @@ def _pad_int(a, pad=16):
     return buf, buf[pad:]
 
 
-def reference_set_globals(n, cfg):
-    L = reference()
+def reference_set_globals(n, cfg, L=None):
+    L = L or reference()
     itf = _Interface.in_dll(L, "d_physics_interface")
     itf.dim, itf.nfringe, itf.nfields, itf.nelem_subgrid = 2, 2, 4, n
     itf.extern_cell_size, itf.extern_face_size = 3, 11
@@ -237,10 +276,11 @@ def reference_rhs(mesh, soln, n, cfg):
     return out
 
 
-def reference_go(mesh, soln, n, cfg, istep=0):
-    """physics_go (the reference's CPU evolve) on ``soln`` in place."""
-    L = reference()
-    reference_set_globals(n, cfg)
+def reference_go(mesh, soln, n, cfg, istep=0, path=None):
+    """physics_go (the reference's CPU evolve) on ``soln`` in place; path
+    selects a build of the reference library (default: the parity build)."""
+    L = reference(path)
+    reference_set_globals(n, cfg, L)
     buf, ci = _pad_int(mesh.cell_info)
     dim, uns, nf, nn = C.c_int(2), C.c_int(0), C.c_int(4), C.c_int(n)
     nc, ng, nface, dof = C.c_int(mesh.ncell), C.c_int(0), C.c_int(mesh.nface), C.c_int(mesh.dof)
@@ -257,3 +297,40 @@ def reference_go(mesh, soln, n, cfg, istep=0):
                  C.byref(evo), 0, C.byref(tt), C.byref(ct), C.byref(rt))
     return {"istep": ist.value, "regrid": rg.value, "visualize": vis.value, "checkpoint": chk.value,
             "evolve_solution": evo.value, "total_time": tt.value, "abort": L.oracle_mpi_take_abort_code()}
+
+
+def reference_mt_go(shards, states, n, cfg, path=None):
+    """The reference's physics_go on len(shards) ranks at once, one thread
+    each, over the multi-rank MPI stand-in (mt_driver.c): every rank evolves
+    its own state in ``states`` (local quads then ghost quads, AoS) with the
+    ghost exchange of physics_mpi_real_to_ghost every stage. ``shards`` are
+    objects with ``mesh`` (external_t arrays of the rank) and
+    ``reference_lists()`` (send / recv (cell, rank) pairs). Returns the
+    per-rank flags and the slowest rank's seconds in physics_go."""
+    L = reference(path or REFERENCE_MT)
+    reference_set_globals(n, cfg, L)
+    P = len(shards)
+    ranks = (MtRank * P)()
+    keep = []
+    for r, (sh, st) in enumerate(zip(shards, states)):
+        m = sh.mesh
+        buf, ci = _pad_int(m.cell_info)
+        send, recv = sh.reference_lists()
+        send = np.ascontiguousarray(send if len(send) else np.zeros(2, np.int32), np.int32)
+        recv = np.ascontiguousarray(recv if len(recv) else np.zeros(2, np.int32), np.int32)
+        nall = len(m.cell_info) // 3
+        sizes = np.full(max(nall, 1), 4 * n * n, np.int32)
+        fi = np.ascontiguousarray(m.face_info, np.int32)
+        geom = np.ascontiguousarray(m.geom, np.float64)
+        R = ranks[r]
+        R.ncell, R.nghost, R.nface, R.dof = m.ncell, nall - m.ncell, m.nface, m.dof
+        R.nsend, R.nrecv = len(sh.reference_lists()[0]) // 2, len(sh.reference_lists()[1]) // 2
+        R.cell_info, R.face_info, R.send, R.recv, R.sizes = ip(ci), ip(fi), ip(send), ip(recv), ip(sizes)
+        R.geom, R.soln = dp(geom), dp(st)
+        R.istep, R.evolve_solution = 0, 1
+        keep += [buf, ci, fi, geom, send, recv, sizes, st]
+    rc = L.oracle_mt_go(P, n, ranks)
+    if rc != 0:
+        raise RuntimeError("oracle_mt_go: the rank threads could not be started")
+    return {"istep": [ranks[r].istep for r in range(P)], "evolve_solution": [ranks[r].evolve_solution for r in range(P)],
+            "wall": max(ranks[r].wall for r in range(P)), "abort": L.oracle_mpi_take_abort_code()}

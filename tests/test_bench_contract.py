@@ -33,7 +33,21 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
     assert cb["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
-    assert "workload" in d["config"]
+    assert "workload" in d["config"] and d["ms_per_step"] > 0
+    assert cb["same_config"] is True and cb["one_rank"]["value"] > 0
+
+
+def test_reference_arm_loads_no_product_library():
+    """The CPU baseline builds its mesh in NumPy and runs only the
+    reference's own C code (oracle/_ref): libamrgpu.so is never mapped."""
+    code = ("import sys, json; sys.argv=['bench.py']; sys.path.insert(0, %r); import bench; "
+            "cb = bench.cpu_baseline(steps=1, one_rank_steps=1); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'amrgpu': 'libamrgpu' in maps, 'ref': 'libref_physics' in maps}))" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    assert d == {"amrgpu": False, "ref": True}
 
 
 def test_reference_arm_prints_nothing_on_other_ranks():
