@@ -78,6 +78,8 @@ PROTOTYPES = {
     # Part 2: errors and configuration
     "amrgpu_last_error": (C.c_int, []),
     "amrgpu_evolve_config": (C.c_int, [C.c_int, C.POINTER(ConfigStruct)]),
+    "amrgpu_set_comm_ops": (C.c_int, [C.c_void_p]),
+    "amrgpu_has_comm_ops": (C.c_int, []),
     "amrgpu_session_autotune": (C.c_int, [C.c_void_p, C.c_int]),
     "amrgpu_session_launch_variant_info": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, i32p, i32p]),
     "amrgpu_tune_cache_get": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, i32p, i32p, i32p, f64p]),

@@ -2054,20 +2054,89 @@ bool resolve_config(bool from_reference_layer, PhysicsConfig &out)
     return false;
 }
 
+// The caller's MPI operations (amrgpu_set_comm_ops), process-wide.
+std::mutex g_comm_mu;
+amrgpu_comm_ops_t g_comm_ops{};
+bool g_comm_set = false;
+
+bool comm_ops(amrgpu_comm_ops_t &out)
+{
+    std::lock_guard<std::mutex> lk(g_comm_mu);
+    if (g_comm_set) out = g_comm_ops;
+    return g_comm_set;
+}
+
+// Ghost-exchange buffers of a multi-rank evolve session: the send-list
+// records and the ghost records on the device and in pinned host memory,
+// plus a pinned word for the CFL step's cross-rank MIN.
+struct HaloBuffers {
+    double *d_send = nullptr, *d_recv = nullptr, *h_send = nullptr, *h_recv = nullptr;
+    unsigned long long *h_dt = nullptr;
+    size_t send_cap = 0, recv_cap = 0;
+
+    void release()
+    {
+        cudaFree(d_send);
+        cudaFree(d_recv);
+        cudaFreeHost(h_send);
+        cudaFreeHost(h_recv);
+        cudaFreeHost(h_dt);
+        *this = HaloBuffers{};
+    }
+    bool reserve(size_t nsend_doubles, size_t nrecv_doubles)
+    {
+        if (!h_dt && !cuda_ok(cudaMallocHost(&h_dt, sizeof(unsigned long long)), "pinned dt word")) return false;
+        if (nsend_doubles > send_cap) {
+            cudaFree(d_send);
+            cudaFreeHost(h_send);
+            d_send = h_send = nullptr;
+            send_cap = 0;
+            if (!cuda_ok(cudaMalloc(&d_send, sizeof(double) * nsend_doubles), "halo send buffer") ||
+                !cuda_ok(cudaMallocHost(&h_send, sizeof(double) * nsend_doubles), "pinned halo send buffer"))
+                return false;
+            send_cap = nsend_doubles;
+        }
+        if (nrecv_doubles > recv_cap) {
+            cudaFree(d_recv);
+            cudaFreeHost(h_recv);
+            d_recv = h_recv = nullptr;
+            recv_cap = 0;
+            if (!cuda_ok(cudaMalloc(&d_recv, sizeof(double) * nrecv_doubles), "halo receive buffer") ||
+                !cuda_ok(cudaMallocHost(&h_recv, sizeof(double) * nrecv_doubles), "pinned halo receive buffer"))
+                return false;
+            recv_cap = nrecv_doubles;
+        }
+        return true;
+    }
+};
+
 struct EvolveCache {
     amrgpu_session *s = nullptr;
     // the mesh the session was built from, kept to compare byte for byte
     std::vector<int> cell_info, face_info;
     std::vector<double> geom;
+    std::vector<int> send, recv;  // the rank's (quad, peer) lists
     int ncell = -1, nghost = -1, nface = -1, dof = -1;
     uint64_t cfg_hash = 0;
     double sim_time = 0.0;
     int end_istep = -1;  // *istep at the end of the last call
+    HaloBuffers halo;
+
+    ~EvolveCache()
+    {
+        // at thread exit (ranks run as threads) or process exit; CUDA
+        // calls during the runtime's own teardown return an error and
+        // free nothing, which is harmless here
+        if (s) amrgpu_session_destroy(s);
+        halo.release();
+    }
 };
 
+// One cache per calling thread: ranks that run as threads of one process
+// each keep their own session.
 EvolveCache &cache()
 {
-    static EvolveCache c;
+    static thread_local EvolveCache c;
     return c;
 }
 
@@ -2099,12 +2168,114 @@ bool same_mesh(const EvolveCache &ec, int ncell, int nghost, int nface, int dof,
            std::memcmp(ec.geom.data(), geom, sizeof(double) * 12 * nc) == 0;
 }
 
-void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *ncell,
-            int *nghost, int *nface, int *dof, int *cell_info, int *face_info, int *nsend, int *nrecv, int *sizes,
-            double *geom, double *soln, int *istep, int *regrid, int *visualize, int *checkpoint,
-            int *evolve_solution, double *total_time, double *compute_time, double *residual_time)
+// The send / receive lists of a multi-rank call against what the GPU path
+// needs: send entries name local quads, ghost k is receive entry k (the
+// reference's driver stacks ghosts by owner rank after the local quads,
+// physics_mpi.c:54 relies on it), every record is 4 n^2 doubles.
+bool check_rank_lists(int ncell, int nghost, int nsend, int nrecv, const int *send, const int *recv,
+                      const int *sizes, int stride, int n)
 {
-    (void)sizes;
+    auto fail = [](const std::string &m) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "multi-rank evolve: " + m);
+        return false;
+    };
+    if (stride < 2) return fail("extern_mpi_comm_size < 2");
+    if (nsend < 0 || nrecv < 0 || nghost < 0) return fail("negative list size");
+    if (nrecv != nghost) return fail("nrecv != nghost");
+    if ((nsend > 0 && !send) || (nrecv > 0 && !recv) || !sizes) return fail("missing send / recv / sizes");
+    for (int k = 0; k < nsend; ++k)
+        if (send[stride * k] < 0 || send[stride * k] >= ncell)
+            return fail("send entry " + std::to_string(k) + " is not a local quad");
+    for (int k = 0; k < nrecv; ++k)
+        if (recv[stride * k] != ncell + k)
+            return fail("receive entry " + std::to_string(k) + " is not ghost quad " + std::to_string(ncell + k));
+    for (int q = 0; q < ncell + nghost; ++q)
+        if (sizes[q] != 4 * n * n) return fail("sizes[" + std::to_string(q) + "] != 4 n^2");
+    return true;
+}
+
+// A multi-rank segment of `steps` steps on an uploaded session: before
+// every stage the send-list records go to the peers and the ghost records
+// come back (pack on the device, one pinned copy each way, the caller's
+// exchange); after the upload and after every step the CFL step is the
+// MIN over ranks. Stops early once final_time is reached (every rank sees
+// the same time). Returns the steps taken, or -1 on error.
+int run_multirank(amrgpu_session *s, EvolveCache &ec, const amrgpu_comm_ops_t &ops, amrgpu_comm_t comm,
+                  int stride, int steps, double final_time, amrgpu_report_t &rep)
+{
+    const int nsend = int(ec.send.size()) / stride, nrecv = int(ec.recv.size()) / stride;
+    const size_t rec = size_t(4) * size_t(s->n) * size_t(s->n);
+    HaloBuffers &hb = ec.halo;
+    auto reduce_dt = [&]() -> bool {
+        unsigned long long *slot = amrgpu_session_dt_slot(s);
+        if (!cuda_ok(cudaMemcpyAsync(hb.h_dt, slot, sizeof(*slot), cudaMemcpyDeviceToHost, s->stream), "D2H dt") ||
+            !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
+            return false;
+        double v;
+        std::memcpy(&v, hb.h_dt, sizeof(v));
+        if (ops.allreduce(comm, &v, 0) != 0) {
+            set_error(AMRGPU_ERR_CUDA, "multi-rank evolve: the caller's MIN all-reduce failed");
+            return false;
+        }
+        std::memcpy(hb.h_dt, &v, sizeof(v));
+        return cuda_ok(cudaMemcpyAsync(slot, hb.h_dt, sizeof(*slot), cudaMemcpyHostToDevice, s->stream), "H2D dt") &&
+               cuda_ok(cudaStreamSynchronize(s->stream), "sync");
+    };
+    auto exchange = [&]() -> bool {
+        if (nsend > 0) {
+            if (amrgpu_session_halo_pack(s, 0, nsend, hb.d_send) != AMRGPU_OK ||
+                !cuda_ok(cudaMemcpyAsync(hb.h_send, hb.d_send, sizeof(double) * rec * size_t(nsend),
+                                         cudaMemcpyDeviceToHost, s->stream),
+                         "D2H halo"))
+                return false;
+        }
+        if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return false;
+        if (ops.exchange(comm, nsend, ec.send.data(), nrecv, ec.recv.data(), stride, int(rec), hb.h_send,
+                         hb.h_recv) != 0) {
+            set_error(AMRGPU_ERR_CUDA, "multi-rank evolve: the caller's ghost exchange failed");
+            return false;
+        }
+        if (nrecv > 0) {
+            if (!cuda_ok(cudaMemcpyAsync(hb.d_recv, hb.h_recv, sizeof(double) * rec * size_t(nrecv),
+                                         cudaMemcpyHostToDevice, s->stream),
+                         "H2D halo") ||
+                amrgpu_session_halo_unpack(s, 0, nrecv, hb.d_recv) != AMRGPU_OK)
+                return false;
+        }
+        return true;
+    };
+    if (!reduce_dt()) return -1;
+    int taken = 0;
+    for (int k = 0; k < steps; ++k) {
+        int st = 0, per = 0;
+        do {
+            if (!exchange() || amrgpu_session_step_stage(s, &st, &per) != AMRGPU_OK) return -1;
+        } while (st != per);
+        if (!reduce_dt()) return -1;
+        ++taken;
+        if (final_time > 0.0) {
+            if (amrgpu_session_sync(s, &rep) != AMRGPU_OK) return -1;
+            if (rep.time >= final_time) break;
+        }
+    }
+    if (amrgpu_session_sync(s, &rep) != AMRGPU_OK) return -1;
+    double nsq = s->h_scal.norm_sq;
+    if (ops.allreduce(comm, &nsq, 1) != 0) {
+        set_error(AMRGPU_ERR_CUDA, "multi-rank evolve: the caller's SUM all-reduce failed");
+        return -1;
+    }
+    rep.residual_norm = std::sqrt(nsq);
+    if (std::isnan(nsq)) rep.nan_detected = 1;
+    return taken;
+}
+
+void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *ncell,
+            int *nghost, int *nface, int *dof, int *cell_info, int *face_info, int *nsend, int *nrecv, int *send,
+            int *recv, int *sizes, double *geom, double *soln, int *istep, int *regrid, int *visualize,
+            int *checkpoint, int *evolve_solution, amrgpu_comm_t comm, double *total_time, double *compute_time,
+            double *residual_time)
+{
+    set_error(AMRGPU_OK, "");  // amrgpu_last_error() reports this call
     PhysicsConfig c;
     if (!resolve_config(from_reference_layer, c)) {
         *evolve_solution = 0;
@@ -2120,10 +2291,21 @@ void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields
         *evolve_solution = 0;
         return;
     }
-    if (*nsend != 0 || *nrecv != 0 || *nghost != 0) {
-        set_error(AMRGPU_ERR_UNSUPPORTED, "GPU path: one rank, no ghost exchange");
-        *evolve_solution = 0;
-        return;
+    const bool multirank = *nsend != 0 || *nrecv != 0 || *nghost != 0;
+    amrgpu_comm_ops_t ops{};
+    const int stride = c.extern_mpi_comm_size;
+    if (multirank) {
+        if (!comm_ops(ops)) {
+            set_error(AMRGPU_ERR_UNSUPPORTED,
+                      "multi-rank evolve (ghost quads) needs the caller's MPI operations: include "
+                      "physics_go_gpu.h in the MPI program or call amrgpu_set_comm_ops");
+            *evolve_solution = 0;
+            return;
+        }
+        if (!check_rank_lists(*ncell, *nghost, *nsend, *nrecv, send, recv, sizes, stride, *nelem_subgrid)) {
+            *evolve_solution = 0;
+            return;
+        }
     }
     c.dim = *dim;
     c.nfields = *nfields;
@@ -2138,7 +2320,13 @@ void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields
     // to the istep the last call returned, and not a fresh start at 0
     const bool continuing = ec.s && ec.cfg_hash == ch && *istep > 0 && *istep == ec.end_istep;
     if (!continuing) ec.sim_time = 0.0;
-    if (ec.cfg_hash != ch || !same_mesh(ec, *ncell, *nghost, *nface, *dof, cell_info, face_info, geom)) {
+    const size_t nsend_ints = multirank ? size_t(stride) * size_t(*nsend) : 0;
+    const size_t nrecv_ints = multirank ? size_t(stride) * size_t(*nrecv) : 0;
+    const bool same_lists = ec.send.size() == nsend_ints && ec.recv.size() == nrecv_ints &&
+                            (nsend_ints == 0 || std::memcmp(ec.send.data(), send, sizeof(int) * nsend_ints) == 0) &&
+                            (nrecv_ints == 0 || std::memcmp(ec.recv.data(), recv, sizeof(int) * nrecv_ints) == 0);
+    if (ec.cfg_hash != ch || !same_lists ||
+        !same_mesh(ec, *ncell, *nghost, *nface, *dof, cell_info, face_info, geom)) {
         if (ec.s) amrgpu_session_destroy(ec.s);
         ec.s = nullptr;
         amrgpu_mesh_t m{*ncell, *nghost, *nface, *dof, cell_info, face_info, geom};
@@ -2147,6 +2335,19 @@ void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields
         if (rc != AMRGPU_OK) {
             *evolve_solution = 0;
             return;
+        }
+        ec.send.assign(send, send + nsend_ints);
+        ec.recv.assign(recv, recv + nrecv_ints);
+        if (multirank) {
+            std::vector<int> quads(static_cast<size_t>(*nsend));
+            for (int k = 0; k < *nsend; ++k) quads[size_t(k)] = send[stride * k];
+            const size_t rec = size_t(4) * size_t(*nelem_subgrid) * size_t(*nelem_subgrid);
+            if (amrgpu_session_set_halo(s, quads.data(), *nsend) != AMRGPU_OK ||
+                !ec.halo.reserve(rec * size_t(std::max(*nsend, 1)), rec * size_t(std::max(*nrecv, 1)))) {
+                amrgpu_session_destroy(s);
+                *evolve_solution = 0;
+                return;
+            }
         }
         const size_t nc = size_t(*ncell + *nghost);
         ec.s = s;
@@ -2185,7 +2386,18 @@ void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields
     }
     amrgpu_report_t rep{};
     int taken = 0;
-    if (c.final_time > 0.0) {
+    if (multirank) {
+        taken = run_multirank(s, ec, ops, comm, stride, steps, c.final_time, rep);
+        if (taken < 0) {
+            *evolve_solution = 0;
+            ec.end_istep = -1;
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return;
+        }
+        if (c.final_time > 0.0 && rep.time >= c.final_time) *evolve_solution = 0;
+        steps = taken;
+    } else if (c.final_time > 0.0) {
         // the device clips dt at final_time; run in chunks and stop once reached
         int left = steps;
         while (left > 0) {
@@ -2224,10 +2436,23 @@ void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields
     *residual_time += ms * 1e-3;
     // physics_go.c:105-118 and physics_runtime_statistics.c:82-86
     int cells = *dof / *nfields;
-    double resid = rep.residual_norm / std::pow(double(cells), 1.0 / double(*dim));
-    if (!std::getenv("AMRGPU_QUIET")) {
+    double cmin = cells, cmax = cells, ctot = cells;
+    int rank = 0, nranks = 1;
+    if (multirank) {
+        // the same collectives on every rank, in the same order
+        ops.allreduce(comm, &cmin, 0);
+        ops.allreduce(comm, &cmax, 2);
+        ops.allreduce(comm, &ctot, 1);
+        double one = 1.0;
+        ops.allreduce(comm, &one, 1);
+        nranks = int(one);
+        ops.rank(comm, &rank);
+    }
+    double resid = rep.residual_norm / std::pow(ctot, 1.0 / double(*dim));
+    if (!std::getenv("AMRGPU_QUIET") && rank == 0) {
         std::printf("[ amr ] istep: %d\n", *istep);
-        std::printf("[ amr ] processor dofs (min,max,avg,total): %d, %d, %d, %d \n", cells, cells, cells, cells);
+        std::printf("[ amr ] processor dofs (min,max,avg,total): %d, %d, %d, %d \n", int(cmin), int(cmax),
+                    int(ctot / double(nranks)), int(ctot));
         std::printf("[physics] iterations: %d, gpu time: %e, residual: %1.15e\n", steps, ms * 1e-3, resid);
         int nres = c.time_scheme;
         if (steps > 0 && cells > 0)
@@ -2261,12 +2486,9 @@ void hpc_amr_evolve_solver(int *dim, int *unstructured, int *nfields, int *nsub_
                            int *visualize, int *checkpoint, int *evolve_solution, amrgpu_comm_t mpicomm_ext,
                            double *total_time, double *compute_time, double *residual_time)
 {
-    (void)send;
-    (void)recv;
-    (void)mpicomm_ext;
     evolve(false, dim, unstructured, nfields, nsub_elem, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
-           sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, total_time, compute_time,
-           residual_time);
+           send, recv, sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, mpicomm_ext,
+           total_time, compute_time, residual_time);
 }
 
 void physics_go_gpu(int *dim, int *unstructured, int *nfields, int *nelem_subgrid, int *ncell, int *nghost,
@@ -2275,12 +2497,24 @@ void physics_go_gpu(int *dim, int *unstructured, int *nfields, int *nelem_subgri
                     int *checkpoint, int *evolve_solution, amrgpu_comm_t mpicomm_ext, double *total_time,
                     double *compute_time, double *residual_time)
 {
-    (void)send;
-    (void)recv;
-    (void)mpicomm_ext;
     evolve(true, dim, unstructured, nfields, nelem_subgrid, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
-           sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, total_time, compute_time,
-           residual_time);
+           send, recv, sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, mpicomm_ext,
+           total_time, compute_time, residual_time);
+}
+
+int amrgpu_set_comm_ops(const amrgpu_comm_ops_t *ops)
+{
+    if (ops && (!ops->rank || !ops->exchange || !ops->allreduce)) return AMRGPU_ERR_ARG;
+    std::lock_guard<std::mutex> lk(g_comm_mu);
+    if (ops) g_comm_ops = *ops;
+    g_comm_set = ops != nullptr;
+    return AMRGPU_OK;
+}
+
+int amrgpu_has_comm_ops(void)
+{
+    amrgpu_comm_ops_t o;
+    return comm_ops(o) ? 1 : 0;
 }
 
 }  // extern "C"

@@ -88,11 +88,16 @@ void hpc_amr_refine_operator_2d(int *unstructured, int *nfields, int *nsub_elem,
  *     sets those flags, advances *istep, copies soln back;
  *   - accumulates *total_time, *compute_time, *residual_time (seconds).
  * Device buffers persist across calls and are rebuilt when the mesh
- * (cell_info / face_info / geom) changes. Errors are reported through
+ * (cell_info / face_info / geom) changes. Each call first clears the
+ * calling thread's error; errors are reported through
  * amrgpu_last_error(); a non-finite residual sets AMRGPU_ERR_NONFINITE (and
  * exits with code 3 when AMRGPU_ABORT_ON_NAN=1, as the reference's
- * MPI_Abort(comm,3) does). Only 2D structured meshes on one rank
- * (nsend == nrecv == 0) are accepted. */
+ * MPI_Abort(comm,3) does). Only 2D structured meshes are accepted. A rank
+ * with ghost quads (nghost, nsend, nrecv > 0) needs the caller's MPI
+ * operations (amrgpu_comm_ops_t below) and exchanges ghost records before
+ * every stage; without them the call is refused (AMRGPU_ERR_UNSUPPORTED).
+ * Device state is kept per calling thread (ranks run as threads each get
+ * their own). */
 void hpc_amr_evolve_solver(int *dim, int *unstructured, int *nfields, int *nsub_elem,
                            int *ncell, int *nghost, int *nface, int *dof, int *cell_info,
                            int *face_info, int *nsend, int *nrecv, int *send, int *recv,
@@ -182,6 +187,41 @@ int amrgpu_config_set(const amrgpu_config_t *cfg);
  * and so does this call. The library's extensions (form, final_time, IC
  * parameters) always come from its own configuration. */
 int amrgpu_evolve_config(int from_reference_layer, amrgpu_config_t *out);
+
+/* ---------------- the caller's MPI, for multi-rank evolve calls ----------
+ * hpc_amr_evolve_solver / physics_go_gpu with ghost quads (nghost, nsend,
+ * nrecv > 0) run the reference's multi-rank step on the GPU: before every
+ * stage the records of the send-list quads are packed on the device and
+ * moved to the ranks that hold them as ghosts (physics_mpi_real_to_ghost,
+ * physics_mpi.c:47-122, called by every stage of rk_time_integrators.c), the
+ * CFL step is the MIN over ranks (MPI_Allreduce,
+ * physics_runge_kutta_interface.c:96,149,205,262,316) and the squared
+ * residual norm the SUM (rk_time_integrators.c:74,162,274). This library
+ * links no MPI, so the caller supplies these three operations once.
+ * physics_go_gpu.h does that automatically in the reference's -D_GPU_
+ * build (a load-time constructor compiled against the caller's <mpi.h>);
+ * other callers call amrgpu_set_comm_ops themselves. Every rank of a call
+ * must make the same calls (they are collectives). Ghost quads must follow
+ * the local quads in receive-list order (recv[k*stride] == ncell + k, as
+ * the reference's AMR driver numbers them, amr_external.c). */
+typedef struct {
+    /* *rank = the caller's rank in comm; 0 on success. */
+    int (*rank)(amrgpu_comm_t comm, int *rank);
+    /* Moves whole-quad records: sendbuf holds record_doubles doubles per
+     * send-list entry, in list order; recvbuf receives one record per
+     * receive-list entry, in list order. Entries are (quad, peer rank)
+     * pairs `stride` ints apart, grouped by peer. 0 on success. */
+    int (*exchange)(amrgpu_comm_t comm, int nsend, const int *send, int nrecv, const int *recv, int stride,
+                    int record_doubles, const double *sendbuf, double *recvbuf);
+    /* In-place all-reduce of one double over comm: op 0 MIN, 1 SUM, 2 MAX.
+     * 0 on success. */
+    int (*allreduce)(amrgpu_comm_t comm, double *value, int op);
+} amrgpu_comm_ops_t;
+
+/* Installs (copies) the operations; NULL removes them. Process-wide. */
+int amrgpu_set_comm_ops(const amrgpu_comm_ops_t *ops);
+/* 1 when operations are installed. */
+int amrgpu_has_comm_ops(void);
 
 /* ---------------- device-resident sessions ---------------- */
 typedef struct amrgpu_session amrgpu_session_t;

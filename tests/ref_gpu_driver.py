@@ -14,6 +14,14 @@ loaded as a dependency of the reference's physics layer, not before it.
     python tests/ref_gpu_driver.py config <workdir>
     python tests/ref_gpu_driver.py evolve <workdir> <golden.npz>
     python tests/ref_gpu_driver.py unconfigured <workdir> <golden.npz>
+    python tests/ref_gpu_driver.py multirank <workdir> <case.npz>
+
+multirank: the same layer built over the multi-rank MPI stand-in
+(oracle/_ref/libref_physics_gpu_mt.so): P ranks as P threads, each entering
+physics_evolve_interface -> physics_go_gpu with its shard (local quads, ghost
+quads, send / recv lists); the ghost exchange and the reductions go through
+the MPI operations physics_go_gpu.h installs. <case.npz> holds the shards and
+every rank's expected local state.
 
 <workdir> must hold input.physics. Prints one JSON line.
 """
@@ -27,10 +35,13 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 REF_GPU = os.path.join(ROOT, "oracle", "_ref", "libref_physics_gpu.so")
+REF_GPU_MT = os.path.join(ROOT, "oracle", "_ref", "libref_physics_gpu_mt.so")
 LIBAMRGPU = os.path.join(ROOT, "amr-demo_b200", "lib", "libamrgpu.so")
 sys.path.insert(0, os.path.join(ROOT, "amr-demo_b200"))
+sys.path.insert(0, ROOT)
 
 from amrgpu._lib import ConfigStruct  # noqa: E402  (no library is loaded by this import)
+from oracle.oracle import MtRank  # noqa: E402  (ctypes layout only; loads no library)
 
 i32p = C.POINTER(C.c_int)
 f64p = C.POINTER(C.c_double)
@@ -106,6 +117,53 @@ def evolve(L, z):
                   "evolve_solution": evo.value}
 
 
+def multirank(z):
+    """oracle_mt_evolve over the shards in z; per-rank comparison of the
+    local quads with the expected state."""
+    L = C.CDLL(REF_GPU_MT)  # loads libamrgpu.so as its dependency
+    n, P = int(z["n"]), int(z["nranks"])
+    initialize(L, n, float(z["coarse_grid_h"]))
+    L.oracle_mt_evolve.restype = C.c_int
+    L.oracle_mt_evolve.argtypes = [C.c_int, C.c_int, C.POINTER(MtRank)]
+    ranks = (MtRank * P)()
+    keep = []
+    for r in range(P):
+        g = lambda k: z[f"r{r}_{k}"]  # noqa: E731
+        # the reference reads cell_info[3*(-1)] for absent neighbours
+        # (physics_rhs_structured.c:97-128): 16 ints of -1 in front
+        cbuf = np.full(len(g("cell_info")) + 16, -1, np.int32)
+        cbuf[16:] = g("cell_info")
+        ci = cbuf[16:]
+        fi = np.ascontiguousarray(g("face_info"), np.int32)
+        geom = np.ascontiguousarray(g("geom"), np.float64)
+        send = np.ascontiguousarray(g("send"), np.int32)
+        recv = np.ascontiguousarray(g("recv"), np.int32)
+        sizes = np.ascontiguousarray(g("sizes"), np.int32)
+        st = np.ascontiguousarray(g("state0"), np.float64).copy()
+        R = ranks[r]
+        R.ncell, R.nghost, R.nface, R.dof = int(g("ncell")), int(g("nghost")), int(g("nface")), int(g("dof"))
+        R.nsend, R.nrecv = len(send) // 2, len(recv) // 2
+        if R.nsend == 0:
+            send = np.zeros(2, np.int32)
+        if R.nrecv == 0:
+            recv = np.zeros(2, np.int32)
+        R.cell_info, R.face_info, R.send, R.recv, R.sizes = ip(ci), ip(fi), ip(send), ip(recv), ip(sizes)
+        R.geom, R.soln = dp(geom), dp(st)
+        R.istep, R.evolve_solution = 0, 1
+        keep.append((cbuf, fi, geom, send, recv, sizes, st))
+    rc = L.oracle_mt_evolve(P, n, ranks)
+    out = {"rc": rc, "error": L.amrgpu_last_error(), "istep": [], "evolve_solution": [], "bitwise": [],
+           "maxdiff": []}
+    for r in range(P):
+        got = keep[r][6][: int(z[f"r{r}_dof"])]
+        want = z[f"r{r}_expected"]
+        out["istep"].append(ranks[r].istep)
+        out["evolve_solution"].append(ranks[r].evolve_solution)
+        out["bitwise"].append(bool(np.array_equal(got, want)))
+        out["maxdiff"].append(float(np.abs(got - want).max()) if len(want) else 0.0)
+    return out
+
+
 def main():
     mode, workdir = sys.argv[1], sys.argv[2]
     os.environ.setdefault("AMRGPU_QUIET", "1")
@@ -120,6 +178,9 @@ def main():
         cfg = ConfigStruct()
         out["evolve_config_rc"] = L.amrgpu_evolve_config(0, C.byref(cfg))
         print(json.dumps(out))
+        return
+    if mode == "multirank":
+        print(json.dumps(multirank(np.load(sys.argv[3]))))
         return
     L = C.CDLL(REF_GPU)  # loads libamrgpu.so as its dependency
     L.amrgpu_evolve_config.argtypes = [C.c_int, C.POINTER(ConfigStruct)]
