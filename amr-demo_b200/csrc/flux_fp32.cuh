@@ -130,58 +130,141 @@ __device__ __forceinline__ void cell_prims_fp32(const double q[4], float P[8])
     P[7] = rv;
 }
 
-// flux_roe_2d on FP32 records. Axis-aligned faces (every face of a brick
-// mesh) take the rotated form: with n = (h,0) the normal velocity is u and
-// the tangential-correction terms of rows 2/3 reduce to 0 and
-// rhobar*(v_R - v_L); Mcoeff = 1/(1+|un/a|) = a/(a+|un|). Four MUFU
-// operations per face (three approximate reciprocals, one reciprocal square
-// root). Other normals use roe_flux_fp32 on conserved states.
-// Axis-aligned face with a positive normal of length h, direction known at
-// compile time (DIR 0: n = (h,0), DIR 1: n = (0,h)): the same algebra as
-// roe_flux_prim_fp32 without any run-time selects.
+// Lane arithmetic for the axis-aligned flux below: one face per lane
+// (float) or two faces per lane in packed pairs (float2, sm_100's paired
+// FP32 add / multiply / fused multiply-add, one instruction for both
+// halves). Every operation is an explicitly rounded intrinsic, so the
+// compiler cannot contract or reorder it, and a float2 half gets exactly
+// the bits the float version gives for the same inputs. Min, max, absolute
+// value and the SFU approximations act per half.
+struct LaneF1 {
+    using T = float;
+    static __device__ __forceinline__ T c(float v) { return v; }
+    static __device__ __forceinline__ T add(T a, T b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ T sub(T a, T b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ T mul(T a, T b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ T fma(T a, T b, T d) { return __fmaf_rn(a, b, d); }
+    static __device__ __forceinline__ T max(T a, T b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ T min(T a, T b) { return fminf(a, b); }
+    static __device__ __forceinline__ T abs(T a) { return fabsf(a); }
+    static __device__ __forceinline__ T rcp(T a) { return frcp(a); }
+    static __device__ __forceinline__ T rsqrt(T a) { return frsqrt(a); }
+};
+
+struct LaneF2 {
+    using T = float2;
+    static __device__ __forceinline__ T c(float v) { return make_float2(v, v); }
+    static __device__ __forceinline__ T add(T a, T b) { return __fadd2_rn(a, b); }
+    // a - b = RN(a + (-1) b): the same single rounding as a subtraction
+    static __device__ __forceinline__ T sub(T a, T b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+    static __device__ __forceinline__ T mul(T a, T b) { return __fmul2_rn(a, b); }
+    static __device__ __forceinline__ T fma(T a, T b, T d) { return __ffma2_rn(a, b, d); }
+    static __device__ __forceinline__ T max(T a, T b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+    static __device__ __forceinline__ T min(T a, T b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+    static __device__ __forceinline__ T abs(T a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+    static __device__ __forceinline__ T rcp(T a) { return make_float2(frcp(a.x), frcp(a.y)); }
+    static __device__ __forceinline__ T rsqrt(T a) { return make_float2(frsqrt(a.x), frsqrt(a.y)); }
+};
+
+// One side of an axis-aligned face in the face's frame: normal and
+// tangential velocity (n, t) and momentum (mn, mt); (u, v) for a face with
+// normal +x, (v, u) for normal +y.
+template <typename T>
+struct AxisSide {
+    T rho, n, t, p, H, sr, mn, mt;
+};
+
+// flux_roe_2d (flux_2d_module.F90:63-182) for a face with positive normal
+// of length h, L on the low side, in the face's frame. The algebra is
+// arranged for fused operations: with hinv = h/(b1-b2) the flux rows are
+// h*(b1 fl - b2 fr)/(b1-b2) + h*bcoeff*jump - h*bM*corr
+//   = hb1 fl - hb2 fr + hbc jump - hbM corr,
+// hb1 = b1 hinv, hb2 = b2 hinv, hbc = b1 hb2 = h bcoeff and
+// hbM = hbc abar/(abar + |un|) = h bM (Mcoeff = 1/(1+|un/a|)); the wave
+// speeds b1 = max(max(un, unr) + a, 0) and b2 = min(min(un, unl) - a, 0)
+// equal the reference's max/min of the sums (rounding is monotone); 1/a^2
+// is the square of the SFU's 1/sqrt(a^2). Out: mass, normal-momentum,
+// tangential-momentum and energy rows.
+template <typename Op>
+__device__ __forceinline__ void roe_flux_rot(const AxisSide<typename Op::T> &L, const AxisSide<typename Op::T> &R,
+                                             typename Op::T h, typename Op::T out[4])
+{
+    using T = typename Op::T;
+    const T inv = Op::rcp(Op::add(L.sr, R.sr));
+    const T rhobar = Op::mul(L.sr, R.sr);
+    const T nbar = Op::mul(Op::fma(L.n, L.sr, Op::mul(R.n, R.sr)), inv);
+    const T tbar = Op::mul(Op::fma(L.t, L.sr, Op::mul(R.t, R.sr)), inv);
+    const T Hbar = Op::mul(Op::fma(L.H, L.sr, Op::mul(R.H, R.sr)), inv);
+    const T q2 = Op::fma(nbar, nbar, Op::mul(tbar, tbar));
+    const T a2 = Op::fma(Op::c(-0.2f), q2, Op::mul(Op::c(0.4f), Hbar));
+    const T ra = Op::rsqrt(a2);
+    const T abar = Op::mul(a2, ra);
+    const T b1 = Op::max(Op::add(Op::max(nbar, R.n), abar), Op::c(0.0f));
+    const T b2 = Op::min(Op::sub(Op::min(nbar, L.n), abar), Op::c(0.0f));
+    const T hinv = Op::mul(h, Op::rcp(Op::sub(b1, b2)));
+    const T hb1 = Op::mul(b1, hinv), hb2 = Op::mul(b2, hinv);
+    const T hbc = Op::mul(b1, hb2);
+    const T drho = Op::sub(R.rho, L.rho);
+    const T delta1 = Op::fma(Op::sub(L.p, R.p), Op::mul(ra, ra), drho);
+    const T hbM = Op::mul(Op::mul(hbc, abar), Op::rcp(Op::add(abar, Op::abs(nbar))));
+    const T nhbM = Op::sub(Op::c(0.0f), hbM);
+    auto row = [&](T fl, T fr, T jump, T corr) {
+        return Op::fma(hbc, jump, Op::fma(nhbM, corr, Op::sub(Op::mul(hb1, fl), Op::mul(hb2, fr))));
+    };
+    const T rHl = Op::mul(L.rho, L.H), rHr = Op::mul(R.rho, R.H);
+    out[0] = row(L.mn, R.mn, drho, delta1);
+    out[1] = row(Op::fma(L.mn, L.n, L.p), Op::fma(R.mn, R.n, R.p), Op::sub(R.mn, L.mn), Op::mul(delta1, nbar));
+    out[2] = row(Op::mul(L.mn, L.t), Op::mul(R.mn, R.t), Op::sub(R.mt, L.mt),
+                 Op::fma(delta1, tbar, Op::mul(rhobar, Op::sub(R.t, L.t))));
+    out[3] = row(Op::mul(rHl, L.n), Op::mul(rHr, R.n), Op::sub(rHr, rHl),
+                 Op::fma(delta1, Hbar, Op::mul(rhobar, Op::sub(R.H, L.H))));
+}
+
+// A record [rho, u, v, p, H, sqrt(rho), rho u, rho v] as one side of a face
+// with normal +x (DIR 0) or +y (DIR 1).
+template <int DIR>
+__device__ __forceinline__ AxisSide<float> axis_side(const float *P)
+{
+    return AxisSide<float>{P[0], P[DIR == 0 ? 1 : 2], P[DIR == 0 ? 2 : 1], P[3],
+                           P[4], P[5], P[DIR == 0 ? 6 : 7], P[DIR == 0 ? 7 : 6]};
+}
+
+// The flux of an axis-aligned face with a positive normal of length h,
+// direction known at compile time (DIR 0: n = (h,0), DIR 1: n = (0,h)).
 template <int DIR>
 __device__ __forceinline__ void roe_flux_axis_fp32(const float *L, const float *R, float h, float flux[4])
 {
-    const float rhol = L[0], ul = L[1], vl = L[2], pl = L[3], Hl = L[4], srl = L[5];
-    const float rhor = R[0], ur = R[1], vr = R[2], pr = R[3], Hr = R[4], srr = R[5];
-    const float unl = DIR == 0 ? ul : vl;
-    const float unr = DIR == 0 ? ur : vr;
-    const float inv = frcp(__fadd_rn(srl, srr));
-    const float rhobar = __fmul_rn(srl, srr);
-    const float ubar = __fmul_rn(__fmaf_rn(ul, srl, __fmul_rn(ur, srr)), inv);
-    const float vbar = __fmul_rn(__fmaf_rn(vl, srl, __fmul_rn(vr, srr)), inv);
-    const float Hbar = __fmul_rn(__fmaf_rn(Hl, srl, __fmul_rn(Hr, srr)), inv);
-    const float a2 =
-        __fmul_rn(0.4f, __fsub_rn(Hbar, __fmul_rn(0.5f, __fmaf_rn(ubar, ubar, __fmul_rn(vbar, vbar)))));
-    const float ra = frsqrt(a2);  // 1/abar: abar = a2/abar, 1/a2 = ra^2
-    const float abar = __fmul_rn(a2, ra);
-    const float unbar = DIR == 0 ? ubar : vbar;
-    const float b1 = fmaxf(fmaxf(__fadd_rn(unbar, abar), __fadd_rn(unr, abar)), 0.0f);
-    const float b2 = fminf(fminf(__fsub_rn(unbar, abar), __fsub_rn(unl, abar)), 0.0f);
-    const float inv_db = frcp(__fsub_rn(b1, b2));
-    const float bcoeff = __fmul_rn(__fmul_rn(b1, b2), inv_db);
-    const float drho = __fsub_rn(rhor, rhol);
-    const float delta1 = __fsub_rn(drho, __fmul_rn(__fsub_rn(pr, pl), __fmul_rn(ra, ra)));
-    const float bM = __fmul_rn(__fmul_rn(bcoeff, abar), frcp(__fadd_rn(abar, fabsf(unbar))));
-    const float ml = DIR == 0 ? L[6] : L[7];
-    const float mr = DIR == 0 ? R[6] : R[7];
-    const float rHl = __fmul_rn(rhol, Hl), rHr = __fmul_rn(rhor, Hr);
-    const float hb1 = __fmul_rn(__fmul_rn(h, b1), inv_db), hb2 = __fmul_rn(__fmul_rn(h, b2), inv_db);
-    // flux = hb1 * fl - hb2 * fr + h * d with d = bcoeff * jump - bM * corr
-    auto row = [&](float fl, float fr, float jump, float corr) {
-        const float d = __fsub_rn(__fmul_rn(bcoeff, jump), __fmul_rn(bM, corr));
-        return __fmaf_rn(h, d, __fsub_rn(__fmul_rn(hb1, fl), __fmul_rn(hb2, fr)));
+    float o[4];
+    roe_flux_rot<LaneF1>(axis_side<DIR>(L), axis_side<DIR>(R), h, o);
+    flux[0] = o[0];
+    flux[DIR == 0 ? 1 : 2] = o[1];
+    flux[DIR == 0 ? 2 : 1] = o[2];
+    flux[3] = o[3];
+}
+
+// A cell's two interior faces at once in packed pairs: its x-face (low
+// side Lx, normal +x, length hx_face) in the first half and its y-face (low
+// side Ly, normal +y, length hy_face) in the second, both with high side P.
+// Each half carries exactly the bits roe_flux_axis_fp32 gives that face.
+__device__ __forceinline__ void roe_flux_axis_pair_fp32(const float *Lx, const float *Ly, const float *P,
+                                                        float hx_face, float hy_face, float fx[4], float fy[4])
+{
+    const AxisSide<float> lx = axis_side<0>(Lx), ly = axis_side<1>(Ly), rx = axis_side<0>(P), ry = axis_side<1>(P);
+    auto pair = [](const AxisSide<float> &a, const AxisSide<float> &b) {
+        return AxisSide<float2>{make_float2(a.rho, b.rho), make_float2(a.n, b.n), make_float2(a.t, b.t),
+                                make_float2(a.p, b.p),     make_float2(a.H, b.H), make_float2(a.sr, b.sr),
+                                make_float2(a.mn, b.mn),   make_float2(a.mt, b.mt)};
     };
-    const float tang = DIR == 0 ? __fmul_rn(rhobar, __fsub_rn(vr, vl)) : __fmul_rn(rhobar, __fsub_rn(ur, ul));
-    flux[0] = row(ml, mr, drho, delta1);
-    flux[1] = row(DIR == 0 ? __fmaf_rn(ml, ul, pl) : __fmul_rn(ml, ul),
-                  DIR == 0 ? __fmaf_rn(mr, ur, pr) : __fmul_rn(mr, ur), __fsub_rn(R[6], L[6]),
-                  DIR == 0 ? __fmul_rn(delta1, ubar) : __fmaf_rn(delta1, ubar, tang));
-    flux[2] = row(DIR == 0 ? __fmul_rn(ml, vl) : __fmaf_rn(ml, vl, pl),
-                  DIR == 0 ? __fmul_rn(mr, vr) : __fmaf_rn(mr, vr, pr), __fsub_rn(R[7], L[7]),
-                  DIR == 0 ? __fmaf_rn(delta1, vbar, tang) : __fmul_rn(delta1, vbar));
-    flux[3] = row(__fmul_rn(rHl, unl), __fmul_rn(rHr, unr), __fsub_rn(rHr, rHl),
-                  __fmaf_rn(delta1, Hbar, __fmul_rn(rhobar, __fsub_rn(Hr, Hl))));
+    float2 o[4];
+    roe_flux_rot<LaneF2>(pair(lx, ly), pair(rx, ry), make_float2(hx_face, hy_face), o);
+    fx[0] = o[0].x;
+    fx[1] = o[1].x;
+    fx[2] = o[2].x;
+    fx[3] = o[3].x;
+    fy[0] = o[0].y;
+    fy[2] = o[1].y;
+    fy[1] = o[2].y;
+    fy[3] = o[3].y;
 }
 
 __device__ __forceinline__ void roe_flux_prim_fp32(const float *L, const float *R, float n0, float n1,

@@ -18,17 +18,19 @@
 //           (a cell adds -F at its low face and +F at its high face);
 //   sweep   R steps; at step t lane (i, h) loads cell (i, Rh+t) straight
 //           from HBM (N lanes read 8N contiguous bytes per field), builds
-//           its record in registers, computes the x-face flux at i-1/2 with
-//           the left neighbour's record taken by a warp shuffle, hands that
-//           flux to lane i-1 (which needs it as its i+1/2 face) by a second
-//           shuffle, and the y-face flux at j-1/2 from the record it kept of
-//           the row below. Row j-1 is then complete: -F(x-1/2) +F(x+1/2)
+//           its record in registers, and evaluates the x-face flux at i-1/2
+//           (the left neighbour's record taken by a warp shuffle) and the
+//           y-face flux at j-1/2 (the record it kept of the row below)
+//           together, one face per half of sm_100's paired FP32
+//           instructions; it hands the x-face flux to lane i-1 (which needs
+//           it as its i+1/2 face) by a second shuffle. Row j-1 is then
+//           complete: -F(x-1/2) +F(x+1/2)
 //           -F(y-1/2) +F(y+1/2), summed in FP64, divided by the volume,
 //           negated, and the stage update is written.
 //
-// Per cell-stage this is about 2.1 flux evaluations, one record, 12
-// shuffles and the update: no per-face index decoding, no record stores and
-// reloads, no barrier between the record, face and cell phases.
+// Per cell-stage this is about 1.1 (packed) flux evaluations, one record,
+// 12 shuffles and the update: no per-face index decoding, no record stores
+// and reloads, no barrier between the record, face and cell phases.
 #pragma once
 
 #include "flux_fp32.cuh"
@@ -195,11 +197,17 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
             }
             float P[8];
             cell_prims_fp32(q4, P);
-            // x-face at i-1/2 (lane 0's left face is an edge face)
-            float L[8], fx[4], fxr[4];
+            // the x-face at i-1/2 (lane 0's left face is an edge face) and
+            // the y-face at j-1/2 in one packed evaluation (the first row's
+            // y-face is an edge or the row R-1/R face: its half is unused)
+            float L[8], fx[4], fy[4], fxr[4];
 #pragma unroll
             for (int k = 0; k < 8; ++k) L[k] = __shfl_up_sync(FULL, P[k], 1, N);
-            roe_flux_axis_fp32<0>(L, P, fhy, fx);
+            if (t == 0) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) below[k] = P[k];
+            }
+            roe_flux_axis_pair_fp32(L, below, P, fhy, fhx, fx, fy);
 #pragma unroll
             for (int f = 0; f < 4; ++f) fxr[f] = __shfl_down_sync(FULL, fx[f], 1, N);
             double xp[4];
@@ -215,8 +223,6 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
 #pragma unroll
                 for (int f = 0; f < 4; ++f) gy[f] = h == 0 ? sedge[w][sub][2][i][f] : sedge[w][sub][4][i][f];
             } else {
-                float fy[4];
-                roe_flux_axis_fp32<1>(below, P, fhx, fy);
 #pragma unroll
                 for (int f = 0; f < 4; ++f) gy[f] = (double)fy[f];
                 finish(j - 1, gy);
