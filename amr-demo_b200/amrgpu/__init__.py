@@ -101,9 +101,13 @@ class Config:
 
 # --------------------------------------------------------------------- mesh
 class Mesh:
-    """Flat arrays of one mesh epoch, as src/amr/src/amr_external.c builds them."""
+    """Flat arrays of one mesh epoch, as src/amr/src/amr_external.c builds them.
 
-    def __init__(self, n, cell_info, face_info, geom, nface, dof, nghost=0):
+    ``sizes`` (optional): the patch size of every quad for a mesh that mixes
+    8x8 and 16x16 patches; cell_info[3q+2] is then the running sum of
+    4 n^2 (the reference's own offset layout) and ``n`` the largest size."""
+
+    def __init__(self, n, cell_info, face_info, geom, nface, dof, nghost=0, sizes=None):
         self.n = int(n)
         self.cell_info = np.ascontiguousarray(cell_info, dtype=np.int32)
         self.face_info = np.ascontiguousarray(face_info, dtype=np.int32)
@@ -112,10 +116,17 @@ class Mesh:
         self.dof = int(dof)
         self.nghost = int(nghost)
         self.ncell = len(self.cell_info) // 3 - self.nghost
+        self.sizes = None if sizes is None else np.ascontiguousarray(sizes, dtype=np.int32)
 
     @property
     def ncells(self):
+        if self.sizes is not None:
+            return int((self.sizes.astype(np.int64) ** 2).sum())
         return self.ncell * self.n * self.n
+
+    def offsets(self):
+        """First cell of every quad (cell_info[2] / 4)."""
+        return (self.cell_info[2::3][: self.ncell] // NFIELDS).astype(np.int64)
 
     def struct(self):
         return MeshStruct(self.ncell, self.nghost, self.nface, self.dof, ip(self.cell_info),
@@ -294,10 +305,35 @@ class Forest:
         return Mesh(n, cell_info, face_info[: 11 * nface.value].copy(), geom, nface.value, dof.value)
 
     def initialize(self, n):
-        """Initial condition of every quad from the global configuration (AoS)."""
-        soln = np.zeros(NFIELDS * n * n * self.num_quads, np.float64)
-        check(lib().amrgpu_forest_initialize(self._f, int(n), dp(soln)), "forest_initialize")
-        return soln
+        """Initial condition of every quad from the global configuration (AoS).
+        ``n`` may be a per-quad array of patch sizes (a mixed mesh): every
+        quad then gets its own size's initial patch, in mesh order."""
+        if np.ndim(n) == 0:
+            soln = np.zeros(NFIELDS * int(n) * int(n) * self.num_quads, np.float64)
+            check(lib().amrgpu_forest_initialize(self._f, int(n), dp(soln)), "forest_initialize")
+            return soln
+        sizes = np.asarray(n, np.int64)
+        per = {int(k): self.initialize(int(k)).reshape(self.num_quads, -1) for k in np.unique(sizes)}
+        return np.concatenate([per[int(k)][q] for q, k in enumerate(sizes)]) if len(sizes) else np.zeros(0)
+
+    def patch_sizes(self, size_of_level):
+        """Per-quad patch sizes from a level -> size rule (a callable, or a
+        sequence indexed by level)."""
+        _, level, _, _ = self.quads()
+        f = size_of_level if callable(size_of_level) else (lambda lv: size_of_level[lv])
+        return np.array([int(f(int(lv))) for lv in level], np.int32)
+
+    def mesh_mixed(self, sizes):
+        """The mesh with per-quad patch sizes (8 or 16): the forest's arrays
+        with cell_info[3q+2] = 4 * (cells of the quads before q) and dof the
+        sum of 4 n^2."""
+        sizes = np.asarray(sizes, np.int32)
+        m = self.mesh(int(sizes.max()) if len(sizes) else 16)
+        cells = sizes.astype(np.int64) ** 2
+        off = np.concatenate([[0], np.cumsum(cells)[:-1]]) if len(cells) else np.zeros(0, np.int64)
+        ci = m.cell_info.copy()
+        ci[2::3] = (NFIELDS * off).astype(np.int32)
+        return Mesh(m.n, ci, m.face_info, m.geom, m.nface, int(NFIELDS * cells.sum()), sizes=sizes)
 
 
 # --------------------------------------------------------------------- session

@@ -104,14 +104,21 @@ def host_tags(n, rho_tol, method=5):
     return tag
 
 
-def regrid(forest, session, n, min_level, max_level, config=None, form=None, device_mesh=True):
+def regrid(forest, session, n, min_level, max_level, config=None, form=None, device_mesh=True, size_of_level=None):
     """One regrid of the session in place (its mesh and state follow the
     forest); returns the session. device_mesh: the 2:1 balance passes and
     the quad descriptors run on the GPU (Forest.balance(session=...),
     Session.regrid_forest); otherwise the host balances, lists the mesh
-    arrays and the session decodes them."""
+    arrays and the session decodes them. size_of_level: mixed patch sizes
+    (a level -> 8 / 16 rule, Forest.patch_sizes): the host path, with the
+    mesh of Forest.mesh_mixed."""
     tags = session.tag()
-    if device_mesh:
+    if size_of_level is not None:
+        forest.adapt(tags, 1, 0, min_level, max_level)
+        forest.balance()
+        kind, src = forest.remap()
+        session.regrid(forest.mesh_mixed(forest.patch_sizes(size_of_level)), kind, src)
+    elif device_mesh:
         forest.adapt(tags, 1, 0, min_level, max_level)
         session.balance_regrid(forest)
     else:
@@ -128,12 +135,20 @@ def regrid(forest, session, n, min_level, max_level, config=None, form=None, dev
     return session
 
 
-def run(forest, soln, n, config, form, final_time, regrid_interval, min_level, max_level, max_steps=10 ** 7):
+def run(forest, soln, n, config, form, final_time, regrid_interval, min_level, max_level, max_steps=10 ** 7,
+        size_of_level=None):
     """Evolve to final_time with a regrid every regrid_interval steps.
+    size_of_level: mixed 8x8 / 16x16 patches by level (soln is then
+    ignored: the initial state is evaluated at each quad's size).
     Returns (session, stats)."""
     config["final_time"] = final_time
     config.apply()
-    mesh = forest.mesh(n)
+    if size_of_level is not None:
+        sizes = forest.patch_sizes(size_of_level)
+        mesh = forest.mesh_mixed(sizes)
+        soln = forest.initialize(sizes)
+    else:
+        mesh = forest.mesh(n)
     s = Session(mesh, config, form=form)
     s.upload(soln)
     steps = 0
@@ -156,7 +171,7 @@ def run(forest, soln, n, config, form, final_time, regrid_interval, min_level, m
             break
         if time_now >= final_time:
             break
-        regrid(forest, s, n, min_level, max_level)
+        regrid(forest, s, n, min_level, max_level, size_of_level=size_of_level)
         regrids += 1
         t_regrid += time.perf_counter() - t1
     return s, {"steps": steps, "time": time_now, "cell_updates": cell_updates, "solve_s": t_solve,

@@ -33,6 +33,29 @@ struct QuadDesc {
 };
 static_assert(sizeof(QuadDesc) == 160, "QuadDesc layout");
 
+// Mixed patch sizes (8x8 and 16x16 quads in one mesh; extension): per quad
+// its patch size n, the offset of its first cell in the state arrays
+// (cells, not doubles: cell_info[2] / 4) and its level, and per side the
+// neighbour's patch size, the cell offsets of nbr0 / nbr1, and for a
+// kSideFineHang side which half of the coarse edge this quad covers (0: the
+// half at the coarse edge's lower coordinate). Read only by the mixed-size
+// kernels; uniform meshes keep QuadDesc alone.
+struct MixSide {
+    int n;
+    int base0;
+    int base1;
+    int half;
+};
+
+struct MixDesc {
+    int n;
+    int base;
+    int level;
+    int pad;
+    MixSide side[4];
+};
+static_assert(sizeof(MixDesc) == 80, "MixDesc layout");
+
 // Per-step scalars kept on the device, cycled over three slots so that a
 // step reads slot s%3, writes its successor's dt candidates into (s+1)%3 and
 // re-arms (s+2)%3 without racing concurrently running blocks.

@@ -22,6 +22,9 @@ struct StageLaunch {
 
 int stage_table_fp64(const StageLaunch **out);
 int stage_table_fp32(const StageLaunch **out);
+// The mixed-size row sweep (8x8 and 16x16 quads in one work list, FP32-flux
+// form): n = 0, never a uniform mesh's launch.
+const StageLaunch *stage_launch_mixed();
 
 // CFL step of a state (prologue of a segment): min over cells of the
 // reference's candidate, folded into scal->slot[slot].dt_bits.

@@ -6,6 +6,7 @@
 namespace amrgpu {
 
 struct QuadDesc;
+struct MixDesc;
 struct DeviceScalars;
 
 struct TagMethods {
@@ -26,5 +27,16 @@ cudaError_t launch_rearm(DeviceScalars *scal, int slot_now, double cap, cudaStre
 cudaError_t launch_remap(int n, const double *qold, long long stride_old, double *qnew,
                          long long stride_new, const int *kind, const int *src, int nquad_new,
                          cudaStream_t st);
+
+// mixed patch sizes (mixed.cu)
+const void *cfl_kernel_mixed();
+int totals_mixed_grid(int nquad);
+cudaError_t launch_totals_mixed(const QuadDesc *quads, const MixDesc *mix, const double *q, long long stride,
+                                int nquad, double *partials, int grid, cudaStream_t st);
+cudaError_t launch_tag_mixed(const double *rho, const QuadDesc *quads, const MixDesc *mix, int nquad, int nmeth,
+                             const TagMethods &m, int *tags, cudaStream_t st);
+cudaError_t launch_remap_mixed(const double *qold, long long stride_old, const MixDesc *mold, double *qnew,
+                               long long stride_new, const MixDesc *mnew, const int *kind, const int *src,
+                               int nquad_new, cudaStream_t st);
 
 }  // namespace amrgpu

@@ -157,6 +157,18 @@ struct amrgpu_session {
     bool primed = false;
     double t0 = 0.0;
     int sms = 148;
+    // mixed patch sizes (8x8 and 16x16 quads in one mesh; extension)
+    bool mixed = false;
+    std::vector<int> qn;              // patch size of each quad
+    std::vector<MixDesc> h_mix;
+    MixDesc *d_mix = nullptr;         // per-quad sizes and offsets of the current mesh
+    int cap_mix = 0;
+    MixDesc *d_mix_old = nullptr;     // ... of the mesh before a regrid (remap source)
+    int cap_mix_old = 0;
+    int *d_work = nullptr;            // work list: the 16x16 quads, then the 8x8 quads
+    std::vector<int> h_work;
+    int cap_work = 0;
+    int nwork16 = 0, nwork8 = 0;
 };
 
 namespace {
@@ -170,6 +182,46 @@ int scheme_of(const amrgpu_session *s)
     return sc;
 }
 
+// Patch sizes of a mesh from the reference's own layout: quad q's state
+// starts at cell_info[3q+2] and holds 4 n^2 doubles (the reference's
+// sizes[] array, physics_go.c:78-86, gives the same numbers). A mesh whose
+// offsets are 4 n^2 q for the configured n is uniform; otherwise every quad
+// must hold an 8x8 or a 16x16 patch (mixed sizes, an extension), with no
+// ghost quads. On success cells = the local quads' cells.
+int mesh_sizes(const amrgpu_mesh_t *m, int n, bool &mixed, std::vector<int> &qn, long long &cells)
+{
+    const int nq = m->ncell, ntot = m->ncell + m->nghost;
+    const long long nftm = 4LL * n * n;
+    bool uniform = (long long)m->dof == nftm * nq;
+    for (int q = 0; q < ntot && uniform; ++q)
+        if ((long long)m->cell_info[3 * q + 2] != nftm * q) uniform = false;
+    mixed = !uniform;
+    qn.assign(size_t(nq), n);
+    cells = (long long)nq * n * n;
+    if (uniform) return AMRGPU_OK;
+    if (m->nghost != 0) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: ghost quads are not supported");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    if (nq > 0 && m->cell_info[2] != 0) {
+        set_error(AMRGPU_ERR_MESH, "cell_info[2] of quad 0 is not 0");
+        return AMRGPU_ERR_MESH;
+    }
+    for (int q = 0; q < nq; ++q) {
+        const long long a = m->cell_info[3 * q + 2];
+        const long long b = (q + 1 < nq) ? (long long)m->cell_info[3 * (q + 1) + 2] : (long long)m->dof;
+        const long long sz = b - a;
+        if (sz != 4 * 64 && sz != 4 * 256) {
+            set_error(AMRGPU_ERR_MESH, "quad " + std::to_string(q) + " holds " + std::to_string(sz) +
+                                           " doubles: patches must be uniform or 8x8 / 16x16 (4*64 / 4*256)");
+            return AMRGPU_ERR_MESH;
+        }
+        qn[size_t(q)] = sz == 4 * 64 ? 8 : 16;
+    }
+    cells = (long long)m->dof / 4;
+    return AMRGPU_OK;
+}
+
 // face_info -> per-quad side descriptors, following the decode of
 // physics_rhs_structured.c:73-262 (side parity picks left/right, side_plus,
 // level_l / level_r for cell_h, ind < dof guards real quads).
@@ -179,7 +231,7 @@ int decode_mesh(amrgpu_session *s, const amrgpu_mesh_t *m)
     const int n = s->n;
     const int nftm = 4 * n * n;
     s->h_quads.assign(size_t(nq), QuadDesc{});
-    for (int q = 0; q < ntot; ++q) {
+    for (int q = 0; q < ntot && !s->mixed; ++q) {
         int off = m->cell_info[3 * q + 2];
         if (off != nftm * q) {
             set_error(AMRGPU_ERR_MESH, "cell_info[2] is not 4*n*n*id (quads must be contiguous)");
@@ -252,6 +304,114 @@ int decode_mesh(amrgpu_session *s, const amrgpu_mesh_t *m)
     return AMRGPU_OK;
 }
 
+// Mixed-size descriptors and work list of a decoded mesh (s->h_quads,
+// s->qn): per quad its size, first cell and level; per side the
+// neighbour's size and first cells, and the geometric order of a hanging
+// edge's two fine quads (half: for a coarse side 1 when nbr1 lies at the
+// edge's lower coordinate, for a fine side 1 when this quad covers the
+// upper half). The work list holds the 16x16 quads in mesh order, then the
+// 8x8 quads.
+int build_mix(amrgpu_session *s, const amrgpu_mesh_t *m)
+{
+    const int nq = s->nquad;
+    s->h_mix.assign(size_t(nq), MixDesc{});
+    auto base = [&](int q) { return m->cell_info[3 * q + 2] / 4; };
+    // lower coordinate of quad q along the edge of side k (y for the x
+    // sides 0 / 1, x for the y sides 2 / 3)
+    auto along = [&](int q, int k) { return s->h_quads[size_t(q)].corner[k < 2 ? 1 : 0]; };
+    auto edge_len = [&](int q, int k) {
+        const double *g = s->h_quads[size_t(q)].corner;
+        return k < 2 ? std::fabs(g[5] - g[1]) : std::fabs(g[2] - g[0]);
+    };
+    for (int q = 0; q < nq; ++q) {
+        MixDesc &md = s->h_mix[size_t(q)];
+        md.n = s->qn[size_t(q)];
+        md.base = base(q);
+        md.level = m->cell_info[3 * q + 1];
+        for (int k = 0; k < 4; ++k) {
+            const SideDesc &d = s->h_quads[size_t(q)].side[k];
+            MixSide &ms = md.side[k];
+            ms.n = md.n;
+            ms.base0 = ms.base1 = 0;
+            ms.half = 0;
+            if (d.kind == kSideFull || d.kind == kSideCoarseHang || d.kind == kSideFineHang) {
+                ms.n = s->qn[size_t(d.nbr0)];
+                ms.base0 = base(d.nbr0);
+            }
+            if (d.kind == kSideCoarseHang) {
+                if (s->qn[size_t(d.nbr1)] != s->qn[size_t(d.nbr0)]) {
+                    set_error(AMRGPU_ERR_MESH, "mixed patch sizes: the two fine quads on quad " + std::to_string(q) +
+                                                   "'s hanging side " + std::to_string(k) +
+                                                   " differ in size (siblings must share one patch size)");
+                    return AMRGPU_ERR_MESH;
+                }
+                ms.base1 = base(d.nbr1);
+                ms.half = along(d.nbr1, k) < along(d.nbr0, k) ? 1 : 0;
+            } else if (d.kind == kSideFineHang) {
+                ms.half = along(q, k) - along(d.nbr0, k) > 0.25 * edge_len(q, k) ? 1 : 0;
+            }
+        }
+    }
+    std::vector<int> work;
+    work.reserve(size_t(nq));
+    for (int q = 0; q < nq; ++q)
+        if (s->qn[size_t(q)] == 16) work.push_back(q);
+    s->nwork16 = int(work.size());
+    for (int q = 0; q < nq; ++q)
+        if (s->qn[size_t(q)] == 8) work.push_back(q);
+    s->nwork8 = int(work.size()) - s->nwork16;
+    s->h_work = std::move(work);
+    return AMRGPU_OK;
+}
+
+// Descriptors and work list of a mixed mesh to the device (grown buffers).
+// keep_old: the current descriptors move to d_mix_old first (the remap of
+// a regrid reads the old mesh's offsets).
+int upload_mix(amrgpu_session *s, bool keep_old)
+{
+    const int nq = s->nquad;
+    if (keep_old) {
+        std::swap(s->d_mix, s->d_mix_old);
+        std::swap(s->cap_mix, s->cap_mix_old);
+    }
+    if (nq > s->cap_mix || !s->d_mix) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->d_mix);
+        s->d_mix = nullptr;
+        s->cap_mix = 0;
+        const int c = std::max(2 * nq, 1);
+        if (!cuda_ok(cudaMalloc(&s->d_mix, sizeof(MixDesc) * size_t(c)), "cudaMalloc mixed descriptors"))
+            return AMRGPU_ERR_CUDA;
+        s->cap_mix = c;
+    }
+    if (nq > s->cap_work || !s->d_work) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(s->d_work);
+        s->d_work = nullptr;
+        s->cap_work = 0;
+        const int c = std::max(2 * nq, 1);
+        if (!cuda_ok(cudaMalloc(&s->d_work, sizeof(int) * size_t(c)), "cudaMalloc work list")) return AMRGPU_ERR_CUDA;
+        s->cap_work = c;
+    }
+    if (nq > 0 &&
+        (!cuda_ok(cudaMemcpyAsync(s->d_mix, s->h_mix.data(), sizeof(MixDesc) * size_t(nq), cudaMemcpyHostToDevice,
+                                  s->stream),
+                  "upload mixed descriptors") ||
+         !cuda_ok(cudaMemcpyAsync(s->d_work, s->h_work.data(), sizeof(int) * size_t(nq), cudaMemcpyHostToDevice,
+                                  s->stream),
+                  "upload work list")))
+        return AMRGPU_ERR_CUDA;
+    // the host vectors stay alive until the next build (the copies above
+    // read them asynchronously)
+    return AMRGPU_OK;
+}
+
+// Cells of the local quads.
+long long local_cells(const amrgpu_session *s)
+{
+    return s->mixed ? s->ncells_total : (long long)s->nquad * s->n * s->n;
+}
+
 // The FP32-flux form takes face normals and volumes from each quad's
 // spacing, which needs axis-aligned rectangular quads (every brick mesh).
 bool quads_are_rectangles(const amrgpu_session *s)
@@ -291,6 +451,13 @@ const StageLaunch *default_launch(int form, int n, int nquad)
     return first;
 }
 
+// The launch a session uses: the mixed-size sweep for a mixed mesh, else
+// default_launch.
+const StageLaunch *session_default_launch(const amrgpu_session *s)
+{
+    return s->mixed ? stage_launch_mixed() : default_launch(s->form, s->n, s->nquad);
+}
+
 const StageLaunch *find_launch(int form, int n, int qpb, int threads)
 {
     const StageLaunch *tab;
@@ -311,6 +478,10 @@ int configure_launch(amrgpu_session *s, const StageLaunch *L)
         set_error(AMRGPU_ERR_UNSUPPORTED, "the FP32-flux form needs axis-aligned rectangular quads");
         return AMRGPU_ERR_UNSUPPORTED;
     }
+    if (s->mixed && (s->form != AMRGPU_FORM_FP32_FLUX || L != stage_launch_mixed())) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: the FP32-flux form's mixed-size sweep only");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
     if (s->occ_kernel != L->kernel) {
         if (!cuda_ok(cudaFuncSetAttribute(L->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L->smem)),
                      "cudaFuncSetAttribute"))
@@ -325,6 +496,12 @@ int configure_launch(amrgpu_session *s, const StageLaunch *L)
     int per_sm = s->occ_per_sm;
     if (per_sm < 1) per_sm = 1;
     int groups = (s->nquad + L->qpb - 1) / L->qpb;
+    if (s->mixed) {
+        // work items (a 16x16 quad or a pair of 8x8 quads) per block = warps
+        const int items = s->nwork16 + (s->nwork8 + 1) / 2;
+        const int warps = L->threads / 32;
+        groups = (items + warps - 1) / warps;
+    }
     int g = std::min(groups, per_sm * s->sms);
     if (g < 1) g = 1;
     if (g > s->partial_cap) {
@@ -366,16 +543,21 @@ int prime(amrgpu_session *s, bool keep_time = false)
     bool cfl_on = s->cfg.time_scheme != 2;
     if (cfl_on && s->nquad > 0) {
         CflArgs a;
+        std::memset(&a, 0, sizeof(a));
         a.quads = s->d_quads;
+        a.mix = s->d_mix;
         a.qin = rolebuf(s, RX);
         a.scal = s->d_scal;
         a.stride = s->stride;
         a.nquad = s->nquad;
         a.slot = p;
         a.cfl = s->cfg.cfl;
-        const void *k = s->form == AMRGPU_FORM_FP32_FLUX ? cfl_kernel_fp32(s->n) : cfl_kernel_fp64(s->n);
-        long long cells = (long long)s->nquad * s->n * s->n;
+        const void *k = s->mixed ? cfl_kernel_mixed()
+                                 : (s->form == AMRGPU_FORM_FP32_FLUX ? cfl_kernel_fp32(s->n) : cfl_kernel_fp64(s->n));
+        long long cells = local_cells(s);
         int g = int(std::min<long long>((cells + 255) / 256, (long long)s->sms * 8));
+        if (s->mixed) g = int(std::min<long long>(((long long)s->nquad * 32 + 255) / 256, (long long)s->sms * 8));
+        if (g < 1) g = 1;
         void *args[] = {&a};
         if (!cuda_ok(cudaLaunchKernel(k, dim3(g), dim3(256), args, 0, s->stream), "cfl kernel"))
             return AMRGPU_ERR_CUDA;
@@ -420,6 +602,10 @@ int enqueue_stage(amrgpu_session *s, size_t st)
     a.a1 = rolebuf(s, plan[st].a1);
     a.out0 = rolebuf(s, plan[st].out0);
     a.out1 = rolebuf(s, plan[st].out1);
+    a.mix = s->d_mix;
+    a.work = s->d_work;
+    a.nwork16 = s->nwork16;
+    a.nwork8 = s->nwork8;
     void *args[] = {&a};
     cudaError_t e = cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args,
                                      s->launch->smem, s->stream);
@@ -481,6 +667,10 @@ bool launch_rhs_stage(amrgpu_session *s)
         double ms = s->cfg.ic_params[0] != 0.0 ? s->cfg.ic_params[0] : 2.0;
         amrgpu::shock_state(s->cfg.gamma, ms, 1.0, 1.0, a.qinflow);
     }
+    a.mix = s->d_mix;
+    a.work = s->d_work;
+    a.nwork16 = s->nwork16;
+    a.nwork8 = s->nwork8;
     void *args[] = {&a};
     if (!cuda_ok(cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args, s->launch->smem,
                                   s->stream),
@@ -516,7 +706,7 @@ bool tune_candidate(const amrgpu_session *s, const StageLaunch &L, const StageLa
 int autotune_session(amrgpu_session *s, bool retime)
 {
     s->tune_pending = false;
-    if (s->nquad == 0) return AMRGPU_OK;
+    if (s->nquad == 0 || s->mixed) return AMRGPU_OK;  // a mixed mesh has one launch
     const StageLaunch *tab;
     const int cnt = (s->form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
     const StageLaunch *def = default_launch(s->form, s->n, s->nquad);
@@ -636,20 +826,33 @@ int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const Phy
     s->nghost = m->nghost;
     s->nface = m->nface;
     s->dof = m->dof;
-    if (m->dof != 4 * s->n * s->n * m->ncell) {
-        set_error(AMRGPU_ERR_MESH, "dof != 4*n*n*ncell");
-        delete s;
-        return AMRGPU_ERR_MESH;
-    }
-    int rc = decode_mesh(s, m);
+    long long mesh_cells = 0;
+    int rc = mesh_sizes(m, s->n, s->mixed, s->qn, mesh_cells);
     if (rc != AMRGPU_OK) {
         delete s;
         return rc;
     }
+    if (s->mixed && s->form != AMRGPU_FORM_FP32_FLUX) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: the FP32-flux form only (gpu_form: 1)");
+        delete s;
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    rc = decode_mesh(s, m);
+    if (rc != AMRGPU_OK) {
+        delete s;
+        return rc;
+    }
+    if (s->mixed) {
+        rc = build_mix(s, m);
+        if (rc != AMRGPU_OK) {
+            delete s;
+            return rc;
+        }
+    }
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, dev);
-    s->ncells_total = (long long)(m->ncell + m->nghost) * s->n * s->n;
+    s->ncells_total = s->mixed ? mesh_cells : (long long)(m->ncell + m->nghost) * s->n * s->n;
     s->stride = ((s->ncells_total + 31) / 32) * 32;
     if (s->stride == 0) s->stride = 32;
     // state buffers hold a quarter more cells than the mesh, so that a regrid
@@ -672,6 +875,7 @@ int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const Phy
                          "upload quads");
     }
     if (ok) ok = cuda_ok(cudaMalloc(&s->d_tot, sizeof(double) * 4 * size_t(totals_grid(s->cap_stride))), "cudaMalloc totals");
+    if (ok && s->mixed) ok = upload_mix(s, false) == AMRGPU_OK;
     s->cap_quads = std::max(s->nquad, 1);
     s->cap_desc = s->nquad;
     s->rect = quads_are_rectangles(s);
@@ -681,10 +885,10 @@ int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const Phy
         amrgpu_session_destroy(s);
         return AMRGPU_ERR_CUDA;
     }
-    const StageLaunch *L = default_launch(s->form, s->n, s->nquad);
+    const StageLaunch *L = session_default_launch(s);
     const char *env_q = std::getenv("AMRGPU_QPB");
     const char *env_t = std::getenv("AMRGPU_THREADS");
-    if (env_q || env_t) {
+    if ((env_q || env_t) && !s->mixed) {
         const StageLaunch *L2 = find_launch(s->form, s->n, env_q ? std::atoi(env_q) : 0, env_t ? std::atoi(env_t) : 0);
         if (L2) {
             L = L2;
@@ -697,7 +901,7 @@ int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const Phy
         return rc;
     }
     s->gpu_name = device_name(dev);
-    s->tune_pending = !s->launch_pinned;
+    s->tune_pending = !s->launch_pinned && !s->mixed;
     *out = s;
     return AMRGPU_OK;
 }
@@ -728,6 +932,9 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_remap0);
     cudaFree(s->d_bal_work);
     cudaFreeHost(s->h_stage);
+    cudaFree(s->d_mix);
+    cudaFree(s->d_mix_old);
+    cudaFree(s->d_work);
     s->ring.release();
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -737,6 +944,10 @@ int amrgpu_session_set_form(amrgpu_session_t *s, int form)
 {
     if (!s || (form != AMRGPU_FORM_FP64_EXACT && form != AMRGPU_FORM_FP32_FLUX)) return AMRGPU_ERR_ARG;
     if (form == s->form) return AMRGPU_OK;
+    if (s->mixed) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: the FP32-flux form only");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
     // keep the current state where the canonical X role points
     s->form = form;
     s->cfg.form = form;
@@ -843,7 +1054,7 @@ int amrgpu_session_upload(amrgpu_session_t *s, const double *soln)
 int amrgpu_session_download(amrgpu_session_t *s, double *soln)
 {
     if (!s || !soln) return AMRGPU_ERR_ARG;
-    long long cells = (long long)s->nquad * s->n * s->n;
+    long long cells = local_cells(s);
     if (cells) {
         if (!cuda_ok(launch_soa_to_aos(rolebuf(s, RX), s->d_aos, cells, s->stride, s->stream), "soa_to_aos"))
             return AMRGPU_ERR_CUDA;
@@ -897,6 +1108,10 @@ unsigned long long *amrgpu_session_dt_slot(amrgpu_session_t *s)
 int amrgpu_session_set_halo(amrgpu_session_t *s, const int *send_quads, int nsend)
 {
     if (!s || nsend < 0 || (nsend > 0 && !send_quads)) return AMRGPU_ERR_ARG;
+    if (s->mixed && nsend > 0) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: no ghost exchange");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
     for (int k = 0; k < nsend; ++k)
         if (send_quads[k] < 0 || send_quads[k] >= s->nquad) {
             set_error(AMRGPU_ERR_ARG, "set_halo: send entry " + std::to_string(k) + " is not a local quad");
@@ -1060,7 +1275,7 @@ int amrgpu_session_rhs(amrgpu_session_t *s, double *rhs)
     if (s->nquad == 0) return AMRGPU_OK;
     if (!launch_rhs_stage(s)) return AMRGPU_ERR_CUDA;
     s->launches++;
-    long long cells = (long long)s->nquad * s->n * s->n;
+    long long cells = local_cells(s);
     if (!cuda_ok(launch_soa_to_aos(rolebuf(s, RZ), s->d_aos, cells, s->stride, s->stream), "soa_to_aos"))
         return AMRGPU_ERR_CUDA;
     s->launches++;
@@ -1090,7 +1305,7 @@ const double *amrgpu_session_state_device(amrgpu_session_t *s, int field)
     return rolebuf(s, RX) + size_t(field) * size_t(s->stride);
 }
 
-int amrgpu_session_cells(const amrgpu_session_t *s) { return s ? int((long long)s->nquad * s->n * s->n) : 0; }
+int amrgpu_session_cells(const amrgpu_session_t *s) { return s ? int(local_cells(s)) : 0; }
 
 void *amrgpu_session_stream(amrgpu_session_t *s) { return s ? (void *)s->stream : nullptr; }
 
@@ -1158,6 +1373,10 @@ namespace amrgpu {
 bool session_view(amrgpu_session_t *s, SessionView *v)
 {
     if (!s || !v) return false;
+    if (s->mixed) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: not supported by this call (uniform meshes only)");
+        return false;
+    }
     v->n = s->n;
     v->nquad = s->nquad;
     v->stride = s->stride;
@@ -1194,11 +1413,18 @@ extern "C" {
 int amrgpu_session_totals(amrgpu_session_t *s, double totals[4])
 {
     if (!s || !totals) return AMRGPU_ERR_ARG;
-    long long cells = (long long)s->nquad * s->n * s->n;
+    long long cells = local_cells(s);
     int g = totals_grid(std::max<long long>(cells, 1));
-    if (!cuda_ok(launch_totals(s->n, s->d_quads, rolebuf(s, RX), s->stride, s->nquad, s->d_tot, g, s->stream),
-                 "totals"))
+    if (s->mixed) {
+        g = std::min(g, totals_mixed_grid(std::max(s->nquad, 1)));
+        if (!cuda_ok(launch_totals_mixed(s->d_quads, s->d_mix, rolebuf(s, RX), s->stride, s->nquad, s->d_tot, g,
+                                         s->stream),
+                     "totals"))
+            return AMRGPU_ERR_CUDA;
+    } else if (!cuda_ok(launch_totals(s->n, s->d_quads, rolebuf(s, RX), s->stride, s->nquad, s->d_tot, g, s->stream),
+                        "totals")) {
         return AMRGPU_ERR_CUDA;
+    }
     s->launches++;
     std::vector<double> h(size_t(4 * g));
     if (!cuda_ok(cudaMemcpyAsync(h.data(), s->d_tot, sizeof(double) * 4 * size_t(g), cudaMemcpyDeviceToHost, s->stream),
@@ -1223,7 +1449,9 @@ int amrgpu_session_tag(amrgpu_session_t *s, int *tags)
         m.method[k] = k < nm ? s->cfg.amr_tag_methods[size_t(k)] : 0;
         m.tol[k] = k < nm ? s->cfg.amr_tag_tolerances[size_t(k)] : 0.0;
     }
-    bool ok = cuda_ok(launch_tag(s->n, rolebuf(s, RX), s->d_quads, s->nquad, nm, m, s->d_tags, s->stream),
+    bool ok = cuda_ok(s->mixed ? launch_tag_mixed(rolebuf(s, RX), s->d_quads, s->d_mix, s->nquad, nm, m, s->d_tags,
+                                                  s->stream)
+                               : launch_tag(s->n, rolebuf(s, RX), s->d_quads, s->nquad, nm, m, s->d_tags, s->stream),
                       "tag kernel");
     s->launches++;
     if (ok)
@@ -1237,6 +1465,10 @@ int amrgpu_session_tag(amrgpu_session_t *s, int *tags)
 int amrgpu_session_remap(amrgpu_session_t *dst, amrgpu_session_t *src, const int *kind, const int *src_index)
 {
     if (!dst || !src || !kind || !src_index || dst->n != src->n) return AMRGPU_ERR_ARG;
+    if (dst->mixed || src->mixed) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: use amrgpu_session_regrid (in place)");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
     for (int q = 0; q < dst->nquad; ++q) {
         int lim = kind[q] == 0 ? src->nquad - 1 : src->nquad - 4;
         if (src_index[q] < 0 || src_index[q] > lim) {
@@ -1308,9 +1540,9 @@ int ensure_desc(amrgpu_session *s, QuadDesc **buf, int *cap, int nq)
 // The state moves to the new mesh of nq quads (descriptors already in
 // d_quads, remap kind / source in d_kind / d_src): into the spare buffer Y
 // of the same capacity, or a fresh set when the mesh outgrew the capacity.
-int apply_regrid(amrgpu_session *s, int nq, int nface)
+int apply_regrid(amrgpu_session *s, int nq, int nface, long long mixed_cells = -1)
 {
-    const long long cells = (long long)nq * s->n * s->n;
+    const long long cells = mixed_cells >= 0 ? mixed_cells : (long long)nq * s->n * s->n;
     const long long stride = std::max<long long>(((cells + 31) / 32) * 32, 32);
     double *qold = rolebuf(s, RX);
     const long long old_stride = s->stride;
@@ -1342,8 +1574,13 @@ int apply_regrid(amrgpu_session *s, int nq, int nface)
     }
     double *qnew = fresh[0] ? fresh[0] : rolebuf(s, RY);
     if (nq > 0) {
-        ok = cuda_ok(launch_remap(s->n, qold, old_stride, qnew, stride, s->d_kind, s->d_src, nq, s->stream),
-                     "remap kernel");
+        if (mixed_cells >= 0)
+            ok = cuda_ok(launch_remap_mixed(qold, old_stride, s->d_mix_old, qnew, stride, s->d_mix, s->d_kind, s->d_src,
+                                            nq, s->stream),
+                         "remap kernel");
+        else
+            ok = cuda_ok(launch_remap(s->n, qold, old_stride, qnew, stride, s->d_kind, s->d_src, nq, s->stream),
+                         "remap kernel");
         s->launches++;
     }
     if (!ok) {
@@ -1364,12 +1601,12 @@ int apply_regrid(amrgpu_session *s, int nq, int nface)
     s->nquad = nq;
     s->nghost = 0;
     s->nface = nface;
-    s->dof = 4 * s->n * s->n * nq;
+    s->dof = int(4 * cells);
     s->ncells_total = cells;
     s->stride = stride;
     // a launch chosen by the caller stays; the default follows the mesh size
-    int rc = configure_launch(s, s->launch_pinned ? s->launch : default_launch(s->form, s->n, nq));
-    if (!s->launch_pinned) s->tune_pending = true;
+    int rc = configure_launch(s, (s->launch_pinned && !s->mixed) ? s->launch : session_default_launch(s));
+    if (!s->launch_pinned && !s->mixed) s->tune_pending = true;
     if (rc != AMRGPU_OK) return rc;
     return prime(s, s->primed);
 }
@@ -1487,12 +1724,32 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
         set_error(AMRGPU_ERR_UNSUPPORTED, "session_regrid: ghost quads need a ghost exchange after the remap");
         return AMRGPU_ERR_UNSUPPORTED;
     }
-    if (m->dof != 4 * s->n * s->n * m->ncell) {
-        set_error(AMRGPU_ERR_MESH, "dof != 4*n*n*ncell");
-        return AMRGPU_ERR_MESH;
+    bool mixed_new = false;
+    std::vector<int> qn_new;
+    long long cells_new = 0;
+    if (int e = mesh_sizes(m, s->n, mixed_new, qn_new, cells_new)) return e;
+    // a mixed regrid (either mesh mixed) runs the mixed-size path from here
+    // on; it needs the FP32-flux form and a launch the session chose
+    const bool mixed_path = mixed_new || s->mixed;
+    if (mixed_path && (s->form != AMRGPU_FORM_FP32_FLUX || (s->launch_pinned && !s->mixed))) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: the FP32-flux form with the library's launch only");
+        return AMRGPU_ERR_UNSUPPORTED;
     }
     if (!check_remap(s, m->ncell, kind, src_index)) return AMRGPU_ERR_ARG;
+    if (mixed_path && !s->mixed) {
+        // the old (uniform) mesh's descriptors for the remap's source side
+        s->qn.assign(size_t(s->nquad), s->n);
+        s->h_mix.assign(size_t(s->nquad), MixDesc{});
+        for (int q = 0; q < s->nquad; ++q) {
+            s->h_mix[size_t(q)].n = s->n;
+            s->h_mix[size_t(q)].base = q * s->n * s->n;
+        }
+        s->h_work.assign(size_t(s->nquad), 0);
+        if (int e = upload_mix(s, false)) return e;
+    }
     std::vector<QuadDesc> old = std::move(s->h_quads);
+    const bool was_mixed = s->mixed;
+    s->mixed = mixed_path;
     int rc = decode_mesh(s, m);
     if (rc == AMRGPU_OK && s->form == AMRGPU_FORM_FP32_FLUX && !quads_are_rectangles(s)) {
         set_error(AMRGPU_ERR_UNSUPPORTED, "the FP32-flux form needs axis-aligned rectangular quads");
@@ -1500,9 +1757,38 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
     }
     if (rc != AMRGPU_OK) {
         s->h_quads = std::move(old);
+        s->mixed = was_mixed;
         return rc;
     }
     const int nq = m->ncell;
+    if (mixed_path) {
+        const int nq_old = s->nquad;
+        s->nquad = nq;
+        std::vector<int> qn_keep = std::move(s->qn);
+        std::vector<MixDesc> mix_keep = std::move(s->h_mix);
+        std::vector<int> work_keep = std::move(s->h_work);
+        const int n16_keep = s->nwork16, n8_keep = s->nwork8;
+        s->qn = std::move(qn_new);
+        rc = build_mix(s, m);
+        if (rc != AMRGPU_OK) {
+            // the session stays on the old mesh
+            s->qn = std::move(qn_keep);
+            s->h_mix = std::move(mix_keep);
+            s->h_work = std::move(work_keep);
+            s->nwork16 = n16_keep;
+            s->nwork8 = n8_keep;
+            s->h_quads = std::move(old);
+            s->mixed = was_mixed;
+            s->nquad = nq_old;
+            return rc;
+        }
+        rc = upload_mix(s, true);
+        if (rc != AMRGPU_OK) {
+            s->nquad = nq_old;
+            return rc;
+        }
+        s->nquad = nq_old;  // apply_regrid moves the session to the new mesh
+    }
     rc = ensure_quad_arrays(s, nq);
     if (rc == AMRGPU_OK) rc = ensure_desc(s, &s->d_quads, &s->cap_desc, nq);
     if (rc != AMRGPU_OK) {
@@ -1520,12 +1806,16 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
                      "upload quads");
     if (!ok) return AMRGPU_ERR_CUDA;
     s->rect = (s->form != AMRGPU_FORM_FP32_FLUX) ? quads_are_rectangles(s) : true;
-    return apply_regrid(s, nq, m->nface);
+    return apply_regrid(s, nq, m->nface, mixed_path ? cells_new : -1);
 }
 
 int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f)
 {
     if (!s || !f || !f->f) return AMRGPU_ERR_ARG;
+    if (s->mixed) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: regrid through amrgpu_session_regrid");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
     if (s->stage_pos != 0) {
         set_error(AMRGPU_ERR_ARG, "session_regrid_forest: a step begun with step_stage is not finished");
         return AMRGPU_ERR_ARG;
@@ -1887,6 +2177,10 @@ extern "C" {
 int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
 {
     if (!f || !f->f || !s) return -AMRGPU_ERR_ARG;
+    if (s->mixed) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: regrid through amrgpu_session_regrid");
+        return -AMRGPU_ERR_UNSUPPORTED;
+    }
     int live = 0;
     return balance_impl(s, f->f, &live, false);
 }
@@ -1894,6 +2188,10 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
 int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f)
 {
     if (!s || !f || !f->f) return AMRGPU_ERR_ARG;
+    if (s->mixed) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: regrid through amrgpu_session_regrid");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
     if (s->stage_pos != 0) {
         set_error(AMRGPU_ERR_ARG, "session_balance_regrid: a step begun with step_stage is not finished");
         return AMRGPU_ERR_ARG;

@@ -115,4 +115,10 @@ int stage_table_fp32(const StageLaunch **out)
     return int(sizeof(kTable32) / sizeof(kTable32[0]));
 }
 
+// two warps per block, 128 registers: 16 resident warps per SM, as the
+// uniform sweeps' default
+static const StageLaunch kMixed{0, 2, 64, 8, 0, (const void *)sweep_mixed_kernel<2, 8>, 1};
+
+const StageLaunch *stage_launch_mixed() { return &kMixed; }
+
 }  // namespace amrgpu

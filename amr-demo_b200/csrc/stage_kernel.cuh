@@ -75,10 +75,18 @@ struct StageArgs {
     double dt_cap;
     double final_time;    // > 0: clip the step at this time
     double qinflow[4];    // bc 3 state (extension)
+    // mixed patch sizes: per-quad sizes and offsets, and the work list
+    // (the 16x16 quads first, nwork16 of them, then the 8x8 quads in pairs,
+    // nwork8 of them)
+    const MixDesc *mix;
+    const int *work;
+    int nwork16;
+    int nwork8;
 };
 
 struct CflArgs {
     const QuadDesc *quads;
+    const MixDesc *mix;  // mixed patch sizes: per-quad n and offset (else null)
     const double *qin;
     DeviceScalars *scal;
     long long stride;

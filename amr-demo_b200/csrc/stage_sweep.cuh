@@ -39,49 +39,62 @@
 
 namespace amrgpu {
 
-template <int N, int WARPS>
-__device__ __forceinline__ void sweep_body(const StageArgs &a)
+// Neighbour cell facing position p of side s (the cell on the neighbour's
+// opposite side) in a patch of run-time size n.
+__device__ __forceinline__ int facing_cell_rt(int s, int p, int n)
+{
+    if (s == 0) return p * n + (n - 1);
+    if (s == 1) return p * n;
+    if (s == 2) return (n - 1) * n + p;
+    return p;
+}
+
+// Per-warp scalars of the sweep's block reductions.
+struct SweepAcc {
+    double dt_min;
+    double norm;
+    int flags;
+};
+
+// One work item of the row sweep: the warp's QPW quads, this lane's quad
+// `quad` (computed but neither stored nor reduced when !valid). sedge is the
+// warp's edge table, [quad of the warp][side 0..3, 4 = faces between rows
+// R-1 and R][position][field].
+//
+// MIXED: the mesh holds 8x8 and 16x16 quads (extension, no reference
+// counterpart): the quad's state starts at mix[quad].base, and an edge whose
+// neighbour has another patch size pairs cells by position along the edge.
+// The edge is cut into pieces of the finer side's cell length; each piece
+// pairs the own cell and the neighbour cell that cover it, and its flux
+// (normal length = the finer cell length) goes to both, evaluated by each
+// quad from the same two records at the same call site, so the pair sees
+// the same bits (exact conservation). A coarser own cell sums its pieces in
+// FP64 in edge order, as a coarse hanging edge sums its two fluxes. Sides
+// whose neighbour has this quad's patch size keep the reference's pairing
+// (physics_residual_face_*_structured.c: the same position, a coarse
+// hanging edge's two index-paired fluxes).
+template <int N, bool MIXED>
+__device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5][N][4], int quad, bool valid,
+                                           int lane, double dt, const float qinf[4], SweepAcc &acc)
 {
     static_assert(N == 16 || N == 8, "row sweep for 16x16 and 8x8 patches");
     constexpr int NN = N * N;
-    constexpr int QPW = 32 / (2 * N);  // quads per warp
     constexpr int R = N / 2;           // rows per half-patch
     constexpr unsigned FULL = 0xffffffffu;
-    // edge fluxes per warp and quad: [side 0..3, 4 = faces between rows R-1
-    // and R][position][field]
-    __shared__ double sedge[WARPS][QPW][5][N][4];
-    __shared__ double red[64];
-    __shared__ int s_last;
-
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int sub = lane / (2 * N), l = lane % (2 * N);
     const int i = l % N, h = l / N;
     const long long stride = a.stride;
-
-    const double dt = sweep_step_dt(a);
-    const float qinf[4] = {(float)a.qinflow[0], (float)a.qinflow[1], (float)a.qinflow[2], (float)a.qinflow[3]};
-
-    double my_dt_min = a.dt_cap;
-    double my_norm = 0.0;
-    int my_flags = 0;
-
-    // Work items (QPW consecutive quads each): each warp's first one by its
-    // index, then the next free one from a counter (work_next, reset to 0 by
-    // the last block), so that warps and SMs that finish early take more and
-    // the tail stays short. A quad past the end (odd count, 8x8) is computed
-    // on its item's first quad and neither stored nor reduced.
-    const int nwarps = gridDim.x * WARPS;
-    const int nitems = (a.nquad + QPW - 1) / QPW;
-    int item = blockIdx.x * WARPS + w;
-    while (item < nitems) {
-        const bool valid = item * QPW + sub < a.nquad;
-        const int quad = valid ? item * QPW + sub : item * QPW;
+    double &my_dt_min = acc.dt_min;
+    double &my_norm = acc.norm;
+    int &my_flags = acc.flags;
+    {
         const QuadDesc &qd = a.quads[quad];
         const double *g = qd.corner;
         const double hx = (g[2] - g[0]) / (double)N, hy = (g[5] - g[1]) / (double)N;
         const double vol = hx * hy, inv_vol = 1.0 / (hx * hy);
         const float fhx = (float)hx, fhy = (float)hy;
-        const double *Qq = a.qin + (long long)quad * NN;
+        const long long qbase = MIXED ? (long long)a.mix[quad].base : (long long)quad * NN;
+        const double *Qq = a.qin + qbase;
         auto load_rec = [&](const double *base, int cell, float P[8], double q[4]) {
 #pragma unroll
             for (int f = 0; f < 4; ++f) q[f] = base[f * stride + cell];
@@ -109,25 +122,73 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
                 // one flux site for a side's one or two neighbours: the
                 // neighbour quad computes the same face at the same site, so
                 // both see bit-identical values (conservation)
-                const int fc = facing_cell<N>(s, m);
-                const int nk = (d.kind == kSideCoarseHang) ? 2 : 1;
 #pragma unroll
                 for (int f = 0; f < 4; ++f) E[f] = 0.0;
+                // pieces of this edge cell: k-th piece's neighbour (0 / 1),
+                // its position along the neighbour's edge, the normal length
+                int nk = (d.kind == kSideCoarseHang) ? 2 : 1;
+                int nn = N, ratio = 0, hang_swap = 0, hang_half = 0;
+                long long nb0 = 0, nb1 = 0;
+                float hp = hc;
+                if constexpr (MIXED) {
+                    const MixSide ms = a.mix[quad].side[s];
+                    nb0 = ms.base0;
+                    nb1 = ms.base1;
+                    if (ms.n != N) {
+                        nn = ms.n;
+                        hang_half = ms.half;
+                        hang_swap = ms.half;
+                        double hn;
+                        if (d.kind == kSideFull) {
+                            ratio = nn > N ? nn / N : 1;
+                            hn = cell_h_of(a.h_base, d.level, nn);
+                            hp = (float)fmin(cell_h_of(a.h_base, d.level, N), hn);
+                        } else if (d.kind == kSideCoarseHang) {
+                            ratio = 2 * nn >= N ? 2 * nn / N : 1;
+                            hn = cell_h_of(a.h_base, d.level, nn);
+                            hp = (float)fmin(cell_h_of(a.h_base, d.level - 1, N), hn);
+                        } else {
+                            ratio = 1;
+                            hn = cell_h_of(a.h_base, d.level - 1, nn);
+                            hp = (float)fmin(cell_h_of(a.h_base, d.level, N), hn);
+                        }
+                        nk = ratio;
+                    }
+                }
 #pragma unroll 1
                 for (int k = 0; k < nk; ++k) {
                     float Pn[8];
                     double qn4[4];
-                    load_rec(a.qin + (long long)(k == 0 ? d.nbr0 : d.nbr1) * NN, fc, Pn, qn4);
+                    long long nb;
+                    if constexpr (MIXED) nb = k == 0 ? nb0 : nb1;
+                    else nb = (long long)(k == 0 ? d.nbr0 : d.nbr1) * NN;
+                    int fc = facing_cell<N>(s, m);
+                    if (MIXED && ratio > 0) {
+                        // geometric pairing with a neighbour of another size
+                        int p, which = 0;
+                        if (d.kind == kSideFull) {
+                            p = nn > N ? m * ratio + k : m * nn / N;
+                        } else if (d.kind == kSideCoarseHang) {
+                            const int g = 2 * nn >= N ? m * ratio + k : m * 2 * nn / N;
+                            which = (g / nn) ^ hang_swap;
+                            p = g % nn;
+                        } else {
+                            p = (hang_half * N + m) * nn / (2 * N);
+                        }
+                        nb = which ? nb1 : nb0;
+                        fc = facing_cell_rt(s, p, nn);
+                    }
+                    load_rec(a.qin + nb, fc, Pn, qn4);
                     const float *L = (s & 1) ? Po : Pn;
                     const float *R = (s & 1) ? Pn : Po;
-                    if (round == 0) roe_flux_axis_fp32<0>(L, R, hc, fl);
-                    else roe_flux_axis_fp32<1>(L, R, hc, fl);
+                    if (round == 0) roe_flux_axis_fp32<0>(L, R, hp, fl);
+                    else roe_flux_axis_fp32<1>(L, R, hp, fl);
 #pragma unroll
                     for (int f = 0; f < 4; ++f) E[f] = E[f] + (double)fl[f];
                 }
             }
 #pragma unroll
-            for (int f = 0; f < 4; ++f) sedge[w][sub][s][m][f] = E[f];
+            for (int f = 0; f < 4; ++f) sedge[sub][s][m][f] = E[f];
         }
         // ---------------- the faces between rows R-1 and R (column i)
         {
@@ -139,7 +200,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
             if (h == 0) {
                 roe_flux_axis_fp32<1>(P, O, fhx, fl);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) sedge[w][sub][4][i][f] = (double)fl[f];
+                for (int f = 0; f < 4; ++f) sedge[sub][4][i][f] = (double)fl[f];
             }
         }
         __syncwarp();
@@ -152,7 +213,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
         double a0next[4] = {0.0, 0.0, 0.0, 0.0};   // ... of the current row, loaded a row ahead of its use
         const bool has_a0 = a.a0 != nullptr;
         auto finish = [&](int jr, const double gup[4]) {
-            const long long gi = (long long)quad * NN + jr * N + i;
+            const long long gi = qbase + jr * N + i;
             double kv[4], qn[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
@@ -193,7 +254,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 a0below[f] = a0next[f];
-                a0next[f] = has_a0 ? a.a0[f * stride + (long long)quad * NN + j * N + i] : 0.0;
+                a0next[f] = has_a0 ? a.a0[f * stride + qbase + j * N + i] : 0.0;
             }
             float P[8];
             cell_prims_fp32(q4, P);
@@ -213,15 +274,15 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
             double xp[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                const double fl = (i == 0) ? sedge[w][sub][0][j][f] : (double)fx[f];
-                const double fr = (i == N - 1) ? sedge[w][sub][1][j][f] : (double)fxr[f];
+                const double fl = (i == 0) ? sedge[sub][0][j][f] : (double)fx[f];
+                const double fr = (i == N - 1) ? sedge[sub][1][j][f] : (double)fxr[f];
                 xp[f] = fr - fl;
             }
             // y-face at j-1/2 (the first row's is an edge or the row R-1/R face)
             double gy[4];
             if (t == 0) {
 #pragma unroll
-                for (int f = 0; f < 4; ++f) gy[f] = h == 0 ? sedge[w][sub][2][i][f] : sedge[w][sub][4][i][f];
+                for (int f = 0; f < 4; ++f) gy[f] = h == 0 ? sedge[sub][2][i][f] : sedge[sub][4][i][f];
             } else {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) gy[f] = (double)fy[f];
@@ -239,18 +300,83 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
             double gtop[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                gtop[f] = h == 0 ? sedge[w][sub][4][i][f] : sedge[w][sub][3][i][f];
+                gtop[f] = h == 0 ? sedge[sub][4][i][f] : sedge[sub][3][i][f];
                 a0below[f] = a0next[f];
             }
             finish(R * h + R - 1, gtop);
         }
         __syncwarp();  // the next item rewrites this warp's edge table
+    }
+}
+
+// The uniform-size row sweep. Work items (QPW consecutive quads each): each
+// warp's first one by its index, then the next free one from a counter
+// (work_next, reset to 0 by the last block), so that warps and SMs that
+// finish early take more and the tail stays short. A quad past the end (odd
+// count, 8x8) is computed on its item's first quad and neither stored nor
+// reduced.
+template <int N, int WARPS>
+__device__ __forceinline__ void sweep_body(const StageArgs &a)
+{
+    constexpr int QPW = 32 / (2 * N);
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ double sedge[WARPS][QPW][5][N][4];
+    __shared__ double red[64];
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sub = lane / (2 * N);
+    const double dt = sweep_step_dt(a);
+    const float qinf[4] = {(float)a.qinflow[0], (float)a.qinflow[1], (float)a.qinflow[2], (float)a.qinflow[3]};
+    SweepAcc acc{a.dt_cap, 0.0, 0};
+    const int nwarps = gridDim.x * WARPS;
+    const int nitems = (a.nquad + QPW - 1) / QPW;
+    int item = blockIdx.x * WARPS + w;
+    while (item < nitems) {
+        const bool valid = item * QPW + sub < a.nquad;
+        const int quad = valid ? item * QPW + sub : item * QPW;
+        sweep_quad<N, false>(a, sedge[w], quad, valid, lane, dt, qinf, acc);
         unsigned nxt = 0;
         if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);
         item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
     }
+    sweep_reduce<WARPS>(a, acc.dt_min, acc.norm, acc.flags, red, &s_last);
+}
 
-    sweep_reduce<WARPS>(a, my_dt_min, my_norm, my_flags, red, &s_last);
+// The mixed-size row sweep: one launch over a work list of the 16x16 quads
+// (one item each) followed by the 8x8 quads (two per item), claimed from
+// one counter as above; an item's patch size decides which body runs (the
+// choice is uniform over the warp). The two bodies share one per-warp edge
+// table (320 doubles for either size).
+template <int WARPS>
+__device__ __forceinline__ void sweep_body_mixed(const StageArgs &a)
+{
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ double sedge_raw[WARPS][5 * 16 * 4];
+    __shared__ double red[64];
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const double dt = sweep_step_dt(a);
+    const float qinf[4] = {(float)a.qinflow[0], (float)a.qinflow[1], (float)a.qinflow[2], (float)a.qinflow[3]};
+    SweepAcc acc{a.dt_cap, 0.0, 0};
+    const int nwarps = gridDim.x * WARPS;
+    const int nitems = a.nwork16 + (a.nwork8 + 1) / 2;
+    int item = blockIdx.x * WARPS + w;
+    while (item < nitems) {
+        if (item < a.nwork16) {
+            sweep_quad<16, true>(a, reinterpret_cast<double(*)[5][16][4]>(sedge_raw[w]), a.work[item], true, lane,
+                                 dt, qinf, acc);
+        } else {
+            const int k = 2 * (item - a.nwork16) + lane / 16;
+            const bool valid = k < a.nwork8;
+            const int quad = a.work[a.nwork16 + (valid ? k : k - 1)];
+            sweep_quad<8, true>(a, reinterpret_cast<double(*)[5][8][4]>(sedge_raw[w]), quad, valid, lane, dt,
+                                qinf, acc);
+        }
+        unsigned nxt = 0;
+        if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);
+        item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
+    }
+    sweep_reduce<WARPS>(a, acc.dt_min, acc.norm, acc.flags, red, &s_last);
 }
 
 template <int WARPS, int MINB>
@@ -263,6 +389,12 @@ template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep8_kernel(const StageArgs a)
 {
     sweep_body<8, WARPS>(a);
+}
+
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) sweep_mixed_kernel(const StageArgs a)
+{
+    sweep_body_mixed<WARPS>(a);
 }
 
 }  // namespace amrgpu

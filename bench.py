@@ -388,11 +388,20 @@ def amr_workload(args):
     import amrgpu as ag
     from amrgpu import amr, workloads as W
     t0 = time.perf_counter()
+    rule = None
     if args.workload == "four_quadrant":
         f, mesh, cfg, soln = W.four_quadrant(seed=0, min_level=4, max_level=9, n=16, form=args.amr_form)
         desc = ("four-quadrant Riemann problem, unit square, levels 4-9, 16x16 patches, density-jump tol 0.05, "
                 "SSP-RK3 CFL 0.5, regrid every 5 steps")
         lo, hi = 4, 9
+        if args.mixed:
+            # 8x8 patches on the two coarsest levels (the smooth far field),
+            # 16x16 on the refined levels; host-side balance and mesh arrays
+            rule = lambda lv: 8 if lv <= lo + 1 else 16  # noqa: E731
+            sizes = f.patch_sizes(rule)
+            mesh = f.mesh_mixed(sizes)
+            soln = f.initialize(sizes)
+            desc = desc.replace("16x16 patches", "mixed patches (8x8 at levels 4-5, 16x16 at 6-9, one work list)")
     else:
         f, mesh, cfg, soln = W.shock_bubble(seed=0, min_level=5, max_level=args.max_level, n=16, form=args.amr_form)
         desc = (f"Mach-2 shock-bubble interaction, [0,2]x[0,1] (2x1 trees), levels 5-{args.max_level}, 16x16 "
@@ -406,7 +415,7 @@ def amr_workload(args):
     for _ in range(max(1, args.warmup // 5)):
         s.step(5)
         s.sync()
-        amr.regrid(f, s, 16, lo, hi)
+        amr.regrid(f, s, 16, lo, hi, size_of_level=rule)
     import numpy as np
     solve = reg = 0.0
     cu = steps = 0
@@ -426,7 +435,12 @@ def amr_workload(args):
         c = time.perf_counter()
         f.adapt(tags, 1, 0, lo, hi)
         d = time.perf_counter()
-        s.balance_regrid(f)
+        if rule is None:
+            s.balance_regrid(f)
+        else:
+            f.balance()
+            kind, src = f.remap()
+            s.regrid(f.mesh_mixed(f.patch_sizes(rule)), kind, src)
         h = time.perf_counter()
         for k, v in zip(parts, (c - b, d - c, h - d)):
             parts[k] += v
@@ -725,6 +739,8 @@ def main():
                     help="vortex: the headline line; vortex_period: both forms to t = 10 with their errors; "
                          "the others time one adaptive workload")
     ap.add_argument("--amr-form", type=int, default=1, help="form of the adaptive workloads (0 FP64, 1 FP32 flux)")
+    ap.add_argument("--mixed", action="store_true",
+                    help="four_quadrant with mixed patch sizes (8x8 on the coarsest two levels, 16x16 above)")
     ap.add_argument("--max-level", type=int, default=11, help="finest level of the shock-bubble workload")
     args = ap.parse_args()
     if args.warmup < 3:
