@@ -142,29 +142,33 @@ class ForestMesh:
     face_info, geom) from amrgpu_forest_external on first use -- valid while
     the forest is unchanged."""
 
-    def __init__(self, forest, n, nface):
+    def __init__(self, forest, n, nface, rule=None):
         self.forest = forest
         self.n = int(n)
         self.ncell = forest.num_quads
         self.nghost = 0
         self.nface = int(nface)
-        self.dof = NFIELDS * self.n * self.n * self.ncell
+        # mixed patch sizes by the session's level rule
+        self.sizes = None if rule is None else forest.patch_sizes(rule)
+        self.dof = NFIELDS * (self.ncells if self.sizes is not None else self.n * self.n * self.ncell)
         self._version = forest.version
         self._full = None
 
     @property
     def ncells(self):
+        if self.sizes is not None:
+            return int((self.sizes.astype(np.int64) ** 2).sum())
         return self.ncell * self.n * self.n
 
     def full(self):
         if self._full is None:
             if self.forest.version != self._version:
                 raise RuntimeError("the forest changed since this mesh was built")
-            self._full = self.forest.mesh(self.n)
+            self._full = self.forest.mesh(self.n) if self.sizes is None else self.forest.mesh_mixed(self.sizes)
         return self._full
 
     def __getattr__(self, name):
-        if name in ("cell_info", "face_info", "geom", "struct", "levels"):
+        if name in ("cell_info", "face_info", "geom", "struct", "levels", "offsets"):
             return getattr(self.full(), name)
         raise AttributeError(name)
 
@@ -320,8 +324,12 @@ class Forest:
         """Per-quad patch sizes from a level -> size rule (a callable, or a
         sequence indexed by level)."""
         _, level, _, _ = self.quads()
-        f = size_of_level if callable(size_of_level) else (lambda lv: size_of_level[lv])
-        return np.array([int(f(int(lv))) for lv in level], np.int32)
+        if callable(size_of_level):
+            table = np.array([int(size_of_level(lv)) for lv in range(32)], np.int32)
+        else:
+            t = np.asarray(size_of_level, np.int32)
+            table = t[np.minimum(np.arange(32), len(t) - 1)]
+        return table[level]
 
     def mesh_mixed(self, sizes):
         """The mesh with per-quad patch sizes (8 or 16): the forest's arrays
@@ -460,12 +468,26 @@ class Session:
         check(lib().amrgpu_session_regrid(self._s, C.byref(ms), ip(k), ip(s)), "regrid")
         self.mesh = mesh
 
+    def set_patch_rule(self, size_of_level):
+        """Mixed 8x8 / 16x16 patches by level for the regrids built on the
+        device (a callable level -> size, a sequence indexed by level, or
+        None to clear); see amrgpu_session_set_patch_rule."""
+        if size_of_level is None:
+            check(lib().amrgpu_session_set_patch_rule(self._s, None, 0), "set_patch_rule")
+            self._rule = None
+            return
+        f = size_of_level if callable(size_of_level) else (lambda lv: size_of_level[min(lv, len(size_of_level) - 1)])
+        table = np.array([int(f(lv)) for lv in range(32)], np.int32)
+        check(lib().amrgpu_session_set_patch_rule(self._s, ip(table), 32), "set_patch_rule")
+        self._rule = [int(v) for v in table]
+
     def regrid_forest(self, forest):
         """In place, from the forest after refine / coarsen / balance: quad
         descriptors built on the device, state remapped by the forest's
         remap table (amrgpu_session_regrid_forest)."""
         check(lib().amrgpu_session_regrid_forest(self._s, C.c_void_p(forest._f)), "regrid_forest")
-        self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s))
+        self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s),
+                               getattr(self, "_rule", None))
 
     def balance_regrid(self, forest):
         """forest.balance(session=self) and self.regrid_forest(forest) in one
@@ -473,7 +495,8 @@ class Session:
         device (amrgpu_session_balance_regrid)."""
         forest.version += 1
         check(lib().amrgpu_session_balance_regrid(self._s, C.c_void_p(forest._f)), "balance_regrid")
-        self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s))
+        self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s),
+                               getattr(self, "_rule", None))
 
     def quad_descriptors(self):
         """The device quad descriptors as a structured array (kind, nbr0,

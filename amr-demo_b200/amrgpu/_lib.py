@@ -79,6 +79,7 @@ PROTOTYPES = {
     "amrgpu_last_error": (C.c_int, []),
     "amrgpu_evolve_config": (C.c_int, [C.c_int, C.POINTER(ConfigStruct)]),
     "amrgpu_set_comm_ops": (C.c_int, [C.c_void_p]),
+    "amrgpu_session_set_patch_rule": (C.c_int, [C.c_void_p, i32p, C.c_int]),
     "amrgpu_has_comm_ops": (C.c_int, []),
     "amrgpu_session_autotune": (C.c_int, [C.c_void_p, C.c_int]),
     "amrgpu_session_launch_variant_info": (C.c_int, [C.c_void_p, C.c_int, i32p, i32p, i32p, i32p]),

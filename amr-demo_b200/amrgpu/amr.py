@@ -113,12 +113,14 @@ def regrid(forest, session, n, min_level, max_level, config=None, form=None, dev
     (a level -> 8 / 16 rule, Forest.patch_sizes): the host path, with the
     mesh of Forest.mesh_mixed."""
     tags = session.tag()
-    if size_of_level is not None:
+    if size_of_level is not None and not device_mesh:
         forest.adapt(tags, 1, 0, min_level, max_level)
         forest.balance()
         kind, src = forest.remap()
         session.regrid(forest.mesh_mixed(forest.patch_sizes(size_of_level)), kind, src)
     elif device_mesh:
+        if size_of_level is not None:
+            session.set_patch_rule(size_of_level)
         forest.adapt(tags, 1, 0, min_level, max_level)
         session.balance_regrid(forest)
     else:

@@ -29,7 +29,18 @@ cudaError_t launch_remap(int n, const double *qold, long long stride_old, double
                          cudaStream_t st);
 
 // mixed patch sizes (mixed.cu)
+struct SizeRule {
+    int size[32];  // patch size (8 or 16) of a quad at each level
+};
 const void *cfl_kernel_mixed();
+// Descriptors and work list of a mixed mesh from a forest's leaves (tree,
+// level, x, y) and its new quad descriptors: cells / flag16 / base / pos16
+// hold nq + 1 ints each; status (3 ints): [0] 1 when a hanging edge's two
+// fine quads differ in size, [1] the cells, [2] the 16x16 quads.
+size_t build_mix_scan_bytes(int nq);
+cudaError_t launch_build_mix(const int4 *leaves, const QuadDesc *quads, int nq, const SizeRule &rule, MixDesc *out,
+                             int *work, int *cells, int *flag16, int *base, int *pos16, void *scan_tmp,
+                             size_t scan_bytes, int *status, cudaStream_t st);
 int totals_mixed_grid(int nquad);
 cudaError_t launch_totals_mixed(const QuadDesc *quads, const MixDesc *mix, const double *q, long long stride,
                                 int nquad, double *partials, int grid, cudaStream_t st);

@@ -11,7 +11,13 @@
 //                        pairs (geometric position for unequal sizes)
 //   remap_mixed_kernel   refine / coarsen / copy of a regrid, with a size
 //                        change resampled by position
+//   build_mix (3 kernels + 2 scans)  the descriptors and work list of a
+//                        forest regridded on the device, sizes by level
 #include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
 
 #include "device_common.cuh"
 #include "flux_fp32.cuh"
@@ -248,6 +254,87 @@ __global__ void remap_mixed_kernel(const double *__restrict__ qold, long long st
             qnew[f * stride_new + nb + r] = v;
         }
     }
+}
+
+// ---- descriptors of a mixed mesh built on the device (the forest's
+// leaves and the new quad descriptors already there; sizes by level)
+
+__global__ void mix_sizes_kernel(const int4 *leaves, int nq, SizeRule rule, int *cells, int *flag16)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q > nq) return;
+    if (q == nq) {  // the scans' closing element
+        cells[q] = 0;
+        flag16[q] = 0;
+        return;
+    }
+    const int n = rule.size[leaves[q].y & 31];
+    cells[q] = n * n;
+    flag16[q] = n == 16 ? 1 : 0;
+}
+
+__global__ void mix_desc_kernel(const int4 *leaves, const QuadDesc *quads, int nq, SizeRule rule, const int *base,
+                                const int *pos16, MixDesc *out, int *work, int *status)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q == 0) {
+        status[1] = base[nq];   // cells
+        status[2] = pos16[nq];  // 16x16 quads
+    }
+    if (q >= nq) return;
+    const int n = rule.size[leaves[q].y & 31];
+    MixDesc md;
+    md.n = n;
+    md.base = base[q];
+    md.level = leaves[q].y;
+    md.pad = 0;
+    const QuadDesc &qd = quads[q];
+    for (int k = 0; k < 4; ++k) {
+        const SideDesc &d = qd.side[k];
+        MixSide ms{n, 0, 0, 0};
+        auto along = [&](int p) { return quads[p].corner[k < 2 ? 1 : 0]; };
+        if (d.kind == kSideFull || d.kind == kSideCoarseHang || d.kind == kSideFineHang) {
+            ms.n = rule.size[leaves[d.nbr0].y & 31];
+            ms.base0 = base[d.nbr0];
+        }
+        if (d.kind == kSideCoarseHang) {
+            if (rule.size[leaves[d.nbr1].y & 31] != ms.n) atomicOr(&status[0], 1);
+            ms.base1 = base[d.nbr1];
+            ms.half = along(d.nbr1) < along(d.nbr0) ? 1 : 0;
+        } else if (d.kind == kSideFineHang) {
+            const double *g = qd.corner;
+            const double len = k < 2 ? fabs(g[5] - g[1]) : fabs(g[2] - g[0]);
+            ms.half = along(q) - along(d.nbr0) > 0.25 * len ? 1 : 0;
+        }
+        md.side[k] = ms;
+    }
+    out[q] = md;
+    const int c16 = pos16[nq];
+    work[n == 16 ? pos16[q] : c16 + (q - pos16[q])] = q;
+}
+
+size_t build_mix_scan_bytes(int nq)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int *)nullptr, (int *)nullptr, (nq > 0 ? nq : 1) + 1);
+    return bytes;
+}
+
+cudaError_t launch_build_mix(const int4 *leaves, const QuadDesc *quads, int nq, const SizeRule &rule, MixDesc *out,
+                             int *work, int *cells, int *flag16, int *base, int *pos16, void *scan_tmp,
+                             size_t scan_bytes, int *status, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(status, 0, 3 * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    const int g = (nq + 1 + 255) / 256;
+    mix_sizes_kernel<<<g, 256, 0, st>>>(leaves, nq, rule, cells, flag16);
+    e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, cells, base, nq + 1, st);
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, flag16, pos16, nq + 1, st);
+    if (e != cudaSuccess) return e;
+    mix_desc_kernel<<<(std::max(nq, 1) + 255) / 256, 256, 0, st>>>(leaves, quads, nq, rule, base, pos16, out, work,
+                                                                   status);
+    return cudaGetLastError();
 }
 
 static int warps_grid(int nquad)

@@ -167,6 +167,10 @@ struct amrgpu_session {
     int cap_mix_old = 0;
     int *d_work = nullptr;            // work list: the 16x16 quads, then the 8x8 quads
     std::vector<int> h_work;
+    bool has_rule = false;            // patch size by level for regrids built on the device
+    SizeRule rule{};
+    void *d_mix_scratch = nullptr;    // sizes / offsets / scans of the device build
+    size_t mix_scratch_bytes = 0;
     int cap_work = 0;
     int nwork16 = 0, nwork8 = 0;
 };
@@ -367,9 +371,8 @@ int build_mix(amrgpu_session *s, const amrgpu_mesh_t *m)
 // Descriptors and work list of a mixed mesh to the device (grown buffers).
 // keep_old: the current descriptors move to d_mix_old first (the remap of
 // a regrid reads the old mesh's offsets).
-int upload_mix(amrgpu_session *s, bool keep_old)
+int mix_buffers(amrgpu_session *s, int nq, bool keep_old)
 {
-    const int nq = s->nquad;
     if (keep_old) {
         std::swap(s->d_mix, s->d_mix_old);
         std::swap(s->cap_mix, s->cap_mix_old);
@@ -393,6 +396,13 @@ int upload_mix(amrgpu_session *s, bool keep_old)
         if (!cuda_ok(cudaMalloc(&s->d_work, sizeof(int) * size_t(c)), "cudaMalloc work list")) return AMRGPU_ERR_CUDA;
         s->cap_work = c;
     }
+    return AMRGPU_OK;
+}
+
+int upload_mix(amrgpu_session *s, bool keep_old)
+{
+    const int nq = s->nquad;
+    if (int rc = mix_buffers(s, nq, keep_old)) return rc;
     if (nq > 0 &&
         (!cuda_ok(cudaMemcpyAsync(s->d_mix, s->h_mix.data(), sizeof(MixDesc) * size_t(nq), cudaMemcpyHostToDevice,
                                   s->stream),
@@ -404,6 +414,20 @@ int upload_mix(amrgpu_session *s, bool keep_old)
     // the host vectors stay alive until the next build (the copies above
     // read them asynchronously)
     return AMRGPU_OK;
+}
+
+// Sizes and offsets of a uniform session's current mesh into d_mix (the
+// remap source of a regrid that turns it into a mixed one).
+int upload_uniform_mix(amrgpu_session *s)
+{
+    s->qn.assign(size_t(s->nquad), s->n);
+    s->h_mix.assign(size_t(s->nquad), MixDesc{});
+    for (int q = 0; q < s->nquad; ++q) {
+        s->h_mix[size_t(q)].n = s->n;
+        s->h_mix[size_t(q)].base = q * s->n * s->n;
+    }
+    s->h_work.assign(size_t(s->nquad), 0);
+    return upload_mix(s, false);
 }
 
 // Cells of the local quads.
@@ -935,6 +959,7 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_mix);
     cudaFree(s->d_mix_old);
     cudaFree(s->d_work);
+    cudaFree(s->d_mix_scratch);
     s->ring.release();
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -1667,7 +1692,7 @@ int build_and_apply(amrgpu_session *s, const ForestDev &F)
     const size_t q4 = al(sizeof(int) * 4 * size_t(std::max(nq, 1)));
     const size_t o_emit = 0, o_scan = q4, o_emtr = 2 * q4, o_tmp = 3 * q4;
     const size_t o_stat = o_tmp + al(scan_bytes);
-    rc = ensure_dev(s, &s->d_mesh_scratch, &s->mesh_scratch_bytes, o_stat + 256);
+    rc = ensure_dev(s, &s->d_mesh_scratch, &s->mesh_scratch_bytes, o_stat + 256);  // status: 2 + 2 pad + 3 ints
     if (rc) return rc;
     char *base = static_cast<char *>(s->d_mesh_scratch);
     int *d_status = reinterpret_cast<int *>(base + o_stat);
@@ -1677,12 +1702,36 @@ int build_and_apply(amrgpu_session *s, const ForestDev &F)
                  "build quads"))
         return AMRGPU_ERR_CUDA;
     s->launches += nq > 0 ? 4 : 0;
+    // mixed patch sizes by the session's level rule: sizes, offsets,
+    // neighbour descriptors and the work list from the new descriptors
+    int *d_mstat = d_status + 4;
+    if (s->has_rule) {
+        if (!s->mixed && (rc = upload_uniform_mix(s))) return rc;
+        if ((rc = mix_buffers(s, nq, true))) return rc;
+        const size_t n1 = al(sizeof(int) * (size_t(nq) + 1));
+        const size_t sb = build_mix_scan_bytes(nq);
+        if ((rc = ensure_dev(s, &s->d_mix_scratch, &s->mix_scratch_bytes, 4 * n1 + al(sb)))) return rc;
+        char *mb = static_cast<char *>(s->d_mix_scratch);
+        if (!cuda_ok(launch_build_mix(F.leaves, s->d_quads_alt, nq, s->rule, s->d_mix, s->d_work,
+                                      reinterpret_cast<int *>(mb), reinterpret_cast<int *>(mb + n1),
+                                      reinterpret_cast<int *>(mb + 2 * n1), reinterpret_cast<int *>(mb + 3 * n1),
+                                      mb + 4 * n1, sb, d_mstat, s->stream),
+                     "build mixed descriptors"))
+            return AMRGPU_ERR_CUDA;
+        s->launches += 4;
+    }
     int *status = reinterpret_cast<int *>(s->h_stage);  // staging is at least 64 bytes
-    if (!cuda_ok(cudaMemcpyAsync(status, d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->stream), "D2H status") ||
+    if (!cuda_ok(cudaMemcpyAsync(status, d_status, (s->has_rule ? 7 : 2) * sizeof(int), cudaMemcpyDeviceToHost,
+                                 s->stream),
+                 "D2H status") ||
         !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
         return AMRGPU_ERR_CUDA;
     if (status[0]) {
         set_error(AMRGPU_ERR_MESH, "session regrid from a forest: the forest is not 2:1 balanced");
+        return AMRGPU_ERR_MESH;
+    }
+    if (s->has_rule && status[4]) {
+        set_error(AMRGPU_ERR_MESH, "mixed patch sizes: the two fine quads of a hanging edge differ in size");
         return AMRGPU_ERR_MESH;
     }
     const int nface = nq > 0 ? status[1] : 0;
@@ -1690,6 +1739,15 @@ int build_and_apply(amrgpu_session *s, const ForestDev &F)
     std::swap(s->cap_desc, s->cap_desc_alt);
     s->h_quads.clear();  // the live descriptors exist on the device only
     s->rect = true;      // brick quads are axis-aligned rectangles
+    if (s->has_rule) {
+        s->mixed = true;
+        s->h_mix.clear();  // (device only, like the quad descriptors)
+        s->h_work.clear();
+        s->qn.clear();
+        s->nwork16 = status[6];
+        s->nwork8 = nq - status[6];
+        return apply_regrid(s, nq, nface, (long long)status[5]);
+    }
     return apply_regrid(s, nq, nface);
 }
 
@@ -1737,15 +1795,7 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
     }
     if (!check_remap(s, m->ncell, kind, src_index)) return AMRGPU_ERR_ARG;
     if (mixed_path && !s->mixed) {
-        // the old (uniform) mesh's descriptors for the remap's source side
-        s->qn.assign(size_t(s->nquad), s->n);
-        s->h_mix.assign(size_t(s->nquad), MixDesc{});
-        for (int q = 0; q < s->nquad; ++q) {
-            s->h_mix[size_t(q)].n = s->n;
-            s->h_mix[size_t(q)].base = q * s->n * s->n;
-        }
-        s->h_work.assign(size_t(s->nquad), 0);
-        if (int e = upload_mix(s, false)) return e;
+        if (int e = upload_uniform_mix(s)) return e;
     }
     std::vector<QuadDesc> old = std::move(s->h_quads);
     const bool was_mixed = s->mixed;
@@ -1812,8 +1862,9 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
 int amrgpu_session_regrid_forest(amrgpu_session_t *s, const amrgpu_forest_t *f)
 {
     if (!s || !f || !f->f) return AMRGPU_ERR_ARG;
-    if (s->mixed) {
-        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: regrid through amrgpu_session_regrid");
+    if (s->mixed && !s->has_rule) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: set a patch-size rule (amrgpu_session_set_patch_rule) "
+                                          "or regrid through amrgpu_session_regrid");
         return AMRGPU_ERR_UNSUPPORTED;
     }
     if (s->stage_pos != 0) {
@@ -2177,10 +2228,7 @@ extern "C" {
 int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
 {
     if (!f || !f->f || !s) return -AMRGPU_ERR_ARG;
-    if (s->mixed) {
-        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: regrid through amrgpu_session_regrid");
-        return -AMRGPU_ERR_UNSUPPORTED;
-    }
+
     int live = 0;
     return balance_impl(s, f->f, &live, false);
 }
@@ -2188,8 +2236,9 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s)
 int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f)
 {
     if (!s || !f || !f->f) return AMRGPU_ERR_ARG;
-    if (s->mixed) {
-        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: regrid through amrgpu_session_regrid");
+    if (s->mixed && !s->has_rule) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: set a patch-size rule (amrgpu_session_set_patch_rule) "
+                                          "or regrid through amrgpu_session_regrid");
         return AMRGPU_ERR_UNSUPPORTED;
     }
     if (s->stage_pos != 0) {
@@ -2798,6 +2847,31 @@ void physics_go_gpu(int *dim, int *unstructured, int *nfields, int *nelem_subgri
     evolve(true, dim, unstructured, nfields, nelem_subgrid, ncell, nghost, nface, dof, cell_info, face_info, nsend, nrecv,
            send, recv, sizes, geom, soln, istep, regrid, visualize, checkpoint, evolve_solution, mpicomm_ext,
            total_time, compute_time, residual_time);
+}
+
+int amrgpu_session_set_patch_rule(amrgpu_session_t *s, const int *size_of_level, int nlevels)
+{
+    if (!s || nlevels < 0 || nlevels > 32 || (nlevels > 0 && !size_of_level)) return AMRGPU_ERR_ARG;
+    if (nlevels == 0) {
+        s->has_rule = false;
+        return AMRGPU_OK;
+    }
+    if (s->form != AMRGPU_FORM_FP32_FLUX || (s->launch_pinned && !s->mixed) || s->nghost != 0) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: the FP32-flux form with the library's launch, no ghosts");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    SizeRule r{};
+    for (int l = 0; l < 32; ++l) {
+        const int v = size_of_level[std::min(l, nlevels - 1)];
+        if (v != 8 && v != 16) {
+            set_error(AMRGPU_ERR_ARG, "patch-size rule: sizes must be 8 or 16");
+            return AMRGPU_ERR_ARG;
+        }
+        r.size[l] = v;
+    }
+    s->rule = r;
+    s->has_rule = true;
+    return AMRGPU_OK;
 }
 
 int amrgpu_set_comm_ops(const amrgpu_comm_ops_t *ops)

@@ -396,7 +396,7 @@ def amr_workload(args):
         lo, hi = 4, 9
         if args.mixed:
             # 8x8 patches on the two coarsest levels (the smooth far field),
-            # 16x16 on the refined levels; host-side balance and mesh arrays
+            # 16x16 on the refined levels
             rule = lambda lv: 8 if lv <= lo + 1 else 16  # noqa: E731
             sizes = f.patch_sizes(rule)
             mesh = f.mesh_mixed(sizes)
@@ -411,6 +411,8 @@ def amr_workload(args):
     cells0 = mesh.ncells
     cfg["final_time"] = 0.0
     s = ag.Session(mesh, cfg, form=args.amr_form)
+    if rule is not None:
+        s.set_patch_rule(rule)  # regrids build the mixed mesh on the device
     s.upload(soln)
     for _ in range(max(1, args.warmup // 5)):
         s.step(5)
@@ -435,12 +437,7 @@ def amr_workload(args):
         c = time.perf_counter()
         f.adapt(tags, 1, 0, lo, hi)
         d = time.perf_counter()
-        if rule is None:
-            s.balance_regrid(f)
-        else:
-            f.balance()
-            kind, src = f.remap()
-            s.regrid(f.mesh_mixed(f.patch_sizes(rule)), kind, src)
+        s.balance_regrid(f)
         h = time.perf_counter()
         for k, v in zip(parts, (c - b, d - c, h - d)):
             parts[k] += v
@@ -655,6 +652,26 @@ def run_gpu(args):
     amr = None
     if not args.no_learned:
         amr = learned_amr(args)
+    config3 = None
+    if not args.no_amr:
+        # config 3: the four-quadrant AMR loop (levels 4-9, regrid every 5
+        # steps, regrid time included) with 16x16 patches and with mixed
+        # 8x8 / 16x16 patches in one work list
+        import argparse as _ap
+        config3 = {}
+        for key, mixed in (("uniform_16", False), ("mixed_8_16", True)):
+            a3 = _ap.Namespace(workload="four_quadrant", mixed=mixed, amr_form=1, steps=60, warmup=10,
+                               max_level=args.max_level)
+            r3 = amr_workload(a3)
+            config3[key] = {k: r3[k] for k in ("value", "solve_only", "steps", "regrids", "cells_min", "cells_max",
+                                               "error", "regrid_ms")}
+            # the same steps (same finest cell, same dt) for both: wall time
+            # per step, regrid included, is the like-for-like figure
+            config3[key]["wall_ms_per_step"] = 1e3 * (r3["solve_s"] + r3["regrid_s"]) / max(r3["steps"], 1)
+            config3[key]["workload"] = r3["config"]["workload"]
+        config3["mixed_over_uniform"] = config3["mixed_8_16"]["value"] / config3["uniform_16"]["value"]
+        config3["uniform_over_mixed_wall_time"] = (config3["uniform_16"]["wall_ms_per_step"] /
+                                                   config3["mixed_8_16"]["wall_ms_per_step"])
     head = out[1]
     # the committed ncu traffic figure is for the default workload (16x16, level 6)
     traffic = traffic_per_launch(1) if (args.patch == 16 and args.level == 6) else None
@@ -683,6 +700,7 @@ def run_gpu(args):
         "e2e": e2e,
         "e2e_pinned": e2e_pinned,
         "learned_amr": amr,
+        "amr_config3": config3,
         "clocks": clocks,
         "gpu_launches": int(out[0]["launches"] + out[1]["launches"]),
         "cpu_baseline": cpu,
@@ -739,6 +757,7 @@ def main():
                     help="vortex: the headline line; vortex_period: both forms to t = 10 with their errors; "
                          "the others time one adaptive workload")
     ap.add_argument("--amr-form", type=int, default=1, help="form of the adaptive workloads (0 FP64, 1 FP32 flux)")
+    ap.add_argument("--no-amr", action="store_true", help="skip the adaptive config-3 lines (uniform and mixed)")
     ap.add_argument("--mixed", action="store_true",
                     help="four_quadrant with mixed patch sizes (8x8 on the coarsest two levels, 16x16 above)")
     ap.add_argument("--max-level", type=int, default=11, help="finest level of the shock-bubble workload")

@@ -22,8 +22,9 @@ extern "C" {
 #endif
 
 /* The communicator argument of the reference ABI. A caller built with MPI
- * passes its MPI_Comm (see physics_go_gpu.h); this single-process library
- * accepts it and does not use it. */
+ * passes its MPI_Comm (see physics_go_gpu.h); the library links no MPI and
+ * only hands it to the caller's MPI operations (amrgpu_comm_ops_t) in a
+ * multi-rank call. */
 #ifndef AMRGPU_COMM_T
 #define AMRGPU_COMM_T intptr_t
 #endif
@@ -415,6 +416,20 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s);
  * descend from (no remap table built or uploaded by the host after the
  * balance). */
 int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f);
+/* Mixed patch sizes (extension; the reference fixes one size per build):
+ * the patch size (8 or 16) of a quad at each level, size_of_level[l] for
+ * l < nlevels (the last entry for deeper levels); nlevels = 0 clears it.
+ * With a rule set, amrgpu_session_balance_regrid / _regrid_forest build a
+ * mesh of mixed sizes on the device (sizes, cell offsets as the running
+ * sum of n^2, neighbour sizes, the work list of the mixed-size sweep) and
+ * remap the state, resampling by position where a quad's size changes.
+ * A mesh passed to amrgpu_session_create / _regrid with per-quad sizes in
+ * cell_info[2] (the running sum of 4 n^2) is mixed without a rule. Mixed
+ * meshes: FP32-flux form only, no ghost quads, the two fine quads of a
+ * hanging edge share one size; an edge between two sizes pairs the cells
+ * that cover each piece of the finer side's length, one flux per piece for
+ * both quads (conservative). */
+int amrgpu_session_set_patch_rule(amrgpu_session_t *s, const int *size_of_level, int nlevels);
 /* Copies up to cap quad descriptors (160 bytes each: 4 sides x {kind, nbr0,
  * nbr1, face rank, level, bc} ints, then 8 corner doubles) to host memory;
  * returns the session's quad count. */

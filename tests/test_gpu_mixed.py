@@ -284,7 +284,7 @@ def test_adaptive_four_quadrant_with_mixed_patches(ag):
     from amrgpu import amr, workloads as W
     out = {}
     for mixed in (False, True):
-        f, mesh, cfg, soln = W.four_quadrant(seed=3, min_level=4, max_level=6, n=16, form=1)
+        f, mesh, cfg, soln = W.four_quadrant(seed=0, min_level=4, max_level=6, n=16, form=1)
         rule = (lambda lv: 8 if lv <= 5 else 16) if mixed else None
         s, st = amr.run(f, soln, 16, cfg, 1, 0.05, 5, 4, 6, size_of_level=rule)
         q = s.download()
@@ -296,3 +296,43 @@ def test_adaptive_four_quadrant_with_mixed_patches(ag):
     l1 = np.abs(b - a).sum() / np.abs(a).sum()
     assert l1 <= 2e-2, l1
     assert out[True][1] < out[False][1]  # fewer cells per step
+
+
+def test_device_built_mixed_regrid_equals_the_host_built_one(ag):
+    """A regrid with a patch-size rule built on the device (GPU 2:1 balance,
+    descriptors, sizes / offsets / work list by scans) gives the state the
+    host-built mixed mesh gives, bit for bit, after the remap and after
+    further steps -- from a uniform 16x16 session that turns mixed, and
+    again from the mixed one."""
+    rule = lambda lv: 8 if lv <= 2 else 16  # noqa: E731
+    runs = []
+    for device in (False, True):
+        f = meshes.two_level_ring(16, periodic=(1, 1))
+        cfg = config(16)
+        s0 = meshes.perturbed(f.initialize(16), 13, amp=1e-2)
+        s = ag.Session(f.mesh(16), cfg, form=ag.FORM_FP32_FLUX)
+        s.upload(s0)
+        s.step(2)
+        s.sync()
+        states = []
+        for cycle in range(2):
+            tags = s.tag()
+            tags[: max(1, len(tags) // 5)] = 1  # refine some, coarsen the rest where possible
+            if device:
+                s.set_patch_rule(rule)
+                f.adapt(tags, 1, 0, 1, 4)
+                s.balance_regrid(f)
+            else:
+                f.adapt(tags, 1, 0, 1, 4)
+                f.balance()
+                kind, src = f.remap()
+                s.regrid(f.mesh_mixed(f.patch_sizes(rule)), kind, src)
+            states.append(s.download())
+            s.step(3)
+            rep = s.sync()
+            assert rep["error"] == 0
+            states.append(s.download())
+        s.close()
+        runs.append(states)
+    for a, b in zip(*runs):
+        assert a.shape == b.shape and np.array_equal(a, b)
