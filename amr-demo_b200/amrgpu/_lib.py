@@ -125,6 +125,8 @@ PROTOTYPES = {
     "amrgpu_session_set_halo": (C.c_int, [C.c_void_p, i32p, C.c_int]),
     "amrgpu_session_halo_pack": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "amrgpu_session_halo_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "amrgpu_session_halo_unpack_edges": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "amrgpu_session_halo_pack_edges": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "amrgpu_session_local_scalars": (C.c_int, [C.c_void_p, f64p, i32p]),
     "amrgpu_session_tag": (C.c_int, [C.c_void_p, i32p]),
     "amrgpu_session_remap": (C.c_int, [C.c_void_p, C.c_void_p, i32p, i32p]),

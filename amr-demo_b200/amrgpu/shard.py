@@ -89,8 +89,15 @@ class Shard:
 
     @property
     def record(self):
-        """Doubles of one quad's halo record."""
+        """Doubles of one quad's whole patch (4 fields x n*n)."""
         return RECORD_FIELDS * self.mesh.n * self.mesh.n
+
+    @property
+    def halo_record(self):
+        """Doubles of one ghost quad on the wire: its four one-cell edge
+        strips per field (16*n), the only cells the stage kernels read of a
+        ghost (amrgpu_session_halo_pack_edges)."""
+        return RECORD_FIELDS * 4 * self.mesh.n
 
     def local_state(self, global_aos):
         """This rank's AoS input: its quads, then its ghosts."""
@@ -203,7 +210,7 @@ class GpuRank:
         check(lib().amrgpu_session_set_halo(self.session._s, sq.ctypes.data_as(C.POINTER(C.c_int)), len(sq)),
               "set_halo")
         self.device = torch.device("cuda", torch.cuda.current_device())
-        rec = shard.record
+        rec = shard.halo_record
         self.sendbuf = torch.empty(max(len(sq), 1) * rec, dtype=torch.float64, device=self.device)
         self.recvbuf = torch.empty(max(len(shard.ghosts), 1) * rec, dtype=torch.float64, device=self.device)
         self.stream = torch.cuda.ExternalStream(self.session.stream(), device=self.device)
@@ -221,12 +228,14 @@ class GpuRank:
     def pack(self):
         nsend = len(self.shard.send_quads)
         if nsend:
-            check(lib().amrgpu_session_halo_pack(self.session._s, 0, nsend, self.sendbuf.data_ptr()), "halo_pack")
+            check(lib().amrgpu_session_halo_pack_edges(self.session._s, 0, nsend, self.sendbuf.data_ptr()),
+                  "halo_pack")
 
     def unpack(self):
         ng = len(self.shard.ghosts)
         if ng:
-            check(lib().amrgpu_session_halo_unpack(self.session._s, 0, ng, self.recvbuf.data_ptr()), "halo_unpack")
+            check(lib().amrgpu_session_halo_unpack_edges(self.session._s, 0, ng, self.recvbuf.data_ptr()),
+                  "halo_unpack")
 
     def stage(self):
         """Runs the next stage; True when it was the step's last."""
@@ -293,7 +302,7 @@ class Distributed:
         plan = getattr(self, "_a2a", None)
         if plan is None:
             r = self.r
-            rec = r.shard.record
+            rec = r.shard.halo_record
             out_split = [0] * self.nranks
             in_split = [0] * self.nranks
             for peer, _, count in r.shard.send:
@@ -413,7 +422,7 @@ class LocalCluster:
                     r.pack()
                 self._sync_streams()
                 for dst, gfirst, src, sfirst, cnt in self.routes:
-                    rec = dst.shard.record
+                    rec = dst.shard.halo_record
                     dst.recvbuf[gfirst * rec:(gfirst + cnt) * rec].copy_(src.sendbuf[sfirst * rec:(sfirst + cnt) * rec])
                 self._sync_device()
                 ends = []

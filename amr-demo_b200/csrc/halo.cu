@@ -15,6 +15,14 @@
 // ncell .. ncell+count-1 (the reference's receives straight into the ghost
 // storage, physics_mpi.c:60-77). Both move 2 doubles per thread; n*n is even
 // for every supported patch size.
+//
+// Edge-strip format (pack_edges / unpack_edges): the stage kernels read a
+// ghost quad only at the cells that face their own quads -- its one-cell
+// edge rows and columns -- so a ghost can travel as its four edge strips:
+// per field the n cells of side 0 (column 0), side 1 (column n-1), side 2
+// (row 0), side 3 (row n-1), 16*n doubles (corner cells twice), 4x fewer
+// than the whole patch at 16x16, 2x at 8x8. A ghost's interior cells are
+// left as they were; nothing reads them.
 #include <cuda_runtime.h>
 
 #include "halo_kernels.h"
@@ -52,6 +60,43 @@ __global__ void halo_unpack_kernel(double *__restrict__ q, long long stride, int
     }
 }
 
+// Cell of a patch of size n at position p of side s's edge strip.
+__device__ __forceinline__ int strip_cell(int s, int p, int n)
+{
+    if (s == 0) return p * n;
+    if (s == 1) return p * n + n - 1;
+    if (s == 2) return p;
+    return (n - 1) * n + p;
+}
+
+__global__ void halo_pack_edges_kernel(const double *__restrict__ q, long long stride, int n,
+                                       const int *__restrict__ list, int count, double *__restrict__ out)
+{
+    const int per = 16 * n;  // doubles per quad: 4 fields x 4 sides x n
+    const long long total = (long long)count * per;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(e / per);
+        const int r = (int)(e - (long long)k * per);
+        const int f = r / (4 * n), s = (r / n) & 3, p = r % n;
+        out[e] = q[(long long)f * stride + (long long)__ldg(list + k) * n * n + strip_cell(s, p, n)];
+    }
+}
+
+__global__ void halo_unpack_edges_kernel(double *__restrict__ q, long long stride, int n, int first_quad,
+                                         int count, const double *__restrict__ in)
+{
+    const int per = 16 * n;
+    const long long total = (long long)count * per;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(e / per);
+        const int r = (int)(e - (long long)k * per);
+        const int f = r / (4 * n), s = (r / n) & 3, p = r % n;
+        q[(long long)f * stride + (long long)(first_quad + k) * n * n + strip_cell(s, p, n)] = in[e];
+    }
+}
+
 namespace {
 int halo_grid(long long pairs, int sms)
 {
@@ -78,6 +123,24 @@ cudaError_t launch_halo_unpack(double *q, long long stride, int n, int first_qua
     const int nn = n * n;
     halo_unpack_kernel<<<halo_grid((long long)count * 2 * nn, sms), 256, 0, st>>>(q, stride, nn, first_quad,
                                                                                    count, in);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_halo_pack_edges(const double *q, long long stride, int n, const int *list, int count,
+                                   double *out, int sms, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    halo_pack_edges_kernel<<<halo_grid((long long)count * 16 * n, sms), 256, 0, st>>>(q, stride, n, list, count,
+                                                                                       out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_halo_unpack_edges(double *q, long long stride, int n, int first_quad, int count,
+                                     const double *in, int sms, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    halo_unpack_edges_kernel<<<halo_grid((long long)count * 16 * n, sms), 256, 0, st>>>(q, stride, n, first_quad,
+                                                                                         count, in);
     return cudaGetLastError();
 }
 

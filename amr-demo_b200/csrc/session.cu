@@ -1186,6 +1186,34 @@ int amrgpu_session_halo_unpack(amrgpu_session_t *s, int first_ghost, int count, 
     return AMRGPU_OK;
 }
 
+int amrgpu_session_halo_pack_edges(amrgpu_session_t *s, int first, int count, double *d_out)
+{
+    if (!s || first < 0 || count < 0 || first + count > s->nsend || (count > 0 && !d_out)) return AMRGPU_ERR_ARG;
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme_of(s), swap_xy);
+    const double *q = rolebuf(s, plan[size_t(s->stage_pos)].in);
+    if (!cuda_ok(launch_halo_pack_edges(q, s->stride, s->n, s->d_send + first, count, d_out, s->sms, s->stream),
+                 "halo pack"))
+        return AMRGPU_ERR_CUDA;
+    if (count > 0) s->launches++;
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_halo_unpack_edges(amrgpu_session_t *s, int first_ghost, int count, const double *d_in)
+{
+    if (!s || first_ghost < 0 || count < 0 || first_ghost + count > s->nghost || (count > 0 && !d_in))
+        return AMRGPU_ERR_ARG;
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme_of(s), swap_xy);
+    double *q = rolebuf(s, plan[size_t(s->stage_pos)].in);
+    if (!cuda_ok(launch_halo_unpack_edges(q, s->stride, s->n, s->nquad + first_ghost, count, d_in, s->sms,
+                                          s->stream),
+                 "halo unpack"))
+        return AMRGPU_ERR_CUDA;
+    if (count > 0) s->launches++;
+    return AMRGPU_OK;
+}
+
 int amrgpu_session_local_scalars(amrgpu_session_t *s, double *norm_sq, int *flags)
 {
     if (!s) return AMRGPU_ERR_ARG;
@@ -2551,7 +2579,9 @@ int run_multirank(amrgpu_session *s, EvolveCache &ec, const amrgpu_comm_ops_t &o
                   int stride, int steps, double final_time, amrgpu_report_t &rep)
 {
     const int nsend = int(ec.send.size()) / stride, nrecv = int(ec.recv.size()) / stride;
-    const size_t rec = size_t(4) * size_t(s->n) * size_t(s->n);
+    // ghost records in the edge-strip format: the stage kernels read only a
+    // ghost's cells that face this rank's quads
+    const size_t rec = size_t(16) * size_t(s->n);
     HaloBuffers &hb = ec.halo;
     auto reduce_dt = [&]() -> bool {
         unsigned long long *slot = amrgpu_session_dt_slot(s);
@@ -2570,7 +2600,7 @@ int run_multirank(amrgpu_session *s, EvolveCache &ec, const amrgpu_comm_ops_t &o
     };
     auto exchange = [&]() -> bool {
         if (nsend > 0) {
-            if (amrgpu_session_halo_pack(s, 0, nsend, hb.d_send) != AMRGPU_OK ||
+            if (amrgpu_session_halo_pack_edges(s, 0, nsend, hb.d_send) != AMRGPU_OK ||
                 !cuda_ok(cudaMemcpyAsync(hb.h_send, hb.d_send, sizeof(double) * rec * size_t(nsend),
                                          cudaMemcpyDeviceToHost, s->stream),
                          "D2H halo"))
@@ -2586,7 +2616,7 @@ int run_multirank(amrgpu_session *s, EvolveCache &ec, const amrgpu_comm_ops_t &o
             if (!cuda_ok(cudaMemcpyAsync(hb.d_recv, hb.h_recv, sizeof(double) * rec * size_t(nrecv),
                                          cudaMemcpyHostToDevice, s->stream),
                          "H2D halo") ||
-                amrgpu_session_halo_unpack(s, 0, nrecv, hb.d_recv) != AMRGPU_OK)
+                amrgpu_session_halo_unpack_edges(s, 0, nrecv, hb.d_recv) != AMRGPU_OK)
                 return false;
         }
         return true;
@@ -2688,7 +2718,7 @@ void evolve(bool from_reference_layer, int *dim, int *unstructured, int *nfields
         if (multirank) {
             std::vector<int> quads(static_cast<size_t>(*nsend));
             for (int k = 0; k < *nsend; ++k) quads[size_t(k)] = send[stride * k];
-            const size_t rec = size_t(4) * size_t(*nelem_subgrid) * size_t(*nelem_subgrid);
+            const size_t rec = size_t(16) * size_t(*nelem_subgrid);  // edge-strip records
             if (amrgpu_session_set_halo(s, quads.data(), *nsend) != AMRGPU_OK ||
                 !ec.halo.reserve(rec * size_t(std::max(*nsend, 1)), rec * size_t(std::max(*nrecv, 1)))) {
                 amrgpu_session_destroy(s);

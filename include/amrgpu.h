@@ -320,7 +320,8 @@ int amrgpu_session_totals(amrgpu_session_t *s, double totals[4]);
  * cross-rank MIN of the CFL step before every step
  * (physics_runge_kutta_interface.c:96,149,205,262,316) and the SUM of the
  * squared residual norm (rk_time_integrators.c:74,162,274). One quad's
- * halo record is 4 fields x n*n doubles. */
+ * halo record is 4 fields x n*n doubles (whole patch) or 16*n (edge
+ * strips, below). */
 /* Enqueues the next stage of the current step; reports its 1-based index
  * and the stages of a step. A step begun here is finished here before
  * amrgpu_session_step / step_graph / regrid. */
@@ -341,6 +342,14 @@ int amrgpu_session_halo_pack(amrgpu_session_t *s, int first, int count, double *
 /* Records d_in (device) -> ghost quads first_ghost .. first_ghost+count-1
  * of the next stage's input, on the session stream. */
 int amrgpu_session_halo_unpack(amrgpu_session_t *s, int first_ghost, int count, const double *d_in);
+/* The same two calls with edge-strip records: per quad and field the n
+ * cells of its side 0 (column 0), 1 (column n-1), 2 (row 0) and 3 (row n-1),
+ * 16*n doubles (4x fewer than a whole record at n = 16). The stage kernels
+ * read a ghost quad only at cells facing local quads, i.e. on these strips;
+ * unpack leaves a ghost's interior cells as they were. The reference-named
+ * evolve entry points exchange ghosts in this format. */
+int amrgpu_session_halo_pack_edges(amrgpu_session_t *s, int first, int count, double *d_out);
+int amrgpu_session_halo_unpack_edges(amrgpu_session_t *s, int first_ghost, int count, const double *d_in);
 /* This rank's squared residual norm and flag bits (1 non-finite, 2
  * negative density or pressure) as of the last amrgpu_session_sync. */
 int amrgpu_session_local_scalars(amrgpu_session_t *s, double *norm_sq, int *flags);

@@ -41,9 +41,14 @@ class OracleRank:
         self.oc = O.make_config(self.n, cfg)
         self.scheme = int(cfg["time_scheme"])
         self.stages_per_step = _STAGES[self.scheme]
-        rec = shard.record
+        rec = shard.halo_record
         self.sendbuf = torch.zeros(max(len(shard.send_quads), 1) * rec, dtype=torch.float64)
         self.recvbuf = torch.zeros(max(len(shard.ghosts), 1) * rec, dtype=torch.float64)
+        n = self.n
+        # cells of the edge-strip format: sides 0..3 (column 0, column n-1,
+        # row 0, row n-1), n cells each, as amrgpu_session_halo_pack_edges
+        self.strip = np.array([p * n if s == 0 else p * n + n - 1 if s == 1 else p if s == 2 else (n - 1) * n + p
+                               for s in range(4) for p in range(n)], np.int64)
         self.dt = torch.zeros(1, dtype=torch.int64)
         self.time = 0.0
         self.steps = 0
@@ -72,15 +77,19 @@ class OracleRank:
     def pack(self):
         rec = self.shard.record
         if len(self.shard.send_quads):
-            blocks = self.Q.reshape(-1, rec)[self.shard.send_quads]
-            self.sendbuf[: blocks.size] = torch.from_numpy(blocks.reshape(-1))
+            # per quad and field the strip cells (AoS: cell c field f at 4c + f)
+            blocks = self.Q.reshape(-1, rec)[self.shard.send_quads].reshape(len(self.shard.send_quads), -1, 4)
+            strips = blocks[:, self.strip, :].transpose(0, 2, 1)
+            self.sendbuf[: strips.size] = torch.from_numpy(np.ascontiguousarray(strips).reshape(-1))
 
     def unpack(self):
         rec = self.shard.record
         ng = len(self.shard.ghosts)
         if ng:
             nl = self.shard.nlocal
-            self.Q[nl * rec:(nl + ng) * rec] = self.recvbuf[: ng * rec].numpy()
+            ghosts = self.Q[nl * rec:(nl + ng) * rec].reshape(ng, -1, 4)
+            strips = self.recvbuf[: ng * self.shard.halo_record].numpy().reshape(ng, 4, -1)
+            ghosts[:, self.strip, :] = strips.transpose(0, 2, 1)
 
     def _rhs(self):
         return O.rhs(self.mesh, self.Q, self.oc)

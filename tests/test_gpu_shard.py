@@ -88,7 +88,20 @@ def test_uneven_partition_on_hanging_ring(ag):
         assert np.array_equal(got, ref), form
 
 
-def test_halo_pack_and_unpack_move_whole_records(ag):
+def _stage_input(r):
+    import ctypes as C
+    import torch
+    from amrgpu import shard as S
+    from amrgpu._lib import lib
+    stride = C.c_longlong(0)
+    ptr = lib().amrgpu_session_stage_input(r.session._s, C.byref(stride))
+    return torch.as_tensor(S._DeviceView(ptr, (4, stride.value), "<f8"), device=r.device)
+
+
+def test_halo_moves_edge_strips(ag):
+    """GpuRank packs the send quads' four one-cell edge strips (16 n doubles
+    per quad: per field sides 0..3 -- column 0, column n-1, row 0, row n-1);
+    unpack writes them into the ghosts' edge cells and leaves the interior."""
     from amrgpu import shard as S
     import torch
     m, cfg, s0 = build(ag, 40, 8, 3)
@@ -101,25 +114,51 @@ def test_halo_pack_and_unpack_move_whole_records(ag):
         r.pack()
     r.stream.synchronize()
     n = m.n
-    rec = 4 * n * n
+    strip = np.array([p * n if s == 0 else p * n + n - 1 if s == 1 else p if s == 2 else (n - 1) * n + p
+                      for s in range(4) for p in range(n)])
     aos = loc.reshape(-1, n * n, 4)
-    want = aos[sh.send_quads].transpose(0, 2, 1).reshape(-1)
+    want = aos[sh.send_quads][:, strip, :].transpose(0, 2, 1).reshape(-1)
+    assert sh.halo_record == 16 * n
     assert np.array_equal(r.sendbuf[: len(want)].cpu().numpy(), want)
-    # unpack planted records into the ghosts; a stage reads them back
     ng = len(sh.ghosts)
-    planted = np.arange(ng * rec, dtype=np.float64)
-    r.recvbuf[: ng * rec].copy_(torch.from_numpy(planted))
+    before = _stage_input(r)[:, sh.nlocal * n * n:(sh.nlocal + ng) * n * n].cpu().numpy().reshape(4, ng, n * n)
+    planted = np.arange(ng * sh.halo_record, dtype=np.float64) + 0.5
+    r.recvbuf[: len(planted)].copy_(torch.from_numpy(planted))
     torch.cuda.synchronize()
     r.unpack()
     r.stream.synchronize()
+    g = _stage_input(r)[:, sh.nlocal * n * n:(sh.nlocal + ng) * n * n].cpu().numpy().reshape(4, ng, n * n)
+    expect = before.copy()
+    expect[:, :, strip] = planted.reshape(ng, 4, 4 * n).transpose(1, 0, 2)
+    assert np.array_equal(g, expect)
+    r.close()
+
+
+def test_whole_record_halo_calls(ag):
+    """amrgpu_session_halo_pack / _unpack keep the whole-patch format
+    (4 fields x n*n per quad)."""
+    from amrgpu import shard as S
     from amrgpu._lib import lib
-    import ctypes as C
-    stride = C.c_longlong(0)
-    ptr = lib().amrgpu_session_stage_input(r.session._s, C.byref(stride))
-    view = torch.as_tensor(S._DeviceView(ptr, (4, stride.value), "<f8"), device=r.device)
-    g = view[:, sh.nlocal * n * n:(sh.nlocal + ng) * n * n].cpu().numpy()
+    import torch
+    m, cfg, s0 = build(ag, 41, 8, 3)
+    sh = S.make_shard(m, S.partition(m.ncell, 2), 1)
+    r = S.GpuRank(sh, cfg)
+    loc = sh.local_state(s0)
+    r.upload(loc)
+    n = m.n
+    rec = 4 * n * n
+    ns, ng = len(sh.send_quads), len(sh.ghosts)
+    buf = torch.zeros(max(ns, ng) * rec, dtype=torch.float64, device=r.device)
+    assert lib().amrgpu_session_halo_pack(r.session._s, 0, ns, buf.data_ptr()) == 0
+    r.stream.synchronize()
+    want = loc.reshape(-1, n * n, 4)[sh.send_quads].transpose(0, 2, 1).reshape(-1)
+    assert np.array_equal(buf[: len(want)].cpu().numpy(), want)
+    planted = torch.arange(ng * rec, dtype=torch.float64, device=r.device)
+    assert lib().amrgpu_session_halo_unpack(r.session._s, 0, ng, planted.data_ptr()) == 0
+    r.stream.synchronize()
+    g = _stage_input(r)[:, sh.nlocal * n * n:(sh.nlocal + ng) * n * n].cpu().numpy()
     got = g.reshape(4, ng, n * n).transpose(1, 0, 2).reshape(-1)
-    assert np.array_equal(got, planted)
+    assert np.array_equal(got, planted.cpu().numpy())
     r.close()
 
 

@@ -115,6 +115,36 @@ def test_uneven_partition_with_hanging_faces_across_ranks(ag, oracle):
     assert np.array_equal(cl.download(), ref)
 
 
+def test_ghost_interiors_are_never_read(ag, oracle):
+    """Ghosts travel as their one-cell edge strips: with every ghost quad's
+    interior cells set to NaN after the start, a sharded run still equals
+    the unsharded one bit for bit (nothing reads a ghost off its strips)."""
+    from amrgpu import shard as S
+    n = 4
+    f = meshes.two_level_ring(n, periodic=(1, 1))
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=5, dt=0.01)
+    cfg.apply()
+    m = f.mesh(n)
+    s0 = meshes.perturbed(f.initialize(n), 4, amp=1e-2)
+    ref = s0.copy()
+    out = oracle.evolve(m, ref, oracle.make_config(n, cfg))
+    off = S.partition(m.ncell, 3)
+    ranks = [OracleRank(S.make_shard(m, off, r), cfg) for r in range(3)]
+    cl = S.LocalCluster(ranks)
+    cl.start(s0)
+    interior = np.array([j * n + i for j in range(1, n - 1) for i in range(1, n - 1)], np.int64)
+    poisoned = 0
+    for r in ranks:
+        nl, ng, rec = r.shard.nlocal, len(r.shard.ghosts), r.shard.record
+        if ng:
+            g = r.Q[nl * rec:(nl + ng) * rec].reshape(ng, n * n, 4)
+            g[:, interior, :] = np.nan
+            poisoned += ng
+    assert poisoned > 0
+    cl.step(out["steps"])
+    assert np.array_equal(cl.download(), ref)
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
