@@ -25,6 +25,7 @@ int stage_table_fp32(const StageLaunch **out);
 // The mixed-size row sweep (8x8 and 16x16 quads in one work list, FP32-flux
 // form): n = 0, never a uniform mesh's launch.
 const StageLaunch *stage_launch_mixed();
+int stage_table_mixed(const StageLaunch **out);
 
 // CFL step of a state (prologue of a segment): min over cells of the
 // reference's candidate, folded into scal->slot[slot].dt_bits.

@@ -502,7 +502,7 @@ int configure_launch(amrgpu_session *s, const StageLaunch *L)
         set_error(AMRGPU_ERR_UNSUPPORTED, "the FP32-flux form needs axis-aligned rectangular quads");
         return AMRGPU_ERR_UNSUPPORTED;
     }
-    if (s->mixed && (s->form != AMRGPU_FORM_FP32_FLUX || L != stage_launch_mixed())) {
+    if (s->mixed && (s->form != AMRGPU_FORM_FP32_FLUX || L->n != 0)) {
         set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: the FP32-flux form's mixed-size sweep only");
         return AMRGPU_ERR_UNSUPPORTED;
     }
@@ -719,6 +719,7 @@ int quad_bucket(int nquad)
 // bit for bit among themselves.
 bool tune_candidate(const amrgpu_session *s, const StageLaunch &L, const StageLaunch *def)
 {
+    if (s->mixed) return L.n == 0;
     if (L.n != s->n) return false;
     if (s->form == AMRGPU_FORM_FP32_FLUX && def && L.sweep != def->sweep) return false;
     return true;
@@ -730,15 +731,16 @@ bool tune_candidate(const amrgpu_session *s, const StageLaunch &L, const StageLa
 int autotune_session(amrgpu_session *s, bool retime)
 {
     s->tune_pending = false;
-    if (s->nquad == 0 || s->mixed) return AMRGPU_OK;  // a mixed mesh has one launch
+    if (s->nquad == 0) return AMRGPU_OK;
     const StageLaunch *tab;
-    const int cnt = (s->form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
-    const StageLaunch *def = default_launch(s->form, s->n, s->nquad);
+    const int cnt = s->mixed ? stage_table_mixed(&tab)
+                             : (s->form == AMRGPU_FORM_FP32_FLUX) ? stage_table_fp32(&tab) : stage_table_fp64(&tab);
+    const StageLaunch *def = session_default_launch(s);
     TuneEntry key;
     key.gpu = s->gpu_name;
     key.sms = s->sms;
     key.form = s->form;
-    key.n = s->n;
+    key.n = s->mixed ? 0 : s->n;  // 0: the mixed-size sweep
     key.bucket = quad_bucket(s->nquad);
     TuneEntry hit;
     if (!retime && tune_lookup(key, &hit)) {
@@ -925,7 +927,7 @@ int session_create_cfg(amrgpu_session_t **out, const amrgpu_mesh_t *m, const Phy
         return rc;
     }
     s->gpu_name = device_name(dev);
-    s->tune_pending = !s->launch_pinned && !s->mixed;
+    s->tune_pending = !s->launch_pinned;
     *out = s;
     return AMRGPU_OK;
 }
@@ -1658,8 +1660,9 @@ int apply_regrid(amrgpu_session *s, int nq, int nface, long long mixed_cells = -
     s->ncells_total = cells;
     s->stride = stride;
     // a launch chosen by the caller stays; the default follows the mesh size
-    int rc = configure_launch(s, (s->launch_pinned && !s->mixed) ? s->launch : session_default_launch(s));
-    if (!s->launch_pinned && !s->mixed) s->tune_pending = true;
+    const bool keep = s->launch_pinned && s->launch && (s->launch->n == 0) == s->mixed;
+    int rc = configure_launch(s, keep ? s->launch : session_default_launch(s));
+    if (!s->launch_pinned) s->tune_pending = true;
     if (rc != AMRGPU_OK) return rc;
     return prime(s, s->primed);
 }

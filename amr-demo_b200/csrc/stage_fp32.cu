@@ -115,10 +115,22 @@ int stage_table_fp32(const StageLaunch **out)
     return int(sizeof(kTable32) / sizeof(kTable32[0]));
 }
 
-// two warps per block, 128 registers: 16 resident warps per SM, as the
-// uniform sweeps' default
-static const StageLaunch kMixed{0, 2, 64, 8, 0, (const void *)sweep_mixed_kernel<2, 8>, 1};
+// The mixed-size sweep's shapes (n = 0): two warps per block at 128
+// registers (16 warps per SM; the two bodies spill ~100 bytes there), and at
+// 159 registers without spills (12 warps per SM). Every shape gives the same
+// bits; the autotuner picks one per mesh-size bucket.
+static const StageLaunch kMixed[] = {
+    StageLaunch{0, 2, 64, 8, 0, (const void *)sweep_mixed_kernel<2, 8>, 1},
+    StageLaunch{0, 2, 64, 6, 0, (const void *)sweep_mixed_kernel<2, 6>, 1},
+    StageLaunch{0, 4, 128, 3, 0, (const void *)sweep_mixed_kernel<4, 3>, 1},
+};
 
-const StageLaunch *stage_launch_mixed() { return &kMixed; }
+const StageLaunch *stage_launch_mixed() { return &kMixed[0]; }
+
+int stage_table_mixed(const StageLaunch **out)
+{
+    *out = kMixed;
+    return int(sizeof(kMixed) / sizeof(kMixed[0]));
+}
 
 }  // namespace amrgpu
