@@ -319,7 +319,7 @@ def run(forest, soln, n, config, final_time, regrid_interval, min_level, max_lev
 
 
 def run_checked(make, n, final_time, min_level, max_level, tol, mlp, regrid_interval=10, plain_interval=5,
-                l1_bound=1e-2, **kw):
+                l1_bound=1e-3, **kw):
     """The learned run validated against a plain-indicator run of the same
     problem: both final densities go to the uniform grid of max_level and
     when their relative L1 difference exceeds l1_bound the plain run's
