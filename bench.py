@@ -757,7 +757,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-indicator AMR comparison")
     ap.add_argument("--learned-only", action="store_true", help="run only the learned-indicator AMR comparison")
     ap.add_argument("--learned-seeds", type=int, default=64, help="seeded runs that make the training set")
-    ap.add_argument("--learned-interval", type=int, default=10,
+    ap.add_argument("--learned-interval", type=int, default=20,
                     help="regrid interval of the learned run (its model predicts the plain class that many steps ahead)")
     ap.add_argument("--learned-max-level", type=int, default=7,
                     help="finest level of the learned-indicator workload (8x8 patches; 7 = 1024^2 at the finest)")
