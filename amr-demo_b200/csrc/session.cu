@@ -166,6 +166,8 @@ struct amrgpu_session {
     MixDesc *d_mix_old = nullptr;     // ... of the mesh before a regrid (remap source)
     int cap_mix_old = 0;
     int *d_work = nullptr;            // work list: the 16x16 quads, then the 8x8 quads
+    int *d_work_old = nullptr;        // ... of the mesh before a regrid (kept until it is applied)
+    int cap_work_old = 0;
     std::vector<int> h_work;
     bool has_rule = false;            // patch size by level for regrids built on the device
     SizeRule rule{};
@@ -376,6 +378,8 @@ int mix_buffers(amrgpu_session *s, int nq, bool keep_old)
     if (keep_old) {
         std::swap(s->d_mix, s->d_mix_old);
         std::swap(s->cap_mix, s->cap_mix_old);
+        std::swap(s->d_work, s->d_work_old);
+        std::swap(s->cap_work, s->cap_work_old);
     }
     if (nq > s->cap_mix || !s->d_mix) {
         cudaStreamSynchronize(s->stream);
@@ -414,6 +418,16 @@ int upload_mix(amrgpu_session *s, bool keep_old)
     // the host vectors stay alive until the next build (the copies above
     // read them asynchronously)
     return AMRGPU_OK;
+}
+
+// Undoes mix_buffers(..., true) after a regrid that failed before it was
+// applied: the session's descriptors and work list are the old mesh's again.
+void mix_restore(amrgpu_session *s)
+{
+    std::swap(s->d_mix, s->d_mix_old);
+    std::swap(s->cap_mix, s->cap_mix_old);
+    std::swap(s->d_work, s->d_work_old);
+    std::swap(s->cap_work, s->cap_work_old);
 }
 
 // Sizes and offsets of a uniform session's current mesh into d_mix (the
@@ -961,6 +975,7 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_mix);
     cudaFree(s->d_mix_old);
     cudaFree(s->d_work);
+    cudaFree(s->d_work_old);
     cudaFree(s->d_mix_scratch);
     s->ring.release();
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1736,19 +1751,28 @@ int build_and_apply(amrgpu_session *s, const ForestDev &F)
     // mixed patch sizes by the session's level rule: sizes, offsets,
     // neighbour descriptors and the work list from the new descriptors
     int *d_mstat = d_status + 4;
+    // once the mixed descriptor buffers are swapped, a failure puts the old
+    // mesh's back: the session stays on the old mesh until apply_regrid
+    bool swapped = false;
+    auto fail = [&](int code) {
+        if (swapped) mix_restore(s);
+        return code;
+    };
     if (s->has_rule) {
         if (!s->mixed && (rc = upload_uniform_mix(s))) return rc;
-        if ((rc = mix_buffers(s, nq, true))) return rc;
+        rc = mix_buffers(s, nq, true);
+        swapped = true;
+        if (rc) return fail(rc);
         const size_t n1 = al(sizeof(int) * (size_t(nq) + 1));
         const size_t sb = build_mix_scan_bytes(nq);
-        if ((rc = ensure_dev(s, &s->d_mix_scratch, &s->mix_scratch_bytes, 4 * n1 + al(sb)))) return rc;
+        if ((rc = ensure_dev(s, &s->d_mix_scratch, &s->mix_scratch_bytes, 4 * n1 + al(sb)))) return fail(rc);
         char *mb = static_cast<char *>(s->d_mix_scratch);
         if (!cuda_ok(launch_build_mix(F.leaves, s->d_quads_alt, nq, s->rule, s->d_mix, s->d_work,
                                       reinterpret_cast<int *>(mb), reinterpret_cast<int *>(mb + n1),
                                       reinterpret_cast<int *>(mb + 2 * n1), reinterpret_cast<int *>(mb + 3 * n1),
                                       mb + 4 * n1, sb, d_mstat, s->stream),
                      "build mixed descriptors"))
-            return AMRGPU_ERR_CUDA;
+            return fail(AMRGPU_ERR_CUDA);
         s->launches += 4;
     }
     int *status = reinterpret_cast<int *>(s->h_stage);  // staging is at least 64 bytes
@@ -1756,14 +1780,14 @@ int build_and_apply(amrgpu_session *s, const ForestDev &F)
                                  s->stream),
                  "D2H status") ||
         !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
-        return AMRGPU_ERR_CUDA;
+        return fail(AMRGPU_ERR_CUDA);
     if (status[0]) {
         set_error(AMRGPU_ERR_MESH, "session regrid from a forest: the forest is not 2:1 balanced");
-        return AMRGPU_ERR_MESH;
+        return fail(AMRGPU_ERR_MESH);
     }
     if (s->has_rule && status[4]) {
         set_error(AMRGPU_ERR_MESH, "mixed patch sizes: the two fine quads of a hanging edge differ in size");
-        return AMRGPU_ERR_MESH;
+        return fail(AMRGPU_ERR_MESH);
     }
     const int nface = nq > 0 ? status[1] : 0;
     std::swap(s->d_quads, s->d_quads_alt);
@@ -1842,6 +1866,15 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
         return rc;
     }
     const int nq = m->ncell;
+    // buffers first (they only grow), so that nothing below fails after the
+    // mixed descriptors are swapped except the copies
+    rc = ensure_quad_arrays(s, nq);
+    if (rc == AMRGPU_OK) rc = ensure_desc(s, &s->d_quads, &s->cap_desc, nq);
+    if (rc != AMRGPU_OK) {
+        s->h_quads = std::move(old);
+        s->mixed = was_mixed;
+        return rc;
+    }
     if (mixed_path) {
         const int nq_old = s->nquad;
         s->nquad = nq;
@@ -1864,17 +1897,18 @@ int amrgpu_session_regrid(amrgpu_session_t *s, const amrgpu_mesh_t *m, const int
             return rc;
         }
         rc = upload_mix(s, true);
+        s->nquad = nq_old;  // apply_regrid moves the session to the new mesh
         if (rc != AMRGPU_OK) {
-            s->nquad = nq_old;
+            mix_restore(s);
+            s->qn = std::move(qn_keep);
+            s->h_mix = std::move(mix_keep);
+            s->h_work = std::move(work_keep);
+            s->nwork16 = n16_keep;
+            s->nwork8 = n8_keep;
+            s->h_quads = std::move(old);
+            s->mixed = was_mixed;
             return rc;
         }
-        s->nquad = nq_old;  // apply_regrid moves the session to the new mesh
-    }
-    rc = ensure_quad_arrays(s, nq);
-    if (rc == AMRGPU_OK) rc = ensure_desc(s, &s->d_quads, &s->cap_desc, nq);
-    if (rc != AMRGPU_OK) {
-        s->h_quads = std::move(old);
-        return rc;
     }
     bool ok = cuda_ok(cudaMemcpyAsync(s->d_kind, kind, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice, s->stream),
                       "H2D remap") &&
