@@ -336,3 +336,36 @@ def test_device_built_mixed_regrid_equals_the_host_built_one(ag):
         runs.append(states)
     for a, b in zip(*runs):
         assert a.shape == b.shape and np.array_equal(a, b)
+
+
+def test_refused_regrid_leaves_the_session_on_its_mesh(ag):
+    """A mixed regrid the library refuses (two fine siblings of different
+    sizes) raises and changes nothing: the session's state and its next
+    steps equal those of a session that never saw the regrid."""
+    f = ring(16)
+    sizes = family_sizes(f, np.random.default_rng(2))
+    m = f.mesh_mixed(sizes)
+    cfg = config(16)
+    s0 = meshes.perturbed(f.initialize(sizes), 6, amp=1e-2)
+    runs = []
+    for attempt in (False, True):
+        s = ag.Session(m, cfg, form=ag.FORM_FP32_FLUX)
+        s.upload(s0)
+        s.step(2)
+        s.sync()
+        if attempt:
+            bad = sizes.copy()
+            fi = m.face_info.reshape(-1, 11)[: m.nface]
+            f0 = int(fi[fi[:, 0] == 3][0, 3])
+            bad[f0] = 24 - bad[f0]
+            kind = np.zeros(len(sizes), np.int32)
+            src = np.arange(len(sizes), dtype=np.int32)
+            with pytest.raises(ag.AmrGpuError):
+                s.regrid(f.mesh_mixed(bad), kind, src)
+            s.mesh = m
+        s.step(3)
+        rep = s.sync()
+        assert rep["error"] == 0
+        runs.append(s.download())
+        s.close()
+    assert np.array_equal(runs[0], runs[1])
