@@ -76,4 +76,19 @@ struct DeviceScalars {
 
 enum { kFlagNonFinite = 1, kFlagNegative = 2, kFlagTimeout = 4 };
 
+// Programmatic dependent launch between the stage kernels of a stream. A
+// stage kernel is launched with programmatic stream serialisation, so the
+// hardware may schedule its blocks into the SM slots that the previous
+// stage's finished blocks free, before that grid has ended. Every stage
+// kernel therefore begins with stage_launch_gate(): it lets the next stage
+// be scheduled (launch_dependents: that kernel waits in turn), then waits
+// until the previous grid has completed and its writes are visible (wait)
+// before any load or store. Launched without the attribute, or after work
+// that is not a stage kernel, both instructions return at once.
+__device__ __forceinline__ void stage_launch_gate()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 }  // namespace amrgpu

@@ -605,6 +605,31 @@ int prime(amrgpu_session *s, bool keep_time = false)
     return AMRGPU_OK;
 }
 
+// Launch of a stage kernel (every one begins with stage_launch_gate) with
+// programmatic stream serialisation: its blocks may be scheduled while the
+// previous stage kernel's last blocks are still running, and wait on the
+// device for that grid to complete, so the launch gap between stages is
+// hidden. AMRGPU_PDL=0 launches with plain stream order instead.
+cudaError_t launch_stage_kernel(const amrgpu_session *s, StageArgs &a)
+{
+    static const bool pdl = [] {
+        const char *e = std::getenv("AMRGPU_PDL");
+        return !(e && std::atoi(e) == 0);
+    }();
+    void *args[] = {&a};
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(s->grid);
+    lc.blockDim = dim3(s->launch->threads);
+    lc.dynamicSmemBytes = s->launch->smem;
+    lc.stream = s->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelExC(&lc, s->launch->kernel, args);
+}
+
 // Stage st (0-based) of the current step: its kernel arguments and launch.
 int enqueue_stage(amrgpu_session *s, size_t st)
 {
@@ -644,10 +669,7 @@ int enqueue_stage(amrgpu_session *s, size_t st)
     a.work = s->d_work;
     a.nwork16 = s->nwork16;
     a.nwork8 = s->nwork8;
-    void *args[] = {&a};
-    cudaError_t e = cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args,
-                                     s->launch->smem, s->stream);
-    if (!cuda_ok(e, "stage kernel")) return AMRGPU_ERR_CUDA;
+    if (!cuda_ok(launch_stage_kernel(s, a), "stage kernel")) return AMRGPU_ERR_CUDA;
     s->launches++;
     return AMRGPU_OK;
 }
@@ -709,11 +731,7 @@ bool launch_rhs_stage(amrgpu_session *s)
     a.work = s->d_work;
     a.nwork16 = s->nwork16;
     a.nwork8 = s->nwork8;
-    void *args[] = {&a};
-    if (!cuda_ok(cudaLaunchKernel(s->launch->kernel, dim3(s->grid), dim3(s->launch->threads), args, s->launch->smem,
-                                  s->stream),
-                 "rhs kernel"))
-        return false;
+    if (!cuda_ok(launch_stage_kernel(s, a), "rhs kernel")) return false;
     s->launches++;
     return true;
 }

@@ -410,6 +410,7 @@ __global__ void __launch_bounds__(T, MINB) stage_kernel(const StageArgs a)
     static_assert(T % 32 == 0, "whole warps");
     static_assert(N <= 32 && QPB <= 64, "face code packing");
 
+    stage_launch_gate();
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     QuadDesc *sdesc = reinterpret_cast<QuadDesc *>(smem + S::o_desc);

@@ -382,18 +382,21 @@ __device__ __forceinline__ void sweep_body_mixed(const StageArgs &a)
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageArgs a)
 {
+    stage_launch_gate();
     sweep_body<16, WARPS>(a);
 }
 
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep8_kernel(const StageArgs a)
 {
+    stage_launch_gate();
     sweep_body<8, WARPS>(a);
 }
 
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep_mixed_kernel(const StageArgs a)
 {
+    stage_launch_gate();
     sweep_body_mixed<WARPS>(a);
 }
 

@@ -365,12 +365,14 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep64_16_kernel(const StageArgs a)
 {
+    stage_launch_gate();
     sweep64_body<16, WARPS>(a);
 }
 
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep64_8_kernel(const StageArgs a)
 {
+    stage_launch_gate();
     sweep64_body<8, WARPS>(a);
 }
 
