@@ -498,6 +498,12 @@ class Session:
         self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s),
                                getattr(self, "_rule", None))
 
+    def reserve(self, cells, quads):
+        """Grows the session's buffers now for meshes of up to `cells` cells
+        and `quads` quads, so that regrids within those bounds allocate
+        nothing (amrgpu_session_reserve)."""
+        check(lib().amrgpu_session_reserve(self._s, int(cells), int(quads)), "reserve")
+
     def quad_descriptors(self):
         """The device quad descriptors as a structured array (kind, nbr0,
         nbr1, rank, level, bc per side; 8 corner doubles)."""

@@ -138,11 +138,13 @@ def regrid(forest, session, n, min_level, max_level, config=None, form=None, dev
 
 
 def run(forest, soln, n, config, form, final_time, regrid_interval, min_level, max_level, max_steps=10 ** 7,
-        size_of_level=None):
+        size_of_level=None, headroom=3.0):
     """Evolve to final_time with a regrid every regrid_interval steps.
     size_of_level: mixed 8x8 / 16x16 patches by level (soln is then
     ignored: the initial state is evaluated at each quad's size).
-    Returns (session, stats)."""
+    headroom: the session's buffers are reserved up front for meshes this
+    many times the initial one (cells and quads), so that regrids within it
+    allocate nothing. Returns (session, stats)."""
     config["final_time"] = final_time
     config.apply()
     if size_of_level is not None:
@@ -152,6 +154,8 @@ def run(forest, soln, n, config, form, final_time, regrid_interval, min_level, m
     else:
         mesh = forest.mesh(n)
     s = Session(mesh, config, form=form)
+    if headroom > 1.0:
+        s.reserve(int(headroom * mesh.ncells), int(headroom * mesh.ncell))
     s.upload(soln)
     steps = 0
     cell_updates = 0

@@ -265,7 +265,8 @@ def to_uniform(forest, soln, n, level):
 
 
 def run(forest, soln, n, config, final_time, regrid_interval, min_level, max_level, tol, lo_frac=0.25, mlp=None,
-        judge_fraction=0.05, judge_bound=0.35, judge_min=200, judge_hard=0.5, form=1, seed=0, max_steps=10 ** 7):
+        judge_fraction=0.05, judge_bound=0.35, judge_min=200, judge_hard=0.5, form=1, seed=0, max_steps=10 ** 7,
+        headroom=3.0):
     """Evolve to final_time with a regrid every regrid_interval steps, tagged
     by the learned indicator (mlp) or the plain one (mlp None).
 
@@ -280,6 +281,10 @@ def run(forest, soln, n, config, final_time, regrid_interval, min_level, max_lev
     leaves room for; an untrained model disagrees on 60% or more."""
     config["final_time"] = final_time
     s = Session(forest.mesh(n), config, form=form)
+    if headroom > 1.0:
+        # buffers for meshes up to headroom x the initial one: no regrid
+        # within it allocates
+        s.reserve(int(headroom * s.mesh.ncells), int(headroom * s.mesh.ncell))
     s.upload(soln)
     steps = cells = regrids = 0
     t_solve = t_regrid = 0.0

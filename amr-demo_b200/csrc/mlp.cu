@@ -685,6 +685,9 @@ bool MlpState::refresh_bf16()
 bool MlpState::ensure_batch(int B)
 {
     if (B <= cap_batch) return true;
+    // twice the old capacity at least (rows stay a multiple of 128): a mesh
+    // that grows a few quads per regrid reallocates rarely
+    B = std::max(B, 2 * cap_batch);
     cudaStreamSynchronize(stream);
     for (void *p : batch_owned) cudaFree(p);
     batch_owned.clear();
@@ -733,6 +736,7 @@ bool MlpState::ensure_data(long long n)
 bool MlpState::ensure_judge(int n)
 {
     if (n <= cap_judge) return true;
+    n = std::max(2 * n, 1024);  // headroom: the judged quads follow the mesh
     cudaStreamSynchronize(stream);
     cudaFree(jump);
     cudaFree(which);

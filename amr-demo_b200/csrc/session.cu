@@ -2052,16 +2052,21 @@ BalLayout bal_layout(int cap, int ntrees)
 }
 
 // Grows the balance buffers to cap leaves, keeping the first keep leaves of
-// buffer `live` (leaves, origin, dirty).
+// buffer `live` (leaves, origin, dirty). The buffers are laid out by the
+// forest's tree count ntrees (bal_layout(cap, ntrees)); they are allocated
+// for max(ntrees, bal_trees) trees, so that a reservation for more trees
+// also serves a forest with fewer.
 int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
 {
+    const int alloc_trees = std::max(ntrees, s->bal_trees);
+    const BalLayout A = bal_layout(cap, alloc_trees);
     const BalLayout L = bal_layout(cap, ntrees);
-    const BalLayout O = bal_layout(s->bal_cap, s->bal_trees);
+    const BalLayout O = bal_layout(s->bal_cap, ntrees);
     void *nb[2] = {nullptr, nullptr};
     void *nw = nullptr;
-    bool ok = cuda_ok(cudaMalloc(&nb[0], L.buf), "cudaMalloc balance") &&
-              cuda_ok(cudaMalloc(&nb[1], L.buf), "cudaMalloc balance") &&
-              cuda_ok(cudaMalloc(&nw, L.work), "cudaMalloc balance");
+    bool ok = cuda_ok(cudaMalloc(&nb[0], A.buf), "cudaMalloc balance") &&
+              cuda_ok(cudaMalloc(&nb[1], A.buf), "cudaMalloc balance") &&
+              cuda_ok(cudaMalloc(&nw, A.work), "cudaMalloc balance");
     if (ok && keep > 0 && s->d_bal[live]) {
         char *src = static_cast<char *>(s->d_bal[live]);
         char *dst = static_cast<char *>(nb[0]);
@@ -2073,7 +2078,7 @@ int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
                                      s->stream),
                      "balance copy");
         // brick tables live in the work area (same forest: same tree count)
-        if (ok && s->d_bal_work && s->bal_trees == ntrees)
+        if (ok && s->d_bal_work && s->bal_trees >= ntrees)
             ok = cuda_ok(cudaMemcpyAsync(static_cast<char *>(nw) + L.o_tx, static_cast<char *>(s->d_bal_work) + O.o_tx,
                                          L.o_tmp - L.o_tx, cudaMemcpyDeviceToDevice, s->stream),
                          "balance copy");
@@ -2092,7 +2097,7 @@ int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
     s->d_bal[1] = nb[1];
     s->d_bal_work = nw;
     s->bal_cap = cap;
-    s->bal_trees = ntrees;
+    s->bal_trees = alloc_trees;
     return AMRGPU_OK;
 }
 
@@ -2154,7 +2159,7 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
             h_tab[2 * ntrees + t] = B.tree_at[t];
         }
         const int cap = std::max(nl + nl / 2, 64);  // passes that outgrow it grow it (2x)
-        if (cap > s->bal_cap || ntrees != s->bal_trees) {
+        if (cap > s->bal_cap || ntrees > s->bal_trees) {
             rc = bal_grow(s, std::max(cap, s->bal_cap), ntrees, 0, 0);
             if (rc) return -rc;
         }
@@ -2352,6 +2357,110 @@ int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f)
     set_brick(F, B, s->cfg.bc);
     F.nq = nq;
     return build_and_apply(s, F);
+}
+
+int amrgpu_session_reserve(amrgpu_session_t *s, long long cells, int quads)
+{
+    if (!s || cells < 0 || quads < 0) {
+        set_error(AMRGPU_ERR_ARG, "session_reserve: null session or negative size");
+        return AMRGPU_ERR_ARG;
+    }
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_reserve: a step begun with step_stage is not finished");
+        return AMRGPU_ERR_ARG;
+    }
+    // buffers may move: captured step graphs hold their addresses
+    if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return AMRGPU_ERR_CUDA;
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    // a device buffer grown to want elements, its first keep elements kept
+    auto grow_keep = [&](void **p, int *cap, size_t elem, int keep, int want) -> bool {
+        if (want <= *cap && *p) return true;
+        void *d = nullptr;
+        if (!cuda_ok(cudaMalloc(&d, elem * size_t(std::max(want, 1))), "cudaMalloc reserve")) return false;
+        if (keep > 0 && *p &&
+            !cuda_ok(cudaMemcpyAsync(d, *p, elem * size_t(keep), cudaMemcpyDeviceToDevice, s->stream), "reserve copy")) {
+            cudaFree(d);
+            return false;
+        }
+        if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) {
+            cudaFree(d);
+            return false;
+        }
+        cudaFree(*p);
+        *p = d;
+        *cap = std::max(want, 1);
+        return true;
+    };
+    // the state: four role buffers (their contents kept, field f of cell c
+    // stays at [f * stride + c]), the AoS staging and the totals partials
+    const long long need = ((std::max<long long>(cells, 1) + 31) / 32) * 32;
+    if (need > s->cap_stride) {
+        double *fresh[4] = {nullptr, nullptr, nullptr, nullptr};
+        double *aos = nullptr, *tot = nullptr;
+        const size_t bytes = sizeof(double) * 4 * size_t(need);
+        bool ok = true;
+        for (int k = 0; k < 4 && ok; ++k) ok = cuda_ok(cudaMalloc(&fresh[k], bytes), "cudaMalloc reserve state");
+        if (ok) ok = cuda_ok(cudaMalloc(&aos, bytes), "cudaMalloc reserve aos");
+        if (ok) ok = cuda_ok(cudaMalloc(&tot, sizeof(double) * 4 * size_t(totals_grid(need))), "cudaMalloc reserve totals");
+        for (int k = 0; k < 4 && ok; ++k)
+            ok = cuda_ok(cudaMemcpyAsync(fresh[k], s->buf[k], sizeof(double) * 4 * size_t(s->stride),
+                                         cudaMemcpyDeviceToDevice, s->stream),
+                         "reserve copy");
+        if (ok) ok = cuda_ok(cudaStreamSynchronize(s->stream), "sync");
+        if (!ok) {
+            for (double *p : fresh) cudaFree(p);
+            cudaFree(aos);
+            cudaFree(tot);
+            return AMRGPU_ERR_CUDA;
+        }
+        for (int k = 0; k < 4; ++k) {
+            cudaFree(s->buf[k]);
+            s->buf[k] = fresh[k];
+        }
+        cudaFree(s->d_aos);
+        cudaFree(s->d_tot);
+        s->d_aos = aos;
+        s->d_tot = tot;
+        s->cap_stride = need;
+    }
+    if (quads == 0) return AMRGPU_OK;
+    // per-quad tables: tags / remap, the live descriptors (kept) and the
+    // build target of the next regrid
+    int rc = ensure_quad_arrays(s, quads);
+    if (rc) return rc;
+    if (!grow_keep(reinterpret_cast<void **>(&s->d_quads), &s->cap_desc, sizeof(QuadDesc), s->nquad, quads))
+        return AMRGPU_ERR_CUDA;
+    if (!grow_keep(reinterpret_cast<void **>(&s->d_quads_alt), &s->cap_desc_alt, sizeof(QuadDesc), 0, quads))
+        return AMRGPU_ERR_CUDA;
+    // mixed patch sizes: the live sizes / work list (kept) and the spare pair
+    if (s->mixed || s->has_rule) {
+        const int keep = s->mixed ? s->nquad : 0;
+        if (!grow_keep(reinterpret_cast<void **>(&s->d_mix), &s->cap_mix, sizeof(MixDesc), keep, quads) ||
+            !grow_keep(reinterpret_cast<void **>(&s->d_work), &s->cap_work, sizeof(int), keep, quads) ||
+            !grow_keep(reinterpret_cast<void **>(&s->d_mix_old), &s->cap_mix_old, sizeof(MixDesc), 0, quads) ||
+            !grow_keep(reinterpret_cast<void **>(&s->d_work_old), &s->cap_work_old, sizeof(int), 0, quads))
+            return AMRGPU_ERR_CUDA;
+        const size_t n1 = al(sizeof(int) * (size_t(quads) + 1));
+        if ((rc = ensure_dev(s, &s->d_mix_scratch, &s->mix_scratch_bytes, 4 * n1 + al(build_mix_scan_bytes(quads)))))
+            return rc;
+    }
+    // descriptor build scratch (as build_and_apply lays it out)
+    const size_t q4 = al(sizeof(int) * 4 * size_t(quads));
+    if ((rc = ensure_dev(s, &s->d_mesh_scratch, &s->mesh_scratch_bytes,
+                         3 * q4 + al(build_quads_scan_bytes(quads)) + 256)))
+        return rc;
+    // balance: pre-balance remap table, leaf buffers for the passes (the
+    // balance sizes them at 1.5 times the leaves), tables for up to 64
+    // trees, pinned staging of the leaves
+    if ((rc = ensure_dev(s, &s->d_remap0, &s->remap0_bytes, 8 * size_t(quads) + 16))) return rc;
+    const int bcap = std::max(quads + quads / 2, 64);
+    const int btrees = std::max(s->bal_trees, 64);
+    if (bcap > s->bal_cap || btrees > s->bal_trees) {
+        if ((rc = bal_grow(s, std::max(bcap, s->bal_cap), btrees, 0, 0))) return rc;
+    }
+    return ensure_stage(s, 32 * size_t(bcap) + 12 * size_t(btrees) + 4096);
 }
 
 int amrgpu_session_quad_descriptors(amrgpu_session_t *s, void *out, int cap)

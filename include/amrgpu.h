@@ -439,6 +439,16 @@ int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f);
  * that cover each piece of the finer side's length, one flux per piece for
  * both quads (conservative). */
 int amrgpu_session_set_patch_rule(amrgpu_session_t *s, const int *size_of_level, int nlevels);
+/* Extension (the reference allocates per regrid through p4est): grows every
+ * device and pinned buffer that a regrid of this session may need -- the
+ * state (its contents kept), quad descriptors, remap and tag tables, mixed
+ * patch tables, balance buffers (forests of up to 64 trees) and the staging
+ * of the forest's leaves -- to hold a mesh of up to `cells` cells and
+ * `quads` quads, so that later regrids within those bounds allocate and
+ * free nothing (large device allocations and frees cost milliseconds each
+ * and synchronise the device). Beyond the bounds the buffers grow as
+ * before. Captured step graphs are released. */
+int amrgpu_session_reserve(amrgpu_session_t *s, long long cells, int quads);
 /* Copies up to cap quad descriptors (160 bytes each: 4 sides x {kind, nbr0,
  * nbr1, face rank, level, bc} ints, then 8 corner doubles) to host memory;
  * returns the session's quad count. */
