@@ -54,7 +54,7 @@ class MeshStruct(C.Structure):
 class JudgeStruct(C.Structure):
     """amrgpu_judge_t."""
 
-    _fields_ = [("judged", C.c_int), ("disagree", C.c_int), ("rate", C.c_double)]
+    _fields_ = [("judged", C.c_int), ("disagree", C.c_int), ("rate", C.c_double), ("coarser", C.c_int)]
 
 
 class ReportStruct(C.Structure):
@@ -164,6 +164,7 @@ PROTOTYPES = {
     "amrgpu_session_jumps": (C.c_int, [C.c_void_p, f64p]),
     "amrgpu_mlp_dataset_append": (C.c_longlong, [C.c_void_p, C.c_void_p, C.c_double, C.c_double]),
     "amrgpu_mlp_dataset_relabel": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_double]),
+    "amrgpu_mlp_dataset_cover": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_double]),
     "amrgpu_mlp_dataset_size": (C.c_longlong, [C.c_void_p]),
     "amrgpu_mlp_dataset_clear": (C.c_int, [C.c_void_p]),
     "amrgpu_mlp_dataset_labels": (C.c_int, [C.c_void_p, i32p, C.c_longlong]),

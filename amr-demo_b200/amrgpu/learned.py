@@ -89,6 +89,12 @@ class Mlp:
         check(lib().amrgpu_mlp_dataset_relabel(self._m, session._s, int(first), float(tol), float(lo_frac)),
               "mlp_dataset_relabel")
 
+    def cover(self, session, first, tol, lo_frac=0.25):
+        """Merges the plain classes of the session's current state into the
+        labels of rows [first, first + nquad), keeping the finer demand."""
+        check(lib().amrgpu_mlp_dataset_cover(self._m, session._s, int(first), float(tol), float(lo_frac)),
+              "mlp_dataset_cover")
+
     def size(self):
         return int(lib().amrgpu_mlp_dataset_size(self._m))
 
@@ -132,7 +138,7 @@ class Mlp:
         check(lib().amrgpu_session_learned_tags(session._s, self._m, float(judge_fraction), C.c_ulonglong(seed),
                                                 float(tol), float(lo_frac), _i32(t), C.byref(j)),
               "session_learned_tags")
-        return t, {"judged": j.judged, "disagree": j.disagree, "rate": j.rate}
+        return t, {"judged": j.judged, "disagree": j.disagree, "rate": j.rate, "coarser": j.coarser}
 
 
 def session_features(session):
@@ -199,11 +205,16 @@ def vortex_amr(seed=0, n=8, min_level=3, max_level=6, tol=0.02, lo_frac=0.25, fo
 
 
 def collect(mlp, seeds, n=8, min_level=3, max_level=6, tol=0.02, lo_frac=0.25, regrid_interval=5, regrids=20,
-            lookahead=True):
+            lookahead=True, cover_every=0):
     """Runs the seeded vortex family under the plain indicator and appends
     every quad of every regrid to the model's dataset; with `lookahead` a
     row's label is the plain class of the same quad at the next regrid
-    (what the indicator will ask for by then), else at the same time."""
+    (what the indicator will ask for by then), else at the same time. With
+    cover_every = k > 0 a row's label covers the whole interval instead:
+    the finest of the plain classes now and every k steps until the next
+    regrid (refine if any asks for it, coarsen only if all do) -- what a
+    plain indicator regridding every k steps would ask of the quad over the
+    interval."""
     for seed in seeds:
         f, cfg, soln, _ = vortex_amr(seed, n, min_level, max_level, tol, lo_frac)
         s = Session(f.mesh(n), cfg, form=1)
@@ -211,10 +222,19 @@ def collect(mlp, seeds, n=8, min_level=3, max_level=6, tol=0.02, lo_frac=0.25, r
         for _ in range(regrids):
             start = mlp.size()
             mlp.append(s, tol, lo_frac)
-            s.step(regrid_interval)
-            s.sync()
-            if lookahead:
-                mlp.relabel(s, start, tol, lo_frac)
+            if cover_every > 0:
+                done = 0
+                while done < regrid_interval:
+                    k = min(cover_every, regrid_interval - done)
+                    s.step(k)
+                    s.sync()
+                    mlp.cover(s, start, tol, lo_frac)
+                    done += k
+            else:
+                s.step(regrid_interval)
+                s.sync()
+                if lookahead:
+                    mlp.relabel(s, start, tol, lo_frac)
             cls = plain_classes(session_jumps(s), tol, lo_frac)
             regrid_by_classes(f, s, n, cls, min_level, max_level)
         s.close()
@@ -266,7 +286,7 @@ def to_uniform(forest, soln, n, level):
 
 def run(forest, soln, n, config, final_time, regrid_interval, min_level, max_level, tol, lo_frac=0.25, mlp=None,
         judge_fraction=0.05, judge_bound=0.35, judge_min=200, judge_hard=0.5, form=1, seed=0, max_steps=10 ** 7,
-        headroom=3.0):
+        headroom=3.0, judge_coarser=False):
     """Evolve to final_time with a regrid every regrid_interval steps, tagged
     by the learned indicator (mlp) or the plain one (mlp None).
 
@@ -278,7 +298,12 @@ def run(forest, soln, n, config, final_time, regrid_interval, min_level, max_lev
     (a broken model). A look-ahead model disagrees with the plain classes
     of the current state by design (it predicts the next regrid's; about
     20% of the quads on the vortex family), which is what judge_bound
-    leaves room for; an untrained model disagrees on 60% or more."""
+    leaves room for; an untrained model disagrees on 60% or more.
+    judge_coarser: the judge counts only the judged quads that the model
+    leaves coarser than the plain indicator would (plain refine and learned
+    not, or learned coarsen and plain not) -- for a model trained on
+    covering labels (collect(cover_every=...)), which asks for more
+    refinement than the plain classes of the moment by design."""
     config["final_time"] = final_time
     s = Session(forest.mesh(n), config, form=form)
     if headroom > 1.0:
@@ -288,7 +313,7 @@ def run(forest, soln, n, config, final_time, regrid_interval, min_level, max_lev
     s.upload(soln)
     steps = cells = regrids = 0
     t_solve = t_regrid = 0.0
-    judged = disagree = 0
+    judged = disagree = coarser = 0
     fallback_at = None
     time_now = 0.0
     while steps < max_steps:
@@ -306,8 +331,10 @@ def run(forest, soln, n, config, final_time, regrid_interval, min_level, max_lev
             cls, j = mlp.tags(s, tol, lo_frac, judge_fraction, seed=seed * 1000003 + regrids)
             judged += j["judged"]
             disagree += j["disagree"]
-            broken = j["judged"] >= 20 and j["rate"] > judge_hard
-            drift = judged >= judge_min and disagree > judge_bound * judged
+            coarser += j["coarser"]
+            bad_now, bad_all = (j["coarser"], coarser) if judge_coarser else (j["disagree"], disagree)
+            broken = j["judged"] >= 20 and bad_now > judge_hard * j["judged"]
+            drift = judged >= judge_min and bad_all > judge_bound * judged
             if broken or drift:
                 fallback_at = regrids
                 cls = plain_classes(session_jumps(s), tol, lo_frac)
@@ -318,7 +345,8 @@ def run(forest, soln, n, config, final_time, regrid_interval, min_level, max_lev
         t_regrid += time.perf_counter() - t1
     return s, {"steps": steps, "time": time_now, "cell_updates": cells, "solve_s": t_solve, "regrid_s": t_regrid,
                "regrids": regrids, "quads": s.mesh.ncell, "judged": judged, "disagree": disagree,
-               "disagree_rate": disagree / judged if judged else 0.0, "fallback_at": fallback_at,
+               "disagree_rate": disagree / judged if judged else 0.0,
+               "coarser_rate": coarser / judged if judged else 0.0, "fallback_at": fallback_at,
                "mean_cells": cells / max(steps, 1),
                "rate": cells / max(t_solve + t_regrid, 1e-30)}
 

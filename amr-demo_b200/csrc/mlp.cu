@@ -520,13 +520,21 @@ __global__ void argmax_kernel(const float *L, int B, int *cls)
 }
 
 // plain three-class label from the jump: refine (1) when J >= tol, coarsen
-// (0) when J < lo_frac * tol, keep (2) in between
-__global__ void label_kernel(const double *J, int n, double tol, double lo_frac, int *cls)
+// (0) when J < lo_frac * tol, keep (2) in between. cover: merged into the
+// label already there, keeping the finer demand (refine if either asks for
+// it, coarsen only if both do, keep otherwise)
+__global__ void label_kernel(const double *J, int n, double tol, double lo_frac, int *cls, int cover)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const double j = J[k];
-    cls[k] = j >= tol ? kClassRefine : (j < lo_frac * tol ? kClassCoarsen : kClassKeep);
+    int c = j >= tol ? kClassRefine : (j < lo_frac * tol ? kClassCoarsen : kClassKeep);
+    if (cover) {
+        const int old = cls[k];
+        c = (old == kClassRefine || c == kClassRefine) ? kClassRefine
+            : (old == kClassCoarsen && c == kClassCoarsen) ? kClassCoarsen : kClassKeep;
+    }
+    cls[k] = c;
 }
 
 // ---------------------------------------------------------------- host side
@@ -560,10 +568,11 @@ cudaError_t mlp_launch_jump(int n, const double *rho, const QuadDesc *quads, con
     return cudaGetLastError();
 }
 
-cudaError_t mlp_launch_labels(const double *J, int n, double tol, double lo_frac, int *cls, cudaStream_t st)
+cudaError_t mlp_launch_labels(const double *J, int n, double tol, double lo_frac, int *cls, cudaStream_t st,
+                              bool cover)
 {
     if (n <= 0) return cudaSuccess;
-    label_kernel<<<(n + 255) / 256, 256, 0, st>>>(J, n, tol, lo_frac, cls);
+    label_kernel<<<(n + 255) / 256, 256, 0, st>>>(J, n, tol, lo_frac, cls, cover ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -165,7 +165,11 @@ long long amrgpu_mlp_dataset_append(amrgpu_mlp_t *m, amrgpu_session_t *s, double
     return ms.n_data;
 }
 
-int amrgpu_mlp_dataset_relabel(amrgpu_mlp_t *m, amrgpu_session_t *s, long long first, double tol, double lo_frac)
+namespace {
+
+// the plain classes of the session's current state into the labels of
+// rows [first, first + nquad): replacing them, or merged (cover)
+int relabel_rows(amrgpu_mlp_t *m, amrgpu_session_t *s, long long first, double tol, double lo_frac, bool cover)
 {
     SessionView v{};
     if (!m || !session_view(s, &v) || !(tol > 0.0) || first < 0 || first + v.nquad > m->st.n_data)
@@ -175,10 +179,22 @@ int amrgpu_mlp_dataset_relabel(amrgpu_mlp_t *m, amrgpu_session_t *s, long long f
     if (!ms.ensure_judge(v.nquad)) return AMRGPU_ERR_CUDA;
     bool ok = ok_cuda(cudaStreamSynchronize(ms.stream), "sync") &&
               ok_cuda(mlp_launch_jump(v.n, v.q, v.quads, nullptr, v.nquad, ms.jump, st), "jump kernel") &&
-              ok_cuda(mlp_launch_labels(ms.jump, v.nquad, tol, lo_frac, ms.yall + first, st), "label kernel") &&
+              ok_cuda(mlp_launch_labels(ms.jump, v.nquad, tol, lo_frac, ms.yall + first, st, cover), "label kernel") &&
               ok_cuda(cudaStreamSynchronize(st), "sync");
     session_count_launches(s, 2);
     return ok ? AMRGPU_OK : AMRGPU_ERR_CUDA;
+}
+
+}  // namespace
+
+int amrgpu_mlp_dataset_relabel(amrgpu_mlp_t *m, amrgpu_session_t *s, long long first, double tol, double lo_frac)
+{
+    return relabel_rows(m, s, first, tol, lo_frac, false);
+}
+
+int amrgpu_mlp_dataset_cover(amrgpu_mlp_t *m, amrgpu_session_t *s, long long first, double tol, double lo_frac)
+{
+    return relabel_rows(m, s, first, tol, lo_frac, true);
 }
 
 long long amrgpu_mlp_dataset_size(const amrgpu_mlp_t *m) { return m ? m->st.n_data : 0; }
@@ -338,7 +354,7 @@ int amrgpu_session_learned_tags(amrgpu_session_t *s, amrgpu_mlp_t *m, double jud
         set_error(AMRGPU_ERR_UNSUPPORTED, "learned tags: patches of 8x8 or 16x16 cells only");
         return AMRGPU_ERR_UNSUPPORTED;
     }
-    if (judge) *judge = amrgpu_judge_t{0, 0, 0.0};
+    if (judge) *judge = amrgpu_judge_t{0, 0, 0.0, 0};
     if (v.nquad == 0) return AMRGPU_OK;
     MlpState &ms = m->st;
     cudaStream_t st = (cudaStream_t)v.stream;
@@ -371,11 +387,16 @@ int amrgpu_session_learned_tags(amrgpu_session_t *s, amrgpu_mlp_t *m, double jud
     session_count_launches(s, launches);
     if (!ok) return AMRGPU_ERR_CUDA;
     if (judge) {
-        int dis = 0;
-        for (int k = 0; k < nj; ++k) dis += jl[size_t(k)] != tags[which[size_t(k)]];
+        int dis = 0, coarser = 0;
+        for (int k = 0; k < nj; ++k) {
+            const int p = jl[size_t(k)], t = tags[which[size_t(k)]];
+            dis += p != t;
+            coarser += (p == kClassRefine && t != kClassRefine) || (t == kClassCoarsen && p != kClassCoarsen);
+        }
         judge->judged = nj;
         judge->disagree = dis;
         judge->rate = nj ? (double)dis / nj : 0.0;
+        judge->coarser = coarser;
     }
     return AMRGPU_OK;
 }

@@ -28,7 +28,8 @@ cudaError_t mlp_launch_features(int n, const double *q, long long stride, const 
                                 __nv_bfloat16 *X, cudaStream_t st);
 cudaError_t mlp_launch_jump(int n, const double *rho, const QuadDesc *quads, const int *which, int count, double *J,
                             cudaStream_t st);
-cudaError_t mlp_launch_labels(const double *J, int n, double tol, double lo_frac, int *cls, cudaStream_t st);
+cudaError_t mlp_launch_labels(const double *J, int n, double tol, double lo_frac, int *cls, cudaStream_t st,
+                              bool cover = false);
 
 struct MlpState {
     // FP32 master parameters and AdamW moments (flat: W1, b1, W2, b2, W3, b3)

@@ -495,6 +495,9 @@ typedef struct {
     int judged;       /* quads the plain indicator re-scored */
     int disagree;     /* of those, where the learned class differs */
     double rate;      /* disagree / judged (0 when none judged) */
+    int coarser;      /* of those, where the learned class leaves the quad
+                         coarser than the plain one: plain refine and learned
+                         not, or learned coarsen and plain not */
 } amrgpu_judge_t;
 int amrgpu_mlp_create(amrgpu_mlp_t **out, unsigned long long seed);
 void amrgpu_mlp_destroy(amrgpu_mlp_t *m);
@@ -514,6 +517,13 @@ long long amrgpu_mlp_dataset_append(amrgpu_mlp_t *m, amrgpu_session_t *s, double
  * labels that look ahead to a later state of the same mesh. */
 int amrgpu_mlp_dataset_relabel(amrgpu_mlp_t *m, amrgpu_session_t *s, long long first, double tol,
                                double lo_frac);
+/* As amrgpu_mlp_dataset_relabel, but each row's label is merged with the
+ * plain class of the current state instead of replaced, keeping the finer
+ * demand: refine if either asks for it, coarsen only if both do, keep
+ * otherwise. Called at several later states of one mesh, it labels each
+ * quad with what the plain indicator asks for at any of them. */
+int amrgpu_mlp_dataset_cover(amrgpu_mlp_t *m, amrgpu_session_t *s, long long first, double tol,
+                             double lo_frac);
 long long amrgpu_mlp_dataset_size(const amrgpu_mlp_t *m);
 int amrgpu_mlp_dataset_clear(amrgpu_mlp_t *m);
 /* Labels of the dataset rows [0, n). */

@@ -125,6 +125,31 @@ def test_dataset_append_and_relabel(ag, L, M):
     s.close()
 
 
+def test_dataset_cover_keeps_the_finer_demand(ag, L, M):
+    """Covering labels: a row's label merged with the plain class of a later
+    state of the same mesh is refine where either asks for it, coarsen where
+    both do, keep otherwise."""
+    tol = 0.02
+    f, cfg, soln, _ = L.vortex_amr(904, 8, 3, 5, tol)
+    m = f.mesh(8)
+    s = ag.Session(m, cfg, form=1)
+    s.upload(soln)
+    mlp = L.Mlp(seed=0)
+    assert mlp.append(s, tol) == m.ncell
+    ya = M.labels(M.jumps(s.download(), m, 8), tol)
+    s.step(60)
+    s.sync()
+    mlp.cover(s, 0, tol)
+    yb = M.labels(M.jumps(s.download(), m, 8), tol)
+    assert not np.array_equal(ya, yb)
+    assert (ya == L.REFINE).any() and (ya == L.COARSEN).any()
+    want = np.where((ya == L.REFINE) | (yb == L.REFINE), L.REFINE,
+                    np.where((ya == L.COARSEN) & (yb == L.COARSEN), L.COARSEN, L.KEEP))
+    assert np.array_equal(mlp.labels(), want)
+    mlp.close()
+    s.close()
+
+
 def test_train_epoch_matches_oracle_adamw_step(ag, L, M):
     """One AdamW step on one batch: the GPU update equals the oracle's
     gradient fed through AdamW (bias-corrected, decay on weights only)."""
@@ -210,6 +235,13 @@ def test_learned_tags_equal_argmax_of_predict_and_judge_counts(ag, L, trained):
     assert j["disagree"] <= j["judged"]
     # the judged quads are a subset: the disagreement cannot exceed the total one
     assert j["disagree"] <= int((tags != plain).sum())
+    assert j["coarser"] <= j["disagree"]
+    # every quad judged: both counts over the whole mesh
+    tags, j = m.tags(s, TOL, judge_fraction=1.0, seed=3)
+    assert j["judged"] == s.mesh.ncell
+    assert j["disagree"] == int((tags != plain).sum())
+    assert j["coarser"] == int((((plain == L.REFINE) & (tags != L.REFINE)) |
+                                ((tags == L.COARSEN) & (plain != L.COARSEN))).sum())
     s.close()
 
 
