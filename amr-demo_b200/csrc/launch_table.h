@@ -18,6 +18,9 @@ struct StageLaunch {
     size_t smem;
     const void *kernel;  // __global__ void(StageArgs)
     int sweep = 0;       // 1: a row-sweep kernel (one warp per qpb*32/threads quads)
+    // the same launch specialised for stages 1..3 of the Shu-Osher RK3 (the
+    // FP32-flux form's scheme), when the variant has them
+    const void *kernel_so[3] = {nullptr, nullptr, nullptr};
 };
 
 int stage_table_fp64(const StageLaunch **out);

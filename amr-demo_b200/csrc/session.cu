@@ -610,7 +610,7 @@ int prime(amrgpu_session *s, bool keep_time = false)
 // previous stage kernel's last blocks are still running, and wait on the
 // device for that grid to complete, so the launch gap between stages is
 // hidden. AMRGPU_PDL=0 launches with plain stream order instead.
-cudaError_t launch_stage_kernel(const amrgpu_session *s, StageArgs &a)
+cudaError_t launch_stage_kernel(const amrgpu_session *s, StageArgs &a, const void *kernel)
 {
     static const bool pdl = [] {
         const char *e = std::getenv("AMRGPU_PDL");
@@ -627,7 +627,7 @@ cudaError_t launch_stage_kernel(const amrgpu_session *s, StageArgs &a)
     at[0].val.programmaticStreamSerializationAllowed = 1;
     lc.attrs = at;
     lc.numAttrs = pdl ? 1 : 0;
-    return cudaLaunchKernelExC(&lc, s->launch->kernel, args);
+    return cudaLaunchKernelExC(&lc, kernel, args);
 }
 
 // Stage st (0-based) of the current step: its kernel arguments and launch.
@@ -669,7 +669,10 @@ int enqueue_stage(amrgpu_session *s, size_t st)
     a.work = s->d_work;
     a.nwork16 = s->nwork16;
     a.nwork8 = s->nwork8;
-    if (!cuda_ok(launch_stage_kernel(s, a), "stage kernel")) return AMRGPU_ERR_CUDA;
+    // the Shu-Osher stages run the variant specialised for them when it exists
+    const void *k = s->launch->kernel;
+    if (scheme == kSchemeRK3ShuOsher && st < 3 && s->launch->kernel_so[st]) k = s->launch->kernel_so[st];
+    if (!cuda_ok(launch_stage_kernel(s, a, k), "stage kernel")) return AMRGPU_ERR_CUDA;
     s->launches++;
     return AMRGPU_OK;
 }
@@ -731,7 +734,7 @@ bool launch_rhs_stage(amrgpu_session *s)
     a.work = s->d_work;
     a.nwork16 = s->nwork16;
     a.nwork8 = s->nwork8;
-    if (!cuda_ok(launch_stage_kernel(s, a), "rhs kernel")) return false;
+    if (!cuda_ok(launch_stage_kernel(s, a, s->launch->kernel), "rhs kernel")) return false;
     s->launches++;
     return true;
 }

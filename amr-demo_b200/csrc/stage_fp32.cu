@@ -85,8 +85,18 @@ const void *cfl_kernel_fp32(int n)
 // row-sweep kernel for 16x16 patches: one warp per quad, "quads per
 // block" = warps per block, no dynamic shared memory; all at 128
 // registers (16 resident warps per SM): fewer registers spill and run slower
-#define AMRGPU_SWEEP16(W, MINB) StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep16_kernel<W, MINB>, 1}
-#define AMRGPU_SWEEP8(W, MINB) StageLaunch{8, 2 * (W), 32 * (W), MINB, 0, (const void *)sweep8_kernel<W, MINB>, 1}
+#define AMRGPU_SWEEP16(W, MINB)                                                                          \
+    StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep16_kernel<W, MINB>, 1,                      \
+                {(const void *)sweep16_kernel<W, MINB, 1>, (const void *)sweep16_kernel<W, MINB, 2>,     \
+                 (const void *)sweep16_kernel<W, MINB, 3>}}
+#define AMRGPU_SWEEP8(W, MINB)                                                                           \
+    StageLaunch{8, 2 * (W), 32 * (W), MINB, 0, (const void *)sweep8_kernel<W, MINB>, 1,                  \
+                {(const void *)sweep8_kernel<W, MINB, 1>, (const void *)sweep8_kernel<W, MINB, 2>,       \
+                 (const void *)sweep8_kernel<W, MINB, 3>}}
+#define AMRGPU_SWEEPMIX(W, MINB)                                                                         \
+    StageLaunch{0, W, 32 * (W), MINB, 0, (const void *)sweep_mixed_kernel<W, MINB>, 1,                   \
+                {(const void *)sweep_mixed_kernel<W, MINB, 1>, (const void *)sweep_mixed_kernel<W, MINB, 2>, \
+                 (const void *)sweep_mixed_kernel<W, MINB, 3>}}
 
 static const StageLaunch kTable32[] = {
     AMRGPU_SWEEP16(4, 4),   // 128 registers, 16 warps per SM
@@ -120,9 +130,9 @@ int stage_table_fp32(const StageLaunch **out)
 // 159 registers without spills (12 warps per SM). Every shape gives the same
 // bits; the autotuner picks one per mesh-size bucket.
 static const StageLaunch kMixed[] = {
-    StageLaunch{0, 2, 64, 8, 0, (const void *)sweep_mixed_kernel<2, 8>, 1},
-    StageLaunch{0, 2, 64, 6, 0, (const void *)sweep_mixed_kernel<2, 6>, 1},
-    StageLaunch{0, 4, 128, 3, 0, (const void *)sweep_mixed_kernel<4, 3>, 1},
+    AMRGPU_SWEEPMIX(2, 8),
+    AMRGPU_SWEEPMIX(2, 6),
+    AMRGPU_SWEEPMIX(4, 3),
 };
 
 const StageLaunch *stage_launch_mixed() { return &kMixed[0]; }

@@ -269,11 +269,16 @@ __device__ __forceinline__ int facing_cell(int s, int m)
 // Shu-Osher RK3 of the FP32-flux form is the extension). kv is the cell's
 // residual, q0v its input state, A0(f) / A1(f) the first / second auxiliary
 // inputs; writes the outputs at gi and returns the new state in qn.
-template <typename A0F, typename A1F>
+// SCHEME / STAGE >= 0 / > 0 fix the scheme and the stage at compile time
+// (the same expressions, without the per-cell switch); -1 / 0 read them
+// from the arguments.
+template <int SCHEME = -1, int STAGE = 0, typename A0F, typename A1F>
 __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long long stride, long long gi,
                                           const double q0v[4], const double kv[4], A0F A0, A1F A1, double qn[4])
 {
-    switch (a.scheme) {
+    const int scheme = SCHEME >= 0 ? SCHEME : a.scheme;
+    const int stage = STAGE > 0 ? STAGE : a.stage;
+    switch (scheme) {
     case kSchemeRhsOnly:
 #pragma unroll
         for (int f = 0; f < 4; ++f) { a.out0[f * stride + gi] = kv[f]; qn[f] = q0v[f]; }
@@ -286,7 +291,7 @@ __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long lo
     }
     case kSchemeRK2: {
         double alpha1 = 1.0 * dt, beta1 = 0.5 * dt, beta2 = 0.5 * dt;
-        if (a.stage == 1) {
+        if (stage == 1) {
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 qn[f] = q0v[f] + alpha1 * kv[f];
@@ -305,14 +310,14 @@ __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long lo
     case kSchemeRK3: {
         double alpha1 = 1.00 * dt, alpha21 = 0.25 * dt, alpha22 = 0.25 * dt;
         double beta1 = 1.0 / 6.0 * dt, beta2 = 1.0 / 6.0 * dt, beta3 = 2.0 / 3.0 * dt;
-        if (a.stage == 1) {
+        if (stage == 1) {
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 qn[f] = q0v[f] + alpha1 * kv[f];
                 a.out0[f * stride + gi] = qn[f];
                 a.out1[f * stride + gi] = kv[f];
             }
-        } else if (a.stage == 2) {
+        } else if (stage == 2) {
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 double Q0 = A0(f);
@@ -333,15 +338,15 @@ __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long lo
     }
     case kSchemeRK4: {
         double alpha1 = 0.5 * dt, alpha2 = 0.5 * dt, alpha3 = 1.0 * dt, beta1 = 1.0 / 6.0 * dt;
-        if (a.stage == 1) {
+        if (stage == 1) {
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 qn[f] = q0v[f] + alpha1 * kv[f];
                 a.out0[f * stride + gi] = qn[f];
                 a.out1[f * stride + gi] = kv[f];
             }
-        } else if (a.stage < 4) {
-            double al = (a.stage == 2) ? alpha2 : alpha3;
+        } else if (stage < 4) {
+            double al = (stage == 2) ? alpha2 : alpha3;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 double Q0 = A0(f);
@@ -363,10 +368,10 @@ __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long lo
     }
     case kSchemeLSERK45: {
         double ra, rb;
-        lserk_coeff(a.stage, ra, rb);
+        lserk_coeff(stage, ra, rb);
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-            double qsv = (a.stage == 1) ? dt * kv[f] : A0(f) * ra + dt * kv[f];
+            double qsv = (stage == 1) ? dt * kv[f] : A0(f) * ra + dt * kv[f];
             qn[f] = q0v[f] + rb * qsv;
             a.out1[f * stride + gi] = qsv;
             a.out0[f * stride + gi] = qn[f];
@@ -374,10 +379,10 @@ __device__ __forceinline__ void rk_update(const StageArgs &a, double dt, long lo
         break;
     }
     default: {  // kSchemeRK3ShuOsher
-        if (a.stage == 1) {
+        if (stage == 1) {
 #pragma unroll
             for (int f = 0; f < 4; ++f) { qn[f] = q0v[f] + dt * kv[f]; a.out0[f * stride + gi] = qn[f]; }
-        } else if (a.stage == 2) {
+        } else if (stage == 2) {
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 qn[f] = 0.75 * A0(f) + 0.25 * (q0v[f] + dt * kv[f]);

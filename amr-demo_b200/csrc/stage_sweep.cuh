@@ -73,7 +73,7 @@ struct SweepAcc {
 // whose neighbour has this quad's patch size keep the reference's pairing
 // (physics_residual_face_*_structured.c: the same position, a coarse
 // hanging edge's two index-paired fluxes).
-template <int N, bool MIXED>
+template <int N, bool MIXED, int SO = 0>
 __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5][N][4], int quad, bool valid,
                                            int lane, double dt, const float qinf[4], SweepAcc &acc)
 {
@@ -211,7 +211,7 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
         double qbelow[4];    // input state of the row below
         double a0below[4] = {0.0, 0.0, 0.0, 0.0};  // first auxiliary input of the row below
         double a0next[4] = {0.0, 0.0, 0.0, 0.0};   // ... of the current row, loaded a row ahead of its use
-        const bool has_a0 = a.a0 != nullptr;
+        const bool has_a0 = SO > 0 ? SO >= 2 : a.a0 != nullptr;
         auto finish = [&](int jr, const double gup[4]) {
             const long long gi = qbase + jr * N + i;
             double kv[4], qn[4];
@@ -223,8 +223,9 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
             if (!valid) return;
             auto A0 = [&](int f) -> double { return a0below[f]; };
             auto A1 = [&](int f) -> double { return a.a1[f * stride + gi]; };
-            rk_update(a, dt, stride, gi, qbelow, kv, A0, A1, qn);
-            if (a.last_stage) {
+            if constexpr (SO > 0) rk_update<kSchemeRK3ShuOsher, SO>(a, dt, stride, gi, qbelow, kv, A0, A1, qn);
+            else rk_update(a, dt, stride, gi, qbelow, kv, A0, A1, qn);
+            if (SO > 0 ? SO == 3 : a.last_stage != 0) {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) my_norm += kv[f] * kv[f];
                 if (a.cfl_on) {
@@ -315,7 +316,7 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
 // finish early take more and the tail stays short. A quad past the end (odd
 // count, 8x8) is computed on its item's first quad and neither stored nor
 // reduced.
-template <int N, int WARPS>
+template <int N, int WARPS, int SO>
 __device__ __forceinline__ void sweep_body(const StageArgs &a)
 {
     constexpr int QPW = 32 / (2 * N);
@@ -332,9 +333,9 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
     const int nitems = (a.nquad + QPW - 1) / QPW;
     int item = blockIdx.x * WARPS + w;
     while (item < nitems) {
-        const bool valid = item * QPW + sub < a.nquad;
+        const bool valid = QPW == 1 || item * QPW + sub < a.nquad;
         const int quad = valid ? item * QPW + sub : item * QPW;
-        sweep_quad<N, false>(a, sedge[w], quad, valid, lane, dt, qinf, acc);
+        sweep_quad<N, false, SO>(a, sedge[w], quad, valid, lane, dt, qinf, acc);
         unsigned nxt = 0;
         if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);
         item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
@@ -347,7 +348,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
 // one counter as above; an item's patch size decides which body runs (the
 // choice is uniform over the warp). The two bodies share one per-warp edge
 // table (320 doubles for either size).
-template <int WARPS>
+template <int WARPS, int SO>
 __device__ __forceinline__ void sweep_body_mixed(const StageArgs &a)
 {
     constexpr unsigned FULL = 0xffffffffu;
@@ -363,14 +364,14 @@ __device__ __forceinline__ void sweep_body_mixed(const StageArgs &a)
     int item = blockIdx.x * WARPS + w;
     while (item < nitems) {
         if (item < a.nwork16) {
-            sweep_quad<16, true>(a, reinterpret_cast<double(*)[5][16][4]>(sedge_raw[w]), a.work[item], true, lane,
-                                 dt, qinf, acc);
+            sweep_quad<16, true, SO>(a, reinterpret_cast<double(*)[5][16][4]>(sedge_raw[w]), a.work[item], true,
+                                     lane, dt, qinf, acc);
         } else {
             const int k = 2 * (item - a.nwork16) + lane / 16;
             const bool valid = k < a.nwork8;
             const int quad = a.work[a.nwork16 + (valid ? k : k - 1)];
-            sweep_quad<8, true>(a, reinterpret_cast<double(*)[5][8][4]>(sedge_raw[w]), quad, valid, lane, dt,
-                                qinf, acc);
+            sweep_quad<8, true, SO>(a, reinterpret_cast<double(*)[5][8][4]>(sedge_raw[w]), quad, valid, lane, dt,
+                                    qinf, acc);
         }
         unsigned nxt = 0;
         if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);
@@ -379,25 +380,28 @@ __device__ __forceinline__ void sweep_body_mixed(const StageArgs &a)
     sweep_reduce<WARPS>(a, acc.dt_min, acc.norm, acc.flags, red, &s_last);
 }
 
-template <int WARPS, int MINB>
+// SO = 0: any scheme and stage, read from the arguments; SO = 1..3: stage
+// SO of the Shu-Osher RK3 (the FP32-flux form's scheme) fixed at compile
+// time, so the row loop carries no per-cell scheme or stage test.
+template <int WARPS, int MINB, int SO = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep16_kernel(const StageArgs a)
 {
     stage_launch_gate();
-    sweep_body<16, WARPS>(a);
+    sweep_body<16, WARPS, SO>(a);
 }
 
-template <int WARPS, int MINB>
+template <int WARPS, int MINB, int SO = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep8_kernel(const StageArgs a)
 {
     stage_launch_gate();
-    sweep_body<8, WARPS>(a);
+    sweep_body<8, WARPS, SO>(a);
 }
 
-template <int WARPS, int MINB>
+template <int WARPS, int MINB, int SO = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep_mixed_kernel(const StageArgs a)
 {
     stage_launch_gate();
-    sweep_body_mixed<WARPS>(a);
+    sweep_body_mixed<WARPS, SO>(a);
 }
 
 }  // namespace amrgpu
