@@ -125,7 +125,14 @@ __device__ __forceinline__ void bilinear_node(const double *g, double xi, double
 // solver_residual_face_full_structured_2d_module.F90:239
 __device__ __forceinline__ double cell_h_of(double h_base, int level, int n)
 {
-    return h_base * (1.0 / ldexp(1.0, level)) / (double)n;
+    // h_base / 2^level / n with n a power of two: both steps scale by a power
+    // of two and are exact, so two multiplications by exact powers of two
+    // (built from their exponent bits) give the same value as the divisions
+    // without the IEEE division sequences; level and n stay far inside the
+    // normal exponent range
+    const double inv_2l = __longlong_as_double((long long)(1023 - level) << 52);
+    const double inv_n = __longlong_as_double((long long)(1023 - (__ffs(n) - 1)) << 52);
+    return h_base * inv_2l * inv_n;
 }
 
 // Volume of the sub-cell with nodes n1..n4:

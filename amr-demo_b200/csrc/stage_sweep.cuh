@@ -33,11 +33,22 @@
 // and reloads, no barrier between the record, face and cell phases.
 #pragma once
 
+#include <type_traits>
+
 #include "flux_fp32.cuh"
 #include "stage_kernel.cuh"
 #include "sweep_common.cuh"
 
 namespace amrgpu {
+
+// a where the mask is all ones, b where it is zero: a select by bitwise
+// operations, which the compiler cannot turn into a branch
+__device__ __forceinline__ double blend_d(unsigned long long mask, double a, double b)
+{
+    const unsigned long long x = (unsigned long long)__double_as_longlong(a);
+    const unsigned long long y = (unsigned long long)__double_as_longlong(b);
+    return __longlong_as_double((long long)((x & mask) | (y & ~mask)));
+}
 
 // Neighbour cell facing position p of side s (the cell on the neighbour's
 // opposite side) in a patch of run-time size n.
@@ -237,16 +248,22 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
                 if (!(rho > 0.0) || !(pe > 0.0)) my_flags |= kFlagNegative;
             }
         };
+        // lanes whose low / high x-face is an edge face: all-ones masks
+        const unsigned long long m_lo = i == 0 ? ~0ull : 0ull, m_hi = i == N - 1 ? ~0ull : 0ull;
         double qnext[4];
 #pragma unroll
         for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (R * h) * N + i];
-#pragma unroll 1
-        for (int t = 0; t < R; ++t) {
+        // one row step. The first row (its y-face below is an edge or the row
+        // R-1/R face, no row below to finish) and the last (no row above to
+        // prefetch) are separate copies, so the loop in between tests neither.
+        auto row = [&](int t, auto first_c, auto last_c) {
+            constexpr bool FIRST = decltype(first_c)::value;
+            constexpr bool LAST = decltype(last_c)::value;
             const int j = R * h + t;
             double q4[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) q4[f] = qnext[f];
-            if (t < R - 1) {
+            if constexpr (!LAST) {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (j + 1) * N + i];
             }
@@ -265,7 +282,7 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
             float L[8], fx[4], fy[4], fxr[4];
 #pragma unroll
             for (int k = 0; k < 8; ++k) L[k] = __shfl_up_sync(FULL, P[k], 1, N);
-            if (t == 0) {
+            if constexpr (FIRST) {
 #pragma unroll
                 for (int k = 0; k < 8; ++k) below[k] = P[k];
             }
@@ -275,15 +292,19 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
             double xp[4];
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                const double fl = (i == 0) ? sedge[sub][0][j][f] : (double)fx[f];
-                const double fr = (i == N - 1) ? sedge[sub][1][j][f] : (double)fxr[f];
+                // every lane reads the edge faces (one address per half) and
+                // converts its interior ones; the choice is a bitwise blend
+                const double el = sedge[sub][0][j][f], er = sedge[sub][1][j][f];
+                const double fl = blend_d(m_lo, el, (double)fx[f]);
+                const double fr = blend_d(m_hi, er, (double)fxr[f]);
                 xp[f] = fr - fl;
             }
             // y-face at j-1/2 (the first row's is an edge or the row R-1/R face)
             double gy[4];
-            if (t == 0) {
+            if constexpr (FIRST) {
+                const double *ge = h == 0 ? sedge[sub][2][i] : sedge[sub][4][i];
 #pragma unroll
-                for (int f = 0; f < 4; ++f) gy[f] = h == 0 ? sedge[sub][2][i][f] : sedge[sub][4][i][f];
+                for (int f = 0; f < 4; ++f) gy[f] = ge[f];
             } else {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) gy[f] = (double)fy[f];
@@ -296,7 +317,11 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
             }
 #pragma unroll
             for (int k = 0; k < 8; ++k) below[k] = P[k];
-        }
+        };
+        row(0, std::true_type{}, std::false_type{});
+#pragma unroll 1
+        for (int t = 1; t < R - 1; ++t) row(t, std::false_type{}, std::false_type{});
+        row(R - 1, std::false_type{}, std::true_type{});
         {
             double gtop[4];
 #pragma unroll
