@@ -86,7 +86,8 @@ struct SweepAcc {
 // hanging edge's two index-paired fluxes).
 template <int N, bool MIXED, int SO = 0>
 __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5][N][4], int quad, bool valid,
-                                           int lane, double dt, const float qinf[4], SweepAcc &acc)
+                                           int lane, double dt, const float qinf[4], SweepAcc &acc,
+                                           unsigned &next_claim)
 {
     static_assert(N == 16 || N == 8, "row sweep for 16x16 and 8x8 patches");
     constexpr int NN = N * N;
@@ -106,94 +107,145 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
         const float fhx = (float)hx, fhy = (float)hy;
         const long long qbase = MIXED ? (long long)a.mix[quad].base : (long long)quad * NN;
         const double *Qq = a.qin + qbase;
-        auto load_rec = [&](const double *base, int cell, float P[8], double q[4]) {
-#pragma unroll
-            for (int f = 0; f < 4; ++f) q[f] = base[f * stride + cell];
-            cell_prims_fp32(q, P);
-        };
 
         // ---------------- edges: round 0 sides 0 / 1, round 1 sides 2 / 3
+        // A side as this lane sees it: its own edge cell, the pieces its edge
+        // cell pairs with (one for a full or fine side, two for a coarse
+        // hanging side, by position along the edge when the neighbour's
+        // patch size differs) and the face normal's length.
+        struct EdgeSide {
+            SideDesc d;
+            int s, own, nk, nn, ratio, hang_half;
+            long long nb0, nb1;
+            float hc, hp;
+        };
+        auto side_info = [&](int round) {
+            EdgeSide e;
+            e.s = 2 * round + h;
+            e.d = qd.side[e.s];
+            const int m = i;
+            e.own = (e.s == 0) ? m * N : (e.s == 1) ? m * N + N - 1 : (e.s == 2) ? m : (N - 1) * N + m;
+            e.hc = (float)cell_h_of(a.h_base, e.d.level, N);
+            e.hp = e.hc;
+            e.nk = (e.d.kind == kSideCoarseHang) ? 2 : 1;
+            e.nn = N;
+            e.ratio = 0;
+            e.hang_half = 0;
+            e.nb0 = e.nb1 = 0;
+            if constexpr (MIXED) {
+                if (e.d.kind != kSideBoundary) {
+                    const MixSide ms = a.mix[quad].side[e.s];
+                    e.nb0 = ms.base0;
+                    e.nb1 = ms.base1;
+                    if (ms.n != N) {
+                        e.nn = ms.n;
+                        e.hang_half = ms.half;
+                        double hn;
+                        if (e.d.kind == kSideFull) {
+                            e.ratio = e.nn > N ? e.nn / N : 1;
+                            hn = cell_h_of(a.h_base, e.d.level, e.nn);
+                            e.hp = (float)fmin(cell_h_of(a.h_base, e.d.level, N), hn);
+                        } else if (e.d.kind == kSideCoarseHang) {
+                            e.ratio = 2 * e.nn >= N ? 2 * e.nn / N : 1;
+                            hn = cell_h_of(a.h_base, e.d.level, e.nn);
+                            e.hp = (float)fmin(cell_h_of(a.h_base, e.d.level - 1, N), hn);
+                        } else {
+                            e.ratio = 1;
+                            hn = cell_h_of(a.h_base, e.d.level - 1, e.nn);
+                            e.hp = (float)fmin(cell_h_of(a.h_base, e.d.level, N), hn);
+                        }
+                        e.nk = e.ratio;
+                    }
+                }
+            }
+            return e;
+        };
+        // state offset (first cell of the quad) and cell of piece k
+        auto piece_src = [&](const EdgeSide &e, int k, long long &nb, int &fc) {
+            const int m = i;
+            if constexpr (MIXED) nb = k == 0 ? e.nb0 : e.nb1;
+            else nb = (long long)(k == 0 ? e.d.nbr0 : e.d.nbr1) * NN;
+            fc = facing_cell<N>(e.s, m);
+            if (MIXED && e.ratio > 0) {
+                // geometric pairing with a neighbour of another size
+                int p, which = 0;
+                if (e.d.kind == kSideFull) {
+                    p = e.nn > N ? m * e.ratio + k : m * e.nn / N;
+                } else if (e.d.kind == kSideCoarseHang) {
+                    const int gp = 2 * e.nn >= N ? m * e.ratio + k : m * 2 * e.nn / N;
+                    which = (gp / e.nn) ^ e.hang_half;
+                    p = gp % e.nn;
+                } else {
+                    p = (e.hang_half * N + m) * e.nn / (2 * N);
+                }
+                nb = which ? e.nb1 : e.nb0;
+                fc = facing_cell_rt(e.s, p, e.nn);
+            }
+        };
+        // every load of the edge phase first, so that their latencies
+        // overlap instead of following one another: the quad's own cells
+        // (both rounds' edge cells, the rows R-1 / R, the sweep's first row)
+        // need no descriptor and go out at once; the first neighbour cell of
+        // each round follows its side descriptor
+        double qo[2][4], qn0[2][4], qmid[4], qnext[4];
 #pragma unroll
         for (int round = 0; round < 2; ++round) {
             const int s = 2 * round + h, m = i;
-            const SideDesc d = qd.side[s];
             const int own = (s == 0) ? m * N : (s == 1) ? m * N + N - 1 : (s == 2) ? m : (N - 1) * N + m;
+#pragma unroll
+            for (int f = 0; f < 4; ++f) qo[round][f] = Qq[f * stride + own];
+        }
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            qmid[f] = Qq[f * stride + (R - 1 + h) * N + i];
+            qnext[f] = Qq[f * stride + (R * h) * N + i];
+        }
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+            const EdgeSide e = side_info(round);
+            long long nb = qbase;
+            int fc = e.own;  // a boundary side reads its own cell again (unused)
+            if (e.d.kind != kSideBoundary) piece_src(e, 0, nb, fc);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) qn0[round][f] = a.qin[nb + f * stride + fc];
+        }
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+            const EdgeSide e = side_info(round);
+            const int s = e.s, m = i;
             float Po[8], fl[4];
-            double qo[4];
-            load_rec(Qq, own, Po, qo);
-            const float hc = (float)cell_h_of(a.h_base, d.level, N);
+            cell_prims_fp32(qo[round], Po);
             double E[4];
-            if (d.kind == kSideBoundary) {
-                const float n0 = round == 0 ? (s == 0 ? -hc : hc) : 0.0f;
-                const float n1 = round == 0 ? 0.0f : (s == 2 ? -hc : hc);
-                bc_flux_rec_fp32(d.bc, Po, n0, n1, qinf, fl);
+            if (e.d.kind == kSideBoundary) {
+                const float n0 = round == 0 ? (s == 0 ? -e.hc : e.hc) : 0.0f;
+                const float n1 = round == 0 ? 0.0f : (s == 2 ? -e.hc : e.hc);
+                bc_flux_rec_fp32(e.d.bc, Po, n0, n1, qinf, fl);
 #pragma unroll
                 for (int f = 0; f < 4; ++f) E[f] = (s & 1) ? (double)fl[f] : -(double)fl[f];
             } else {
                 // one flux site for a side's one or two neighbours: the
                 // neighbour quad computes the same face at the same site, so
                 // both see bit-identical values (conservation)
-#pragma unroll
-                for (int f = 0; f < 4; ++f) E[f] = 0.0;
-                // pieces of this edge cell: k-th piece's neighbour (0 / 1),
-                // its position along the neighbour's edge, the normal length
-                int nk = (d.kind == kSideCoarseHang) ? 2 : 1;
-                int nn = N, ratio = 0, hang_swap = 0, hang_half = 0;
-                long long nb0 = 0, nb1 = 0;
-                float hp = hc;
-                if constexpr (MIXED) {
-                    const MixSide ms = a.mix[quad].side[s];
-                    nb0 = ms.base0;
-                    nb1 = ms.base1;
-                    if (ms.n != N) {
-                        nn = ms.n;
-                        hang_half = ms.half;
-                        hang_swap = ms.half;
-                        double hn;
-                        if (d.kind == kSideFull) {
-                            ratio = nn > N ? nn / N : 1;
-                            hn = cell_h_of(a.h_base, d.level, nn);
-                            hp = (float)fmin(cell_h_of(a.h_base, d.level, N), hn);
-                        } else if (d.kind == kSideCoarseHang) {
-                            ratio = 2 * nn >= N ? 2 * nn / N : 1;
-                            hn = cell_h_of(a.h_base, d.level, nn);
-                            hp = (float)fmin(cell_h_of(a.h_base, d.level - 1, N), hn);
-                        } else {
-                            ratio = 1;
-                            hn = cell_h_of(a.h_base, d.level - 1, nn);
-                            hp = (float)fmin(cell_h_of(a.h_base, d.level, N), hn);
-                        }
-                        nk = ratio;
-                    }
-                }
-#pragma unroll 1
-                for (int k = 0; k < nk; ++k) {
+                auto piece_flux = [&](const double qn4[4]) {
                     float Pn[8];
-                    double qn4[4];
-                    long long nb;
-                    if constexpr (MIXED) nb = k == 0 ? nb0 : nb1;
-                    else nb = (long long)(k == 0 ? d.nbr0 : d.nbr1) * NN;
-                    int fc = facing_cell<N>(s, m);
-                    if (MIXED && ratio > 0) {
-                        // geometric pairing with a neighbour of another size
-                        int p, which = 0;
-                        if (d.kind == kSideFull) {
-                            p = nn > N ? m * ratio + k : m * nn / N;
-                        } else if (d.kind == kSideCoarseHang) {
-                            const int g = 2 * nn >= N ? m * ratio + k : m * 2 * nn / N;
-                            which = (g / nn) ^ hang_swap;
-                            p = g % nn;
-                        } else {
-                            p = (hang_half * N + m) * nn / (2 * N);
-                        }
-                        nb = which ? nb1 : nb0;
-                        fc = facing_cell_rt(s, p, nn);
-                    }
-                    load_rec(a.qin + nb, fc, Pn, qn4);
+                    cell_prims_fp32(qn4, Pn);
                     const float *L = (s & 1) ? Po : Pn;
                     const float *R = (s & 1) ? Pn : Po;
-                    if (round == 0) roe_flux_axis_fp32<0>(L, R, hp, fl);
-                    else roe_flux_axis_fp32<1>(L, R, hp, fl);
+                    if (round == 0) roe_flux_axis_fp32<0>(L, R, e.hp, fl);
+                    else roe_flux_axis_fp32<1>(L, R, e.hp, fl);
+                };
+                piece_flux(qn0[round]);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) E[f] = 0.0 + (double)fl[f];
+#pragma unroll 1
+                for (int k = 1; k < e.nk; ++k) {
+                    long long nb;
+                    int fc;
+                    piece_src(e, k, nb, fc);
+                    double qn4[4];
+#pragma unroll
+                    for (int f = 0; f < 4; ++f) qn4[f] = a.qin[nb + f * stride + fc];
+                    piece_flux(qn4);
 #pragma unroll
                     for (int f = 0; f < 4; ++f) E[f] = E[f] + (double)fl[f];
                 }
@@ -204,8 +256,7 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
         // ---------------- the faces between rows R-1 and R (column i)
         {
             float P[8], O[8], fl[4];
-            double q4[4];
-            load_rec(Qq, (R - 1 + h) * N + i, P, q4);
+            cell_prims_fp32(qmid, P);
 #pragma unroll
             for (int k = 0; k < 8; ++k) O[k] = __shfl_xor_sync(FULL, P[k], N);
             if (h == 0) {
@@ -250,9 +301,6 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
         };
         // lanes whose low / high x-face is an edge face: all-ones masks
         const unsigned long long m_lo = i == 0 ? ~0ull : 0ull, m_hi = i == N - 1 ? ~0ull : 0ull;
-        double qnext[4];
-#pragma unroll
-        for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (R * h) * N + i];
         // one row step. The first row (its y-face below is an edge or the row
         // R-1/R face, no row below to finish) and the last (no row above to
         // prefetch) are separate copies, so the loop in between tests neither.
@@ -266,6 +314,10 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
             if constexpr (!LAST) {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) qnext[f] = Qq[f * stride + (j + 1) * N + i];
+            } else {
+                // the warp's next work item is claimed a row before this one
+                // ends: the atomic's round trip overlaps the last row
+                if (lane == 0) next_claim = atomicAdd(&a.scal->work_next, 1u);
             }
             // the auxiliary input of this row, used when the row is finished
             // in the next step (its load latency is covered by the fluxes)
@@ -337,8 +389,9 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
 
 // The uniform-size row sweep. Work items (QPW consecutive quads each): each
 // warp's first one by its index, then the next free one from a counter
-// (work_next, reset to 0 by the last block), so that warps and SMs that
-// finish early take more and the tail stays short. A quad past the end (odd
+// (work_next, reset to 0 by the last block; claimed during an item's last
+// row), so that warps and SMs that finish early take more and the tail
+// stays short. A quad past the end (odd
 // count, 8x8) is computed on its item's first quad and neither stored nor
 // reduced.
 template <int N, int WARPS, int SO>
@@ -360,9 +413,8 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
     while (item < nitems) {
         const bool valid = QPW == 1 || item * QPW + sub < a.nquad;
         const int quad = valid ? item * QPW + sub : item * QPW;
-        sweep_quad<N, false, SO>(a, sedge[w], quad, valid, lane, dt, qinf, acc);
-        unsigned nxt = 0;
-        if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);
+        unsigned nxt = 0;  // claimed by lane 0 during the item's last row
+        sweep_quad<N, false, SO>(a, sedge[w], quad, valid, lane, dt, qinf, acc, nxt);
         item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
     }
     sweep_reduce<WARPS>(a, acc.dt_min, acc.norm, acc.flags, red, &s_last);
@@ -388,18 +440,17 @@ __device__ __forceinline__ void sweep_body_mixed(const StageArgs &a)
     const int nitems = a.nwork16 + (a.nwork8 + 1) / 2;
     int item = blockIdx.x * WARPS + w;
     while (item < nitems) {
+        unsigned nxt = 0;  // claimed by lane 0 during the item's last row
         if (item < a.nwork16) {
             sweep_quad<16, true, SO>(a, reinterpret_cast<double(*)[5][16][4]>(sedge_raw[w]), a.work[item], true,
-                                     lane, dt, qinf, acc);
+                                     lane, dt, qinf, acc, nxt);
         } else {
             const int k = 2 * (item - a.nwork16) + lane / 16;
             const bool valid = k < a.nwork8;
             const int quad = a.work[a.nwork16 + (valid ? k : k - 1)];
             sweep_quad<8, true, SO>(a, reinterpret_cast<double(*)[5][8][4]>(sedge_raw[w]), quad, valid, lane, dt,
-                                    qinf, acc);
+                                    qinf, acc, nxt);
         }
-        unsigned nxt = 0;
-        if (lane == 0) nxt = atomicAdd(&a.scal->work_next, 1u);
         item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
     }
     sweep_reduce<WARPS>(a, acc.dt_min, acc.norm, acc.flags, red, &s_last);
