@@ -68,9 +68,15 @@ public:
 private:
     CopyPool()
     {
-        int n = 7;
+        // a quarter of the host's hardware threads (4 on the 16-core hosts
+        // measured: the pageable round trip ran at 1.7 / 2.6 / 3.1 / 3.0 /
+        // 2.7 / 1.4 G cell-updates/s with 1 / 2 / 4 / 6 / 8 / 16 threads --
+        // more threads than that contend for the host's memory bandwidth),
+        // the caller included; AMRGPU_COPY_THREADS overrides
+        const int hw = std::max(1, int(std::thread::hardware_concurrency()));
+        int n = std::min(8, std::max(1, hw / 4)) - 1;
         if (const char *e = std::getenv("AMRGPU_COPY_THREADS")) n = std::max(0, std::atoi(e) - 1);
-        n = std::min<int>(n, std::max(0, int(std::thread::hardware_concurrency()) - 1));
+        n = std::min<int>(n, hw - 1);
         for (int k = 0; k < n; ++k) workers_.emplace_back([this] { loop(); });
     }
     void loop()
