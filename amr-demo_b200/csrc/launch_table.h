@@ -18,9 +18,11 @@ struct StageLaunch {
     size_t smem;
     const void *kernel;  // __global__ void(StageArgs)
     int sweep = 0;       // 1: a row-sweep kernel (one warp per qpb*32/threads quads)
-    // the same launch specialised for stages 1..3 of the Shu-Osher RK3 (the
-    // FP32-flux form's scheme), when the variant has them
+    // the same launch specialised for stages 1..3 of one three-stage scheme
+    // (so_scheme: the Shu-Osher RK3 of the FP32-flux form, the reference's
+    // RK3 of the FP64 form), when the variant has them
     const void *kernel_so[3] = {nullptr, nullptr, nullptr};
+    int so_scheme = -1;
 };
 
 int stage_table_fp64(const StageLaunch **out);

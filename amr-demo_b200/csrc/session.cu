@@ -524,6 +524,10 @@ int configure_launch(amrgpu_session *s, const StageLaunch *L)
         if (!cuda_ok(cudaFuncSetAttribute(L->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L->smem)),
                      "cudaFuncSetAttribute"))
             return AMRGPU_ERR_CUDA;
+        for (const void *k : L->kernel_so)
+            if (k && !cuda_ok(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L->smem)),
+                              "cudaFuncSetAttribute"))
+                return AMRGPU_ERR_CUDA;
         int occ = 0;
         if (!cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->kernel, L->threads, L->smem),
                      "occupancy"))
@@ -669,9 +673,10 @@ int enqueue_stage(amrgpu_session *s, size_t st)
     a.work = s->d_work;
     a.nwork16 = s->nwork16;
     a.nwork8 = s->nwork8;
-    // the Shu-Osher stages run the variant specialised for them when it exists
+    // the stages of a three-stage scheme run the variant specialised for
+    // them when the launch has one for this scheme
     const void *k = s->launch->kernel;
-    if (scheme == kSchemeRK3ShuOsher && st < 3 && s->launch->kernel_so[st]) k = s->launch->kernel_so[st];
+    if (scheme == s->launch->so_scheme && st < 3 && s->launch->kernel_so[st]) k = s->launch->kernel_so[st];
     if (!cuda_ok(launch_stage_kernel(s, a, k), "stage kernel")) return AMRGPU_ERR_CUDA;
     s->launches++;
     return AMRGPU_OK;

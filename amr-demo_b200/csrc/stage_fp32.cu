@@ -88,15 +88,18 @@ const void *cfl_kernel_fp32(int n)
 #define AMRGPU_SWEEP16(W, MINB)                                                                          \
     StageLaunch{16, W, 32 * (W), MINB, 0, (const void *)sweep16_kernel<W, MINB>, 1,                      \
                 {(const void *)sweep16_kernel<W, MINB, 1>, (const void *)sweep16_kernel<W, MINB, 2>,     \
-                 (const void *)sweep16_kernel<W, MINB, 3>}}
+                 (const void *)sweep16_kernel<W, MINB, 3>},                                               \
+                kSchemeRK3ShuOsher}
 #define AMRGPU_SWEEP8(W, MINB)                                                                           \
     StageLaunch{8, 2 * (W), 32 * (W), MINB, 0, (const void *)sweep8_kernel<W, MINB>, 1,                  \
                 {(const void *)sweep8_kernel<W, MINB, 1>, (const void *)sweep8_kernel<W, MINB, 2>,       \
-                 (const void *)sweep8_kernel<W, MINB, 3>}}
+                 (const void *)sweep8_kernel<W, MINB, 3>},                                                \
+                kSchemeRK3ShuOsher}
 #define AMRGPU_SWEEPMIX(W, MINB)                                                                         \
     StageLaunch{0, W, 32 * (W), MINB, 0, (const void *)sweep_mixed_kernel<W, MINB>, 1,                   \
                 {(const void *)sweep_mixed_kernel<W, MINB, 1>, (const void *)sweep_mixed_kernel<W, MINB, 2>, \
-                 (const void *)sweep_mixed_kernel<W, MINB, 3>}}
+                 (const void *)sweep_mixed_kernel<W, MINB, 3>},                                            \
+                kSchemeRK3ShuOsher}
 
 static const StageLaunch kTable32[] = {
     AMRGPU_SWEEP16(4, 4),   // 128 registers, 16 warps per SM

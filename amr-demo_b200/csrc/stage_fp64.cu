@@ -94,10 +94,16 @@ const void *cfl_kernel_fp64(int n)
                 (const void *)stage_kernel<N, QPB, T, MINB, false, FluxOpsFP64>}
 
 // row-sweep kernels: one warp per 16x16 quad or per two 8x8 quads
-#define AMRGPU_SWEEP64_16(W, MINB)                                                             \
-    StageLaunch{16, W, 32 * (W), MINB, Sweep64Smem<16>::bytes(W), (const void *)sweep64_16_kernel<W, MINB>, 1}
-#define AMRGPU_SWEEP64_8(W, MINB)                                                              \
-    StageLaunch{8, 2 * (W), 32 * (W), MINB, Sweep64Smem<8>::bytes(W), (const void *)sweep64_8_kernel<W, MINB>, 1}
+#define AMRGPU_SWEEP64_16(W, MINB)                                                                      \
+    StageLaunch{16, W, 32 * (W), MINB, Sweep64Smem<16>::bytes(W), (const void *)sweep64_16_kernel<W, MINB>, 1,  \
+                {(const void *)sweep64_16_kernel<W, MINB, 1>, (const void *)sweep64_16_kernel<W, MINB, 2>,     \
+                 (const void *)sweep64_16_kernel<W, MINB, 3>},                                                 \
+                kSchemeRK3}
+#define AMRGPU_SWEEP64_8(W, MINB)                                                                       \
+    StageLaunch{8, 2 * (W), 32 * (W), MINB, Sweep64Smem<8>::bytes(W), (const void *)sweep64_8_kernel<W, MINB>, 1, \
+                {(const void *)sweep64_8_kernel<W, MINB, 1>, (const void *)sweep64_8_kernel<W, MINB, 2>,       \
+                 (const void *)sweep64_8_kernel<W, MINB, 3>},                                                  \
+                kSchemeRK3}
 
 // Per patch size the first entry is the default launch (a row sweep gives
 // way to the size's first block kernel on meshes too small to fill the GPU

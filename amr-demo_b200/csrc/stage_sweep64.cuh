@@ -60,7 +60,10 @@ struct Sweep64Smem {
     static constexpr size_t bytes(int warps) { return sizeof(double) * (size_t)per_warp * (size_t)warps; }
 };
 
-template <int N, int WARPS>
+// ST = 0: any scheme and stage, read from the arguments; ST = 1..3: stage
+// ST of the reference's RK3 (the FP64 form's default scheme) fixed at
+// compile time -- the same update expressions without the per-cell switch.
+template <int N, int WARPS, int ST>
 __device__ __forceinline__ void sweep64_body(const StageArgs &a)
 {
     static_assert(N == 16 || N == 8, "row sweep for 16x16 and 8x8 patches");
@@ -94,7 +97,10 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
     double my_dt_min = a.dt_cap;
     double my_norm = 0.0;
     int my_flags = 0;
-    const bool has_a0 = a.a0 != nullptr, has_a1 = a.a1 != nullptr;
+    // the reference RK3's auxiliary inputs: none in stage 1, Q0 and k1 in
+    // stage 2, the combination C in stage 3
+    const bool has_a0 = ST > 0 ? ST >= 2 : a.a0 != nullptr;
+    const bool has_a1 = ST > 0 ? ST == 2 : a.a1 != nullptr;
 
     // work items as in the FP32 sweep: first by warp index, then from the
     // quad counter; a quad past the end is computed on the item's first
@@ -103,7 +109,7 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
     const int nitems = (a.nquad + QPW - 1) / QPW;
     int item = blockIdx.x * WARPS + w;
     while (item < nitems) {
-        const bool valid = item * QPW + sub < a.nquad;
+        const bool valid = QPW == 1 || item * QPW + sub < a.nquad;
         const int quad = valid ? item * QPW + sub : item * QPW;
         const QuadDesc &qd = a.quads[quad];
         const double *g = qd.corner;
@@ -228,8 +234,9 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
             if (!valid) return;
             auto A0 = [&](int f) -> double { return ab[32 * f]; };
             auto A1 = [&](int f) -> double { return ab[32 * (4 + f)]; };
-            rk_update(a, dt, stride, gi, q0v, kv, A0, A1, qn);
-            if (a.last_stage) {
+            if constexpr (ST > 0) rk_update<kSchemeRK3, ST>(a, dt, stride, gi, q0v, kv, A0, A1, qn);
+            else rk_update(a, dt, stride, gi, q0v, kv, A0, A1, qn);
+            if (ST > 0 ? ST == 3 : a.last_stage != 0) {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) my_norm += kv[f] * kv[f];
                 if (a.cfl_on) {
@@ -318,10 +325,15 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
 #pragma unroll
                     for (int f = 0; f < 4; ++f) r[f] = 0.0;
                     edge_sum(j, r);
+                    // interior x-faces only (lane 0's low and lane N-1's high
+                    // face are edge faces, summed above): each sum is
+                    // formed and kept or dropped by a select, not a branch
 #pragma unroll
                     for (int f = 0; f < 4; ++f) {
-                        if (i > 0) r[f] = r[f] - F[f];
-                        if (i < N - 1) r[f] = r[f] + Fr[f];
+                        const double rl = r[f] - F[f];
+                        r[f] = i > 0 ? rl : r[f];
+                        const double rr = r[f] + Fr[f];
+                        r[f] = i < N - 1 ? rr : r[f];
                     }
                 } else {
 #pragma unroll
@@ -362,18 +374,18 @@ __device__ __forceinline__ void sweep64_body(const StageArgs &a)
     sweep_reduce<WARPS>(a, my_dt_min, my_norm, my_flags, red, &s_last);
 }
 
-template <int WARPS, int MINB>
+template <int WARPS, int MINB, int ST = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep64_16_kernel(const StageArgs a)
 {
     stage_launch_gate();
-    sweep64_body<16, WARPS>(a);
+    sweep64_body<16, WARPS, ST>(a);
 }
 
-template <int WARPS, int MINB>
+template <int WARPS, int MINB, int ST = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB) sweep64_8_kernel(const StageArgs a)
 {
     stage_launch_gate();
-    sweep64_body<8, WARPS>(a);
+    sweep64_body<8, WARPS, ST>(a);
 }
 
 }  // namespace amrgpu
