@@ -37,6 +37,8 @@
 // count. The result is byte-identical to decode_mesh(forest_external(...)).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cub/device/device_scan.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
@@ -127,27 +129,26 @@ __global__ void keys_kernel(ForestDev F);
 // look at the four corners for a leaf two or more levels finer (the dirty
 // leaf itself is flagged). Splitting a leaf's checks over threads shortens
 // each thread's chain of dependent binary searches; the flags are the same.
-__global__ void balance_check_kernel(ForestDev F, const unsigned char *dirty, unsigned char *flags)
+__device__ __forceinline__ void balance_check_item(const ForestDev &F, const unsigned char *dirty,
+                                                   unsigned char *flags, long long t)
 {
-    const long long total = 16ll * F.nq;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
+    {
         const int i = int(t >> 4), item = int(t & 15);
-        if (!dirty[i]) continue;
+        if (!dirty[i]) return;
         const int4 q = F.leaves[i];
         if (item < 8) {
             // fine side: the neighbour region across a face or a corner
-            if (q.y < 2) continue;
+            if (q.y < 2) return;
             const int d = item < 4 ? item : item + 1;  // 0..8 without the centre 4
             const int dx = d % 3 - 1, dy = d / 3 - 1;
             KeyD k;
-            if (!shifted_d(F, q.x, q.y, q.z, q.w, dx, dy, k)) continue;
+            if (!shifted_d(F, q.x, q.y, q.z, q.w, dx, dy, k)) return;
             const int c = locate_d(F, k.tree, k.x, k.y);
             if (c >= 0 && F.leaves[c].y < q.y - 1) flags[c] = 1;
-            continue;
+            return;
         }
         // coarse side
-        if (q.y + 2 > kMaxLevelG) continue;
+        if (q.y + 2 > kMaxLevelG) return;
         const long long L = qlen_d(q.y);
         const int lim = q.y + 2;
         bool fine = false;
@@ -191,6 +192,14 @@ __global__ void balance_check_kernel(ForestDev F, const unsigned char *dirty, un
     }
 }
 
+__global__ void balance_check_kernel(ForestDev F, const unsigned char *dirty, unsigned char *flags)
+{
+    const long long total = 16ll * F.nq;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x)
+        balance_check_item(F, dirty, flags, t);
+}
+
 // Leaves after a balance pass per leaf: 4 if flagged for refinement, else
 // 1, and 0 past the last leaf (the scan's extra entry holds the total).
 struct BalanceCount {
@@ -202,26 +211,32 @@ using BalanceCountIt = thrust::transform_iterator<BalanceCount, thrust::counting
 
 // flagged leaves -> four z-ordered children at pos[i]..pos[i]+3 (dirty),
 // others copied (clean); origin: the leaf of the pass's input it came from
+__device__ __forceinline__ void balance_refine_item(int i, const int4 *in, const int *orig_in,
+                                                    const unsigned char *flags, const int *pos, int4 *out,
+                                                    int *orig_out, unsigned char *dirty_out)
+{
+    const int4 p = in[i];
+    const int o = orig_in[i];
+    const int at = pos[i];
+    if (flags[i]) {
+        const int h = int(qlen_d(p.y + 1));
+        for (int c = 0; c < 4; ++c) {
+            out[at + c] = make_int4(p.x, p.y + 1, p.z + (c & 1) * h, p.w + ((c >> 1) & 1) * h);
+            orig_out[at + c] = o;
+            dirty_out[at + c] = 1;
+        }
+    } else {
+        out[at] = p;
+        orig_out[at] = o;
+        dirty_out[at] = 0;
+    }
+}
+
 __global__ void balance_refine_kernel(int nq, const int4 *in, const int *orig_in, const unsigned char *flags,
                                       const int *pos, int4 *out, int *orig_out, unsigned char *dirty_out)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
-        const int4 p = in[i];
-        const int o = orig_in[i];
-        const int at = pos[i];
-        if (flags[i]) {
-            const int h = int(qlen_d(p.y + 1));
-            for (int c = 0; c < 4; ++c) {
-                out[at + c] = make_int4(p.x, p.y + 1, p.z + (c & 1) * h, p.w + ((c >> 1) & 1) * h);
-                orig_out[at + c] = o;
-                dirty_out[at + c] = 1;
-            }
-        } else {
-            out[at] = p;
-            orig_out[at] = o;
-            dirty_out[at] = 0;
-        }
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x)
+        balance_refine_item(i, in, orig_in, flags, pos, out, orig_out, dirty_out);
 }
 
 // Remap table of the balanced leaves: leaf k descends from pre-balance leaf
@@ -246,29 +261,33 @@ __global__ void keys_kernel(ForestDev F)
 // Start of a balance pass in one launch: each leaf's Morton key, a cleared
 // refine flag and the first leaf of each tree (tb[t] = first leaf of tree t
 // or of a later tree when t has none; tb[ntrees] = nq).
-__global__ void pass_prep_kernel(ForestDev F, int ntrees, int *tb, unsigned char *flags)
+__device__ __forceinline__ void pass_prep_item(const ForestDev &F, int ntrees, int *tb, unsigned char *flags, int i)
 {
     const int nq = F.nq;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nq; i += gridDim.x * blockDim.x) {
-        if (i == nq) {
-            const int last = nq == 0 ? -1 : F.leaves[nq - 1].x;
-            for (int u = last + 1; u <= ntrees; ++u) tb[u] = nq;
-        } else {
-            const int4 l = F.leaves[i];
-            F.keys[i] = morton_d(l.z, l.w);
-            flags[i] = 0;
-            const int prev = i == 0 ? -1 : F.leaves[i - 1].x;
-            for (int u = prev + 1; u <= l.x; ++u) tb[u] = i;  // trees without leaves start here too
-        }
+    if (i == nq) {
+        const int last = nq == 0 ? -1 : F.leaves[nq - 1].x;
+        for (int u = last + 1; u <= ntrees; ++u) tb[u] = nq;
+    } else {
+        const int4 l = F.leaves[i];
+        F.keys[i] = morton_d(l.z, l.w);
+        flags[i] = 0;
+        const int prev = i == 0 ? -1 : F.leaves[i - 1].x;
+        for (int u = prev + 1; u <= l.x; ++u) tb[u] = i;  // trees without leaves start here too
     }
+}
+
+__global__ void pass_prep_kernel(ForestDev F, int ntrees, int *tb, unsigned char *flags)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= F.nq; i += gridDim.x * blockDim.x)
+        pass_prep_item(F, ntrees, tb, flags, i);
 }
 
 // One thread per (leaf, side): the side descriptor (rank filled later), the
 // emits flag and the emitter slot; the leaf's corners from side 0's thread.
-__global__ void sides_kernel(ForestDev F, QuadDesc *out, int *emits, int *emitter, int *status)
+__device__ __forceinline__ void sides_item(const ForestDev &F, QuadDesc *out, int *emits, int *emitter, int *status,
+                                           int t)
 {
-    const int total = 4 * F.nq;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    {
         const int i = t >> 2, s = t & 3;
         const int4 q = F.leaves[i];  // tree, level, x, y
         const int dx = s == 0 ? -1 : (s == 1 ? 1 : 0);
@@ -370,6 +389,13 @@ __global__ void sides_kernel(ForestDev F, QuadDesc *out, int *emits, int *emitte
     }
 }
 
+__global__ void sides_kernel(ForestDev F, QuadDesc *out, int *emits, int *emitter, int *status)
+{
+    const int total = 4 * F.nq;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x)
+        sides_item(F, out, emits, emitter, status, t);
+}
+
 __global__ void rank_kernel(int nq, QuadDesc *out, const int *emits, const int *scan, const int *emitter,
                             int *status)
 {
@@ -377,6 +403,187 @@ __global__ void rank_kernel(int nq, QuadDesc *out, const int *emits, const int *
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         out[t >> 2].side[t & 3].rank = scan[emitter[t]];
         if (t == total - 1) status[1] = scan[t] + emits[t];
+    }
+}
+
+// ---------------------------------------------------------------- the
+// balance loop and the descriptor build in one cooperative launch.
+//
+// Every phase of every pass runs as a grid-stride loop over all blocks,
+// separated by device-wide barriers, so a whole 2:1 balance (until a pass
+// finds nothing to refine), the quad descriptors of the balanced leaves and
+// their remap table cost one launch and one read-back instead of a few
+// launches and a read-back per pass. The phases are the kernels above, item
+// for item, so the leaves, descriptors and tables are the same.
+
+// Device-wide barrier of a cooperative launch: the last block to arrive
+// resets the count and advances the generation; the others wait for the
+// generation to move, at most kBarrierSpins polls. A wait that runs out
+// sets `abort` and every block leaves at its next barrier, so a fault in the
+// loop's logic ends the kernel with an error instead of hanging it.
+constexpr long long kBarrierSpins = 1ll << 22;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ bool grid_barrier(BalanceCtl *ctl)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = ld_acquire_u32(&ctl->bar_gen);
+        __threadfence();
+        const unsigned arrived = atomicAdd(&ctl->bar_count, 1u) + 1u;
+        int ok = 1;
+        if (arrived == gridDim.x) {
+            atomicExch(&ctl->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&ctl->bar_gen, 1u);
+        } else {
+            long long spins = 0;
+            while (ld_acquire_u32(&ctl->bar_gen) == gen) {
+                if (++spins > kBarrierSpins) {
+                    ok = 0;
+                    atomicExch(&ctl->abort, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok && *(volatile int *)&ctl->abort == 0;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Exclusive scan of cnt(0..n-1) into pos[0..n-1] and the total into pos[n],
+// over all blocks: each block takes a contiguous chunk, each thread a
+// contiguous run of it; block sums go through bsum and a barrier. Returns
+// false when a barrier gave up.
+template <typename Cnt>
+__device__ bool grid_scan(int n, Cnt cnt, int *pos, int *bsum, BalanceCtl *ctl)
+{
+    __shared__ int s_warp[32];
+    __shared__ int s_off, s_tot;
+    const int T = blockDim.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = T >> 5;
+    const int chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int lo = min(n, (int)blockIdx.x * chunk), hi = min(n, lo + chunk);
+    const int per = (chunk + T - 1) / T;
+    const int tlo = min(hi, lo + (int)threadIdx.x * per), thi = min(hi, tlo + per);
+    int sum = 0;
+    for (int i = tlo; i < thi; ++i) sum += cnt(i);
+    int incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    if (lane == 31) s_warp[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int v = lane < nw ? s_warp[lane] : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane >= d) v += u;
+        }
+        if (lane < nw) s_warp[lane] = v;  // inclusive warp prefixes
+    }
+    __syncthreads();
+    const int texcl = incl - sum + (w > 0 ? s_warp[w - 1] : 0);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = s_warp[nw - 1];
+    if (!grid_barrier(ctl)) return false;
+    // this block's offset and the total, from every block's sum
+    int off = 0, tot = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += T) {
+        const int v = __ldcg(bsum + b);
+        tot += v;
+        if (b < (int)blockIdx.x) off += v;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        off += __shfl_xor_sync(0xffffffffu, off, d);
+        tot += __shfl_xor_sync(0xffffffffu, tot, d);
+    }
+    if (threadIdx.x == 0) s_off = s_tot = 0;
+    __syncthreads();
+    if (lane == 0) {
+        atomicAdd(&s_off, off);
+        atomicAdd(&s_tot, tot);
+    }
+    __syncthreads();
+    int run = s_off + texcl;
+    for (int i = tlo; i < thi; ++i) {
+        pos[i] = run;
+        run += cnt(i);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) pos[n] = s_tot;
+    return grid_barrier(ctl);
+}
+
+__global__ void __launch_bounds__(256) balance_loop_kernel(const BalanceLoopArgs a)
+{
+    BalanceCtl *ctl = a.ctl;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    int nl = a.nl, live = a.live, passes = 0;
+    bool ok = true, done = false, overflow = false, refined = false;
+    ForestDev F = a.F;
+    for (int pass = 0; pass < 64 && ok; ++pass) {
+        ++passes;
+        F.leaves = a.leaves[live];
+        F.nq = nl;
+        unsigned char *flags = a.flags;
+        for (int i = gtid; i <= nl; i += gstride) pass_prep_item(F, a.ntrees, a.tree_begin, flags, i);
+        if (!(ok = grid_barrier(ctl))) break;
+        for (long long t = gtid; t < 16ll * nl; t += gstride) balance_check_item(F, a.dirty[live], flags, t);
+        if (!(ok = grid_barrier(ctl))) break;
+        if (!(ok = grid_scan(nl, [&](int i) { return __ldcg(flags + i) ? 4 : 1; }, a.pos, a.bsum, ctl))) break;
+        const int total = __ldcg(a.pos + nl);
+        if (total == nl) {
+            done = true;
+            break;
+        }
+        if (total > a.cap) {
+            overflow = true;
+            break;
+        }
+        for (int i = gtid; i < nl; i += gstride)
+            balance_refine_item(i, a.leaves[live], a.orig[live], flags, a.pos, a.leaves[1 - live], a.orig[1 - live],
+                                a.dirty[1 - live]);
+        if (!(ok = grid_barrier(ctl))) break;
+        live = 1 - live;
+        nl = total;
+        refined = true;
+    }
+    // the balanced leaves' remap table and descriptors (keys and tree starts
+    // are the last pass's, which refined nothing)
+    if (ok && done && a.build) {
+        if (a.kind0) {
+            for (int k = gtid; k < nl; k += gstride) {
+                const int o = a.orig[live][k];
+                a.kind[k] = a.kind0[o];
+                a.src[k] = a.src0[o];
+            }
+        }
+        for (int t = gtid; t < 4 * nl; t += gstride) sides_item(F, a.out, a.emits, a.emitter, a.status, t);
+        ok = grid_barrier(ctl);
+        if (ok) ok = grid_scan(4 * nl, [&](int t) { return __ldcg(a.emits + t); }, a.scan, a.bsum, ctl);
+        if (ok) {
+            for (int t = gtid; t < 4 * nl; t += gstride) a.out[t >> 2].side[t & 3].rank = __ldcg(a.scan + a.emitter[t]);
+            if (gtid == 0) a.status[1] = nl > 0 ? __ldcg(a.scan + 4 * nl) : 0;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->nl = nl;
+        ctl->live = live;
+        ctl->passes = passes;
+        ctl->result = !ok ? kBalanceTimeout : overflow ? kBalanceOverflow : done ? kBalanceDone : kBalanceNoConverge;
+        ctl->refined = refined ? 1 : 0;
     }
 }
 
@@ -448,5 +655,27 @@ cudaError_t launch_build_quads(const ForestDev &F, QuadDesc *out, int *emits, in
     rank_kernel<<<grid_for(4ll * F.nq, sms), 256, 0, st>>>(F.nq, out, emits, scan, emitter, status);
     return cudaGetLastError();
 }
+
+
+cudaError_t launch_balance_loop(const BalanceLoopArgs &a, int sms, cudaStream_t st)
+{
+    // one block per SM at most (a cooperative launch needs every block
+    // resident), fewer for small forests: about 8 of the 16 checks per leaf
+    // per thread, since every block takes part in every barrier
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, balance_loop_kernel, 256, 0);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorLaunchOutOfResources;
+    const long long want = (16ll * std::max(a.nl, 1) + 8 * 256 - 1) / (8 * 256);
+    const int grid = int(std::max(1ll, std::min<long long>(want, (long long)sms)));
+    BalanceLoopArgs args = a;
+    void *p[] = {&args};
+    e = cudaMemsetAsync(a.ctl, 0, sizeof(BalanceCtl), st);
+    if (e == cudaSuccess && a.build) e = cudaMemsetAsync(a.status, 0, 2 * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchCooperativeKernel((const void *)balance_loop_kernel, dim3(grid), dim3(256), p, 0, st);
+}
+
+size_t balance_loop_bsum_ints(int sms) { return size_t(std::max(sms, 1)); }
 
 }  // namespace amrgpu

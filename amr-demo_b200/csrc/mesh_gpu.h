@@ -40,6 +40,40 @@ cudaError_t launch_balance_refine(int nq, const int4 *in, const int *orig_in, co
                                   const int *pos, int4 *out, int *orig_out, unsigned char *dirty_out, int sms,
                                   cudaStream_t st);
 
+// The whole 2:1 balance (passes until one refines nothing), then the quad
+// descriptors of the balanced leaves and their remap table, in one
+// cooperative launch (device-wide barriers between the phases, each wait
+// bounded). Leaf buffers are double-buffered: the loop starts from
+// buffer `live` with nl leaves and ends with ctl->live / ctl->nl.
+enum { kBalanceDone = 1, kBalanceOverflow = 2, kBalanceNoConverge = 3, kBalanceTimeout = 4 };
+struct BalanceCtl {
+    unsigned bar_count, bar_gen;  // the barrier
+    int abort;                    // set by a barrier wait that ran out
+    int nl, live, passes, refined;
+    int result;                   // kBalance*
+};
+struct BalanceLoopArgs {
+    ForestDev F;                  // brick and tree tables; leaves / nq set per pass, keys written
+    int ntrees;
+    int *tree_begin;              // ntrees + 1 entries, rebuilt every pass
+    int4 *leaves[2];
+    int *orig[2];
+    unsigned char *dirty[2];
+    int nl, live, cap;            // leaves at the start, their buffer, each buffer's capacity
+    unsigned char *flags;         // cap
+    int *pos;                     // cap + 1
+    int *bsum;                    // one per block (balance_loop_bsum_ints)
+    BalanceCtl *ctl;
+    int build;                    // then the descriptors of the balanced leaves:
+    QuadDesc *out;                //   cap descriptors
+    int *emits, *scan, *emitter;  //   4 cap (+1 for scan) ints each
+    int *status;                  //   [0] 2:1 violation bits, [1] face count
+    const int *kind0, *src0;      //   remap table of the leaves the loop started from (or null)
+    int *kind, *src;              //   ... gathered for the balanced leaves
+};
+cudaError_t launch_balance_loop(const BalanceLoopArgs &a, int sms, cudaStream_t st);
+size_t balance_loop_bsum_ints(int sms);
+
 // Scratch of the face-numbering scan for nq leaves.
 size_t build_quads_scan_bytes(int nq);
 

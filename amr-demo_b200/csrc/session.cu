@@ -2109,29 +2109,22 @@ int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
     return AMRGPU_OK;
 }
 
-// 2:1 balance of forest fo with every pass on the session's GPU; the
-// balanced leaves stay in d_bal[*live_out] (with the last pass's keys and
-// tree starts in the work area) and are copied back into the host forest.
-// With remap, the remap table of the balanced leaves (kind / source of the
-// pre-balance leaf each one descends from, validated against the session's
-// current quad count) is gathered into d_kind / d_src on the device.
-// Returns the leaf count or -error.
-int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
+// Stages a forest's leaves for the device balance: leaves (int4), origin
+// (identity), dirty marks, brick tables and, with remap, the pre-balance
+// remap kind / source (range-checked against the session's quads) into
+// d_remap0; grows the balance buffers to 1.5 times the leaves.
+int stage_leaves(amrgpu_session *s, std::vector<Leaf> &leaves, const BrickView &B, int ntrees, bool remap)
 {
-    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
-    BrickView B;
-    forest_brick(fo, &B);
-    const int ntrees = B.nx * B.ny;
-    int nl = int(leaves.size());
+    const int nl = int(leaves.size());
     // staging: leaves (int4), origin, remap kind / source (with remap),
     // dirty bytes, brick tables
     const size_t nrm = remap ? 2 * size_t(nl) : 0;
     size_t sb = 16 * size_t(nl) + 4 * size_t(nl) + 4 * nrm + size_t(nl) + 12 * size_t(ntrees) + 64;
     int rc = ensure_stage(s, sb);
-    if (rc) return -rc;
+    if (rc) return rc;
     if (remap) {
         rc = ensure_dev(s, &s->d_remap0, &s->remap0_bytes, 4 * nrm + 16);
-        if (rc) return -rc;
+        if (rc) return rc;
     }
     {
         int *h = static_cast<int *>(s->h_stage);
@@ -2158,7 +2151,7 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
         }
         if (bad) {
             set_error(AMRGPU_ERR_ARG, "remap kind or source index out of range");
-            return -AMRGPU_ERR_ARG;
+            return AMRGPU_ERR_ARG;
         }
         int *h_tab = reinterpret_cast<int *>(h_dirty + ((size_t(nl) + 15) & ~size_t(15)));
         for (int t = 0; t < ntrees; ++t) {
@@ -2169,7 +2162,7 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
         const int cap = std::max(nl + nl / 2, 64);  // passes that outgrow it grow it (2x)
         if (cap > s->bal_cap || ntrees > s->bal_trees) {
             rc = bal_grow(s, std::max(cap, s->bal_cap), ntrees, 0, 0);
-            if (rc) return -rc;
+            if (rc) return rc;
         }
         const BalLayout L = bal_layout(s->bal_cap, ntrees);
         char *b0 = static_cast<char *>(s->d_bal[0]);
@@ -2189,8 +2182,75 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
                           "H2D balance");
         if (ok && remap && nl > 0)
             ok = cuda_ok(cudaMemcpyAsync(s->d_remap0, h_rm, 4 * nrm, cudaMemcpyHostToDevice, s->stream), "H2D remap");
-        if (!ok) return -AMRGPU_ERR_CUDA;
+        if (!ok) return AMRGPU_ERR_CUDA;
     }
+    return AMRGPU_OK;
+}
+
+// The balanced leaves (buffer `live`, nl of them) back into the host
+// forest: coordinates and origin read back, then rewritten in place.
+int leaves_back_to_host(amrgpu_session *s, Forest *fo, int nl, int live, int ntrees)
+{
+    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
+    int rc = ensure_stage(s, 20 * size_t(nl) + 64);
+    if (rc) return rc;
+    const BalLayout L = bal_layout(s->bal_cap, ntrees);
+    char *in = static_cast<char *>(s->d_bal[live]);
+    int *h = static_cast<int *>(s->h_stage);
+    int *h_orig = h + 4 * size_t(nl);
+    if (nl > 0 &&
+        (!cuda_ok(cudaMemcpyAsync(h, in, 16 * size_t(nl), cudaMemcpyDeviceToHost, s->stream), "D2H balance") ||
+         !cuda_ok(cudaMemcpyAsync(h_orig, in + L.o_orig, 4 * size_t(nl), cudaMemcpyDeviceToHost, s->stream),
+                  "D2H balance") ||
+         !cuda_ok(cudaStreamSynchronize(s->stream), "sync")))
+        return AMRGPU_ERR_CUDA;
+    if (nl != int(leaves.size())) {
+        // in place, from the end backwards: balance only refines, so leaf k
+        // comes from input leaf h_orig[k] <= k (non-decreasing in k), which
+        // is read before anything at or below it is overwritten; the prefix
+        // of leaves the balance left alone is not touched. Field by field:
+        // copying a whole leaf right after overwriting some of its fields
+        // stalls on store forwarding.
+        const int n0 = int(leaves.size());
+        int first = 0;
+        while (first < n0 && h_orig[first] == first && h[4 * first + 1] == leaves[size_t(first)].level)
+            leaves[size_t(first++)].dirty = 0;
+        forest_grow_leaves(fo, size_t(nl));
+        for (int k = nl - 1; k >= first; --k) {
+            const Leaf &p = leaves[size_t(h_orig[k])];
+            Leaf &d = leaves[size_t(k)];
+            d.tree = p.tree;
+            d.tag = p.tag;
+            d.type = p.type;
+            d.src = p.src;
+            d.src_kind = p.src_kind;
+            d.level = h[4 * k + 1];
+            d.x = h[4 * k + 2];
+            d.y = h[4 * k + 3];
+            d.dirty = 0;
+        }
+    } else {
+        for (Leaf &q : leaves) q.dirty = 0;
+    }
+    return AMRGPU_OK;
+}
+
+// 2:1 balance of forest fo with every pass on the session's GPU; the
+// balanced leaves stay in d_bal[*live_out] (with the last pass's keys and
+// tree starts in the work area) and are copied back into the host forest.
+// With remap, the remap table of the balanced leaves (kind / source of the
+// pre-balance leaf each one descends from, validated against the session's
+// current quad count) is gathered into d_kind / d_src on the device.
+// Returns the leaf count or -error.
+int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
+{
+    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
+    BrickView B;
+    forest_brick(fo, &B);
+    const int ntrees = B.nx * B.ny;
+    int nl = int(leaves.size());
+    int rc = stage_leaves(s, leaves, B, ntrees, remap);
+    if (rc) return -rc;
     int live = 0;
     bool done = false, refined = false;
     for (int pass = 0; pass < 64 && !done; ++pass) {
@@ -2273,48 +2333,118 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
         for (Leaf &q : leaves) q.dirty = 0;
         return nl;
     }
-    // the balanced leaves back to the host: coordinates and origin
-    rc = ensure_stage(s, 20 * size_t(nl) + 64);
-    if (rc) return -rc;
-    const BalLayout L = bal_layout(s->bal_cap, ntrees);
-    char *in = static_cast<char *>(s->d_bal[live]);
-    int *h = static_cast<int *>(s->h_stage);
-    int *h_orig = h + 4 * size_t(nl);
-    if (nl > 0 &&
-        (!cuda_ok(cudaMemcpyAsync(h, in, 16 * size_t(nl), cudaMemcpyDeviceToHost, s->stream), "D2H balance") ||
-         !cuda_ok(cudaMemcpyAsync(h_orig, in + L.o_orig, 4 * size_t(nl), cudaMemcpyDeviceToHost, s->stream),
-                  "D2H balance") ||
-         !cuda_ok(cudaStreamSynchronize(s->stream), "sync")))
-        return -AMRGPU_ERR_CUDA;
-    if (nl != int(leaves.size())) {
-        // in place, from the end backwards: balance only refines, so leaf k
-        // comes from input leaf h_orig[k] <= k (non-decreasing in k), which
-        // is read before anything at or below it is overwritten; the prefix
-        // of leaves the balance left alone is not touched. Field by field:
-        // copying a whole leaf right after overwriting some of its fields
-        // stalls on store forwarding.
-        const int n0 = int(leaves.size());
-        int first = 0;
-        while (first < n0 && h_orig[first] == first && h[4 * first + 1] == leaves[size_t(first)].level)
-            leaves[size_t(first++)].dirty = 0;
-        forest_grow_leaves(fo, size_t(nl));
-        for (int k = nl - 1; k >= first; --k) {
-            const Leaf &p = leaves[size_t(h_orig[k])];
-            Leaf &d = leaves[size_t(k)];
-            d.tree = p.tree;
-            d.tag = p.tag;
-            d.type = p.type;
-            d.src = p.src;
-            d.src_kind = p.src_kind;
-            d.level = h[4 * k + 1];
-            d.x = h[4 * k + 2];
-            d.y = h[4 * k + 3];
-            d.dirty = 0;
+    rc = leaves_back_to_host(s, fo, nl, live, ntrees);
+    return rc ? -rc : nl;
+}
+
+// The whole regrid of an adapted forest with the balance passes, the quad
+// descriptors of the balanced leaves and their remap table in one
+// cooperative launch (launch_balance_loop) and one read-back; the balanced
+// leaves go back to the host forest, then the state is remapped as by
+// build_and_apply. Sessions with a patch-size rule take balance_impl and
+// build_and_apply instead (the mixed build needs the leaf count first).
+int balance_regrid_fused(amrgpu_session *s, Forest *fo)
+{
+    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
+    BrickView B;
+    forest_brick(fo, &B);
+    const int ntrees = B.nx * B.ny;
+    const int n0 = int(leaves.size());
+    int rc = stage_leaves(s, leaves, B, ntrees, true);
+    if (rc) return rc;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    int nl = n0, live = 0;
+    BalanceCtl ctl{};
+    int status[2] = {0, 0};
+    for (int attempt = 0;; ++attempt) {
+        const int cap = s->bal_cap;
+        if ((rc = ensure_desc(s, &s->d_quads_alt, &s->cap_desc_alt, cap))) return rc;
+        if ((rc = ensure_quad_arrays(s, cap))) return rc;
+        const size_t n4 = al(sizeof(int) * (4 * size_t(cap) + 1));
+        const size_t o_emits = 0, o_scan = n4, o_emitter = 2 * n4, o_status = 3 * n4;
+        const size_t o_bsum = o_status + 256, o_ctl = o_bsum + al(sizeof(int) * balance_loop_bsum_ints(s->sms));
+        if ((rc = ensure_dev(s, &s->d_mesh_scratch, &s->mesh_scratch_bytes, o_ctl + al(sizeof(BalanceCtl)))))
+            return rc;
+        char *base = static_cast<char *>(s->d_mesh_scratch);
+        const BalLayout L = bal_layout(cap, ntrees);
+        char *w = static_cast<char *>(s->d_bal_work);
+        BalanceLoopArgs a{};
+        set_brick(a.F, B, s->cfg.bc);
+        a.F.keys = reinterpret_cast<unsigned long long *>(w + L.o_keys);
+        a.F.tree_begin = reinterpret_cast<const int *>(w + L.o_tb);
+        a.F.tree_tx = reinterpret_cast<const int *>(w + L.o_tx);
+        a.F.tree_ty = reinterpret_cast<const int *>(w + L.o_ty);
+        a.F.tree_at = reinterpret_cast<const int *>(w + L.o_at);
+        a.ntrees = ntrees;
+        a.tree_begin = reinterpret_cast<int *>(w + L.o_tb);
+        for (int k = 0; k < 2; ++k) {
+            char *b = static_cast<char *>(s->d_bal[k]);
+            a.leaves[k] = reinterpret_cast<int4 *>(b);
+            a.orig[k] = reinterpret_cast<int *>(b + L.o_orig);
+            a.dirty[k] = reinterpret_cast<unsigned char *>(b + L.o_dirty);
         }
+        a.nl = nl;
+        a.live = live;
+        a.cap = cap;
+        a.flags = reinterpret_cast<unsigned char *>(w + L.o_flags);
+        a.pos = reinterpret_cast<int *>(w + L.o_pos);
+        a.bsum = reinterpret_cast<int *>(base + o_bsum);
+        a.ctl = reinterpret_cast<BalanceCtl *>(base + o_ctl);
+        a.build = 1;
+        a.out = s->d_quads_alt;
+        a.emits = reinterpret_cast<int *>(base + o_emits);
+        a.scan = reinterpret_cast<int *>(base + o_scan);
+        a.emitter = reinterpret_cast<int *>(base + o_emitter);
+        a.status = reinterpret_cast<int *>(base + o_status);
+        const int *rm = static_cast<const int *>(s->d_remap0);
+        a.kind0 = rm;
+        a.src0 = rm + n0;
+        a.kind = s->d_kind;
+        a.src = s->d_src;
+        if (!cuda_ok(launch_balance_loop(a, s->sms, s->stream), "balance loop")) return AMRGPU_ERR_CUDA;
+        s->launches++;
+        // the staged leaves were read by the uploads before the launch: the
+        // staging takes the results
+        char *h = static_cast<char *>(s->h_stage);
+        if (!cuda_ok(cudaMemcpyAsync(h, a.ctl, sizeof(BalanceCtl), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
+            !cuda_ok(cudaMemcpyAsync(h + 256, a.status, sizeof(status), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
+            !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
+            return AMRGPU_ERR_CUDA;
+        std::memcpy(&ctl, h, sizeof(ctl));
+        std::memcpy(status, h + 256, sizeof(status));
+        if (ctl.result == kBalanceOverflow && attempt < 16) {
+            // more leaves than the buffers hold: grow (keeping the live
+            // leaves, their origin and dirty marks) and go on from there
+            if ((rc = bal_grow(s, 2 * s->bal_cap, ntrees, ctl.live, ctl.nl))) return rc;
+            nl = ctl.nl;
+            live = 0;
+            continue;
+        }
+        break;
+    }
+    if (ctl.result == kBalanceTimeout) {
+        set_error(AMRGPU_ERR_CUDA, "balance loop: a device-wide barrier wait ran out");
+        return AMRGPU_ERR_CUDA;
+    }
+    if (ctl.result != kBalanceDone) {
+        set_error(AMRGPU_ERR_MESH, "forest_balance_device: no balance after 64 passes");
+        return AMRGPU_ERR_MESH;
+    }
+    nl = ctl.nl;
+    if (status[0]) {
+        set_error(AMRGPU_ERR_MESH, "session regrid from a forest: the forest is not 2:1 balanced");
+        return AMRGPU_ERR_MESH;
+    }
+    if (ctl.refined) {
+        if ((rc = leaves_back_to_host(s, fo, nl, ctl.live, ntrees))) return rc;
     } else {
         for (Leaf &q : leaves) q.dirty = 0;
     }
-    return nl;
+    std::swap(s->d_quads, s->d_quads_alt);
+    std::swap(s->cap_desc, s->cap_desc_alt);
+    s->h_quads.clear();  // the live descriptors exist on the device only
+    s->rect = true;      // brick quads are axis-aligned rectangles
+    return apply_regrid(s, nl, nl > 0 ? status[1] : 0);
 }
 
 }  // namespace
@@ -2345,6 +2475,13 @@ int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f)
         set_error(AMRGPU_ERR_UNSUPPORTED, "session_balance_regrid: ghost quads need a ghost exchange after the remap");
         return AMRGPU_ERR_UNSUPPORTED;
     }
+    // one cooperative launch for the balance, the descriptors and the remap
+    // table, unless a patch-size rule needs the mixed build on the way
+    static const bool fused = [] {
+        const char *e = std::getenv("AMRGPU_FUSED_BALANCE");
+        return !(e && std::atoi(e) == 0);
+    }();
+    if (fused && !s->has_rule) return balance_regrid_fused(s, f->f);
     int live = 0;
     const int nq = balance_impl(s, f->f, &live, true);  // remap table into d_kind / d_src
     if (nq < 0) return -nq;
