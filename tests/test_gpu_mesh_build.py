@@ -203,3 +203,46 @@ def test_fused_balance_regrid_equals_host_path(ag, seed):
     b.step(4)
     qa = a.download()
     assert np.isfinite(qa).all() and np.array_equal(qa, b.download())
+
+
+def test_fused_balance_grows_its_buffers_mid_balance(ag):
+    """A deep refinement chain at the centre of a small forest: its 2:1
+    ripple needs more leaves than the balance buffers hold when the leaves
+    are staged (1.5 times as many, at least 64), so the one-launch balance
+    loop stops, the buffers grow keeping the leaves and their marks, and the
+    loop goes on; the leaves, the descriptors and the remapped state equal
+    the host path's."""
+    n = 4
+    fa = ag.Forest(1, 1, periodic=(0, 0), level=2)
+    fb = ag.Forest(1, 1, periodic=(0, 0), level=2)
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.002)
+    cfg.apply()
+    s0 = meshes.perturbed(fa.initialize(n), 5, amp=1e-2)
+    a = ag.Session(fa.mesh(n), cfg, form=0)
+    b = ag.Session(fb.mesh(n), cfg, form=0)
+    for s in (a, b):
+        s.upload(s0)
+        s.step(2)
+    p = (1 << 29) - 1  # just below and left of the centre, in root units
+    for f in (fa, fb):
+        f.begin_regrid()
+        for _ in range(8):
+            _, lev, x, y = f.quads()
+            size = np.left_shift(np.int64(1), 30 - lev.astype(np.int64))
+            hit = (x <= p) & (p < x + size) & (y <= p) & (p < y + size)
+            fl = hit.astype(np.int32)
+            f.refine(fl, max_level=12)
+    staged = fb.num_quads
+    fa.balance()
+    assert fa.num_quads > max(64, staged + staged // 2)  # the ripple outgrows the staged capacity
+    kind, src = fa.remap()
+    a.regrid(fa.mesh(n), kind, src)
+    b.balance_regrid(fb)
+    for u, v in zip(leaves_of(fa), leaves_of(fb)):
+        assert np.array_equal(u, v)
+    assert a.quad_descriptors().tobytes() == b.quad_descriptors().tobytes()
+    assert np.array_equal(a.download(), b.download())
+    for s in (a, b):
+        s.step(3)
+    qa = a.download()
+    assert np.isfinite(qa).all() and np.array_equal(qa, b.download())
