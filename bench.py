@@ -299,6 +299,15 @@ def learned_amr(args):
            "l1_bound": L1_BOUND}
     arms = (("plain_fp64", None, 0, 5), ("plain_fp64_at_I", None, 0, I), ("plain_fp32", None, 1, 5),
             ("plain_fp32_at_I", None, 1, I), ("learned_fp32", m, 1, I))
+    # one untimed run of every arm first (seed 4999): kernels load on their
+    # first launch and the library's autotuner times a launch shape for each
+    # mesh-size bucket it meets first; neither one-time cost should land in
+    # whichever arm happens to run first
+    for key, mlp, form, ri in arms:
+        f, cfg, soln, par = L.vortex_amr(4999, n, lo, hi, tol, form=form)
+        s, _ = L.run(f, soln, n, cfg, final_time=3.0, regrid_interval=ri, min_level=lo, max_level=hi, tol=tol,
+                     mlp=mlp, form=form, seed=4999, judge_coarser=mlp is not None)
+        s.close()
     runs = {k: [] for k, _, _, _ in arms}
     for seed in (5000, 5001, 5002):
         ends = {}
@@ -414,7 +423,19 @@ def amr_workload(args):
     steps: GPU tagging by the density jump, host forest refine / coarsen /
     2:1 balance, in-place GPU remap). --warmup steps untimed, then --steps
     steps timed: cell-updates/s with the regrid time included (the
-    metric's definition for adaptive runs) and of the solve alone."""
+    metric's definition for adaptive runs) and of the solve alone. The
+    whole run is made twice from a fresh forest and session and the second
+    is reported: the first loads the kernels and lets the autotuner time a
+    launch shape for every mesh size the run meets (what a production run
+    has from its tuning cache)."""
+    first = _amr_workload_once(args)
+    out = _amr_workload_once(args)
+    out["note"] = "second of two identical runs (the first loads kernels and tunes launch shapes)"
+    out["first_run_value"] = first["value"]
+    return out
+
+
+def _amr_workload_once(args):
     import amrgpu as ag
     from amrgpu import amr, workloads as W
     t0 = time.perf_counter()
