@@ -123,6 +123,10 @@ PROTOTYPES = {
     "amrgpu_session_step_stage": (C.c_int, [C.c_void_p, i32p, i32p]),
     "amrgpu_session_stage_input": (C.c_void_p, [C.c_void_p, C.POINTER(C.c_longlong)]),
     "amrgpu_session_dt_slot": (C.c_void_p, [C.c_void_p]),
+    "amrgpu_session_capture_mark": (C.c_int, [C.c_void_p]),
+    "amrgpu_session_capture_rewind": (C.c_int, [C.c_void_p]),
+    "amrgpu_session_advance": (C.c_int, [C.c_void_p, C.c_int]),
+    "amrgpu_session_step_index": (C.c_longlong, [C.c_void_p]),
     "amrgpu_session_set_halo": (C.c_int, [C.c_void_p, i32p, C.c_int]),
     "amrgpu_session_halo_pack": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "amrgpu_session_halo_unpack": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),

@@ -352,6 +352,58 @@ class Distributed:
                 self._step()
         self._in_stream(run)
 
+    # -- steps as CUDA graphs ---------------------------------------------
+    # A step's host work -- per stage a pack, the NCCL all-to-all, an unpack
+    # and the stage launch, then the MIN all-reduce of the CFL step -- costs
+    # more host time than the step's kernels on a 1024^2 shard. Captured
+    # once as a CUDA graph per step phase (the device addresses a step uses
+    # repeat every 6 steps: three CFL slots, two buffer-role parities), a
+    # step is one graph launch. The session's counters are saved before the
+    # captures and restored after them (the captured work has not run), and
+    # advanced by one step per replay.
+    def capture(self):
+        """Captures the six step graphs; needs a GPU rank whose first steps
+        ran eagerly (communicators set up, launch tuned). Returns False,
+        leaving the driver eager, when the capture is refused."""
+        import torch
+        r = self.r
+        sess = getattr(r, "session", None)
+        if sess is None or getattr(r, "stream", None) is None:
+            return False
+        L = lib()
+        check(L.amrgpu_session_capture_mark(sess._s), "capture_mark")
+        graphs = {}
+        try:
+            base = int(L.amrgpu_session_step_index(sess._s))
+            for k in range(6):
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=r.stream):
+                    self._step()
+                graphs[(base + k) % 6] = g
+        except Exception:
+            graphs = None
+        check(L.amrgpu_session_capture_rewind(sess._s), "capture_rewind")
+        self._graphs = graphs
+        return graphs is not None
+
+    def release_graphs(self):
+        """Drops the step graphs (they hold the NCCL collectives: release
+        them before the process group is destroyed)."""
+        self._graphs = None
+
+    def step_graphs(self, nsteps):
+        """nsteps steps, each as one replay of its phase's graph on the
+        session's stream (a replay runs on the current stream)."""
+        r = self.r
+        L = lib()
+
+        def run():
+            for _ in range(int(nsteps)):
+                k = int(L.amrgpu_session_step_index(r.session._s)) % 6
+                self._graphs[k].replay()
+                check(L.amrgpu_session_advance(r.session._s, 1), "advance")
+        self._in_stream(run)
+
     def report(self):
         import torch
         rep = self.r.report()

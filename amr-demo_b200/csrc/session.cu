@@ -153,6 +153,10 @@ struct amrgpu_session {
     long long step_index = 0;
     int stage_pos = 0;  // stages of the current step enqueued by step_stage (0: at a step boundary)
     int64_t launches = 0;
+    // counters saved by amrgpu_session_capture_mark
+    long long mark_step = -1;
+    int mark_roles[4] = {0, 1, 2, 3};
+    int64_t mark_launches = 0;
     std::map<int, cudaGraphExec_t> graphs;
     bool primed = false;
     double t0 = 0.0;
@@ -1166,6 +1170,56 @@ double *amrgpu_session_stage_input(amrgpu_session_t *s, long long *field_stride)
     if (field_stride) *field_stride = s->stride;
     return rolebuf(s, plan[size_t(s->stage_pos)].in);
 }
+
+int amrgpu_session_capture_mark(amrgpu_session_t *s)
+{
+    if (!s) return AMRGPU_ERR_ARG;
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_capture_mark: a step begun with step_stage is not finished");
+        return AMRGPU_ERR_ARG;
+    }
+    if (!s->primed) {
+        if (int rc = prime(s)) return rc;
+    }
+    if (s->nquad > 0) {
+        if (int rc = maybe_autotune(s)) return rc;
+    }
+    if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return AMRGPU_ERR_CUDA;
+    s->mark_step = s->step_index;
+    std::memcpy(s->mark_roles, s->role, sizeof(s->role));
+    s->mark_launches = s->launches;
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_capture_rewind(amrgpu_session_t *s)
+{
+    if (!s || s->mark_step < 0) return AMRGPU_ERR_ARG;
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_capture_rewind: the captured work ends inside a step");
+        return AMRGPU_ERR_ARG;
+    }
+    s->step_index = s->mark_step;
+    std::memcpy(s->role, s->mark_roles, sizeof(s->role));
+    s->launches = s->mark_launches;
+    s->mark_step = -1;
+    return AMRGPU_OK;
+}
+
+int amrgpu_session_advance(amrgpu_session_t *s, int nsteps)
+{
+    if (!s || nsteps < 0 || s->stage_pos != 0) return AMRGPU_ERR_ARG;
+    bool swap_xy = false;
+    const auto &plan = plan_of(scheme_of(s), swap_xy);
+    // the step's own launches: stage kernels, and the halo kernels of a
+    // session with a send list (pack and unpack before every stage)
+    const int per_stage = 1 + (s->nsend > 0 ? 1 : 0) + (s->nghost > 0 ? 1 : 0);
+    s->launches += (int64_t)nsteps * (int64_t)plan.size() * per_stage;
+    if (swap_xy && (nsteps % 2)) std::swap(s->role[RX], s->role[RY]);
+    s->step_index += nsteps;
+    return AMRGPU_OK;
+}
+
+long long amrgpu_session_step_index(const amrgpu_session_t *s) { return s ? s->step_index : -1; }
 
 unsigned long long *amrgpu_session_dt_slot(amrgpu_session_t *s)
 {

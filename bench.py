@@ -529,20 +529,31 @@ def time_sharded(ag, S, mesh, cfg, s0, form, steps, warmup, tune_on, world, rank
     drv.step(warmup)
     torch.cuda.synchronize()
     dist.barrier()
+    # each step one CUDA graph launch (its exchanges and the CFL reduction
+    # captured with the kernels) when every rank could capture; else eager
+    graphed = drv.capture()
+    ok = torch.tensor([1 if graphed else 0], dtype=torch.int32, device="cuda")
+    dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+    graphed = bool(ok.item())
+    stepper = drv.step_graphs if graphed else drv.step
+    stepper(3)  # the graphs' first launches
+    torch.cuda.synchronize()
+    dist.barrier()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     l0 = r.session.launch_count()
     for k in range(steps):
         with torch.cuda.stream(r.stream):
             flush.zero_()
             evs[k][0].record(r.stream)
-        drv.step(1)
+        stepper(1)
         evs[k][1].record(r.stream)
     rep = drv.report()
     launches = r.session.launch_count() - l0
     torch.cuda.synchronize()
     ms = [a.elapsed_time(b) for a, b in evs]
     return r, drv, {"ms_steps": ms, "report": rep, "tune": tune, "launches": launches,
-                    "ghosts": int(len(sh.ghosts)), "sends": int(len(sh.send_quads)), "local_quads": sh.nlocal}
+                    "ghosts": int(len(sh.ghosts)), "sends": int(len(sh.send_quads)), "local_quads": sh.nlocal,
+                    "step_graphs": graphed}
 
 
 def e2e_sharded(drv, local, steps, segment):
@@ -608,6 +619,7 @@ def run_sharded(args, world, rank, local):
                "step": f"per rank: upload + {args.segment} RK3 steps (sharded driver) + download, "
                        "slowest rank's wall clock"}
     for form, (r, drv, d) in res.items():
+        drv.release_graphs()  # graphs holding NCCL calls go before the process group
         r.close()
     if rank == 0:
         head = out[1] if 1 in out else out[run_forms[0]]
@@ -626,7 +638,8 @@ def run_sharded(args, world, rank, local):
                        "l2": "flushed between steps (256 MB write; per-step CUDA events exclude it)",
                        "launch": head["tune"],
                        "parallelism": f"dp{world}: Morton-range shards, NCCL ghost exchange before every "
-                                      "stage, MIN all-reduce of the CFL step every step"},
+                                      "stage, MIN all-reduce of the CFL step every step",
+                       "step_graphs": bool(head.get("step_graphs"))},
             "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": hbm, "unit": "GB/s",
                          "frac": head["achieved_gbs"] / hbm, "traffic": traffic_per_launch(hf),
                          "peak_kind": peak_kind, "bytes_per_cell_update": B_ALG[hf],

@@ -333,6 +333,20 @@ double *amrgpu_session_stage_input(amrgpu_session_t *s, long long *field_stride)
  * of a positive double (MIN over ranks = MIN of the doubles). Written by
  * the last stage of a step and by upload. */
 unsigned long long *amrgpu_session_dt_slot(amrgpu_session_t *s);
+/* Extension: a caller's CUDA graph of whole steps made of step_stage and
+ * halo calls (with its own collectives between them). The calls only
+ * enqueue work, but they move the session's step counter, stage position
+ * and buffer roles as if it had run: capture_mark (at a step boundary;
+ * it also runs a pending launch tuning first, which must not be captured)
+ * saves them before the capture, capture_rewind restores them after it,
+ * and advance(nsteps) moves them by the nsteps whole steps a replay runs.
+ * step_index is the session's step counter: the device addresses a step
+ * uses repeat with period 6 (three CFL slots, two buffer-role parities),
+ * so a graph of step k replays correctly at every step = k mod 6. */
+int amrgpu_session_capture_mark(amrgpu_session_t *s);
+int amrgpu_session_capture_rewind(amrgpu_session_t *s);
+int amrgpu_session_advance(amrgpu_session_t *s, int nsteps);
+long long amrgpu_session_step_index(const amrgpu_session_t *s);
 /* Local quads (host array, each < ncell) whose records other ranks need,
  * grouped by destination rank (the reference's send list). */
 int amrgpu_session_set_halo(amrgpu_session_t *s, const int *send_quads, int nsend);

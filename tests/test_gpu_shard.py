@@ -193,3 +193,36 @@ def test_distributed_driver_over_nccl_single_rank(ag):
         dist.destroy_process_group()
     assert np.array_equal(got, ref)
     assert rep["time"] == rep0["time"] and rep["steps"] == 10
+
+
+def test_distributed_step_graphs_single_rank(ag):
+    """The per-process driver's steps captured as CUDA graphs (one per step
+    phase, the CFL-step MIN all-reduce inside) on a one-rank NCCL group:
+    after two eager steps, eight graph replays give the plain session's
+    state and time bit for bit, and the session's counters follow."""
+    import torch
+    import torch.distributed as dist
+    from amrgpu import shard as S
+    m, cfg, s0 = build(ag, 61, 16, 3)
+    ref, rep0 = unsharded(ag, m, cfg, s0, ag.FORM_FP32_FLUX, 10)
+    cfg["form"] = ag.FORM_FP32_FLUX
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        r = S.GpuRank(S.make_shard(m, S.partition(m.ncell, 1), 0), cfg)
+        drv = S.Distributed(r)
+        drv.start(r.shard.local_state(s0))
+        drv.step(2)
+        assert drv.capture()
+        drv.step_graphs(8)
+        rep = drv.report()
+        got = drv.download()
+        step_index = ag.lib().amrgpu_session_step_index(r.session._s)
+        drv.release_graphs()
+        r.close()
+    finally:
+        dist.destroy_process_group()
+    assert step_index == 10
+    assert np.array_equal(got, ref)
+    assert rep["time"] == rep0["time"] and rep["steps"] == 10
