@@ -671,6 +671,7 @@ cudaError_t launch_balance_loop(const BalanceLoopArgs &a, int sms, cudaStream_t 
     BalanceLoopArgs args = a;
     void *p[] = {&args};
     e = cudaMemsetAsync(a.ctl, 0, sizeof(BalanceCtl), st);
+    if (e == cudaSuccess && a.stall_test) e = cudaMemsetAsync(&a.ctl->bar_count, 0x40, sizeof(unsigned), st);
     if (e == cudaSuccess && a.build) e = cudaMemsetAsync(a.status, 0, 2 * sizeof(int), st);
     if (e != cudaSuccess) return e;
     return cudaLaunchCooperativeKernel((const void *)balance_loop_kernel, dim3(grid), dim3(256), p, 0, st);

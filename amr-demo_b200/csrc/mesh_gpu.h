@@ -70,6 +70,8 @@ struct BalanceLoopArgs {
     int *status;                  //   [0] 2:1 violation bits, [1] face count
     const int *kind0, *src0;      //   remap table of the leaves the loop started from (or null)
     int *kind, *src;              //   ... gathered for the balanced leaves
+    int stall_test;               // nonzero: the barrier's arrival count starts out of reach, so
+                                  // every wait runs out (tests of the bounded wait)
 };
 cudaError_t launch_balance_loop(const BalanceLoopArgs &a, int sms, cudaStream_t st);
 size_t balance_loop_bsum_ints(int sms);

@@ -2397,7 +2397,7 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
 // leaves go back to the host forest, then the state is remapped as by
 // build_and_apply. Sessions with a patch-size rule take balance_impl and
 // build_and_apply instead (the mixed build needs the leaf count first).
-int balance_regrid_fused(amrgpu_session *s, Forest *fo)
+int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false)
 {
     std::vector<Leaf> &leaves = forest_leaves_mut(fo);
     BrickView B;
@@ -2455,6 +2455,7 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo)
         a.src0 = rm + n0;
         a.kind = s->d_kind;
         a.src = s->d_src;
+        a.stall_test = stall_test ? 1 : 0;
         if (!cuda_ok(launch_balance_loop(a, s->sms, s->stream), "balance loop")) return AMRGPU_ERR_CUDA;
         s->launches++;
         // the staged leaves were read by the uploads before the launch: the
@@ -2660,6 +2661,12 @@ int amrgpu_session_reserve(amrgpu_session_t *s, long long cells, int quads)
         if ((rc = bal_grow(s, std::max(bcap, s->bal_cap), btrees, 0, 0))) return rc;
     }
     return ensure_stage(s, 32 * size_t(bcap) + 12 * size_t(btrees) + 4096);
+}
+
+int amrgpu_session_balance_stall_test(amrgpu_session_t *s, amrgpu_forest_t *f)
+{
+    if (!s || !f || !f->f || s->has_rule || s->stage_pos != 0 || s->nghost != 0) return AMRGPU_ERR_ARG;
+    return balance_regrid_fused(s, f->f, true);
 }
 
 int amrgpu_session_quad_descriptors(amrgpu_session_t *s, void *out, int cap)

@@ -439,6 +439,14 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s);
  * descend from (no remap table built or uploaded by the host after the
  * balance). */
 int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f);
+/* Test support for the bounded waits of amrgpu_session_balance_regrid's
+ * one-launch balance (device-wide barriers between its phases, each wait
+ * at most 2^22 polls): runs it with the barrier's arrival count started out
+ * of reach, so that every wait runs out (about half a second), the kernel
+ * ends and the call returns AMRGPU_ERR_CUDA; the session keeps its mesh
+ * and state and the forest its leaves. Sessions without a patch-size rule,
+ * at a step boundary, without ghost quads. */
+int amrgpu_session_balance_stall_test(amrgpu_session_t *s, amrgpu_forest_t *f);
 /* Mixed patch sizes (extension; the reference fixes one size per build):
  * the patch size (8 or 16) of a quad at each level, size_of_level[l] for
  * l < nlevels (the last entry for deeper levels); nlevels = 0 clears it.

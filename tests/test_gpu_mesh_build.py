@@ -246,3 +246,44 @@ def test_fused_balance_grows_its_buffers_mid_balance(ag):
         s.step(3)
     qa = a.download()
     assert np.isfinite(qa).all() and np.array_equal(qa, b.download())
+
+
+def test_balance_barrier_wait_runs_out_and_the_session_stays_usable(ag):
+    """The one-launch balance's device-wide barrier with its arrival count
+    started out of reach: every block's wait runs out after its poll limit,
+    the kernel ends with the abort flag set and the call reports an error,
+    within a few seconds; the session keeps its mesh, the forest its leaves,
+    and the same regrid then runs normally and equals the host path."""
+    import time
+    n = 4
+    fa = ag.Forest(2, 1, periodic=(1, 0), level=2)
+    fb = ag.Forest(2, 1, periodic=(1, 0), level=2)
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.002)
+    cfg.apply()
+    s0 = meshes.perturbed(fa.initialize(n), 9, amp=1e-2)
+    a = ag.Session(fa.mesh(n), cfg, form=0)
+    b = ag.Session(fb.mesh(n), cfg, form=0)
+    for s in (a, b):
+        s.upload(s0)
+        s.step(2)
+    rng = np.random.default_rng(5)
+    rf = (rng.random(fa.num_quads) < 0.3).astype(np.int32)
+    for f in (fa, fb):
+        f.begin_regrid()
+        f.refine(rf, max_level=4)
+    before = leaves_of(fb)
+    desc = b.quad_descriptors().tobytes()
+    t0 = time.perf_counter()
+    rc = ag.lib().amrgpu_session_balance_stall_test(b._s, fb._f)
+    assert time.perf_counter() - t0 < 30.0
+    assert rc != 0
+    ag.clear_error()
+    for u, v in zip(before, leaves_of(fb)):
+        assert np.array_equal(u, v)
+    assert b.quad_descriptors().tobytes() == desc
+    fa.balance()
+    kind, src = fa.remap()
+    a.regrid(fa.mesh(n), kind, src)
+    b.balance_regrid(fb)
+    assert a.quad_descriptors().tobytes() == b.quad_descriptors().tobytes()
+    assert np.array_equal(a.download(), b.download())
