@@ -35,6 +35,7 @@
 
 #include <type_traits>
 
+#include "async_copy.cuh"
 #include "flux_fp32.cuh"
 #include "stage_kernel.cuh"
 #include "sweep_common.cuh"
@@ -85,8 +86,8 @@ struct SweepAcc {
 // (physics_residual_face_*_structured.c: the same position, a coarse
 // hanging edge's two index-paired fluxes).
 template <int N, bool MIXED, int SO = 0>
-__device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5][N][4], int quad, bool valid,
-                                           int lane, double dt, const float qinf[4], SweepAcc &acc,
+__device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5][N][4], double *sa0, int quad,
+                                           bool valid, int lane, double dt, const float qinf[4], SweepAcc &acc,
                                            unsigned &next_claim)
 {
     static_assert(N == 16 || N == 8, "row sweep for 16x16 and 8x8 patches");
@@ -271,8 +272,11 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
         float below[8];      // record of the row below (y-face partner)
         double part[4];      // (-F(x-1/2) + F(x+1/2)) - F(y-1/2) of the row below
         double qbelow[4];    // input state of the row below
-        double a0below[4] = {0.0, 0.0, 0.0, 0.0};  // first auxiliary input of the row below
-        double a0next[4] = {0.0, 0.0, 0.0, 0.0};   // ... of the current row, loaded a row ahead of its use
+        // the stage's first auxiliary input (Q0 of the Shu-Osher stages 2-3)
+        // of row j goes by cp.async into this lane's slot j & 1 of the warp's
+        // buffer sa0 ([slot][field][lane]) while row j is swept, and is read
+        // when row j is finished in the next step: prefetched a row ahead
+        // without holding it in registers
         const bool has_a0 = SO > 0 ? SO >= 2 : a.a0 != nullptr;
         auto finish = [&](int jr, const double gup[4]) {
             const long long gi = qbase + jr * N + i;
@@ -283,7 +287,7 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
                 kv[f] = -(r * inv_vol);
             }
             if (!valid) return;
-            auto A0 = [&](int f) -> double { return a0below[f]; };
+            auto A0 = [&](int f) -> double { return has_a0 ? sa0[(jr & 1) * 128 + f * 32 + lane] : 0.0; };
             auto A1 = [&](int f) -> double { return a.a1[f * stride + gi]; };
             if constexpr (SO > 0) rk_update<kSchemeRK3ShuOsher, SO>(a, dt, stride, gi, qbelow, kv, A0, A1, qn);
             else rk_update(a, dt, stride, gi, qbelow, kv, A0, A1, qn);
@@ -320,11 +324,12 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
                 if (lane == 0) next_claim = atomicAdd(&a.scal->work_next, 1u);
             }
             // the auxiliary input of this row, used when the row is finished
-            // in the next step (its load latency is covered by the fluxes)
+            // in the next step (its latency is covered by the fluxes)
+            if (has_a0) {
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                a0below[f] = a0next[f];
-                a0next[f] = has_a0 ? a.a0[f * stride + qbase + j * N + i] : 0.0;
+                for (int f = 0; f < 4; ++f)
+                    cp_async8(sa0 + (j & 1) * 128 + f * 32 + lane, a.a0 + f * stride + qbase + j * N + i);
+                cp_async_commit();
             }
             float P[8];
             cell_prims_fp32(q4, P);
@@ -360,6 +365,7 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
             } else {
 #pragma unroll
                 for (int f = 0; f < 4; ++f) gy[f] = (double)fy[f];
+                if (has_a0) cp_async_wait_group<1>();  // row j-1's input has landed
                 finish(j - 1, gy);
             }
 #pragma unroll
@@ -377,10 +383,8 @@ __device__ __forceinline__ void sweep_quad(const StageArgs &a, double (*sedge)[5
         {
             double gtop[4];
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                gtop[f] = h == 0 ? sedge[sub][4][i][f] : sedge[sub][3][i][f];
-                a0below[f] = a0next[f];
-            }
+            for (int f = 0; f < 4; ++f) gtop[f] = h == 0 ? sedge[sub][4][i][f] : sedge[sub][3][i][f];
+            if (has_a0) cp_async_wait_group<0>();
             finish(R * h + R - 1, gtop);
         }
         __syncwarp();  // the next item rewrites this warp's edge table
@@ -400,6 +404,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
     constexpr int QPW = 32 / (2 * N);
     constexpr unsigned FULL = 0xffffffffu;
     __shared__ double sedge[WARPS][QPW][5][N][4];
+    __shared__ __align__(16) double sa0[WARPS][2 * 4 * 32];
     __shared__ double red[64];
     __shared__ int s_last;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -414,7 +419,7 @@ __device__ __forceinline__ void sweep_body(const StageArgs &a)
         const bool valid = QPW == 1 || item * QPW + sub < a.nquad;
         const int quad = valid ? item * QPW + sub : item * QPW;
         unsigned nxt = 0;  // claimed by lane 0 during the item's last row
-        sweep_quad<N, false, SO>(a, sedge[w], quad, valid, lane, dt, qinf, acc, nxt);
+        sweep_quad<N, false, SO>(a, sedge[w], sa0[w], quad, valid, lane, dt, qinf, acc, nxt);
         item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
     }
     sweep_reduce<WARPS>(a, acc.dt_min, acc.norm, acc.flags, red, &s_last);
@@ -430,6 +435,7 @@ __device__ __forceinline__ void sweep_body_mixed(const StageArgs &a)
 {
     constexpr unsigned FULL = 0xffffffffu;
     __shared__ double sedge_raw[WARPS][5 * 16 * 4];
+    __shared__ __align__(16) double sa0[WARPS][2 * 4 * 32];
     __shared__ double red[64];
     __shared__ int s_last;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -442,14 +448,14 @@ __device__ __forceinline__ void sweep_body_mixed(const StageArgs &a)
     while (item < nitems) {
         unsigned nxt = 0;  // claimed by lane 0 during the item's last row
         if (item < a.nwork16) {
-            sweep_quad<16, true, SO>(a, reinterpret_cast<double(*)[5][16][4]>(sedge_raw[w]), a.work[item], true,
-                                     lane, dt, qinf, acc, nxt);
+            sweep_quad<16, true, SO>(a, reinterpret_cast<double(*)[5][16][4]>(sedge_raw[w]), sa0[w], a.work[item],
+                                     true, lane, dt, qinf, acc, nxt);
         } else {
             const int k = 2 * (item - a.nwork16) + lane / 16;
             const bool valid = k < a.nwork8;
             const int quad = a.work[a.nwork16 + (valid ? k : k - 1)];
-            sweep_quad<8, true, SO>(a, reinterpret_cast<double(*)[5][8][4]>(sedge_raw[w]), quad, valid, lane, dt,
-                                    qinf, acc, nxt);
+            sweep_quad<8, true, SO>(a, reinterpret_cast<double(*)[5][8][4]>(sedge_raw[w]), sa0[w], quad, valid,
+                                    lane, dt, qinf, acc, nxt);
         }
         item = nwarps + (int)__shfl_sync(FULL, nxt, 0);
     }
