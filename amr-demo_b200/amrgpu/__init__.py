@@ -498,6 +498,34 @@ class Session:
         self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s),
                                getattr(self, "_rule", None))
 
+    def adapt_regrid(self, forest, min_level, max_level, tags=None, refine_value=1, coarsen_value=0,
+                     return_tags=False):
+        """The whole regrid in one call (amrgpu_session_adapt_regrid): the
+        session's tags (or `tags`, one per quad), forest.adapt(tags,
+        refine_value, coarsen_value, min_level, max_level) and
+        self.balance_regrid(forest). The refine / coarsen also runs on the
+        device when the session's last regrid came from this unchanged
+        forest. return_tags: also return the tags used."""
+        n = self.mesh.ncell
+        assert forest.num_quads == n
+        tin = None if tags is None else np.ascontiguousarray(tags, dtype=np.int32)
+        if tin is not None:
+            assert len(tin) == n
+        tout = np.zeros(n, np.int32) if return_tags else None
+        forest.version += 1
+        check(lib().amrgpu_session_adapt_regrid(self._s, C.c_void_p(forest._f), None if tin is None else ip(tin),
+                                                 None if tout is None else ip(tout), int(refine_value),
+                                                 int(coarsen_value), int(min_level), int(max_level)),
+              "adapt_regrid")
+        self.mesh = ForestMesh(forest, self.mesh.n, lib().amrgpu_session_face_count(self._s),
+                               getattr(self, "_rule", None))
+        return tout
+
+    def holds_forest(self, forest):
+        """True when the next adapt_regrid of `forest` adapts on the device
+        (amrgpu_session_holds_forest)."""
+        return bool(lib().amrgpu_session_holds_forest(self._s, C.c_void_p(forest._f)))
+
     def reserve(self, cells, quads):
         """Grows the session's buffers now for meshes of up to `cells` cells
         and `quads` quads, so that regrids within those bounds allocate

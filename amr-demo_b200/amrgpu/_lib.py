@@ -117,6 +117,9 @@ PROTOTYPES = {
     "amrgpu_forest_balance_device": (C.c_int, [C.c_void_p, C.c_void_p]),
     "amrgpu_forest_adapt": (C.c_int, [C.c_void_p, i32p, C.c_int, C.c_int, C.c_int, C.c_int]),
     "amrgpu_session_balance_regrid": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "amrgpu_session_adapt_regrid": (C.c_int, [C.c_void_p, C.c_void_p, i32p, i32p, C.c_int, C.c_int, C.c_int,
+                                              C.c_int]),
+    "amrgpu_session_holds_forest": (C.c_int, [C.c_void_p, C.c_void_p]),
     "amrgpu_session_reserve": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int]),
     "amrgpu_session_balance_stall_test": (C.c_int, [C.c_void_p, C.c_void_p]),
     "amrgpu_session_quad_descriptors": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),

@@ -112,17 +112,19 @@ def regrid(forest, session, n, min_level, max_level, config=None, form=None, dev
     arrays and the session decodes them. size_of_level: mixed patch sizes
     (a level -> 8 / 16 rule, Forest.patch_sizes): the host path, with the
     mesh of Forest.mesh_mixed."""
+    if device_mesh:
+        # tags, refine / coarsen and balance in one call (on the device too
+        # when the session's last regrid came from this forest)
+        if size_of_level is not None:
+            session.set_patch_rule(size_of_level)
+        session.adapt_regrid(forest, min_level, max_level)
+        return session
     tags = session.tag()
-    if size_of_level is not None and not device_mesh:
+    if size_of_level is not None:
         forest.adapt(tags, 1, 0, min_level, max_level)
         forest.balance()
         kind, src = forest.remap()
         session.regrid(forest.mesh_mixed(forest.patch_sizes(size_of_level)), kind, src)
-    elif device_mesh:
-        if size_of_level is not None:
-            session.set_patch_rule(size_of_level)
-        forest.adapt(tags, 1, 0, min_level, max_level)
-        session.balance_regrid(forest)
     else:
         _, lev, _, _ = forest.quads()
         forest.begin_regrid()

@@ -169,9 +169,9 @@ def regrid_by_classes(forest, session, n, classes, min_level, max_level):
     """Regrid with indicator classes: refine class-1 quads below max_level,
     coarsen complete families whose children are all class 0 above
     min_level (a refined child inherits its parent's refine tag), 2:1
-    balance, remap in place."""
-    forest.adapt(classes, REFINE, COARSEN, min_level, max_level)
-    session.balance_regrid(forest)
+    balance, remap in place (one Session.adapt_regrid call: on the device
+    too when the session's last regrid came from this forest)."""
+    session.adapt_regrid(forest, min_level, max_level, tags=classes, refine_value=REFINE, coarsen_value=COARSEN)
 
 
 def vortex_amr(seed=0, n=8, min_level=3, max_level=6, tol=0.02, lo_frac=0.25, form=1, beta=None, center=None):

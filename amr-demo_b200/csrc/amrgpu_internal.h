@@ -31,6 +31,9 @@ void forest_destroy(Forest *f);
 int forest_num_quads(const Forest *f);
 const std::vector<Leaf> &forest_leaves(const Forest *f);
 std::vector<Leaf> &forest_leaves_mut(Forest *f);
+// Advanced by every call that may change the leaves (forest_leaves_mut
+// included): equal values mean unchanged leaves.
+uint64_t forest_version(const Forest *f);
 // Resizes the forest's leaves to n, reserving a quarter more when the
 // capacity runs out (a regrid then rarely touches freshly allocated pages).
 void forest_grow_leaves(Forest *f, size_t n);

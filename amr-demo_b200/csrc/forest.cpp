@@ -106,6 +106,9 @@ struct Forest {
     // output buffer of forest_adapt's single pass, swapped with `leaves`
     // afterwards; its capacity is kept from regrid to regrid
     std::vector<Leaf> spare;
+    // advanced by every call that may change the leaves, so that a copy of
+    // them elsewhere (a session's device leaves) can tell it is current
+    uint64_t version = 0;
 
     int tree_of(int tx, int ty) const { return tree_at[size_t(ty) * nx + tx]; }
 
@@ -272,10 +275,17 @@ void forest_destroy(Forest *f) { delete f; }
 int forest_num_quads(const Forest *f) { return int(f->leaves.size()); }
 
 const std::vector<Leaf> &forest_leaves(const Forest *f) { return f->leaves; }
-std::vector<Leaf> &forest_leaves_mut(Forest *f) { return f->leaves; }
+std::vector<Leaf> &forest_leaves_mut(Forest *f)
+{
+    ++f->version;
+    return f->leaves;
+}
+
+uint64_t forest_version(const Forest *f) { return f->version; }
 
 void forest_grow_leaves(Forest *f, size_t n)
 {
+    ++f->version;
     std::vector<Leaf> &L = f->leaves;
     if (L.capacity() < n) L.reserve(n + n / 4);
     L.resize(n);
@@ -392,6 +402,7 @@ void coarsen_in_place(Forest *f, Flag flag, int min_level)
 
 void forest_begin_regrid(Forest *f)
 {
+    ++f->version;
     for (size_t i = 0; i < f->leaves.size(); ++i) {
         f->leaves[i].src = int(i);
         f->leaves[i].src_kind = kRemapCopy;
@@ -400,6 +411,7 @@ void forest_begin_regrid(Forest *f)
 
 int forest_refine(Forest *f, const int *flags, int max_level)
 {
+    ++f->version;
     const std::vector<Leaf> &L = f->leaves;
     // children inherit the refine tag
     refine_in_place(f, [&](size_t i) { return flags[i] && L[i].level < max_level && L[i].level < kMaxLevel; }, 1,
@@ -409,12 +421,14 @@ int forest_refine(Forest *f, const int *flags, int max_level)
 
 int forest_coarsen(Forest *f, const int *flags, int min_level)
 {
+    ++f->version;
     coarsen_in_place(f, [&](size_t i) { return flags[i] != 0; }, min_level);
     return int(f->leaves.size());
 }
 
 int forest_adapt(Forest *f, const int *tags, int refine_value, int coarsen_value, int min_level, int max_level)
 {
+    ++f->version;
     // One pass over the leaves into the spare buffer, equal to begin_regrid,
     // storing the tags, forest_refine and then forest_coarsen: the children
     // of a refined leaf all carry their parent's source index, so they never
@@ -491,6 +505,7 @@ int forest_adapt(Forest *f, const int *tags, int refine_value, int coarsen_value
 
 int forest_balance(Forest *f)
 {
+    ++f->version;
     // Refine until every leaf's face and corner neighbours are at most one
     // level coarser (2:1 across faces and corners). Leaves untouched since
     // the last balance are pairwise balanced, so every violation has a

@@ -526,6 +526,85 @@ __device__ bool grid_scan(int n, Cnt cnt, int *pos, int *bsum, BalanceCtl *ctl)
     return grid_barrier(ctl);
 }
 
+// The adapt phase's decisions for one leaf, those of forest_adapt
+// (forest.cpp): a leaf refines when tagged refine_value below max_level; a
+// complete family of four siblings (consecutive in Morton order, same tree
+// and level, none refining, all tagged coarsen_value above min_level)
+// becomes its parent, written where its first child was. Family starts
+// never overlap (the second to fourth children are not aligned to a parent
+// of their level), so each leaf decides on its own.
+__device__ __forceinline__ bool adapt_refines(const AdaptArgs &ad, const int4 q, int tag)
+{
+    return tag == ad.refine_value && q.y < ad.max_level && q.y < kMaxLevelG;
+}
+
+__device__ __forceinline__ bool adapt_coarsens(const AdaptArgs &ad, const int4 q, int tag)
+{
+    return tag == ad.coarsen_value && q.y > ad.min_level;
+}
+
+__device__ bool adapt_family_start(const AdaptArgs &ad, const int4 *in, int n, int i)
+{
+    const int4 p = in[i];
+    if (!(p.y > 0 && p.y > ad.min_level && i + 3 < n)) return false;
+    const long long P = qlen_d(p.y - 1), h = qlen_d(p.y);
+    const long long px = (p.z / P) * P, py = (p.w / P) * P;
+    if (p.z != px || p.w != py) return false;
+    for (int c = 0; c < 4; ++c) {
+        const int4 b = in[i + c];
+        const int t = ad.tags[i + c];
+        if (b.x != p.x || b.y != p.y || b.z != px + (c & 1) * h || b.w != py + ((c >> 1) & 1) * h ||
+            adapt_refines(ad, b, t) || !adapt_coarsens(ad, b, t))
+            return false;
+    }
+    return true;
+}
+
+// Leaves leaf i of the adapt becomes: 4 (refined), 0 (second to fourth
+// child of a coarsened family), else 1. fs: family-start marks.
+__device__ __forceinline__ int adapt_count(const AdaptArgs &ad, const int4 *in, const unsigned char *fs, int i)
+{
+    if (adapt_refines(ad, in[i], ad.tags[i])) return 4;
+    const bool member = (i >= 1 && __ldcg(fs + i - 1)) || (i >= 2 && __ldcg(fs + i - 2)) ||
+                        (i >= 3 && __ldcg(fs + i - 3));
+    return member ? 0 : 1;
+}
+
+// Writes leaf i's output leaves at pos[i] (the exclusive scan of the
+// counts): children of a refined leaf (new, source = the leaf), a family's
+// parent (new, the mean of the family), or the leaf itself (source = the
+// leaf). Origins are the identity: the balance then refers back to these.
+__device__ __forceinline__ void adapt_write_item(const AdaptArgs &ad, const int4 *in, const unsigned char *fs,
+                                                 const int *pos, int4 *out, int *orig_out,
+                                                 unsigned char *dirty_out, int i)
+{
+    const int4 q = in[i];
+    const int at = __ldcg(pos + i);
+    if (adapt_refines(ad, q, ad.tags[i])) {
+        const int h = int(qlen_d(q.y + 1));
+        for (int c = 0; c < 4; ++c) {
+            out[at + c] = make_int4(q.x, q.y + 1, q.z + (c & 1) * h, q.w + ((c >> 1) & 1) * h);
+            orig_out[at + c] = at + c;
+            dirty_out[at + c] = 1;
+            ad.kind[at + c] = 0;  // injection from the parent
+            ad.src[at + c] = i;
+        }
+        return;
+    }
+    if (__ldcg(pos + i + 1) == at) return;  // absorbed into a family's parent
+    if (__ldcg(fs + i)) {
+        out[at] = make_int4(q.x, q.y - 1, q.z, q.w);  // the first child's corner is the parent's
+        dirty_out[at] = 1;
+        ad.kind[at] = 1;  // mean of the four children
+    } else {
+        out[at] = q;
+        dirty_out[at] = 0;
+        ad.kind[at] = 0;
+    }
+    orig_out[at] = at;
+    ad.src[at] = i;
+}
+
 __global__ void __launch_bounds__(256) balance_loop_kernel(const BalanceLoopArgs a)
 {
     BalanceCtl *ctl = a.ctl;
@@ -533,7 +612,30 @@ __global__ void __launch_bounds__(256) balance_loop_kernel(const BalanceLoopArgs
     int nl = a.nl, live = a.live, passes = 0;
     bool ok = true, done = false, overflow = false, refined = false;
     ForestDev F = a.F;
-    for (int pass = 0; pass < 64 && ok; ++pass) {
+    int adapted = 0, adapt_total = 0;
+    if (a.adapt) {
+        // refine / coarsen by tags from buffer `live` into the other buffer
+        const int4 *in = a.leaves[live];
+        unsigned char *fs = a.flags;
+        for (int i = gtid; i < nl; i += gstride) fs[i] = adapt_family_start(a.ad, in, nl, i) ? 1 : 0;
+        ok = grid_barrier(ctl);
+        if (ok) ok = grid_scan(nl, [&](int i) { return adapt_count(a.ad, in, fs, i); }, a.pos, a.bsum, ctl);
+        if (ok) {
+            adapt_total = __ldcg(a.pos + nl);
+            if (adapt_total > a.cap) {
+                overflow = true;
+            } else {
+                for (int i = gtid; i < nl; i += gstride)
+                    adapt_write_item(a.ad, in, fs, a.pos, a.leaves[1 - live], a.orig[1 - live], a.dirty[1 - live],
+                                     i);
+                ok = grid_barrier(ctl);
+                live = 1 - live;
+                nl = adapt_total;
+                adapted = adapt_total;
+            }
+        }
+    }
+    for (int pass = 0; pass < 64 && ok && !overflow; ++pass) {
         ++passes;
         F.leaves = a.leaves[live];
         F.nq = nl;
@@ -563,7 +665,13 @@ __global__ void __launch_bounds__(256) balance_loop_kernel(const BalanceLoopArgs
     // the balanced leaves' remap table and descriptors (keys and tree starts
     // are the last pass's, which refined nothing)
     if (ok && done && a.build) {
-        if (a.kind0) {
+        if (a.ad.kind) {
+            for (int k = gtid; k < nl; k += gstride) {
+                const int o = __ldcg(a.orig[live] + k);
+                a.kind[k] = __ldcg(a.ad.kind + o);
+                a.src[k] = __ldcg(a.ad.src + o);
+            }
+        } else if (a.kind0) {
             for (int k = gtid; k < nl; k += gstride) {
                 const int o = a.orig[live][k];
                 a.kind[k] = a.kind0[o];
@@ -584,6 +692,8 @@ __global__ void __launch_bounds__(256) balance_loop_kernel(const BalanceLoopArgs
         ctl->passes = passes;
         ctl->result = !ok ? kBalanceTimeout : overflow ? kBalanceOverflow : done ? kBalanceDone : kBalanceNoConverge;
         ctl->refined = refined ? 1 : 0;
+        ctl->adapted = adapted;
+        ctl->adapt_total = adapt_total;
     }
 }
 

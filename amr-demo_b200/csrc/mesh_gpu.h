@@ -51,6 +51,15 @@ struct BalanceCtl {
     int abort;                    // set by a barrier wait that ran out
     int nl, live, passes, refined;
     int result;                   // kBalance*
+    int adapted;                  // leaves after the adapt phase (0: no adapt ran or it overflowed)
+    int adapt_total;              // leaves the adapt phase needs (also on overflow)
+};
+// Refine / coarsen of the loop's starting leaves by per-leaf tags, before
+// the balance: the host forest's forest_adapt, leaf for leaf (forest.cpp).
+struct AdaptArgs {
+    const int *tags;              // one per starting leaf
+    int refine_value, coarsen_value, min_level, max_level;
+    int *kind, *src;              // remap table of the adapted leaves
 };
 struct BalanceLoopArgs {
     ForestDev F;                  // brick and tree tables; leaves / nq set per pass, keys written
@@ -72,6 +81,9 @@ struct BalanceLoopArgs {
     int *kind, *src;              //   ... gathered for the balanced leaves
     int stall_test;               // nonzero: the barrier's arrival count starts out of reach, so
                                   // every wait runs out (tests of the bounded wait)
+    int adapt;                    // nonzero: adapt the starting leaves first (ad)
+    AdaptArgs ad;                 // ad.kind non-null: the balanced leaves' remap table comes from
+                                  //   ad.kind / ad.src (an adapt of this or an earlier launch)
 };
 cudaError_t launch_balance_loop(const BalanceLoopArgs &a, int sms, cudaStream_t st);
 size_t balance_loop_bsum_ints(int sms);

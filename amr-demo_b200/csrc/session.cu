@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <string>
@@ -133,6 +134,14 @@ struct amrgpu_session {
     size_t remap0_bytes = 0;
     int bal_cap = 0;                      // leaves the balance buffers hold
     int bal_trees = 0;                    // trees the balance work area holds tables for
+    // the forest whose leaves the balance buffers still hold (buffer
+    // dev_live, nquad leaves, the session's mesh), at version
+    // dev_forest_version: a regrid of that unchanged forest adapts them on
+    // the device instead of staging the host's leaves
+    const Forest *dev_forest = nullptr;
+    uint64_t dev_forest_version = 0;
+    int dev_live = 0;
+    cudaEvent_t ev_tags = nullptr;        // the tags' copy to the host has landed
     bool rect = true;                 // every quad an axis-aligned rectangle
     bool launch_pinned = false;       // the stage launch was chosen by the caller
     bool tune_pending = false;        // the autotuner runs before the next step
@@ -1002,6 +1011,7 @@ void amrgpu_session_destroy(amrgpu_session_t *s)
     cudaFree(s->d_remap0);
     cudaFree(s->d_bal_work);
     cudaFreeHost(s->h_stage);
+    if (s->ev_tags) cudaEventDestroy(s->ev_tags);
     cudaFree(s->d_mix);
     cudaFree(s->d_mix_old);
     cudaFree(s->d_work);
@@ -1589,21 +1599,37 @@ int amrgpu_session_totals(amrgpu_session_t *s, double totals[4])
     return AMRGPU_OK;
 }
 
-int amrgpu_session_tag(amrgpu_session_t *s, int *tags)
+}  // extern "C"
+
+namespace {
+
+// The session's refinement tags of the current state into d_tags.
+bool launch_tags(amrgpu_session *s)
 {
-    if (!s || !tags) return AMRGPU_ERR_ARG;
-    if (s->nquad == 0) return AMRGPU_OK;
     TagMethods m;
     int nm = std::min(s->cfg.amr_ntag_methods, 5);
     for (int k = 0; k < 5; ++k) {
         m.method[k] = k < nm ? s->cfg.amr_tag_methods[size_t(k)] : 0;
         m.tol[k] = k < nm ? s->cfg.amr_tag_tolerances[size_t(k)] : 0.0;
     }
-    bool ok = cuda_ok(s->mixed ? launch_tag_mixed(rolebuf(s, RX), s->d_quads, s->d_mix, s->nquad, nm, m, s->d_tags,
-                                                  s->stream)
-                               : launch_tag(s->n, rolebuf(s, RX), s->d_quads, s->nquad, nm, m, s->d_tags, s->stream),
-                      "tag kernel");
+    const bool ok = cuda_ok(s->mixed ? launch_tag_mixed(rolebuf(s, RX), s->d_quads, s->d_mix, s->nquad, nm, m,
+                                                        s->d_tags, s->stream)
+                                     : launch_tag(s->n, rolebuf(s, RX), s->d_quads, s->nquad, nm, m, s->d_tags,
+                                                  s->stream),
+                            "tag kernel");
     s->launches++;
+    return ok;
+}
+
+}  // namespace
+
+extern "C" {
+
+int amrgpu_session_tag(amrgpu_session_t *s, int *tags)
+{
+    if (!s || !tags) return AMRGPU_ERR_ARG;
+    if (s->nquad == 0) return AMRGPU_OK;
+    bool ok = launch_tags(s);
     if (ok)
         ok = cuda_ok(cudaMemcpyAsync(tags, s->d_tags, sizeof(int) * size_t(s->nquad), cudaMemcpyDeviceToHost,
                                      s->stream),
@@ -1662,7 +1688,17 @@ int ensure_quad_arrays(amrgpu_session *s, int nq)
         for (int *p : arr) cudaFree(p);
         return AMRGPU_ERR_CUDA;
     }
+    // the tags are kept (a device adapt that grows its buffers reads them
+    // again); kind and source are outputs
+    if (s->d_tags && s->cap_quads > 0)
+        ok = cuda_ok(cudaMemcpyAsync(arr[0], s->d_tags, sizeof(int) * size_t(s->cap_quads), cudaMemcpyDeviceToDevice,
+                                     s->stream),
+                     "tags copy");
     cudaStreamSynchronize(s->stream);
+    if (!ok) {
+        for (int *p : arr) cudaFree(p);
+        return AMRGPU_ERR_CUDA;
+    }
     cudaFree(s->d_tags);
     cudaFree(s->d_kind);
     cudaFree(s->d_src);
@@ -1692,6 +1728,7 @@ int ensure_desc(amrgpu_session *s, QuadDesc **buf, int *cap, int nq)
 // of the same capacity, or a fresh set when the mesh outgrew the capacity.
 int apply_regrid(amrgpu_session *s, int nq, int nface, long long mixed_cells = -1)
 {
+    s->dev_forest = nullptr;  // the new mesh's leaves are the caller's to record
     const long long cells = mixed_cells >= 0 ? mixed_cells : (long long)nq * s->n * s->n;
     const long long stride = std::max<long long>(((cells + 31) / 32) * 32, 32);
     double *qold = rolebuf(s, RX);
@@ -2120,6 +2157,7 @@ BalLayout bal_layout(int cap, int ntrees)
 // also serves a forest with fewer.
 int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
 {
+    s->dev_forest = nullptr;
     const int alloc_trees = std::max(ntrees, s->bal_trees);
     const BalLayout A = bal_layout(cap, alloc_trees);
     const BalLayout L = bal_layout(cap, ntrees);
@@ -2169,6 +2207,7 @@ int bal_grow(amrgpu_session *s, int cap, int ntrees, int live, int keep)
 // d_remap0; grows the balance buffers to 1.5 times the leaves.
 int stage_leaves(amrgpu_session *s, std::vector<Leaf> &leaves, const BrickView &B, int ntrees, bool remap)
 {
+    s->dev_forest = nullptr;
     const int nl = int(leaves.size());
     // staging: leaves (int4), origin, remap kind / source (with remap),
     // dirty bytes, brick tables
@@ -2397,23 +2436,44 @@ int balance_impl(amrgpu_session *s, Forest *fo, int *live_out, bool remap)
 // leaves go back to the host forest, then the state is remapped as by
 // build_and_apply. Sessions with a patch-size rule take balance_impl and
 // build_and_apply instead (the mixed build needs the leaf count first).
-int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false)
+// The balance, descriptors and remap table in one cooperative launch (plus
+// read-backs), then the remap. Staged: the host forest's leaves go to the
+// device first. With ad (device adapt): the loop starts from the leaves the
+// balance buffers still hold for this forest (dev_live), refines / coarsens
+// them by ad's tags on the device, and host_work (the host forest's own
+// adapt, which must reach the same leaves) runs while the launch does.
+int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false, AdaptArgs *ad = nullptr,
+                         const std::function<int()> &host_work = {})
 {
-    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
     BrickView B;
     forest_brick(fo, &B);
     const int ntrees = B.nx * B.ny;
-    const int n0 = int(leaves.size());
-    int rc = stage_leaves(s, leaves, B, ntrees, true);
-    if (rc) return rc;
+    int rc;
+    int n0 = s->nquad, live = 0;
+    if (ad) {
+        live = s->dev_live;
+        // the adapted leaves' remap table, kind then source, at a split
+        // fixed for this regrid (a later growth of the leaf buffers keeps
+        // d_remap0)
+        if ((rc = ensure_dev(s, &s->d_remap0, &s->remap0_bytes, 8 * size_t(s->bal_cap) + 16))) return rc;
+        ad->kind = static_cast<int *>(s->d_remap0);
+        ad->src = ad->kind + s->bal_cap;
+    } else {
+        std::vector<Leaf> &leaves = forest_leaves_mut(fo);
+        n0 = int(leaves.size());
+        if ((rc = stage_leaves(s, leaves, B, ntrees, true))) return rc;
+    }
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-    int nl = n0, live = 0;
+    int nl = n0;
+    bool adapt_pending = ad != nullptr, host_done = !host_work;
+    int adapted = -1;
     BalanceCtl ctl{};
     int status[2] = {0, 0};
     for (int attempt = 0;; ++attempt) {
         const int cap = s->bal_cap;
         if ((rc = ensure_desc(s, &s->d_quads_alt, &s->cap_desc_alt, cap))) return rc;
         if ((rc = ensure_quad_arrays(s, cap))) return rc;
+        if (ad) ad->tags = s->d_tags;  // kept by a growth of the quad arrays
         const size_t n4 = al(sizeof(int) * (4 * size_t(cap) + 1));
         const size_t o_emits = 0, o_scan = n4, o_emitter = 2 * n4, o_status = 3 * n4;
         const size_t o_bsum = o_status + 256, o_ctl = o_bsum + al(sizeof(int) * balance_loop_bsum_ints(s->sms));
@@ -2450,9 +2510,14 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false)
         a.scan = reinterpret_cast<int *>(base + o_scan);
         a.emitter = reinterpret_cast<int *>(base + o_emitter);
         a.status = reinterpret_cast<int *>(base + o_status);
-        const int *rm = static_cast<const int *>(s->d_remap0);
-        a.kind0 = rm;
-        a.src0 = rm + n0;
+        if (ad) {
+            a.adapt = adapt_pending ? 1 : 0;
+            a.ad = *ad;
+        } else {
+            const int *rm = static_cast<const int *>(s->d_remap0);
+            a.kind0 = rm;
+            a.src0 = rm + n0;
+        }
         a.kind = s->d_kind;
         a.src = s->d_src;
         a.stall_test = stall_test ? 1 : 0;
@@ -2462,15 +2527,33 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false)
         // staging takes the results
         char *h = static_cast<char *>(s->h_stage);
         if (!cuda_ok(cudaMemcpyAsync(h, a.ctl, sizeof(BalanceCtl), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
-            !cuda_ok(cudaMemcpyAsync(h + 256, a.status, sizeof(status), cudaMemcpyDeviceToHost, s->stream), "D2H") ||
-            !cuda_ok(cudaStreamSynchronize(s->stream), "sync"))
+            !cuda_ok(cudaMemcpyAsync(h + 256, a.status, sizeof(status), cudaMemcpyDeviceToHost, s->stream), "D2H"))
             return AMRGPU_ERR_CUDA;
+        if (!host_done) {
+            host_done = true;
+            if ((rc = host_work())) {
+                cudaStreamSynchronize(s->stream);
+                return rc;
+            }
+        }
+        if (!cuda_ok(cudaStreamSynchronize(s->stream), "sync")) return AMRGPU_ERR_CUDA;
         std::memcpy(&ctl, h, sizeof(ctl));
         std::memcpy(status, h + 256, sizeof(status));
+        if (adapt_pending && ctl.adapted > 0) {
+            adapt_pending = false;
+            adapted = ctl.adapted;
+        }
         if (ctl.result == kBalanceOverflow && attempt < 16) {
             // more leaves than the buffers hold: grow (keeping the live
-            // leaves, their origin and dirty marks) and go on from there
-            if ((rc = bal_grow(s, 2 * s->bal_cap, ntrees, ctl.live, ctl.nl))) return rc;
+            // leaves, their origin and dirty marks) and go on from there;
+            // an adapt that did not fit runs again from its own leaves
+            const int need = adapt_pending ? ctl.adapt_total + ctl.adapt_total / 2 : 0;
+            if ((rc = bal_grow(s, std::max(2 * s->bal_cap, need), ntrees, ctl.live, ctl.nl))) return rc;
+            if (adapt_pending) {
+                if ((rc = ensure_dev(s, &s->d_remap0, &s->remap0_bytes, 8 * size_t(s->bal_cap) + 16))) return rc;
+                ad->kind = static_cast<int *>(s->d_remap0);
+                ad->src = ad->kind + s->bal_cap;
+            }
             nl = ctl.nl;
             live = 0;
             continue;
@@ -2490,6 +2573,11 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false)
         set_error(AMRGPU_ERR_MESH, "session regrid from a forest: the forest is not 2:1 balanced");
         return AMRGPU_ERR_MESH;
     }
+    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
+    if (ad && adapted != int(leaves.size())) {
+        set_error(AMRGPU_ERR_MESH, "device adapt: the leaves differ from the host forest's adapt");
+        return AMRGPU_ERR_MESH;
+    }
     if (ctl.refined) {
         if ((rc = leaves_back_to_host(s, fo, nl, ctl.live, ntrees))) return rc;
     } else {
@@ -2499,7 +2587,13 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false)
     std::swap(s->cap_desc, s->cap_desc_alt);
     s->h_quads.clear();  // the live descriptors exist on the device only
     s->rect = true;      // brick quads are axis-aligned rectangles
-    return apply_regrid(s, nl, nl > 0 ? status[1] : 0);
+    if ((rc = apply_regrid(s, nl, nl > 0 ? status[1] : 0))) return rc;
+    // the balance buffers hold this forest's leaves: the next regrid of it
+    // can adapt them on the device
+    s->dev_forest = fo;
+    s->dev_forest_version = forest_version(fo);
+    s->dev_live = ctl.live;
+    return AMRGPU_OK;
 }
 
 }  // namespace
@@ -2557,6 +2651,84 @@ int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f)
     set_brick(F, B, s->cfg.bc);
     F.nq = nq;
     return build_and_apply(s, F);
+}
+
+int amrgpu_session_adapt_regrid(amrgpu_session_t *s, amrgpu_forest_t *f, const int *tags, int *tags_out,
+                                int refine_value, int coarsen_value, int min_level, int max_level)
+{
+    if (!s || !f || !f->f) return AMRGPU_ERR_ARG;
+    Forest *fo = f->f;
+    const int nq = s->nquad;
+    if (forest_num_quads(fo) != nq) {
+        set_error(AMRGPU_ERR_ARG, "session_adapt_regrid: the forest's quads are not the session's mesh");
+        return AMRGPU_ERR_ARG;
+    }
+    if (s->mixed && !s->has_rule) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "mixed patch sizes: set a patch-size rule (amrgpu_session_set_patch_rule) "
+                                          "or regrid through amrgpu_session_regrid");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    if (s->stage_pos != 0) {
+        set_error(AMRGPU_ERR_ARG, "session_adapt_regrid: a step begun with step_stage is not finished");
+        return AMRGPU_ERR_ARG;
+    }
+    if (s->nghost != 0) {
+        set_error(AMRGPU_ERR_UNSUPPORTED, "session_adapt_regrid: ghost quads need a ghost exchange after the remap");
+        return AMRGPU_ERR_UNSUPPORTED;
+    }
+    static const bool fused = [] {
+        const char *e = std::getenv("AMRGPU_FUSED_BALANCE");
+        return !(e && std::atoi(e) == 0);
+    }();
+    const bool device = fused && !s->has_rule && nq > 0 && s->dev_forest == fo &&
+                        s->dev_forest_version == forest_version(fo);
+    // the tags on the device (the tag kernel, or the caller's) and on the
+    // host (copied back while the device goes on), in the staging after
+    // the balance's read-back slots
+    int rc = ensure_quad_arrays(s, std::max(nq, s->bal_cap));
+    if (!rc) rc = ensure_stage(s, 512 + sizeof(int) * size_t(nq));
+    if (rc) return rc;
+    if (!s->ev_tags && !cuda_ok(cudaEventCreateWithFlags(&s->ev_tags, cudaEventDisableTiming), "event"))
+        return AMRGPU_ERR_CUDA;
+    int *h_tags = reinterpret_cast<int *>(static_cast<char *>(s->h_stage) + 512);
+    if (nq > 0) {
+        bool ok;
+        if (tags) {
+            std::memcpy(h_tags, tags, sizeof(int) * size_t(nq));
+            ok = cuda_ok(cudaMemcpyAsync(s->d_tags, h_tags, sizeof(int) * size_t(nq), cudaMemcpyHostToDevice,
+                                         s->stream),
+                         "H2D tags");
+        } else {
+            ok = launch_tags(s) && cuda_ok(cudaMemcpyAsync(h_tags, s->d_tags, sizeof(int) * size_t(nq),
+                                                           cudaMemcpyDeviceToHost, s->stream),
+                                           "D2H tags");
+        }
+        if (!ok || !cuda_ok(cudaEventRecord(s->ev_tags, s->stream), "event")) return AMRGPU_ERR_CUDA;
+    }
+    // the host forest's own adapt, with the tags as they arrive
+    auto host_adapt = [&]() -> int {
+        if (nq > 0 && !tags && !cuda_ok(cudaEventSynchronize(s->ev_tags), "sync")) return AMRGPU_ERR_CUDA;
+        if (tags_out && nq > 0) std::memcpy(tags_out, h_tags, sizeof(int) * size_t(nq));
+        forest_adapt(fo, h_tags, refine_value, coarsen_value, min_level, max_level);
+        return AMRGPU_OK;
+    };
+    if (!device) {
+        if ((rc = host_adapt())) return rc;
+        return amrgpu_session_balance_regrid(s, f);
+    }
+    AdaptArgs ad{};
+    ad.tags = s->d_tags;
+    ad.refine_value = refine_value;
+    ad.coarsen_value = coarsen_value;
+    ad.min_level = min_level;
+    ad.max_level = max_level;
+    return balance_regrid_fused(s, fo, false, &ad, host_adapt);
+}
+
+int amrgpu_session_holds_forest(const amrgpu_session_t *s, const amrgpu_forest_t *f)
+{
+    if (!s || !f || !f->f) return 0;
+    return s->dev_forest == f->f && s->dev_forest_version == forest_version(f->f) ? 1 : 0;
 }
 
 int amrgpu_session_reserve(amrgpu_session_t *s, long long cells, int quads)

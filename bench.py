@@ -476,10 +476,11 @@ def _amr_workload_once(args):
     solve = reg = 0.0
     cu = steps = 0
     cells = []
-    parts = dict(tag=0.0, forest=0.0, balance_regrid=0.0)
     cycles = max(1, args.steps // 5)
     for _ in range(cycles):
-        # the regrid of amr.regrid, timed part by part
+        # the regrid of amr.regrid: tags, refine / coarsen (on the device
+        # too, overlapped with the host forest's), balance, descriptors and
+        # remap in one call
         a = time.perf_counter()
         s.step(5)
         rep = s.sync()
@@ -487,14 +488,8 @@ def _amr_workload_once(args):
         cu += rep["steps"] * s.mesh.ncells
         steps += rep["steps"]
         cells.append(s.mesh.ncells)
-        tags = s.tag()
-        c = time.perf_counter()
-        f.adapt(tags, 1, 0, lo, hi)
-        d = time.perf_counter()
-        s.balance_regrid(f)
+        s.adapt_regrid(f, lo, hi)
         h = time.perf_counter()
-        for k, v in zip(parts, (c - b, d - c, h - d)):
-            parts[k] += v
         solve += b - a
         reg += h - b
     err = rep["error"]
@@ -504,7 +499,7 @@ def _amr_workload_once(args):
             "value": cu / (solve + reg), "unit": UNIT, "solve_only": cu / solve, "steps": steps,
             "regrids": steps // 5, "cells_start": cells0, "cells_min": min(cells), "cells_max": max(cells),
             "solve_s": solve, "regrid_s": reg, "setup_s": t_setup, "error": err,
-            "regrid_ms": {k: 1e3 * v / cycles for k, v in parts.items()},
+            "regrid_ms": 1e3 * reg / cycles,
             "solve_ms_per_5_steps": 1e3 * solve / cycles}
 
 

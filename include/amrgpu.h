@@ -439,6 +439,24 @@ int amrgpu_forest_balance_device(amrgpu_forest_t *f, amrgpu_session_t *s);
  * descend from (no remap table built or uploaded by the host after the
  * balance). */
 int amrgpu_session_balance_regrid(amrgpu_session_t *s, amrgpu_forest_t *f);
+/* One whole regrid of the session and its forest f (whose leaves are the
+ * session's mesh): the refinement tags (the session's tag kernel on its
+ * current state when tags is NULL, else the caller's, one per quad), then
+ * amrgpu_forest_adapt(f, tags, refine_value, coarsen_value, min_level,
+ * max_level) and amrgpu_session_balance_regrid(s, f) -- the same forest,
+ * mesh and state. When the session's last regrid came from f and f has not
+ * changed since, the refine / coarsen also runs on the device, at the head
+ * of the balance's single launch, from the leaves the session still holds
+ * (no upload of the forest), while the host adapts f from the tags copied
+ * back; the two must agree (AMRGPU_ERR_MESH otherwise). tags_out (NULL or
+ * one int per quad) receives the tags used. Replaces the tagging, refine /
+ * coarsen and balance of the reference's amr_regrid.c:82-125 in one call. */
+int amrgpu_session_adapt_regrid(amrgpu_session_t *s, amrgpu_forest_t *f, const int *tags, int *tags_out,
+                                int refine_value, int coarsen_value, int min_level, int max_level);
+/* 1 when the session still holds f's current leaves on the device (its
+ * last regrid came from f and f has not changed since), so that the next
+ * amrgpu_session_adapt_regrid of f adapts them there; else 0. */
+int amrgpu_session_holds_forest(const amrgpu_session_t *s, const amrgpu_forest_t *f);
 /* Test support for the bounded waits of amrgpu_session_balance_regrid's
  * one-launch balance (device-wide barriers between its phases, each wait
  * at most 2^22 polls): runs it with the barrier's arrival count started out
