@@ -2281,12 +2281,16 @@ int stage_leaves(amrgpu_session *s, std::vector<Leaf> &leaves, const BrickView &
 }
 
 // The balanced leaves (buffer `live`, nl of them) back into the host
-// forest: coordinates and origin read back, then rewritten in place.
-int leaves_back_to_host(amrgpu_session *s, Forest *fo, int nl, int live, int ntrees)
+// forest: coordinates and origin read back (leaves_back_enqueue, which
+// records ev_tags when they have landed), then rewritten in place
+// (leaves_back_finish, after waiting for that event). The device may go on
+// with other work in between.
+int leaves_back_enqueue(amrgpu_session *s, int nl, int live, int ntrees)
 {
-    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
     int rc = ensure_stage(s, 20 * size_t(nl) + 64);
     if (rc) return rc;
+    if (!s->ev_tags && !cuda_ok(cudaEventCreateWithFlags(&s->ev_tags, cudaEventDisableTiming), "event"))
+        return AMRGPU_ERR_CUDA;
     const BalLayout L = bal_layout(s->bal_cap, ntrees);
     char *in = static_cast<char *>(s->d_bal[live]);
     int *h = static_cast<int *>(s->h_stage);
@@ -2294,9 +2298,17 @@ int leaves_back_to_host(amrgpu_session *s, Forest *fo, int nl, int live, int ntr
     if (nl > 0 &&
         (!cuda_ok(cudaMemcpyAsync(h, in, 16 * size_t(nl), cudaMemcpyDeviceToHost, s->stream), "D2H balance") ||
          !cuda_ok(cudaMemcpyAsync(h_orig, in + L.o_orig, 4 * size_t(nl), cudaMemcpyDeviceToHost, s->stream),
-                  "D2H balance") ||
-         !cuda_ok(cudaStreamSynchronize(s->stream), "sync")))
+                  "D2H balance")))
         return AMRGPU_ERR_CUDA;
+    return cuda_ok(cudaEventRecord(s->ev_tags, s->stream), "event") ? AMRGPU_OK : AMRGPU_ERR_CUDA;
+}
+
+int leaves_back_finish(amrgpu_session *s, Forest *fo, int nl)
+{
+    std::vector<Leaf> &leaves = forest_leaves_mut(fo);
+    if (!cuda_ok(cudaEventSynchronize(s->ev_tags), "sync")) return AMRGPU_ERR_CUDA;
+    const int *h = static_cast<const int *>(s->h_stage);
+    const int *h_orig = h + 4 * size_t(nl);
     if (nl != int(leaves.size())) {
         // in place, from the end backwards: balance only refines, so leaf k
         // comes from input leaf h_orig[k] <= k (non-decreasing in k), which
@@ -2326,6 +2338,12 @@ int leaves_back_to_host(amrgpu_session *s, Forest *fo, int nl, int live, int ntr
         for (Leaf &q : leaves) q.dirty = 0;
     }
     return AMRGPU_OK;
+}
+
+int leaves_back_to_host(amrgpu_session *s, Forest *fo, int nl, int live, int ntrees)
+{
+    const int rc = leaves_back_enqueue(s, nl, live, ntrees);
+    return rc ? rc : leaves_back_finish(s, fo, nl);
 }
 
 // 2:1 balance of forest fo with every pass on the session's GPU; the
@@ -2578,16 +2596,19 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false,
         set_error(AMRGPU_ERR_MESH, "device adapt: the leaves differ from the host forest's adapt");
         return AMRGPU_ERR_MESH;
     }
-    if (ctl.refined) {
-        if ((rc = leaves_back_to_host(s, fo, nl, ctl.live, ntrees))) return rc;
-    } else {
-        for (Leaf &q : leaves) q.dirty = 0;
-    }
+    // the balanced leaves' copy back is queued before the remap and the
+    // next step's CFL minimum; the host forest is rebuilt while they run
+    if (ctl.refined && (rc = leaves_back_enqueue(s, nl, ctl.live, ntrees))) return rc;
     std::swap(s->d_quads, s->d_quads_alt);
     std::swap(s->cap_desc, s->cap_desc_alt);
     s->h_quads.clear();  // the live descriptors exist on the device only
     s->rect = true;      // brick quads are axis-aligned rectangles
     if ((rc = apply_regrid(s, nl, nl > 0 ? status[1] : 0))) return rc;
+    if (ctl.refined) {
+        if ((rc = leaves_back_finish(s, fo, nl))) return rc;
+    } else {
+        for (Leaf &q : leaves) q.dirty = 0;
+    }
     // the balance buffers hold this forest's leaves: the next regrid of it
     // can adapt them on the device
     s->dev_forest = fo;
