@@ -100,11 +100,23 @@ __device__ bool shifted_d(const ForestDev &F, int tree, int level, long long x, 
     return true;
 }
 
-// last leaf of the tree whose corner precedes (x,y) on the Morton curve
+// last leaf of the tree whose corner precedes (x,y) on the Morton curve.
+// With the cell table: the leaves of a level-kCellTabLevel cell are
+// contiguous, so the search covers only the cell's leaves, and a leaf that
+// covers the whole cell is the answer at once.
 __device__ int locate_d(const ForestDev &F, int tree, long long x, long long y)
 {
     const unsigned long long m = morton_d(x, y);
     int lo = F.tree_begin[tree], hi = F.tree_begin[tree + 1];  // upper_bound in [lo, hi)
+    if (F.cell_tab) {
+        constexpr int sh = kMaxLevelG - kCellTabLevel;
+        const int c = int(morton_d(x >> sh, y >> sh));
+        const int *tab = F.cell_tab + size_t(tree) * kCellTabCells;
+        const int first = tab[c];
+        if (F.leaves[first].y <= kCellTabLevel) return first;
+        lo = first;
+        hi = c + 1 < kCellTabCells ? tab[c + 1] : hi;
+    }
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (F.keys[mid] <= m) lo = mid + 1;
@@ -273,6 +285,20 @@ __device__ __forceinline__ void pass_prep_item(const ForestDev &F, int ntrees, i
         flags[i] = 0;
         const int prev = i == 0 ? -1 : F.leaves[i - 1].x;
         for (int u = prev + 1; u <= l.x; ++u) tb[u] = i;  // trees without leaves start here too
+        if (F.cell_tab) {
+            // a leaf at or above the table's level is the first leaf of every
+            // cell it covers (a Morton-contiguous run); a finer one is the
+            // first of its cell when it holds the cell's lower corner
+            constexpr int sh = kMaxLevelG - kCellTabLevel;
+            int *tab = F.cell_tab + size_t(l.x) * kCellTabCells;
+            const int c0 = int(morton_d(l.z >> sh, l.w >> sh));
+            if (l.y <= kCellTabLevel) {
+                const int run = 1 << (2 * (kCellTabLevel - l.y));
+                for (int k = 0; k < run; ++k) tab[c0 + k] = i;
+            } else if (((l.z | l.w) & ((1 << sh) - 1)) == 0) {
+                tab[c0] = i;
+            }
+        }
     }
 }
 

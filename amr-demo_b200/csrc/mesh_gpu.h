@@ -11,6 +11,12 @@ namespace amrgpu {
 struct QuadDesc;
 
 // Device view of a forest's leaves and brick.
+// Point location over a tree's leaves starts in a table of the tree's
+// level-kCellTabLevel cells (Morton order): the first leaf in each cell.
+constexpr int kCellTabLevel = 7;
+constexpr int kCellTabCells = 1 << (2 * kCellTabLevel);
+constexpr int kCellTabMaxTrees = 256;  // larger bricks search whole trees
+
 struct ForestDev {
     const int4 *leaves;        // (tree, level, x, y) per leaf, Morton order within trees
     unsigned long long *keys;  // Morton key per leaf (written by the build)
@@ -21,6 +27,9 @@ struct ForestDev {
     double scale;
     int bc[4];
     int nq;
+    // null, or kCellTabCells entries per tree: the first leaf of each
+    // level-kCellTabLevel cell (the one-launch balance fills it every pass)
+    int *cell_tab = nullptr;
 };
 
 // One 2:1 balance pass over F's leaves in three launches (F.keys written,

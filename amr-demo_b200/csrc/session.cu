@@ -2125,7 +2125,7 @@ namespace {
 // total), keys, tree begin, brick tables, scan temp.
 struct BalLayout {
     size_t o_orig, o_dirty, buf;
-    size_t o_flags, o_pos, o_keys, o_tb, o_tx, o_ty, o_at, o_tmp, work;
+    size_t o_flags, o_pos, o_keys, o_tb, o_tx, o_ty, o_at, o_cell, o_tmp, work;
     size_t scan_bytes;
 };
 
@@ -2145,7 +2145,12 @@ BalLayout bal_layout(int cap, int ntrees)
     L.o_tx = L.o_tb + al(4 * size_t(ntrees + 1));
     L.o_ty = L.o_tx + al(4 * size_t(ntrees));
     L.o_at = L.o_ty + al(4 * size_t(ntrees));
-    L.o_tmp = L.o_at + al(4 * size_t(ntrees));
+    L.o_cell = L.o_at + al(4 * size_t(ntrees));
+    // the one-launch balance's cell table, used for bricks of up to
+    // kCellTabMaxTrees trees (sized monotonically in ntrees: a work area
+    // allocated for more trees serves a forest with fewer)
+    const size_t cell = 4 * size_t(std::min(ntrees, kCellTabMaxTrees)) * kCellTabCells;
+    L.o_tmp = L.o_cell + al(cell);
     L.work = L.o_tmp + al(L.scan_bytes);
     return L;
 }
@@ -2507,6 +2512,7 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false,
         a.F.tree_tx = reinterpret_cast<const int *>(w + L.o_tx);
         a.F.tree_ty = reinterpret_cast<const int *>(w + L.o_ty);
         a.F.tree_at = reinterpret_cast<const int *>(w + L.o_at);
+        if (ntrees <= kCellTabMaxTrees) a.F.cell_tab = reinterpret_cast<int *>(w + L.o_cell);
         a.ntrees = ntrees;
         a.tree_begin = reinterpret_cast<int *>(w + L.o_tb);
         for (int k = 0; k < 2; ++k) {
