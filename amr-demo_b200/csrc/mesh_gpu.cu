@@ -141,12 +141,9 @@ __global__ void keys_kernel(ForestDev F);
 // look at the four corners for a leaf two or more levels finer (the dirty
 // leaf itself is flagged). Splitting a leaf's checks over threads shortens
 // each thread's chain of dependent binary searches; the flags are the same.
-__device__ __forceinline__ void balance_check_item(const ForestDev &F, const unsigned char *dirty,
-                                                   unsigned char *flags, long long t)
+__device__ __forceinline__ void balance_check_leaf(const ForestDev &F, unsigned char *flags, int i, int item)
 {
     {
-        const int i = int(t >> 4), item = int(t & 15);
-        if (!dirty[i]) return;
         const int4 q = F.leaves[i];
         if (item < 8) {
             // fine side: the neighbour region across a face or a corner
@@ -202,6 +199,13 @@ __device__ __forceinline__ void balance_check_item(const ForestDev &F, const uns
         }
         if (fine) flags[i] = 1;
     }
+}
+
+__device__ __forceinline__ void balance_check_item(const ForestDev &F, const unsigned char *dirty,
+                                                   unsigned char *flags, long long t)
+{
+    const int i = int(t >> 4);
+    if (dirty[i]) balance_check_leaf(F, flags, i, int(t & 15));
 }
 
 __global__ void balance_check_kernel(ForestDev F, const unsigned char *dirty, unsigned char *flags)
@@ -661,6 +665,7 @@ __global__ void __launch_bounds__(256) balance_loop_kernel(const BalanceLoopArgs
             }
         }
     }
+    int ndirty = -1;  // -1: check every leaf marked dirty (the first pass)
     for (int pass = 0; pass < 64 && ok && !overflow; ++pass) {
         ++passes;
         F.leaves = a.leaves[live];
@@ -668,7 +673,13 @@ __global__ void __launch_bounds__(256) balance_loop_kernel(const BalanceLoopArgs
         unsigned char *flags = a.flags;
         for (int i = gtid; i <= nl; i += gstride) pass_prep_item(F, a.ntrees, a.tree_begin, flags, i);
         if (!(ok = grid_barrier(ctl))) break;
-        for (long long t = gtid; t < 16ll * nl; t += gstride) balance_check_item(F, a.dirty[live], flags, t);
+        if (ndirty >= 0) {
+            // the leaves the previous pass created, listed by its refinement
+            for (int t = gtid; t < 16 * ndirty; t += gstride)
+                balance_check_leaf(F, flags, __ldcg(a.dirty_list + (t >> 4)), t & 15);
+        } else {
+            for (long long t = gtid; t < 16ll * nl; t += gstride) balance_check_item(F, a.dirty[live], flags, t);
+        }
         if (!(ok = grid_barrier(ctl))) break;
         if (!(ok = grid_scan(nl, [&](int i) { return __ldcg(flags + i) ? 4 : 1; }, a.pos, a.bsum, ctl))) break;
         const int total = __ldcg(a.pos + nl);
@@ -680,10 +691,18 @@ __global__ void __launch_bounds__(256) balance_loop_kernel(const BalanceLoopArgs
             overflow = true;
             break;
         }
-        for (int i = gtid; i < nl; i += gstride)
+        for (int i = gtid; i < nl; i += gstride) {
             balance_refine_item(i, a.leaves[live], a.orig[live], flags, a.pos, a.leaves[1 - live], a.orig[1 - live],
                                 a.dirty[1 - live]);
+            if (__ldcg(flags + i)) {
+                // leaves flagged before i: (pos[i] - i) / 3; their children
+                // come first in the list
+                const int at = __ldcg(a.pos + i), k = 4 * ((at - i) / 3);
+                for (int c = 0; c < 4; ++c) a.dirty_list[k + c] = at + c;
+            }
+        }
         if (!(ok = grid_barrier(ctl))) break;
+        ndirty = 4 * ((total - nl) / 3);
         live = 1 - live;
         nl = total;
         refined = true;

@@ -80,6 +80,7 @@ struct BalanceLoopArgs {
     int nl, live, cap;            // leaves at the start, their buffer, each buffer's capacity
     unsigned char *flags;         // cap
     int *pos;                     // cap + 1
+    int *dirty_list;              // cap: the leaves a pass created, for the next pass's checks
     int *bsum;                    // one per block (balance_loop_bsum_ints)
     BalanceCtl *ctl;
     int build;                    // then the descriptors of the balanced leaves:

@@ -2125,7 +2125,7 @@ namespace {
 // total), keys, tree begin, brick tables, scan temp.
 struct BalLayout {
     size_t o_orig, o_dirty, buf;
-    size_t o_flags, o_pos, o_keys, o_tb, o_tx, o_ty, o_at, o_cell, o_tmp, work;
+    size_t o_flags, o_pos, o_keys, o_tb, o_tx, o_ty, o_at, o_cell, o_tmp, o_dlist, work;
     size_t scan_bytes;
 };
 
@@ -2151,7 +2151,8 @@ BalLayout bal_layout(int cap, int ntrees)
     // allocated for more trees serves a forest with fewer)
     const size_t cell = 4 * size_t(std::min(ntrees, kCellTabMaxTrees)) * kCellTabCells;
     L.o_tmp = L.o_cell + al(cell);
-    L.work = L.o_tmp + al(L.scan_bytes);
+    L.o_dlist = L.o_tmp + al(L.scan_bytes);
+    L.work = L.o_dlist + al(4 * c);
     return L;
 }
 
@@ -2526,6 +2527,7 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false,
         a.cap = cap;
         a.flags = reinterpret_cast<unsigned char *>(w + L.o_flags);
         a.pos = reinterpret_cast<int *>(w + L.o_pos);
+        a.dirty_list = reinterpret_cast<int *>(w + L.o_dlist);
         a.bsum = reinterpret_cast<int *>(base + o_bsum);
         a.ctl = reinterpret_cast<BalanceCtl *>(base + o_ctl);
         a.build = 1;
