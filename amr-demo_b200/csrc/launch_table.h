@@ -37,5 +37,9 @@ int stage_table_mixed(const StageLaunch **out);
 struct CflArgs;
 const void *cfl_kernel_fp64(int n);
 const void *cfl_kernel_fp32(int n);  // the FP32-flux form's candidate
+// The remap of an in-place regrid fused with the CFL minimum of the
+// remapped state (remap_cfl.cuh), per form: __global__ void(RemapCflArgs).
+const void *remap_cfl_kernel_fp64(int n);
+const void *remap_cfl_kernel_fp32(int n);
 
 }  // namespace amrgpu

@@ -1726,7 +1726,10 @@ int ensure_desc(amrgpu_session *s, QuadDesc **buf, int *cap, int nq)
 // The state moves to the new mesh of nq quads (descriptors already in
 // d_quads, remap kind / source in d_kind / d_src): into the spare buffer Y
 // of the same capacity, or a fresh set when the mesh outgrew the capacity.
-int apply_regrid(amrgpu_session *s, int nq, int nface, long long mixed_cells = -1)
+// fuse_cfl: the remap also folds the next segment's first CFL minimum
+// (remap_cfl_kernel; s->d_quads must hold the new mesh's descriptors), so
+// no separate CFL pass follows.
+int apply_regrid(amrgpu_session *s, int nq, int nface, long long mixed_cells = -1, bool fuse_cfl = false)
 {
     s->dev_forest = nullptr;  // the new mesh's leaves are the caller's to record
     const long long cells = mixed_cells >= 0 ? mixed_cells : (long long)nq * s->n * s->n;
@@ -1760,7 +1763,33 @@ int apply_regrid(amrgpu_session *s, int nq, int nface, long long mixed_cells = -
         s->d_tot = tot;
     }
     double *qnew = fresh[0] ? fresh[0] : rolebuf(s, RY);
-    if (nq > 0) {
+    const void *rcfl = nullptr;
+    if (fuse_cfl && mixed_cells < 0 && nq > 0 && s->primed && s->cfg.time_scheme != 2)
+        rcfl = s->form == AMRGPU_FORM_FP32_FLUX ? remap_cfl_kernel_fp32(s->n) : remap_cfl_kernel_fp64(s->n);
+    if (rcfl) {
+        // the slots re-armed (dt cap) first, as prime() does
+        const int p = int(s->step_index % 3);
+        ok = cuda_ok(launch_rearm(s->d_scal, p, s->cfg.dt, s->stream), "rearm scalars");
+        s->launches++;
+        RemapCflArgs ra;
+        std::memset(&ra, 0, sizeof(ra));
+        ra.qold = qold;
+        ra.stride_old = old_stride;
+        ra.qnew = qnew;
+        ra.kind = s->d_kind;
+        ra.src = s->d_src;
+        ra.cfl.quads = s->d_quads;
+        ra.cfl.scal = s->d_scal;
+        ra.cfl.stride = stride;
+        ra.cfl.nquad = nq;
+        ra.cfl.slot = p;
+        ra.cfl.cfl = s->cfg.cfl;
+        const long long cells_new = (long long)nq * s->n * s->n;
+        const int g = int(std::max(1ll, std::min<long long>((cells_new + 255) / 256, (long long)s->sms * 16)));
+        void *args[] = {&ra};
+        if (ok) ok = cuda_ok(cudaLaunchKernel(rcfl, dim3(g), dim3(256), args, 0, s->stream), "remap + CFL kernel");
+        s->launches++;
+    } else if (nq > 0) {
         if (mixed_cells >= 0)
             ok = cuda_ok(launch_remap_mixed(qold, old_stride, s->d_mix_old, qnew, stride, s->d_mix, s->d_kind, s->d_src,
                                             nq, s->stream),
@@ -1796,6 +1825,7 @@ int apply_regrid(amrgpu_session *s, int nq, int nface, long long mixed_cells = -
     int rc = configure_launch(s, keep ? s->launch : session_default_launch(s));
     if (!s->launch_pinned) s->tune_pending = true;
     if (rc != AMRGPU_OK) return rc;
+    if (rcfl) return AMRGPU_OK;  // re-armed and the CFL minimum folded already
     return prime(s, s->primed);
 }
 
@@ -2611,7 +2641,7 @@ int balance_regrid_fused(amrgpu_session *s, Forest *fo, bool stall_test = false,
     std::swap(s->cap_desc, s->cap_desc_alt);
     s->h_quads.clear();  // the live descriptors exist on the device only
     s->rect = true;      // brick quads are axis-aligned rectangles
-    if ((rc = apply_regrid(s, nl, nl > 0 ? status[1] : 0))) return rc;
+    if ((rc = apply_regrid(s, nl, nl > 0 ? status[1] : 0, -1, true))) return rc;
     if (ctl.refined) {
         if ((rc = leaves_back_finish(s, fo, nl))) return rc;
     } else {

@@ -7,6 +7,7 @@
 #include "flux_fp32.cuh"
 #include "flux_fp64.cuh"
 #include "launch_table.h"
+#include "remap_cfl.cuh"
 #include "stage_kernel.cuh"
 #include "stage_sweep.cuh"
 
@@ -64,6 +65,29 @@ __global__ void __launch_bounds__(256) cfl_kernel_f32(const CflArgs a)
     if (threadIdx.x == 0) {
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = (red[w] < best) ? red[w] : best;
         atomicMin(&a.scal->slot[a.slot].dt_bits, (unsigned long long)__double_as_longlong(best));
+    }
+}
+
+// cfl_kernel_f32's candidate of one cell from its values, for
+// remap_cfl_kernel
+struct CflCandFP32 {
+    template <int N>
+    __device__ static __forceinline__ double candidate(const CflArgs &a, int q, int, const double q4[4])
+    {
+        const double *g = a.quads[q].corner;
+        const double hx = (g[2] - g[0]) / (double)N, hy = (g[5] - g[1]) / (double)N;
+        return cfl_candidate_fp32(q4, hx * hy, a.cfl);
+    }
+};
+
+const void *remap_cfl_kernel_fp32(int n)
+{
+    switch (n) {
+    case 2: return (const void *)remap_cfl_kernel<2, CflCandFP32>;
+    case 4: return (const void *)remap_cfl_kernel<4, CflCandFP32>;
+    case 8: return (const void *)remap_cfl_kernel<8, CflCandFP32>;
+    case 16: return (const void *)remap_cfl_kernel<16, CflCandFP32>;
+    default: return nullptr;
     }
 }
 

@@ -7,6 +7,7 @@
 
 #include "flux_fp64.cuh"
 #include "launch_table.h"
+#include "remap_cfl.cuh"
 #include "stage_kernel.cuh"
 #include "stage_sweep64.cuh"
 
@@ -75,6 +76,38 @@ __global__ void __launch_bounds__(256) cfl_kernel(const CflArgs a)
     if (threadIdx.x == 0) {
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = (red[w] < best) ? red[w] : best;
         atomicMin(&a.scal->slot[a.slot].dt_bits, (unsigned long long)__double_as_longlong(best));
+    }
+}
+
+// cfl_kernel's candidate of one cell from its values (the subcell volume
+// from the quad's bilinear corners), for remap_cfl_kernel
+struct CflCandFP64 {
+    template <int N>
+    __device__ static __forceinline__ double candidate(const CflArgs &a, int q, int r, const double q4[4])
+    {
+        const double s = 2.0 / (double)N;
+        const int i = r % N, j = r / N;
+        const double *g = a.quads[q].corner;
+        double v1 = s * (double)j - 1.0, v2 = s * (double)(j + 1) - 1.0;
+        double w1 = s * (double)i - 1.0, w2 = s * (double)(i + 1) - 1.0;
+        double x1, y1, x2, y2, x3, y3, x4, y4;
+        bilinear_node(g, w1, v1, x1, y1);
+        bilinear_node(g, w2, v1, x2, y2);
+        bilinear_node(g, w1, v2, x3, y3);
+        bilinear_node(g, w2, v2, x4, y4);
+        const double vol = subcell_volume(x1, y1, x2, y2, x3, y3, x4, y4);
+        return cfl_candidate_fp64(q4, vol, a.cfl);
+    }
+};
+
+const void *remap_cfl_kernel_fp64(int n)
+{
+    switch (n) {
+    case 2: return (const void *)remap_cfl_kernel<2, CflCandFP64>;
+    case 4: return (const void *)remap_cfl_kernel<4, CflCandFP64>;
+    case 8: return (const void *)remap_cfl_kernel<8, CflCandFP64>;
+    case 16: return (const void *)remap_cfl_kernel<16, CflCandFP64>;
+    default: return nullptr;
     }
 }
 

@@ -95,6 +95,18 @@ struct CflArgs {
     double cfl;
 };
 
+// Arguments of remap_cfl_kernel (remap_cfl.cuh): the remap's old state,
+// kind and source per new quad, and the CFL prologue's arguments for the
+// new mesh (cfl.qin unused; cfl.stride is the new state's field stride).
+struct RemapCflArgs {
+    const double *qold;
+    long long stride_old;
+    double *qnew;
+    const int *kind;
+    const int *src;
+    CflArgs cfl;
+};
+
 // LSERK45 coefficients, rk_time_integrators.c:439-448.
 __device__ __forceinline__ void lserk_coeff(int stage, double &ra, double &rb)
 {
