@@ -148,3 +148,47 @@ def test_adapt_regrid_with_a_patch_rule(ag):
         same(a, b)
     for f, s in (a, b):
         s.close()
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_adapt_regrid_equals_the_host_path_on_bricks(ag, seed):
+    """Against code that shares nothing with the device path: the host
+    forest's adapt and balance, its mesh arrays, decoded by the session
+    (Session.regrid). Random refine / coarsen tags on bricks of up to 3x2
+    periodic trees, eight regrids (the device adapt from the second on);
+    leaves, descriptors and states bit for bit."""
+    import meshes
+    n = 8
+    rng = np.random.default_rng(700 + seed)
+    nx, ny = int(rng.integers(1, 4)), int(rng.integers(1, 3))
+    per = (int(rng.integers(2)), int(rng.integers(2)))
+    fa = ag.Forest(nx, ny, periodic=per, level=2)
+    fb = ag.Forest(nx, ny, periodic=per, level=2)
+    cfg = meshes.make_config(n, time_scheme=3, time_steps=10 ** 6, dt=0.005, h=1.0)
+    cfg.apply()
+    s0 = meshes.perturbed(fa.initialize(n), seed, amp=1e-2)
+    a = ag.Session(fa.mesh(n), cfg, form=1)
+    b = ag.Session(fb.mesh(n), cfg, form=1)
+    for s in (a, b):
+        s.upload(s0)
+    for rnd in range(8):
+        for s in (a, b):
+            s.step(2)
+        u = rng.random(fa.num_quads)
+        tags = np.where(u < 0.2, 1, np.where(u < 0.8, 0, 2)).astype(np.int32)
+        fa.adapt(tags, 1, 0, 1, 6)
+        fa.balance()
+        kind, src = fa.remap()
+        a.regrid(fa.mesh(n), kind, src)
+        assert b.holds_forest(fb) == (rnd > 0)
+        b.adapt_regrid(fb, 1, 6, tags=tags)
+        for x, y in zip(fa.quads(), fb.quads()):
+            assert np.array_equal(x, y), rnd
+        assert a.quad_descriptors().tobytes() == b.quad_descriptors().tobytes(), rnd
+        qa = a.download()
+        assert np.isfinite(qa).all() and np.array_equal(qa, b.download()), rnd
+    for s in (a, b):
+        s.step(3)
+    assert np.array_equal(a.download(), b.download())
+    a.close()
+    b.close()
