@@ -213,25 +213,28 @@ def test_host_tag_feature_matches_restated_fortran(ag, oracle):
             assert tag.value == expect
 
 
-@pytest.mark.parametrize("seed,rv,cv", [(3, 1, 0), (4, 2, 1), (5, 1, 2), (6, 0, 1)])
-def test_adapt_equals_the_step_by_step_regrid(ag, seed, rv, cv):
+@pytest.mark.parametrize("seed,rv,cv,level,lo,hi,rounds", [(3, 1, 0, 3, 1, 6, 8), (4, 2, 1, 3, 1, 6, 8),
+                                                             (5, 1, 2, 3, 1, 6, 8), (6, 0, 1, 3, 1, 6, 8),
+                                                             (7, 1, 0, 7, 5, 9, 3)])
+def test_adapt_equals_the_step_by_step_regrid(ag, seed, rv, cv, level, lo, hi, rounds):
     """Forest.adapt (begin_regrid, tags, refine, coarsen in one pass) gives
     the same leaves, tags and remap table as the separate calls, also when
-    the coarsen tag is the one refined children carry (1)."""
+    the coarsen tag is the one refined children carry (1); also on a forest
+    of 32k+ leaves."""
     import numpy as np
     rng = np.random.default_rng(seed)
-    fa = ag.Forest(2, 1, periodic=(1, 0), level=3)
-    fb = ag.Forest(2, 1, periodic=(1, 0), level=3)
-    for rnd in range(8):
+    fa = ag.Forest(2, 1, periodic=(1, 0), level=level)
+    fb = ag.Forest(2, 1, periodic=(1, 0), level=level)
+    for rnd in range(rounds):
         tags = rng.integers(0, 3, fa.num_quads).astype(np.int32)
         _, lev, _, _ = fa.quads()
         fa.begin_regrid()
         fa.set_tags(tags)
-        fa.refine(((tags == rv) & (lev < 6)).astype(np.int32), max_level=6)
+        fa.refine(((tags == rv) & (lev < hi)).astype(np.int32), max_level=hi)
         t2 = fa.get_tags()
         _, lev2, _, _ = fa.quads()
-        fa.coarsen(((t2 == cv) & (lev2 > 1)).astype(np.int32), min_level=1)
-        nb = fb.adapt(tags, rv, cv, 1, 6)
+        fa.coarsen(((t2 == cv) & (lev2 > lo)).astype(np.int32), min_level=lo)
+        nb = fb.adapt(tags, rv, cv, lo, hi)
         assert nb == fa.num_quads == fb.num_quads
         for u, v in zip(fa.quads() + fa.remap() + (fa.get_tags(),), fb.quads() + fb.remap() + (fb.get_tags(),)):
             assert np.array_equal(u, v), rnd
